@@ -1,0 +1,330 @@
+"""Benchmark: hydro leaf-cell-updates/s of the unsplit MUSCL-Hancock step.
+
+Workload (one GPU): the supersonic turbulent box, uniform 256^3
+(levelmin=levelmax=8, periodic), ln(rho) and solenoidal velocity seeded
+Gaussian fields with P(k) ~ k^-4 (sigma=1, RMS Mach 5), P = 0.01 rho,
+gamma = 1.001, hllc, slope_type = 2, courant_factor = 0.8. A "step" is one
+coarse hydro step of the whole box (courant_fine, godunov_fine, set_uold).
+
+Headline value: FP32-mixed path, state resident in HBM. Reported beside it:
+the FP64 drop-in path, the L1(rho) difference FP32-mixed vs FP64 (the FP64
+path is bit-identical to the CPU oracle in the parity tests), an end-to-end
+number through the C ABI with host buffers, the roofline of the dominant
+kernel and a CPU baseline (the FP64 oracle on the host cores).
+
+--gpus N (under torchrun): N independent replicas (the path runs on one GPU;
+there is no data-path collective); value = total cell updates of all ranks
+divided by the slowest rank's device time.
+
+--impl reference: the CPU restatement of the reference (oracle) on a bounded
+sample of the same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "hydro leaf-cell-updates/s FP32-mix vs FP64 at L1(rho)<=1e-5; %HBM peak; p99"
+UNIT = "cell-updates/s"
+BYTES_PER_CELL_UPDATE = 80  # read uold (5 x 8 B) + write unew (5 x 8 B) per leaf-cell update
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--level", type=int, default=8)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-octs", type=int, default=32768)
+    return ap.parse_args()
+
+
+def workload(level, seed):
+    from ramses_b200 import ics, mesh
+    from ramses_b200.params import HydroParams
+    hp = HydroParams(gamma=1.001, riemann="hllc", slope_type=2, courant_factor=0.8)
+    tree = mesh.uniform_tree(level)
+    q = ics.turbulent_box_prim_grid(2 ** level, seed=seed, gamma=hp.gamma)
+    u = ics.fill_uniform_level_from_grid(tree, level, q, hp.gamma)
+    return tree, hp, u
+
+
+def config_dict(level, n_gpus):
+    n = 2 ** level
+    return {"workload": "turbulent box %d^3 uniform (levelmin=levelmax=%d), periodic, hllc, slope_type=2, "
+                        "gamma=1.001, Mach 5, courant 0.8" % (n, level),
+            "cells": n ** 3, "riemann": "hllc", "slope_type": 2, "precision": "fp32-mixed",
+            "l2_policy": "inputs larger than L2 (state %.0f MB per copy > 126 MB L2)" % (n ** 3 * 40 / 1e6),
+            "parallelism": "replicas" if n_gpus > 1 else "single-gpu"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the mixed tile kernel from the committed ncu
+    summary (line 'traffic_bytes_per_launch: N'), scaled to this workload."""
+    f = ROOT / "profiles" / "godunov_tile_mixed_turb256.md"
+    if not f.exists():
+        return None
+    for ln in f.read_text().splitlines():
+        if ln.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_sample(tree, hp, u, nocts, reps, warmup):
+    """Time the oracle's hydro step (courant_fine, set_unew, godunov_fine,
+    set_uold) on the first ``nocts`` octs (Morton order) of the finest level,
+    with all host threads. Returns (cell-updates/s, cores, description)."""
+    import copy
+
+    import oracle
+    level = tree.nlevelmax
+    sub = copy.copy(tree)
+    sub.active = list(tree.active)
+    sub.active[level] = tree.active[level][:nocts]
+    cores = os.cpu_count() or 1
+    run = oracle.OracleRun(sub, hp, u, nthreads=cores)
+    times = []
+    for i in range(warmup + reps):
+        t0 = time.perf_counter()
+        dt, *_ = run.courant_fine(level)
+        run.set_unew(level)
+        run.godunov_fine(level, dt)
+        run.set_uold(level)
+        t1 = time.perf_counter()
+        if i >= warmup:
+            times.append(t1 - t0)
+    cells = nocts * 8
+    value = cells * len(times) / sum(times)
+    desc = ("oracle (C restatement, OpenMP %d threads) hydro step on %d of %d octs (%d cells, Morton-contiguous) "
+            "of the same workload, %d timed repetitions" % (cores, nocts, tree.noct(level), cells, len(times)))
+    return value, cores, desc
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    tree, hp, u = workload(args.level, args.seed)
+    nocts = min(args.cpu_sample_octs, tree.noct(args.level))
+    value, cores, desc = cpu_sample(tree, hp, u, nocts, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": nocts * 8 / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(args.level, 1) | {"precision": "fp64", "sample_octs": nocts},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    from ramses_b200 import runtime
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    runtime.load()
+    runtime.select_device(local)
+
+    tree, hp, u = workload(args.level, args.seed)
+    level = args.level
+    cells = tree.leaf_cells(level)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- FP32-mixed, device resident (headline) -------------------------
+    mixed = runtime.Solver(tree, hp, precision="mixed", uold=u)
+    mixed.uniform_run(args.warmup, graph=False)
+    barrier()
+    mixed.synchronize()
+    with ClockSampler(local) as clk:
+        mixed.uniform_run(args.steps, graph=False)
+        mixed.synchronize()
+    barrier()
+    run_ms = max_over_ranks(mixed.last_run_ms())
+    kern_ms = mixed.last_kernel_ms()
+    value = cells * args.steps * world / (run_ms / 1e3)
+    u_mixed = mixed.download_state()
+
+    # ---- FP64 drop-in path on the same steps ----------------------------
+    f64 = runtime.Solver(tree, hp, precision="fp64", uold=u)
+    f64.uniform_run(args.warmup, graph=False)
+    barrier()
+    f64.uniform_run(args.steps, graph=False)
+    barrier()
+    f64_ms = max_over_ranks(f64.last_run_ms())
+    f64_kern = f64.last_kernel_ms()
+    f64_value = cells * args.steps * world / (f64_ms / 1e3)
+    u_f64 = f64.download_state()
+    idx = tree.cell_index(level).reshape(-1) - 1
+    rm, rf = u_mixed[0, idx], u_f64[0, idx]
+    l1_rho = float(np.abs(rm - rf).sum() / np.abs(rf).sum())
+    linf_rho = float(np.max(np.abs(rm - rf) / np.abs(rf)))
+    f64.close()
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    # every step: H2D of the full Fortran-layout state from pinned memory,
+    # the coarse step (CFL + fused update), D2H of the result state.
+    import ctypes
+    nbytes = 5 * tree.ncell * 8
+    host = np.empty((5, tree.ncell))
+    try:
+        import torch
+        pinned = torch.empty((5, tree.ncell), dtype=torch.float64, pin_memory=True)
+        host = pinned.numpy()
+    except Exception:
+        pass
+    host[:] = u_mixed
+    mixed.upload_state(host)
+    mixed.uniform_run(1, graph=False)
+    barrier()
+    mixed.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        mixed.upload_state(host)
+        mixed.uniform_run(1, graph=False)
+        host[:] = mixed.download_state()
+    mixed.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = cells * args.e2e_steps * world / e2e_s
+    mixed.close()
+
+    peak, peak_kind = hbm_peak()
+    achieved = BYTES_PER_CELL_UPDATE * cells / (kern_ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        nocts = min(args.cpu_sample_octs, tree.noct(level))
+        v, cores, desc = cpu_sample(tree, hp, u, nocts, reps=5, warmup=1)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": run_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": config_dict(level, world),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "steps": args.e2e_steps,
+                    "path": "rb_upload_state + rb_uniform_run(1) + rb_download_state, pinned host buffers"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "godunov_tile_kernel<float,8,8,8> (fused update + CFL partials)",
+                         "bytes_per_cell_update": BYTES_PER_CELL_UPDATE, "kernel_ms": kern_ms,
+                         "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": 2 * args.steps,
+            "fp64": {"value": f64_value, "ms_per_step": f64_ms / args.steps, "kernel_ms": f64_kern,
+                     "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak},
+            "mixed_over_fp64": value / f64_value,
+            "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,
+                         "steps_compared": args.warmup + args.steps},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

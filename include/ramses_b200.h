@@ -1,0 +1,126 @@
+/*
+ * ramses_b200.h -- C ABI of the B200 hydro step (RAMSES unsplit MUSCL-Hancock,
+ * NDIM=3, nvar=5). Plain pointers, sizes and status codes; no C++ or torch
+ * types. Every entry point returns an int status (RB_OK = 0); the text of the
+ * last error of the calling thread is available from rb_last_error().
+ *
+ * Array conventions at this boundary are RAMSES's own (Fortran column-major,
+ * 1-based cell and grid indices stored as int32):
+ *   uold(1:ncell,1:5)  : double[5*ncell], element (icell,ivar) at (ivar-1)*ncell+icell-1
+ *   son(1:ncell)       : int32[ncell]
+ *   father(1:ngridmax) : int32[ngridmax]
+ *   nbor(1:ngridmax,6) : int32[6*ngridmax]
+ *   icell = ncoarse + (ind-1)*ngridmax + igrid, ind = 1..8
+ * The state lives on the GPU between calls (device-resident mirrors); the host
+ * copy is only read or written by rb_upload_state / rb_download_state.
+ *
+ * Reference interfaces replaced (paths within ramses-organisation/ramses):
+ *   godunov_fine(ilevel)               hydro/godunov_fine.f90:5-35   -> rb_godunov_fine
+ *   unsplit(uin,gravin,pin,flux,tmp,dx,dy,dz,dt,ngrid)
+ *                                      hydro/umuscl.f90:22-171        -> rb_unsplit
+ *   courant_fine(ilevel)               hydro/courant_fine.f90:1-159   -> rb_courant_fine
+ *   set_unew(ilevel)                   hydro/godunov_fine.f90:40-130  -> rb_set_unew
+ *   set_uold(ilevel)                   hydro/godunov_fine.f90:135-232 -> rb_set_uold
+ *   upload_fine(ilevel)                hydro/interpol_hydro.f90:5-68  -> rb_upload_fine
+ *   amr_step hydro sequence            amr/amr_step.f90:320-445       -> rb_coarse_step
+ *   &HYDRO_PARAMS                      hydro/read_hydro_params.f90:43-54 -> rb_hydro_params
+ */
+#ifndef RAMSES_B200_H
+#define RAMSES_B200_H
+
+#include <stdint.h>
+
+#include "../ramses_b200/csrc/rb_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rb_context rb_context;
+
+/* Library version string. */
+const char *rb_version(void);
+/* Human-readable text for a status code. */
+const char *rb_status_string(int status);
+/* Text of the calling thread's last error (empty if none). */
+const char *rb_last_error(void);
+/* Number of visible CUDA devices (0 when none); never fails. */
+int rb_device_count(void);
+/* Make `device` the calling thread's current device for rb_create. */
+int rb_select_device(int device);
+
+/* Create a context on the current CUDA device. precision = RB_PREC_FP64
+ * (drop-in) or RB_PREC_MIXED (FP32 slopes/trace/Riemann, FP64 state).
+ * Replaces the namelist read (read_hydro_params.f90:43-54,138) + init_hydro
+ * allocation (init_hydro.f90:31-32). Unsupported namelist values are rejected. */
+int rb_create(const rb_hydro_params *hp, const rb_mesh_params *mp, int precision, rb_context **out);
+int rb_destroy(rb_context *ctx);
+
+/* Upload the octree (son, father, nbor as RAMSES stores them) and the active
+ * grid lists: numbl[l-1] octs at level l, concatenated 1-based igrids in
+ * active_igrid. Builds the device tile and interpolation tables. */
+int rb_sync_tree(rb_context *ctx, const int32_t *son, const int32_t *father, const int32_t *nbor,
+                 const int32_t *numbl, const int32_t *active_igrid);
+
+/* Fortran-layout uold(ncell,5) host <-> device mirror of uold. */
+int rb_upload_state(rb_context *ctx, const double *uold);
+int rb_download_state(rb_context *ctx, double *uold);
+/* Same for unew (for callers that interleave host work with a level step). */
+int rb_upload_unew(rb_context *ctx, const double *unew);
+int rb_download_unew(rb_context *ctx, double *unew);
+
+/* Level operations on the device mirrors (same semantics as the Fortran). */
+int rb_set_unew(rb_context *ctx, int ilevel);
+int rb_set_uold(rb_context *ctx, int ilevel);
+int rb_godunov_fine(rb_context *ctx, int ilevel, double dt);
+int rb_upload_fine(rb_context *ctx, int ilevel);
+/* dt_io: in = current dtnew(ilevel); out = min(in, CFL dt of the level's leaf
+ * cells). mass/ekin/eint: the level's totals (any may be NULL). */
+int rb_courant_fine(rb_context *ctx, int ilevel, double *dt_io, double *mass, double *ekin, double *eint);
+
+/* One coarse time step: the amr_step(levelmin) hydro call sequence with
+ * subcycling, followed by the restriction of levels levelmin-1..1. t_io is
+ * advanced by the step; dtnew_out (may be NULL) receives dtnew(1..nlevelmax). */
+int rb_coarse_step(rb_context *ctx, double *t_io, double *dtnew_out);
+/* Leaf-cell updates done by this context so far (one per leaf cell per step of its level). */
+int rb_cell_updates(rb_context *ctx, int64_t *out);
+
+/* Choose the tile shape of level ilevel's godunov kernel: shape >= 0 forces
+ * one (see rb_tile_shape_info), shape < 0 times every shape on the current
+ * state and keeps the fastest (the state is left unchanged). */
+int rb_set_tile_shape(rb_context *ctx, int ilevel, int shape);
+int rb_get_tile_shape(rb_context *ctx, int ilevel, int *shape);
+int rb_tile_shape_info(int shape, int *tx, int *ty, int *tz, int *nthreads);
+
+/* unsplit with the reference's argument list and Fortran layouts
+ * (umuscl.f90:22-38): uin(nvector,-1:4,-1:4,-1:4,5),
+ * gravin(nvector,-1:4,-1:4,-1:4,3) (may be NULL = zero gravity), pin unused,
+ * flux(nvector,1:3,1:3,1:3,5,3), tmp(nvector,1:3,1:3,1:3,2,3). Host pointers;
+ * FP64 only. */
+int rb_unsplit(const rb_hydro_params *hp, const double *uin, const double *gravin, const double *pin,
+               double *flux, double *tmp, double dx, double dy, double dz, double dt, int ngrid,
+               int nvector);
+
+/* Device-resident uniform-grid stepper (configs with one complete level):
+ * state kept as uold/unew in the device layout, one fused kernel per step
+ * (gather, fluxes, update, next-step CFL partials) and a single-thread dt
+ * finalisation; nsteps steps are captured as one CUDA graph when
+ * use_graph != 0. dt of each step is the CFL dt of the state it starts from,
+ * as newdt_fine/courant_fine give it. t_io advanced; dt_last_out may be NULL. */
+int rb_uniform_run(rb_context *ctx, int nsteps, int use_graph, double *t_io, double *dt_last_out);
+
+/* Wait for all work queued on the context's stream. */
+int rb_synchronize(rb_context *ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that order their own work. */
+int rb_get_stream(rb_context *ctx, void **stream);
+/* Mean device milliseconds per godunov tile-kernel launch of the last
+ * rb_godunov_fine call or un-graphed rb_uniform_run (CUDA events around the
+ * kernel alone). */
+int rb_last_kernel_ms(rb_context *ctx, float *ms);
+/* Device milliseconds of the whole last rb_uniform_run (all steps). */
+int rb_last_run_ms(rb_context *ctx, float *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

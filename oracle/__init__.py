@@ -1,0 +1,201 @@
+"""ctypes wrapper of the CPU oracle (``ramses_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and ``bench.py``'s CPU-baseline / reference arm, as the checker. The product
+package ``ramses_b200`` never imports it.
+
+Parity status: restatement of the reference Fortran, pinned physically to the
+reference's Sod known-answer table; bit-level parity with the Fortran binary
+is unpinned (no Fortran compiler in the build image).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+BUILD = HERE / "_build"
+LIB_PATH = BUILD / "liboracle.so"
+SRC = HERE / "ramses_oracle.c"
+HDR = HERE / "ramses_oracle.h"
+CFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c11"]
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with gcc (no FMA contraction)."""
+    BUILD.mkdir(exist_ok=True)
+    if (not force and LIB_PATH.exists()
+            and LIB_PATH.stat().st_mtime >= max(SRC.stat().st_mtime, HDR.stat().st_mtime)):
+        return LIB_PATH
+    tmp = LIB_PATH.with_suffix(".so.tmp%d" % os.getpid())
+    subprocess.run(["gcc", *CFLAGS, str(SRC), "-o", str(tmp), "-lm"], check=True)
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(str(build()))
+        _declare(_lib)
+    return _lib
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [("gamma", ctypes.c_double), ("smallr", ctypes.c_double),
+                ("smallc", ctypes.c_double), ("courant_factor", ctypes.c_double),
+                ("slope_theta", ctypes.c_double), ("riemann", ctypes.c_int32),
+                ("slope_type", ctypes.c_int32), ("interpol_var", ctypes.c_int32),
+                ("interpol_type", ctypes.c_int32)]
+
+
+MAXLEVEL = 32
+_P32 = ctypes.POINTER(ctypes.c_int32)
+_P64 = ctypes.POINTER(ctypes.c_int64)
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+class OrcMesh(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("ncoarse", ctypes.c_int32), ("ngridmax", ctypes.c_int32),
+                ("nlevelmax", ctypes.c_int32), ("levelmin", ctypes.c_int32),
+                ("nvector", ctypes.c_int32), ("boxlen", ctypes.c_double),
+                ("son", _P32), ("father", _P32), ("nbor", _P32), ("active", _P32),
+                ("active_off", _P64), ("uold", _PD), ("unew", _PD),
+                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1)),
+                ("dtnew", ctypes.c_double * (MAXLEVEL + 1)),
+                ("dtold", ctypes.c_double * (MAXLEVEL + 1)),
+                ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
+                ("mass_tot", ctypes.c_double), ("ekin_tot", ctypes.c_double),
+                ("eint_tot", ctypes.c_double), ("cell_updates", ctypes.c_int64),
+                ("nthreads", ctypes.c_int32)]
+
+
+def _declare(L):
+    P = ctypes.POINTER(OrcParams)
+    M = ctypes.POINTER(OrcMesh)
+    L.orc_unsplit.argtypes = [P, _PD, _PD, _PD, _PD, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.orc_cmpdt.argtypes = [P, _PD, _PD, ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.orc_cmpdt.restype = ctypes.c_double
+    for name in ("orc_set_unew", "orc_set_uold", "orc_upload_fine"):
+        getattr(L, name).argtypes = [P, M, ctypes.c_int]
+    L.orc_godunov_fine.argtypes = [P, M, ctypes.c_int, ctypes.c_double]
+    L.orc_courant_fine.argtypes = [P, M, ctypes.c_int, _PD, _PD, _PD, _PD]
+    L.orc_coarse_step.argtypes = [P, M]
+    L.orc_get3cubefather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
+    L.orc_getnborfather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
+    L.orc_interpol_hydro.argtypes = [P, _PD, _PD, ctypes.c_int]
+
+
+def params_struct(hp) -> OrcParams:
+    hp.validate()
+    return OrcParams(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta,
+                     hp.riemann_code, hp.slope_type, hp.interpol_var, hp.interpol_type)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def unsplit(hp, uin, gravin, dx, dt, ngrid=None):
+    """Fortran-layout unsplit: uin (5,6,6,6,nvector) C-order == Fortran
+    uin(nvector,-1:4,-1:4,-1:4,5). Returns (flux (3,5,3,3,3,nv), tmp (3,2,3,3,3,nv))."""
+    uin = np.ascontiguousarray(uin, dtype=np.float64)
+    nv = uin.shape[-1]
+    if gravin is None:
+        gravin = np.zeros((3, 6, 6, 6, nv))
+    gravin = np.ascontiguousarray(gravin, dtype=np.float64)
+    flux = np.zeros((3, 5, 3, 3, 3, nv))
+    tmp = np.zeros((3, 2, 3, 3, 3, nv))
+    p = params_struct(hp)
+    rc = lib().orc_unsplit(ctypes.byref(p), _ptr(uin, _PD), _ptr(gravin, _PD), _ptr(flux, _PD),
+                           _ptr(tmp, _PD), dx, dx, dx, dt, nv if ngrid is None else ngrid, nv)
+    if rc:
+        raise RuntimeError("orc_unsplit failed: %d" % rc)
+    return flux, tmp
+
+
+class OracleRun:
+    """One hydro problem held in Fortran-layout host arrays, stepped by the
+    oracle with RAMSES's amr_step hydro call sequence."""
+
+    def __init__(self, tree, hp, uold, nsubcycle=None, nvector=32, nthreads=0):
+        self.tree = tree
+        self.hp = hp
+        self.p = params_struct(hp)
+        self.son = np.ascontiguousarray(tree.son, dtype=np.int32)
+        self.father = np.ascontiguousarray(tree.father, dtype=np.int32)
+        self.nbor = np.ascontiguousarray(tree.nbor, dtype=np.int32)
+        self.active, self.active_off = tree.active_concat()
+        self.uold = np.ascontiguousarray(uold, dtype=np.float64).copy()
+        assert self.uold.shape == (5, tree.ncell)
+        self.unew = self.uold.copy()
+        m = OrcMesh()
+        m.nx, m.ny, m.nz = tree.nx, tree.ny, tree.nz
+        m.ncoarse, m.ngridmax = tree.ncoarse, tree.ngridmax
+        m.nlevelmax, m.levelmin, m.nvector = tree.nlevelmax, tree.levelmin, nvector
+        m.boxlen = tree.boxlen
+        m.son, m.father, m.nbor = _ptr(self.son, _P32), _ptr(self.father, _P32), _ptr(self.nbor, _P32)
+        m.active, m.active_off = _ptr(self.active, _P32), _ptr(self.active_off, _P64)
+        m.uold, m.unew = _ptr(self.uold, _PD), _ptr(self.unew, _PD)
+        ns = nsubcycle or [2] * (MAXLEVEL + 1)
+        for i in range(MAXLEVEL + 1):
+            m.nsubcycle[i] = ns[i] if i < len(ns) else 2
+        m.nthreads = nthreads
+        self.m = m
+
+    def _check(self, rc, what):
+        if rc:
+            raise RuntimeError("%s failed: %d" % (what, rc))
+
+    def coarse_step(self):
+        self._check(lib().orc_coarse_step(ctypes.byref(self.p), ctypes.byref(self.m)), "coarse_step")
+
+    def godunov_fine(self, ilevel, dt):
+        self._check(lib().orc_godunov_fine(ctypes.byref(self.p), ctypes.byref(self.m), ilevel, dt), "godunov_fine")
+
+    def set_unew(self, ilevel):
+        lib().orc_set_unew(ctypes.byref(self.p), ctypes.byref(self.m), ilevel)
+
+    def set_uold(self, ilevel):
+        lib().orc_set_uold(ctypes.byref(self.p), ctypes.byref(self.m), ilevel)
+
+    def upload_fine(self, ilevel):
+        lib().orc_upload_fine(ctypes.byref(self.p), ctypes.byref(self.m), ilevel)
+
+    def courant_fine(self, ilevel, dt_in=None):
+        dt = ctypes.c_double(self.tree.boxlen / self.hp.smallc if dt_in is None else dt_in)
+        ma, ek, ei = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(lib().orc_courant_fine(ctypes.byref(self.p), ctypes.byref(self.m), ilevel,
+                                           ctypes.byref(dt), ctypes.byref(ma), ctypes.byref(ek),
+                                           ctypes.byref(ei)), "courant_fine")
+        return dt.value, ma.value, ek.value, ei.value
+
+    @property
+    def t(self):
+        return self.m.t
+
+    @property
+    def cell_updates(self):
+        return self.m.cell_updates
+
+    def dtnew(self, level):
+        return self.m.dtnew[level]
+
+    def get3cubefather(self, cell, ilevel):
+        out = np.zeros(27, np.int32)
+        self._check(lib().orc_get3cubefather(ctypes.byref(self.m), cell, ilevel, _ptr(out, _P32)), "get3cubefather")
+        return out
+
+    def getnborfather(self, cell, ilevel):
+        out = np.zeros(7, np.int32)
+        self._check(lib().orc_getnborfather(ctypes.byref(self.m), cell, ilevel, _ptr(out, _P32)), "getnborfather")
+        return out

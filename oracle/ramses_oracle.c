@@ -1,0 +1,1151 @@
+/*
+ * ramses_oracle.c -- CPU restatement of RAMSES's unsplit MUSCL-Hancock hydro
+ * step (NDIM=3, NENER=0, nvar=5, real*8). TEST INFRASTRUCTURE ONLY: the
+ * parity checker for the CUDA library and the timed CPU baseline; the
+ * product library never links or calls it.
+ *
+ * Parity status: line-by-line restatement of the cited Fortran, pinned
+ * physically against the reference's Sod known-answer table; bit-level
+ * parity with the Fortran binary is unpinned (no Fortran compiler here).
+ *
+ * Every expression keeps the Fortran evaluation order (left-to-right for
+ * operators of equal precedence, unary minus binding looser than '*'), and
+ * the file is compiled with -ffp-contract=off so that no multiply-add is
+ * fused, as in the reference's x86-64 gfortran -O3 build.
+ * Fortran sign(one,x) is copysign(1.0,x); x**2 is x*x.
+ */
+#include "ramses_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NV ORC_NVAR
+static const double zero = 0.0, half = 0.5, one = 1.0, two = 2.0;
+
+static inline double fmaxd(double a, double b) { return a > b ? a : (b > a ? b : a); }
+static inline double fmind(double a, double b) { return a < b ? a : (b < a ? b : a); }
+
+/* ------------------------------------------------------------------------ */
+/* Fortran-layout index helpers for the 6x6x6 stencil arrays (iu1=-1..iu2=4) */
+/* ------------------------------------------------------------------------ */
+#define S6(nv, l, i, j, k) ((size_t)(l) + (size_t)(nv) * ((size_t)((i) + 1) + 6u * ((size_t)((j) + 1) + 6u * (size_t)((k) + 1))))
+#define ST(nv) ((size_t)(nv) * 216u)
+/* q(nvector,-1:4,-1:4,-1:4,nvar) */
+#define QI(nv, l, i, j, k, v) (S6(nv, l, i, j, k) + ST(nv) * (size_t)((v) - 1))
+/* dq/qm/qp(nvector,-1:4,-1:4,-1:4,nvar,ndim) */
+#define QD(nv, l, i, j, k, v, d) (QI(nv, l, i, j, k, v) + ST(nv) * NV * (size_t)((d) - 1))
+/* flux(nvector,1:3,1:3,1:3,nvar,ndim) */
+#define FI(nv, l, i, j, k, v, d) ((size_t)(l) + (size_t)(nv) * ((size_t)((i) - 1) + 3u * ((size_t)((j) - 1) + 3u * ((size_t)((k) - 1) + 3u * ((size_t)((v) - 1) + (size_t)NV * (size_t)((d) - 1))))))
+/* tmp(nvector,1:3,1:3,1:3,2,ndim) */
+#define TI(nv, l, i, j, k, v, d) ((size_t)(l) + (size_t)(nv) * ((size_t)((i) - 1) + 3u * ((size_t)((j) - 1) + 3u * ((size_t)((k) - 1) + 3u * ((size_t)((v) - 1) + 2u * (size_t)((d) - 1))))))
+
+/* ------------------------------------------------------------------------ */
+/* ctoprim: hydro/umuscl.f90:861-965                                         */
+/* ------------------------------------------------------------------------ */
+static void ctoprim(const orc_params *p, const double *uin, double *q, double *c,
+                    const double *gravin, double dt, int ngrid, int nv) {
+  const double gamma = p->gamma;
+  const double smalle = p->smallc * p->smallc / gamma / (gamma - one); /* :891 */
+  const double dtxhalf = dt * half;
+  for (int k = -1; k <= 4; k++)
+    for (int j = -1; j <= 4; j++)
+      for (int i = -1; i <= 4; i++)
+        for (int l = 0; l < ngrid; l++) {
+          double q1 = fmaxd(uin[QI(nv, l, i, j, k, 1)], p->smallr); /* :901 */
+          double oneoverrho = one / q1;
+          double q2 = uin[QI(nv, l, i, j, k, 2)] * oneoverrho;
+          double q3 = uin[QI(nv, l, i, j, k, 3)] * oneoverrho;
+          double q4 = uin[QI(nv, l, i, j, k, 4)] * oneoverrho;
+          double eken = half * q2 * q2; /* :916-922 */
+          eken = eken + half * q3 * q3;
+          eken = eken + half * q4 * q4;
+          double erad = zero;
+          double eint = fmaxd(uin[QI(nv, l, i, j, k, 5)] * oneoverrho - eken - erad, smalle); /* :932 */
+          double q5 = (gamma - one) * q1 * eint;
+          double cc = gamma * q5; /* :936 */
+          cc = sqrt(cc * oneoverrho);
+          /* gravity predictor :944-951 */
+          q2 = q2 + gravin[QI(nv, l, i, j, k, 1)] * dtxhalf;
+          q3 = q3 + gravin[QI(nv, l, i, j, k, 2)] * dtxhalf;
+          q4 = q4 + gravin[QI(nv, l, i, j, k, 3)] * dtxhalf;
+          q[QI(nv, l, i, j, k, 1)] = q1;
+          q[QI(nv, l, i, j, k, 2)] = q2;
+          q[QI(nv, l, i, j, k, 3)] = q3;
+          q[QI(nv, l, i, j, k, 4)] = q4;
+          q[QI(nv, l, i, j, k, 5)] = q5;
+          c[S6(nv, l, i, j, k)] = cc;
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* uslope, 3D branch: hydro/umuscl.f90:970-1005, 1240-1478                   */
+/* ------------------------------------------------------------------------ */
+static inline double q_at(const double *q, int nv, int l, int i, int j, int k, int n) {
+  return q[QI(nv, l, i, j, k, n)];
+}
+
+static int uslope(const orc_params *p, const double *q, double *dq, int ngrid, int nv) {
+  const int st = p->slope_type;
+  if (st == 0) { /* :1002-1005 dq=zero */
+    memset(dq, 0, sizeof(double) * ST(nv) * NV * 3);
+    return 0;
+  }
+  if (st != 1 && st != 2 && st != 3 && st != 7 && st != 8) return -1; /* :1474 */
+  const double slope_type = (double)st;
+  const double theta = p->slope_theta;
+  static const int di[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int n = 1; n <= NV; n++)
+    for (int k = 0; k <= 3; k++)
+      for (int j = 0; j <= 3; j++)
+        for (int i = 0; i <= 3; i++) {
+          if (st == 3) { /* :1328-1392 positivity preserving */
+            for (int l = 0; l < ngrid; l++) {
+              double qc = q_at(q, nv, l, i, j, k, n);
+              double vmin = 0, vmax = 0;
+              int first = 1;
+              /* min/max over the 27 differences in the Fortran argument order
+               * (dflll, dflml, dflrl, dfmll, ... : i fastest, then j, then k) */
+              for (int kk = -1; kk <= 1; kk++)
+                for (int ii = -1; ii <= 1; ii++)
+                  for (int jj = -1; jj <= 1; jj++) {
+                    double d = q_at(q, nv, l, i + ii, j + jj, k + kk, n) - qc;
+                    if (first) { vmin = d; vmax = d; first = 0; }
+                    else { vmin = fmind(vmin, d); vmax = fmaxd(vmax, d); }
+                  }
+              double dfx = half * (q_at(q, nv, l, i + 1, j, k, n) - q_at(q, nv, l, i - 1, j, k, n));
+              double dfy = half * (q_at(q, nv, l, i, j + 1, k, n) - q_at(q, nv, l, i, j - 1, k, n));
+              double dfz = half * (q_at(q, nv, l, i, j, k + 1, n) - q_at(q, nv, l, i, j, k - 1, n));
+              double dff = half * (fabs(dfx) + fabs(dfy) + fabs(dfz));
+              double slop;
+              if (dff > zero) slop = fmind(one, fmind(fabs(vmin), fabs(vmax)) / dff);
+              else slop = one;
+              double dlim = slop;
+              dq[QD(nv, l, i, j, k, n, 1)] = dlim * dfx;
+              dq[QD(nv, l, i, j, k, n, 2)] = dlim * dfy;
+              dq[QD(nv, l, i, j, k, n, 3)] = dlim * dfz;
+            }
+            continue;
+          }
+          for (int d = 0; d < 3; d++) {
+            const int ox = di[d][0], oy = di[d][1], oz = di[d][2];
+            for (int l = 0; l < ngrid; l++) {
+              double qm1 = q_at(q, nv, l, i - ox, j - oy, k - oz, n);
+              double q0 = q_at(q, nv, l, i, j, k, n);
+              double qp1 = q_at(q, nv, l, i + ox, j + oy, k + oz, n);
+              double out;
+              if (st == 1) { /* minmod :1241-1285 */
+                double dlft = q0 - qm1;
+                double drgt = qp1 - q0;
+                if ((dlft * drgt) <= zero) out = zero;
+                else if (dlft > 0) out = fmind(dlft, drgt);
+                else out = fmaxd(dlft, drgt);
+              } else if (st == 2) { /* moncen :1286-1327 */
+                double dlft = slope_type * (q0 - qm1);
+                double drgt = slope_type * (qp1 - q0);
+                double dcen = half * (dlft + drgt) / slope_type;
+                double dsgn = copysign(one, dcen);
+                double slop = fmind(fabs(dlft), fabs(drgt));
+                double dlim = slop;
+                if ((dlft * drgt) <= zero) dlim = zero;
+                out = dsgn * fmind(dlim, fabs(dcen));
+              } else if (st == 7) { /* van Leer :1393-1431 */
+                double dlft = (q0 - qm1);
+                double drgt = (qp1 - q0);
+                if ((dlft * drgt) <= zero) out = zero;
+                else out = (2 * dlft * drgt / (dlft + drgt));
+              } else { /* st == 8, generalised moncen :1432-1473 */
+                double dlft = (q0 - qm1);
+                double drgt = (qp1 - q0);
+                double dcen = half * (dlft + drgt);
+                double dsgn = copysign(one, dcen);
+                double slop = fmind(theta * fabs(dlft), theta * fabs(drgt));
+                double dlim = slop;
+                if ((dlft * drgt) <= zero) dlim = zero;
+                out = dsgn * fmind(dlim, fabs(dcen));
+              }
+              dq[QD(nv, l, i, j, k, n, d + 1)] = out;
+            }
+          }
+        }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* trace3d: hydro/umuscl.f90:483-708                                         */
+/* ------------------------------------------------------------------------ */
+static void trace3d(const orc_params *p, const double *q, const double *dq, double *qm,
+                    double *qp, double dx, double dy, double dz, double dt, int ngrid,
+                    int nv) {
+  const double gamma = p->gamma, smallr = p->smallr;
+  const double dtdx = dt / dx, dtdy = dt / dy, dtdz = dt / dz; /* :523-525 */
+  enum { ir = 1, iu = 2, iv = 3, iw = 4, ip = 5 };
+  for (int k = 0; k <= 3; k++)
+    for (int j = 0; j <= 3; j++)
+      for (int i = 0; i <= 3; i++)
+        for (int l = 0; l < ngrid; l++) {
+          double r = q[QI(nv, l, i, j, k, ir)];
+          double u = q[QI(nv, l, i, j, k, iu)];
+          double v = q[QI(nv, l, i, j, k, iv)];
+          double w = q[QI(nv, l, i, j, k, iw)];
+          double pp = q[QI(nv, l, i, j, k, ip)];
+          double drx = dq[QD(nv, l, i, j, k, ir, 1)], dpx = dq[QD(nv, l, i, j, k, ip, 1)];
+          double dux = dq[QD(nv, l, i, j, k, iu, 1)], dvx = dq[QD(nv, l, i, j, k, iv, 1)];
+          double dwx = dq[QD(nv, l, i, j, k, iw, 1)];
+          double dry = dq[QD(nv, l, i, j, k, ir, 2)], dpy = dq[QD(nv, l, i, j, k, ip, 2)];
+          double duy = dq[QD(nv, l, i, j, k, iu, 2)], dvy = dq[QD(nv, l, i, j, k, iv, 2)];
+          double dwy = dq[QD(nv, l, i, j, k, iw, 2)];
+          double drz = dq[QD(nv, l, i, j, k, ir, 3)], dpz = dq[QD(nv, l, i, j, k, ip, 3)];
+          double duz = dq[QD(nv, l, i, j, k, iu, 3)], dvz = dq[QD(nv, l, i, j, k, iv, 3)];
+          double dwz = dq[QD(nv, l, i, j, k, iw, 3)];
+          /* :576-580 */
+          double sr0 = -(u * drx) - v * dry - w * drz - (dux + dvy + dwz) * r;
+          double sp0 = -(u * dpx) - v * dpy - w * dpz - (dux + dvy + dwz) * gamma * pp;
+          double su0 = -(u * dux) - v * duy - w * duz - (dpx) / r;
+          double sv0 = -(u * dvx) - v * dvy - w * dvz - (dpy) / r;
+          double sw0 = -(u * dwx) - v * dwy - w * dwz - (dpz) / r;
+          const double dtd[3] = {dtdx, dtdy, dtdz};
+          const double dr[3] = {drx, dry, drz}, dp_[3] = {dpx, dpy, dpz};
+          const double du[3] = {dux, duy, duz}, dv[3] = {dvx, dvy, dvz}, dw[3] = {dwx, dwy, dwz};
+          for (int d = 0; d < 3; d++) { /* :592-696 */
+            double t = dtd[d];
+            double *P = qp, *M = qm;
+            double v_;
+            v_ = r - half * dr[d] + sr0 * t * half;
+            P[QD(nv, l, i, j, k, ir, d + 1)] = v_;
+            P[QD(nv, l, i, j, k, ip, d + 1)] = pp - half * dp_[d] + sp0 * t * half;
+            P[QD(nv, l, i, j, k, iu, d + 1)] = u - half * du[d] + su0 * t * half;
+            P[QD(nv, l, i, j, k, iv, d + 1)] = v - half * dv[d] + sv0 * t * half;
+            P[QD(nv, l, i, j, k, iw, d + 1)] = w - half * dw[d] + sw0 * t * half;
+            if (v_ < smallr) P[QD(nv, l, i, j, k, ir, d + 1)] = r;
+            v_ = r + half * dr[d] + sr0 * t * half;
+            M[QD(nv, l, i, j, k, ir, d + 1)] = v_;
+            M[QD(nv, l, i, j, k, ip, d + 1)] = pp + half * dp_[d] + sp0 * t * half;
+            M[QD(nv, l, i, j, k, iu, d + 1)] = u + half * du[d] + su0 * t * half;
+            M[QD(nv, l, i, j, k, iv, d + 1)] = v + half * dv[d] + sv0 * t * half;
+            M[QD(nv, l, i, j, k, iw, d + 1)] = w + half * dw[d] + sw0 * t * half;
+            if (v_ < smallr) M[QD(nv, l, i, j, k, ir, d + 1)] = r;
+          }
+        }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Riemann solvers: hydro/godunov_utils.f90                                  */
+/* ql/qr = (rho, u_normal, P, u_t1, u_t2); fg = 6 fluxes (5 + thermal)       */
+/* ------------------------------------------------------------------------ */
+static void riemann_llf(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  /* :660-820 */
+  const double gamma = p->gamma;
+  const double smallp = p->smallc * p->smallc / gamma;
+  const double entho = one / (gamma - one);
+  double rl = fmaxd(ql[0], p->smallr), ul = ql[1], pl = fmaxd(ql[2], rl * smallp);
+  double cl = gamma * pl;
+  cl = sqrt(cl / rl);
+  double rr = fmaxd(qr[0], p->smallr), ur = qr[1], pr = fmaxd(qr[2], rr * smallp);
+  double cr = gamma * pr;
+  cr = sqrt(cr / rr);
+  double cmax = fmaxd(fabs(ul) + cl, fabs(ur) + cr);
+  double uL[6], uR[6], fL[6], fR[6];
+  uL[0] = ql[0];
+  uR[0] = qr[0];
+  uL[1] = ql[0] * ql[1];
+  uR[1] = qr[0] * qr[1];
+  uL[2] = ql[2] * entho + half * ql[0] * (ql[1] * ql[1]);
+  uR[2] = qr[2] * entho + half * qr[0] * (qr[1] * qr[1]);
+  uL[2] = uL[2] + half * ql[0] * (ql[3] * ql[3]);
+  uR[2] = uR[2] + half * qr[0] * (qr[3] * qr[3]);
+  uL[2] = uL[2] + half * ql[0] * (ql[4] * ql[4]);
+  uR[2] = uR[2] + half * qr[0] * (qr[4] * qr[4]);
+  for (int n = 3; n < 5; n++) {
+    uL[n] = ql[0] * ql[n];
+    uR[n] = qr[0] * qr[n];
+  }
+  uL[5] = ql[2] * entho;
+  uR[5] = qr[2] * entho;
+  fL[0] = ql[1] * uL[0];
+  fR[0] = qr[1] * uR[0];
+  fL[1] = ql[1] * uL[1] + ql[2];
+  fR[1] = qr[1] * uR[1] + qr[2];
+  fL[2] = ql[1] * (uL[2] + ql[2]);
+  fR[2] = qr[1] * (uR[2] + qr[2]);
+  for (int n = 3; n < 6; n++) {
+    fL[n] = ql[1] * uL[n];
+    fR[n] = qr[1] * uR[n];
+  }
+  for (int n = 0; n < 6; n++) fg[n] = half * (fL[n] + fR[n] - cmax * (uR[n] - uL[n]));
+}
+
+static void riemann_hll(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  /* :825-983 */
+  const double gamma = p->gamma;
+  const double smallp = p->smallc * p->smallc / gamma;
+  const double entho = one / (gamma - one);
+  double rl = fmaxd(ql[0], p->smallr), ul = ql[1], pl = fmaxd(ql[2], rl * smallp);
+  double cl = gamma * pl;
+  cl = sqrt(cl / rl);
+  double rr = fmaxd(qr[0], p->smallr), ur = qr[1], pr = fmaxd(qr[2], rr * smallp);
+  double cr = gamma * pr;
+  cr = sqrt(cr / rr);
+  double SL = fmind(fmind(ul, ur) - fmaxd(cl, cr), zero);
+  double SR = fmaxd(fmaxd(ul, ur) + fmaxd(cl, cr), zero);
+  double uL[6], uR[6], fL[6], fR[6];
+  uL[0] = ql[0];
+  uR[0] = qr[0];
+  uL[1] = ql[0] * ql[1];
+  uR[1] = qr[0] * qr[1];
+  uL[2] = ql[2] * entho + half * ql[0] * (ql[1] * ql[1]);
+  uR[2] = qr[2] * entho + half * qr[0] * (qr[1] * qr[1]);
+  uL[2] = uL[2] + half * ql[0] * (ql[3] * ql[3]);
+  uR[2] = uR[2] + half * qr[0] * (qr[3] * qr[3]);
+  uL[2] = uL[2] + half * ql[0] * (ql[4] * ql[4]);
+  uR[2] = uR[2] + half * qr[0] * (qr[4] * qr[4]);
+  for (int n = 3; n < 5; n++) {
+    uL[n] = ql[0] * ql[n];
+    uR[n] = qr[0] * qr[n];
+  }
+  uL[5] = ql[2] * entho;
+  uR[5] = qr[2] * entho;
+  fL[0] = uL[1];
+  fR[0] = uR[1];
+  fL[1] = ql[2] + uL[1] * ql[1];
+  fR[1] = qr[2] + uR[1] * qr[1];
+  fL[2] = ql[1] * (uL[2] + ql[2]);
+  fR[2] = qr[1] * (uR[2] + qr[2]);
+  for (int n = 3; n < 6; n++) {
+    fL[n] = ql[1] * uL[n];
+    fR[n] = qr[1] * uR[n];
+  }
+  for (int n = 0; n < 6; n++)
+    fg[n] = (SR * fL[n] - SL * fR[n] + SR * SL * (uR[n] - uL[n])) / (SR - SL);
+}
+
+static void riemann_hllc(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  /* :988-1209 */
+  const double gamma = p->gamma, smallc = p->smallc;
+  const double smallp = smallc * smallc / gamma;
+  const double entho = one / (gamma - one);
+  double rl = fmaxd(ql[0], p->smallr);
+  double Pl = fmaxd(ql[2], rl * smallp);
+  double ul = ql[1];
+  double el = Pl * entho;
+  double ecinl = half * rl * ul * ul;
+  ecinl = ecinl + half * rl * (ql[3] * ql[3]);
+  ecinl = ecinl + half * rl * (ql[4] * ql[4]);
+  double etotl = el + ecinl;
+  double Ptotl = Pl;
+  double rr = fmaxd(qr[0], p->smallr);
+  double Pr = fmaxd(qr[2], rr * smallp);
+  double ur = qr[1];
+  double er = Pr * entho;
+  double ecinr = half * rr * ur * ur;
+  ecinr = ecinr + half * rr * (qr[3] * qr[3]);
+  ecinr = ecinr + half * rr * (qr[4] * qr[4]);
+  double etotr = er + ecinr;
+  double Ptotr = Pr;
+  double cfastl = gamma * Pl;
+  cfastl = sqrt(fmaxd(cfastl / rl, smallc * smallc));
+  double cfastr = gamma * Pr;
+  cfastr = sqrt(fmaxd(cfastr / rr, smallc * smallc));
+  double SL = fmind(ul, ur) - fmaxd(cfastl, cfastr);
+  double SR = fmaxd(ul, ur) + fmaxd(cfastl, cfastr);
+  double rcl = rl * (ul - SL);
+  double rcr = rr * (SR - ur);
+  double ustar = (rcr * ur + rcl * ul + (Ptotl - Ptotr)) / (rcr + rcl);
+  double Ptotstar = (rcr * Ptotl + rcl * Ptotr + rcl * rcr * (ul - ur)) / (rcr + rcl);
+  double rstarl = rl * (SL - ul) / (SL - ustar);
+  double etotstarl = ((SL - ul) * etotl - Ptotl * ul + Ptotstar * ustar) / (SL - ustar);
+  double estarl = el * (SL - ul) / (SL - ustar);
+  double rstarr = rr * (SR - ur) / (SR - ustar);
+  double etotstarr = ((SR - ur) * etotr - Ptotr * ur + Ptotstar * ustar) / (SR - ustar);
+  double estarr = er * (SR - ur) / (SR - ustar);
+  double ro, uo, Ptoto, etoto, eo;
+  if (SL > 0.0) {
+    ro = rl; uo = ul; Ptoto = Ptotl; etoto = etotl; eo = el;
+  } else if (ustar > 0.0) {
+    ro = rstarl; uo = ustar; Ptoto = Ptotstar; etoto = etotstarl; eo = estarl;
+  } else if (SR > 0.0) {
+    ro = rstarr; uo = ustar; Ptoto = Ptotstar; etoto = etotstarr; eo = estarr;
+  } else {
+    ro = rr; uo = ur; Ptoto = Ptotr; etoto = etotr; eo = er;
+  }
+  fg[0] = ro * uo;
+  fg[1] = ro * uo * uo + Ptoto;
+  fg[2] = (etoto + Ptoto) * uo;
+  for (int n = 3; n < 5; n++) {
+    if (ustar > 0) fg[n] = ro * uo * ql[n];
+    else fg[n] = ro * uo * qr[n];
+  }
+  fg[5] = uo * eo;
+}
+
+/* ------------------------------------------------------------------------ */
+/* cmpflxm: hydro/umuscl.f90:714-856; the left state of face i is qm of cell  */
+/* i-1 (bounds shifted by one in the caller), the right state qp of cell i.  */
+/* ------------------------------------------------------------------------ */
+static int cmpflxm(const orc_params *p, const double *qm, const double *qp, int idim,
+                   int ilo, int ihi, int jlo, int jhi, int klo, int khi, double *fx,
+                   double *tx, int ngrid, int nv) {
+  const int ln = idim + 1;
+  const int lt1 = (idim == 1) ? 3 : 2;
+  const int lt2 = (idim == 3) ? 3 : 4;
+  const int sx = (idim == 1), sy = (idim == 2), sz = (idim == 3);
+  for (int k = klo; k <= khi; k++)
+    for (int j = jlo; j <= jhi; j++)
+      for (int i = ilo; i <= ihi; i++)
+        for (int l = 0; l < ngrid; l++) {
+          double ql[5], qr[5], fg[6];
+          ql[0] = qm[QD(nv, l, i - sx, j - sy, k - sz, 1, idim)];
+          qr[0] = qp[QD(nv, l, i, j, k, 1, idim)];
+          ql[1] = qm[QD(nv, l, i - sx, j - sy, k - sz, ln, idim)];
+          qr[1] = qp[QD(nv, l, i, j, k, ln, idim)];
+          ql[2] = qm[QD(nv, l, i - sx, j - sy, k - sz, 5, idim)];
+          qr[2] = qp[QD(nv, l, i, j, k, 5, idim)];
+          ql[3] = qm[QD(nv, l, i - sx, j - sy, k - sz, lt1, idim)];
+          qr[3] = qp[QD(nv, l, i, j, k, lt1, idim)];
+          ql[4] = qm[QD(nv, l, i - sx, j - sy, k - sz, lt2, idim)];
+          qr[4] = qp[QD(nv, l, i, j, k, lt2, idim)];
+          if (p->riemann == ORC_RIEMANN_LLF) riemann_llf(p, ql, qr, fg);
+          else if (p->riemann == ORC_RIEMANN_HLLC) riemann_hllc(p, ql, qr, fg);
+          else if (p->riemann == ORC_RIEMANN_HLL) riemann_hll(p, ql, qr, fg);
+          else return -1; /* :801-803 unknown Riemann solver */
+          fx[QI(nv, l, i, j, k, 1)] = fg[0];
+          fx[QI(nv, l, i, j, k, ln)] = fg[1];
+          fx[QI(nv, l, i, j, k, lt1)] = fg[3];
+          fx[QI(nv, l, i, j, k, lt2)] = fg[4];
+          fx[QI(nv, l, i, j, k, 5)] = fg[2];
+          tx[S6(nv, l, i, j, k)] = half * (ql[1] + qr[1]);
+          tx[S6(nv, l, i, j, k) + ST(nv)] = fg[5];
+        }
+  return 0;
+}
+
+/* Per-thread work arrays (the Fortran 'save' arrays of unsplit). */
+typedef struct work {
+  int nv;
+  double *qin, *cin, *dq, *qm, *qp, *fx, *tx;
+} work;
+
+static int work_init(work *w, int nv) {
+  w->nv = nv;
+  size_t s = ST(nv);
+  w->qin = (double *)malloc(sizeof(double) * s * NV);
+  w->cin = (double *)malloc(sizeof(double) * s);
+  w->dq = (double *)malloc(sizeof(double) * s * NV * 3);
+  w->qm = (double *)calloc(s * NV * 3, sizeof(double));
+  w->qp = (double *)calloc(s * NV * 3, sizeof(double));
+  w->fx = (double *)malloc(sizeof(double) * s * NV);
+  w->tx = (double *)malloc(sizeof(double) * s * 2);
+  return (w->qin && w->cin && w->dq && w->qm && w->qp && w->fx && w->tx) ? 0 : -1;
+}
+static void work_free(work *w) {
+  free(w->qin); free(w->cin); free(w->dq); free(w->qm); free(w->qp); free(w->fx); free(w->tx);
+}
+
+/* unsplit: hydro/umuscl.f90:22-171 (scheme='muscl', difmag=0) */
+static int unsplit_w(const orc_params *p, work *w, const double *uin, const double *gravin,
+                     double *flux, double *tmp, double dx, double dy, double dz, double dt,
+                     int ngrid) {
+  const int nv = w->nv;
+  ctoprim(p, uin, w->qin, w->cin, gravin, dt, ngrid, nv);
+  if (uslope(p, w->qin, w->dq, ngrid, nv)) return -2;
+  trace3d(p, w->qin, w->dq, w->qm, w->qp, dx, dy, dz, dt, ngrid, nv);
+  const double dd[3] = {dx, dy, dz};
+  for (int idim = 1; idim <= 3; idim++) {
+    /* x: i=if1..if2, j=jlo..jhi, k=klo..khi (:97-99); y, z analogously */
+    int ilo = 1, ihi = 2, jlo = 1, jhi = 2, klo = 1, khi = 2;
+    if (idim == 1) ihi = 3;
+    if (idim == 2) jhi = 3;
+    if (idim == 3) khi = 3;
+    if (cmpflxm(p, w->qm, w->qp, idim, ilo, ihi, jlo, jhi, klo, khi, w->fx, w->tx, ngrid, nv))
+      return -1;
+    const double dd_ = dd[idim - 1];
+    for (int i = ilo; i <= ihi; i++)
+      for (int j = jlo; j <= jhi; j++)
+        for (int k = klo; k <= khi; k++) {
+          for (int ivar = 1; ivar <= NV; ivar++)
+            for (int l = 0; l < ngrid; l++)
+              flux[FI(nv, l, i, j, k, ivar, idim)] = w->fx[QI(nv, l, i, j, k, ivar)] * dt / dd_;
+          for (int ivar = 1; ivar <= 2; ivar++)
+            for (int l = 0; l < ngrid; l++)
+              tmp[TI(nv, l, i, j, k, ivar, idim)] =
+                  w->tx[S6(nv, l, i, j, k) + ST(nv) * (size_t)(ivar - 1)] * dt / dd_;
+        }
+  }
+  return 0;
+}
+
+int orc_unsplit(const orc_params *p, const double *uin, const double *gravin, double *flux,
+                double *tmp, double dx, double dy, double dz, double dt, int ngrid,
+                int nvector) {
+  if (ngrid < 0 || ngrid > nvector) return -3;
+  work w;
+  if (work_init(&w, nvector)) { work_free(&w); return -4; }
+  int rc = unsplit_w(p, &w, uin, gravin, flux, tmp, dx, dy, dz, dt, ngrid);
+  work_free(&w);
+  return rc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* cmpdt: hydro/godunov_utils.f90:5-120; uu(nvector,5), gg(nvector,3)        */
+/* ------------------------------------------------------------------------ */
+double orc_cmpdt(const orc_params *p, double *uu, const double *gg, double dx, int ncell,
+                 int nv) {
+  const double gamma = p->gamma, smallc = p->smallc, C = p->courant_factor;
+  const double smallp = smallc * smallc / gamma;
+#define UU(k, v) uu[(size_t)(k) + (size_t)nv * (size_t)((v) - 1)]
+#define GG(k, d) gg[(size_t)(k) + (size_t)nv * (size_t)((d) - 1)]
+  for (int k = 0; k < ncell; k++) UU(k, 1) = fmaxd(UU(k, 1), p->smallr);
+  for (int idim = 1; idim <= 3; idim++)
+    for (int k = 0; k < ncell; k++) UU(k, idim + 1) = UU(k, idim + 1) / UU(k, 1);
+  for (int idim = 1; idim <= 3; idim++)
+    for (int k = 0; k < ncell; k++)
+      UU(k, 5) = UU(k, 5) - half * UU(k, 1) * (UU(k, idim + 1) * UU(k, idim + 1));
+  for (int k = 0; k < ncell; k++) UU(k, 5) = fmaxd((gamma - one) * UU(k, 5), UU(k, 1) * smallp);
+  for (int k = 0; k < ncell; k++) UU(k, 5) = gamma * UU(k, 5);
+  for (int k = 0; k < ncell; k++) UU(k, 5) = sqrt(UU(k, 5) / UU(k, 1));
+  for (int k = 0; k < ncell; k++) UU(k, 5) = 3.0 * UU(k, 5);
+  for (int idim = 1; idim <= 3; idim++)
+    for (int k = 0; k < ncell; k++) UU(k, 5) = UU(k, 5) + fabs(UU(k, idim + 1));
+  for (int k = 0; k < ncell; k++) UU(k, 1) = zero;
+  for (int idim = 1; idim <= 3; idim++)
+    for (int k = 0; k < ncell; k++) UU(k, 1) = UU(k, 1) + fabs(GG(k, idim));
+  for (int k = 0; k < ncell; k++) {
+    UU(k, 1) = UU(k, 1) * dx / (UU(k, 5) * UU(k, 5));
+    UU(k, 1) = fmaxd(UU(k, 1), 0.0001);
+  }
+  double dt = C * dx / smallc;
+  for (int k = 0; k < ncell; k++) {
+    double dtcell = dx / UU(k, 5) * (sqrt(one + two * C * UU(k, 1)) - one) / UU(k, 1);
+    dt = fmind(dt, dtcell);
+  }
+#undef UU
+#undef GG
+  return dt;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Mesh helpers                                                              */
+/* ------------------------------------------------------------------------ */
+static inline int64_t ncell_of(const orc_mesh *m) {
+  return (int64_t)m->ncoarse + 8 * (int64_t)m->ngridmax;
+}
+static inline int SON(const orc_mesh *m, int icell) { return m->son[icell - 1]; }
+static inline int NBOR(const orc_mesh *m, int igrid, int j) {
+  return m->nbor[(size_t)(j - 1) * (size_t)m->ngridmax + (size_t)(igrid - 1)];
+}
+static inline double *UOLD(const orc_mesh *m, int icell, int ivar) {
+  return &m->uold[(size_t)(ivar - 1) * (size_t)ncell_of(m) + (size_t)(icell - 1)];
+}
+static inline double *UNEW(const orc_mesh *m, int icell, int ivar) {
+  return &m->unew[(size_t)(ivar - 1) * (size_t)ncell_of(m) + (size_t)(icell - 1)];
+}
+static inline int64_t nactive(const orc_mesh *m, int ilevel) {
+  return m->active_off[ilevel + 1] - m->active_off[ilevel];
+}
+static inline const int32_t *active_list(const orc_mesh *m, int ilevel) {
+  return m->active + m->active_off[ilevel];
+}
+
+/* get3cubefather / get3cubepos: amr/nbors_utils.f90:5-300. The tables lll
+ * and mmm of getindices3cube (:305-358) are the geometric map "neighbour at
+ * offset (di,dj,dk) of the cell at position ind lies in the grid reached by
+ * stepping toward the cell's side of its oct"; they are evaluated here from
+ * that geometry, walking z, then y, then x as get3cubepos does. */
+int orc_get3cubefather(const orc_mesh *m, int fcell, int ilevel, int32_t *out27) {
+  if (ilevel == 1) { /* coarse cells, periodic arithmetic :27-138 */
+    if (fcell > m->ncoarse) return -1;
+    int nxny = m->nx * m->ny;
+    int iz = (fcell - 1) / nxny;
+    int iy = (fcell - 1 - iz * nxny) / m->nx;
+    int ix = (fcell - 1 - iy * m->nx - iz * nxny);
+    for (int k1 = 0; k1 <= 2; k1++) {
+      int iiz = iz + k1 - 1;
+      if (iiz < 0) iiz = m->nz - 1;
+      if (iiz > m->nz - 1) iiz = 0;
+      for (int j1 = 0; j1 <= 2; j1++) {
+        int iiy = iy + j1 - 1;
+        if (iiy < 0) iiy = m->ny - 1;
+        if (iiy > m->ny - 1) iiy = 0;
+        for (int i1 = 0; i1 <= 2; i1++) {
+          int iix = ix + i1 - 1;
+          if (iix < 0) iix = m->nx - 1;
+          if (iix > m->nx - 1) iix = 0;
+          out27[i1 + 3 * j1 + 9 * k1] = 1 + iix + iiy * m->nx + iiz * nxny;
+        }
+      }
+    }
+    return 0;
+  }
+  int pos = (fcell - m->ncoarse - 1) / m->ngridmax + 1;
+  int grid = fcell - m->ncoarse - (pos - 1) * m->ngridmax;
+  int c[3] = {(pos - 1) & 1, ((pos - 1) >> 1) & 1, ((pos - 1) >> 2) & 1};
+  /* the 2x2x2 grids: self and the neighbour toward the cell's side */
+  int grids[8];
+  for (int kk = 0; kk <= 1; kk++) {
+    int g1 = grid;
+    if (kk > 0 && g1 > 0) g1 = SON(m, NBOR(m, g1, c[2] ? 6 : 5));
+    for (int jj = 0; jj <= 1; jj++) {
+      int g2 = g1;
+      if (jj > 0 && g2 > 0) g2 = SON(m, NBOR(m, g2, c[1] ? 4 : 3));
+      for (int ii = 0; ii <= 1; ii++) {
+        int g3 = g2;
+        if (ii > 0 && g3 > 0) g3 = SON(m, NBOR(m, g3, c[0] ? 2 : 1));
+        grids[ii + 2 * jj + 4 * kk] = g3;
+      }
+    }
+  }
+  for (int k1 = 0; k1 <= 2; k1++)
+    for (int j1 = 0; j1 <= 2; j1++)
+      for (int i1 = 0; i1 <= 2; i1++) {
+        int o[3] = {i1 - 1, j1 - 1, k1 - 1}, sel = 0, cell = 0;
+        for (int a = 0; a < 3; a++) {
+          int cp = c[a] + o[a];
+          int g = (cp < 0) ? -1 : (cp > 1 ? 1 : 0);
+          if (g != 0) sel |= (1 << a);
+          cell |= ((cp - 2 * g) << a);
+        }
+        int gr = grids[sel];
+        out27[i1 + 3 * j1 + 9 * k1] =
+            gr > 0 ? m->ncoarse + cell * m->ngridmax + gr : 0;
+      }
+  return 0;
+}
+
+/* getnborfather: amr/nbors_utils.f90:404-525 (+ getnborgrids 530-555 and
+ * getnborcells 363-399, evaluated geometrically as above). */
+int orc_getnborfather(const orc_mesh *m, int cell, int ilevel, int32_t *f7) {
+  f7[0] = cell;
+  if (ilevel == 1) {
+    int nxny = m->nx * m->ny;
+    int ib[3] = {m->nx - 1, m->ny - 1, m->nz - 1};
+    int s1[3] = {1, m->nx, nxny};
+    int s2[3] = {m->nx - 1, (m->ny - 1) * m->nx, (m->nz - 1) * nxny};
+    int ix[3];
+    ix[2] = (cell - 1) / nxny;
+    ix[1] = (cell - 1 - ix[2] * nxny) / m->nx;
+    ix[0] = (cell - 1 - ix[1] * m->nx - ix[2] * nxny);
+    for (int d = 0; d < 3; d++) {
+      f7[2 * d + 1] = ix[d] > 0 ? cell - s1[d] : cell + s2[d];
+      f7[2 * d + 2] = ix[d] < ib[d] ? cell + s1[d] : cell - s2[d];
+    }
+    return 0;
+  }
+  int pos = (cell - m->ncoarse - 1) / m->ngridmax + 1;
+  int grid = cell - m->ncoarse - (pos - 1) * m->ngridmax;
+  int c[3] = {(pos - 1) & 1, ((pos - 1) >> 1) & 1, ((pos - 1) >> 2) & 1};
+  for (int j = 1; j <= 6; j++) {
+    int d = (j - 1) / 2, plus = (j - 1) & 1;
+    int inside = plus ? (c[d] == 0) : (c[d] == 1);
+    int g = inside ? grid : SON(m, NBOR(m, grid, j));
+    int cc[3] = {c[0], c[1], c[2]};
+    cc[d] = 1 - c[d];
+    int icell = 0;
+    if (g > 0) icell = m->ncoarse + (cc[0] + 2 * cc[1] + 4 * cc[2]) * m->ngridmax + g;
+    f7[j] = icell > 0 ? icell : NBOR(m, grid, j);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* interpol_hydro + limiters: hydro/interpol_hydro.f90:268-637               */
+/* u1(nn,0:6,5) -> u2(nn,1:8,5), leading dimension nn                        */
+/* ------------------------------------------------------------------------ */
+static void limiter_minmod(const double *a, double *w) { /* :449-476, a[0..6] */
+  for (int idim = 1; idim <= 3; idim++) {
+    double diff_left = 0.5 * (a[2 * idim] - a[0]);
+    double diff_right = 0.5 * (a[0] - a[2 * idim - 1]);
+    double minmod;
+    if (diff_left * diff_right <= 0.0) minmod = 0;
+    else minmod = fmind(fabs(diff_left), fabs(diff_right)) * diff_left / fabs(diff_left);
+    w[idim - 1] = minmod;
+  }
+}
+static void central(const double *a, double *w) { /* :618-637 */
+  for (int idim = 1; idim <= 3; idim++) w[idim - 1] = 0.25 * (a[2 * idim] - a[2 * idim - 1]);
+}
+static void limiter_central(const double *a, double *w) { /* :481-613 */
+  double xc[8][3];
+  for (int ind = 1; ind <= 8; ind++) {
+    int iz = (ind - 1) / 4, iy = (ind - 1 - 4 * iz) / 2, ix = (ind - 1 - 2 * iy - 4 * iz);
+    xc[ind - 1][0] = ((double)ix - 0.5);
+    xc[ind - 1][1] = ((double)iy - 0.5);
+    xc[ind - 1][2] = ((double)iz - 0.5);
+  }
+  for (int idim = 1; idim <= 3; idim++) w[idim - 1] = 0.25 * (a[2 * idim] - a[2 * idim - 1]);
+  double ac[8];
+  for (int ind = 0; ind < 8; ind++) ac[ind] = a[0];
+  for (int idim = 0; idim < 3; idim++)
+    for (int ind = 0; ind < 8; ind++) ac[ind] = ac[ind] + 2.0 * w[idim] * xc[ind][idim];
+  double corner = ac[0];
+  for (int j = 1; j < 8; j++) corner = fmaxd(corner, ac[j]);
+  double kernel = a[1];
+  for (int j = 2; j <= 6; j++) kernel = fmaxd(kernel, a[j]);
+  double diff_kernel = a[0] - kernel, diff_corner = a[0] - corner;
+  double max_limiter = 0.0;
+  if (diff_kernel * diff_corner > 0.0) max_limiter = fmind(1.0, diff_kernel / diff_corner);
+  corner = ac[0];
+  for (int j = 1; j < 8; j++) corner = fmind(corner, ac[j]);
+  kernel = a[1];
+  for (int j = 2; j <= 6; j++) kernel = fmind(kernel, a[j]);
+  diff_kernel = a[0] - kernel;
+  diff_corner = a[0] - corner;
+  double min_limiter = 0.0;
+  if (diff_kernel * diff_corner > 0.0) min_limiter = fmind(1.0, diff_kernel / diff_corner);
+  double limiter = fmind(min_limiter, max_limiter);
+  for (int idim = 0; idim < 3; idim++) w[idim] = w[idim] * limiter;
+}
+
+int orc_interpol_hydro(const orc_params *p, double *u1, double *u2, int nn) {
+#define U1(i, j, v) u1[(size_t)(i) + (size_t)nn * ((size_t)(j) + 7u * (size_t)((v) - 1))]
+#define U2(i, ind, v) u2[(size_t)(i) + (size_t)nn * ((size_t)((ind) - 1) + 8u * (size_t)((v) - 1))]
+  const int ivar_ = p->interpol_var, itype = p->interpol_type;
+  if (itype == 4 && ivar_ != 2) return -1; /* :369-371 */
+  if (ivar_ < 0 || ivar_ > 2 || itype < 0 || itype > 4) return -2;
+  const double oneover_twotondim = 1.0 / 8.0;
+  double xc[8][3];
+  for (int ind = 1; ind <= 8; ind++) {
+    int iz = (ind - 1) / 4, iy = (ind - 1 - 4 * iz) / 2, ix = (ind - 1 - 2 * iy - 4 * iz);
+    xc[ind - 1][0] = ((double)ix - 0.5);
+    xc[ind - 1][1] = ((double)iy - 0.5);
+    xc[ind - 1][2] = ((double)iz - 0.5);
+  }
+  for (int i = 0; i < nn; i++) {
+    if (ivar_ == 1 || ivar_ == 2) { /* :324-352 */
+      for (int j = 0; j <= 6; j++) {
+        double ekin = 0.0;
+        for (int idim = 1; idim <= 3; idim++)
+          ekin = ekin + 0.5 * (U1(i, j, idim + 1) * U1(i, j, idim + 1)) / fmaxd(U1(i, j, 1), p->smallr);
+        double erad = 0.0;
+        U1(i, j, 5) = U1(i, j, 5) - ekin - erad;
+        if (ivar_ == 2)
+          for (int idim = 1; idim <= 3; idim++)
+            U1(i, j, idim + 1) = U1(i, j, idim + 1) / fmaxd(U1(i, j, 1), p->smallr);
+      }
+    }
+    for (int ivar = 1; ivar <= NV; ivar++) { /* :355-394 */
+      double a[7], w[3] = {0.0, 0.0, 0.0};
+      for (int j = 0; j <= 6; j++) a[j] = U1(i, j, ivar);
+      if (itype == 1) limiter_minmod(a, w);
+      if (itype == 2) limiter_central(a, w);
+      if (itype == 3) central(a, w);
+      if (itype == 4) {
+        if (ivar > 1 && ivar <= 4) central(a, w);
+        else limiter_central(a, w);
+      }
+      for (int ind = 1; ind <= 8; ind++) {
+        double v = a[0];
+        for (int idim = 0; idim < 3; idim++) v = v + w[idim] * xc[ind - 1][idim];
+        U2(i, ind, ivar) = v;
+      }
+    }
+    if (ivar_ == 1 || ivar_ == 2) { /* :398-443 */
+      if (ivar_ == 2) {
+        for (int ind = 1; ind <= 8; ind++)
+          for (int idim = 1; idim <= 3; idim++)
+            U2(i, ind, idim + 1) = U2(i, ind, idim + 1) * U2(i, ind, 1);
+        for (int idim = 1; idim <= 3; idim++) {
+          double mom = 0;
+          for (int ind = 1; ind <= 8; ind++) mom = mom + U2(i, ind, idim + 1) * oneover_twotondim;
+          mom = mom - U1(i, 0, idim + 1) * U1(i, 0, 1);
+          for (int ind = 1; ind <= 8; ind++) U2(i, ind, idim + 1) = U2(i, ind, idim + 1) - mom;
+        }
+      }
+      for (int ind = 1; ind <= 8; ind++) {
+        double ekin = 0.0;
+        for (int idim = 1; idim <= 3; idim++)
+          ekin = ekin + 0.5 * (U2(i, ind, idim + 1) * U2(i, ind, idim + 1)) / fmaxd(U2(i, ind, 1), p->smallr);
+        double erad = 0.0;
+        U2(i, ind, 5) = U2(i, ind, 5) + ekin + erad;
+      }
+    }
+  }
+#undef U1
+#undef U2
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* set_unew / set_uold: hydro/godunov_fine.f90:40-130, 135-232               */
+/* (no pressure_fix, no momentum feedback, nvar = ndim+2, one CPU)           */
+/* ------------------------------------------------------------------------ */
+int orc_set_unew(const orc_params *p, orc_mesh *m, int ilevel) {
+  (void)p;
+  const int32_t *act = active_list(m, ilevel);
+  int64_t n = nactive(m, ilevel);
+  for (int ind = 1; ind <= 8; ind++) {
+    int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
+    for (int ivar = 1; ivar <= NV; ivar++)
+      for (int64_t i = 0; i < n; i++) *UNEW(m, act[i] + iskip, ivar) = *UOLD(m, act[i] + iskip, ivar);
+  }
+  return 0;
+}
+
+int orc_set_uold(const orc_params *p, orc_mesh *m, int ilevel) {
+  (void)p;
+  const int32_t *act = active_list(m, ilevel);
+  int64_t n = nactive(m, ilevel);
+  for (int ind = 1; ind <= 8; ind++) {
+    int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
+    for (int ivar = 1; ivar <= NV; ivar++)
+      for (int64_t i = 0; i < n; i++) *UOLD(m, act[i] + iskip, ivar) = *UNEW(m, act[i] + iskip, ivar);
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* upload_fine / upl: hydro/interpol_hydro.f90:5-263                         */
+/* ------------------------------------------------------------------------ */
+int orc_upload_fine(const orc_params *p, orc_mesh *m, int ilevel) {
+  if (ilevel == m->nlevelmax) return 0;
+  const int32_t *act = active_list(m, ilevel);
+  int64_t n = nactive(m, ilevel);
+  for (int64_t i = 0; i < n; i++)
+    for (int ind = 1; ind <= 8; ind++) {
+      int cell = m->ncoarse + (ind - 1) * m->ngridmax + act[i];
+      int gs = SON(m, cell);
+      if (gs <= 0) continue;
+      double getx = 0.0;
+      for (int is = 1; is <= 8; is++)
+        getx = getx + fmaxd(*UOLD(m, m->ncoarse + (is - 1) * m->ngridmax + gs, 1), p->smallr);
+      *UOLD(m, cell, 1) = getx / 8.0;
+      for (int ivar = 2; ivar <= NV; ivar++) {
+        getx = 0.0;
+        for (int is = 1; is <= 8; is++) getx = getx + *UOLD(m, m->ncoarse + (is - 1) * m->ngridmax + gs, ivar);
+        *UOLD(m, cell, ivar) = getx / 8.0;
+      }
+      if (p->interpol_var == 1 || p->interpol_var == 2) {
+        getx = 0.0;
+        for (int is = 1; is <= 8; is++) {
+          int sc = m->ncoarse + (is - 1) * m->ngridmax + gs;
+          double ekin = 0.0;
+          for (int idim = 1; idim <= 3; idim++)
+            ekin = ekin + 0.5 * (*UOLD(m, sc, 1 + idim) * *UOLD(m, sc, 1 + idim)) / fmaxd(*UOLD(m, sc, 1), p->smallr);
+          double erad = 0.0;
+          getx = getx + *UOLD(m, sc, 5) - ekin - erad;
+        }
+        double ekin = 0.0;
+        for (int idim = 1; idim <= 3; idim++)
+          ekin = ekin + 0.5 * (*UOLD(m, cell, 1 + idim) * *UOLD(m, cell, 1 + idim)) / fmaxd(*UOLD(m, cell, 1), p->smallr);
+        double erad = 0.0;
+        *UOLD(m, cell, 5) = getx / 8.0 + ekin + erad;
+      }
+    }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* courant_fine: hydro/courant_fine.f90:1-159                                */
+/* ------------------------------------------------------------------------ */
+int orc_courant_fine(const orc_params *p, orc_mesh *m, int ilevel, double *dt_io,
+                     double *mass, double *ekin, double *eint) {
+  const int nv = m->nvector;
+  double mass_loc = 0, ekin_loc = 0, eint_loc = 0, dt_loc = *dt_io;
+  int nx_loc = m->nx; /* icoarse_max-icoarse_min+1 */
+  double scale = m->boxlen / (double)nx_loc;
+  double dx = pow(0.5, ilevel) * scale;
+  double vol = dx * dx * dx;
+  const int32_t *act = active_list(m, ilevel);
+  int64_t ncache = nactive(m, ilevel);
+  double *uu = (double *)malloc(sizeof(double) * nv * NV);
+  double *gg = (double *)calloc((size_t)nv * 3, sizeof(double));
+  int *leaf = (int *)malloc(sizeof(int) * nv);
+  for (int64_t ig = 0; ig < ncache; ig += nv) {
+    int ngrid = (int)((ncache - ig) < nv ? (ncache - ig) : nv);
+    for (int ind = 1; ind <= 8; ind++) {
+      int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
+      int nleaf = 0;
+      for (int i = 0; i < ngrid; i++) {
+        int c = act[ig + i] + iskip;
+        if (SON(m, c) == 0) leaf[nleaf++] = c;
+      }
+      for (int ivar = 1; ivar <= NV; ivar++)
+        for (int i = 0; i < nleaf; i++) uu[i + (size_t)nv * (ivar - 1)] = *UOLD(m, leaf[i], ivar);
+      for (int i = 0; i < nleaf; i++) mass_loc = mass_loc + uu[i] * vol;
+      for (int i = 0; i < nleaf; i++) ekin_loc = ekin_loc + uu[i + (size_t)nv * 4] * vol;
+      for (int i = 0; i < nleaf; i++) eint_loc = eint_loc + uu[i + (size_t)nv * 4] * vol;
+      for (int iv = 1; iv <= 3; iv++)
+        for (int i = 0; i < nleaf; i++) {
+          double mv = uu[i + (size_t)nv * iv];
+          eint_loc = eint_loc - 0.5 * (mv * mv) / fmaxd(uu[i], p->smallr) * vol;
+        }
+      if (nleaf > 0) {
+        double dt_lev = orc_cmpdt(p, uu, gg, dx, nleaf, nv);
+        dt_loc = fmind(dt_loc, dt_lev);
+      }
+    }
+  }
+  free(uu); free(gg); free(leaf);
+  *dt_io = dt_loc;
+  if (mass) *mass = mass_loc;
+  if (ekin) *ekin = ekin_loc;
+  if (eint) *eint = eint_loc;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* godunov_fine / godfine1: hydro/godunov_fine.f90:5-35, 486-911             */
+/* Flux phase (gather + unsplit + refined-face zeroing) runs batch-parallel; */
+/* the unew updates are then applied serially in the reference batch order.  */
+/* ------------------------------------------------------------------------ */
+typedef struct batch {
+  int ncache;
+  int32_t *grids;   /* [nv] */
+  double *flux;     /* flux(nv,3,3,3,5,3) */
+} batch;
+
+static int godfine1_flux(const orc_params *p, const orc_mesh *m, work *w, const int32_t *ind_grid,
+                         int ncache, int ilevel, double dt, double *uloc, double *gloc,
+                         unsigned char *ok, double *flux, double *tmp, double *u1, double *u2) {
+  const int nv = m->nvector;
+  double scale = m->boxlen / (double)m->nx;
+  double dx = pow(0.5, ilevel) * scale;
+  int32_t nbf[27];
+  /* gathered as (27, nv): nbors_father_cells(i, ind_father) */
+  int32_t *nfc = (int32_t *)malloc(sizeof(int32_t) * 27 * nv);
+  int *ind_exist = (int *)malloc(sizeof(int) * nv), *ind_nexist = (int *)malloc(sizeof(int) * nv);
+  int *igrid_nbor = (int *)malloc(sizeof(int) * nv), *ind_buffer = (int *)malloc(sizeof(int) * nv);
+  int rc = 0;
+  for (int i = 0; i < ncache; i++) {
+    int fc = m->father[ind_grid[i] - 1];
+    if (orc_get3cubefather(m, fc, ilevel, nbf)) { rc = -5; goto done; }
+    for (int j = 0; j < 27; j++) nfc[j * nv + i] = nbf[j];
+  }
+  for (int k1 = 0; k1 <= 2; k1++)
+    for (int j1 = 0; j1 <= 2; j1++)
+      for (int i1 = 0; i1 <= 2; i1++) {
+        int nbuffer = 0, nexist = 0;
+        int ind_father = i1 + 3 * j1 + 9 * k1;
+        for (int i = 0; i < ncache; i++) {
+          int fcell = nfc[ind_father * nv + i];
+          if (fcell <= 0) { rc = -6; goto done; }
+          igrid_nbor[i] = SON(m, fcell);
+          if (igrid_nbor[i] > 0) ind_exist[nexist++] = i;
+          else { ind_nexist[nbuffer] = i; ind_buffer[nbuffer++] = fcell; }
+        }
+        if (nbuffer > 0) {
+          for (int i = 0; i < nbuffer; i++) {
+            int32_t f7[7];
+            orc_getnborfather(m, ind_buffer[i], ilevel, f7);
+            for (int j = 0; j <= 6; j++)
+              for (int ivar = 1; ivar <= NV; ivar++)
+                u1[(size_t)i + (size_t)nbuffer * ((size_t)j + 7u * (size_t)(ivar - 1))] = *UOLD(m, f7[j], ivar);
+          }
+          if (orc_interpol_hydro(p, u1, u2, nbuffer)) { rc = -7; goto done; }
+        }
+        for (int k2 = 0; k2 <= 1; k2++)
+          for (int j2 = 0; j2 <= 1; j2++)
+            for (int i2 = 0; i2 <= 1; i2++) {
+              int ind_son = 1 + i2 + 2 * j2 + 4 * k2;
+              int iskip = m->ncoarse + (ind_son - 1) * m->ngridmax;
+              int i3 = 1 + 2 * (i1 - 1) + i2, j3 = 1 + 2 * (j1 - 1) + j2, k3 = 1 + 2 * (k1 - 1) + k2;
+              for (int ivar = 1; ivar <= NV; ivar++) {
+                for (int e = 0; e < nexist; e++) {
+                  int i = ind_exist[e];
+                  uloc[QI(nv, i, i3, j3, k3, ivar)] = *UOLD(m, iskip + igrid_nbor[i], ivar);
+                }
+                for (int b = 0; b < nbuffer; b++)
+                  uloc[QI(nv, ind_nexist[b], i3, j3, k3, ivar)] =
+                      u2[(size_t)b + (size_t)nbuffer * ((size_t)(ind_son - 1) + 8u * (size_t)(ivar - 1))];
+              }
+              for (int e = 0; e < nexist; e++) {
+                int i = ind_exist[e];
+                ok[S6(nv, i, i3, j3, k3)] = SON(m, iskip + igrid_nbor[i]) > 0;
+              }
+              for (int b = 0; b < nbuffer; b++) ok[S6(nv, ind_nexist[b], i3, j3, k3)] = 0;
+            }
+      }
+  rc = unsplit_w(p, w, uloc, gloc, flux, tmp, dx, dx, dx, dt, ncache);
+  if (rc) goto done;
+  /* Reset flux along direction at refined interface :720-747 */
+  for (int idim = 1; idim <= 3; idim++) {
+    int i0 = idim == 1, j0 = idim == 2, k0 = idim == 3;
+    for (int k3 = 1; k3 <= 2 + k0; k3++)
+      for (int j3 = 1; j3 <= 2 + j0; j3++)
+        for (int i3 = 1; i3 <= 2 + i0; i3++)
+          for (int ivar = 1; ivar <= NV; ivar++)
+            for (int i = 0; i < ncache; i++)
+              if (ok[S6(nv, i, i3 - i0, j3 - j0, k3 - k0)] || ok[S6(nv, i, i3, j3, k3)])
+                flux[FI(nv, i, i3, j3, k3, ivar, idim)] = 0.0;
+  }
+done:
+  free(nfc); free(ind_exist); free(ind_nexist); free(igrid_nbor); free(ind_buffer);
+  return rc;
+}
+
+static void godfine1_update(const orc_mesh *m, const int32_t *ind_grid, int ncache,
+                            const double *flux) {
+  const int nv = m->nvector;
+  const double oneontwotondim = 1.0 / 8.0;
+  /* Conservative update at level ilevel :751-792 */
+  for (int idim = 1; idim <= 3; idim++) {
+    int i0 = idim == 1, j0 = idim == 2, k0 = idim == 3;
+    for (int k2 = 0; k2 <= 1; k2++)
+      for (int j2 = 0; j2 <= 1; j2++)
+        for (int i2 = 0; i2 <= 1; i2++) {
+          int ind_son = 1 + i2 + 2 * j2 + 4 * k2;
+          int iskip = m->ncoarse + (ind_son - 1) * m->ngridmax;
+          int i3 = 1 + i2, j3 = 1 + j2, k3 = 1 + k2;
+          for (int ivar = 1; ivar <= NV; ivar++)
+            for (int i = 0; i < ncache; i++) {
+              double *u = UNEW(m, iskip + ind_grid[i], ivar);
+              *u = *u + (flux[FI(nv, i, i3, j3, k3, ivar, idim)] -
+                         flux[FI(nv, i, i3 + i0, j3 + j0, k3 + k0, ivar, idim)]);
+            }
+        }
+  }
+  /* Conservative update at level ilevel-1 :798-908 */
+  int *buf = (int *)malloc(sizeof(int) * nv), *cel = (int *)malloc(sizeof(int) * nv);
+  for (int idim = 1; idim <= 3; idim++) {
+    int i0 = idim == 1, j0 = idim == 2, k0 = idim == 3;
+    /* left */
+    int nb = 0;
+    for (int i = 0; i < ncache; i++)
+      if (SON(m, NBOR(m, ind_grid[i], 2 * idim - 1)) == 0) {
+        buf[nb] = NBOR(m, ind_grid[i], 2 * idim - 1);
+        cel[nb++] = i;
+      }
+    for (int ivar = 1; ivar <= NV; ivar++)
+      for (int k3 = 1; k3 <= 2 - k0; k3++)
+        for (int j3 = 1; j3 <= 2 - j0; j3++)
+          for (int i3 = 1; i3 <= 2 - i0; i3++)
+            for (int i = 0; i < nb; i++) {
+              double *u = UNEW(m, buf[i], ivar);
+              *u = *u - flux[FI(nv, cel[i], i3, j3, k3, ivar, idim)] * oneontwotondim;
+            }
+    /* right */
+    nb = 0;
+    for (int i = 0; i < ncache; i++)
+      if (SON(m, NBOR(m, ind_grid[i], 2 * idim)) == 0) {
+        buf[nb] = NBOR(m, ind_grid[i], 2 * idim);
+        cel[nb++] = i;
+      }
+    for (int ivar = 1; ivar <= NV; ivar++)
+      for (int k3 = 1 + k0; k3 <= 2; k3++)
+        for (int j3 = 1 + j0; j3 <= 2; j3++)
+          for (int i3 = 1 + i0; i3 <= 2; i3++)
+            for (int i = 0; i < nb; i++) {
+              double *u = UNEW(m, buf[i], ivar);
+              *u = *u + flux[FI(nv, cel[i], i3 + i0, j3 + j0, k3 + k0, ivar, idim)] * oneontwotondim;
+            }
+  }
+  free(buf); free(cel);
+}
+
+int orc_godunov_fine(const orc_params *p, orc_mesh *m, int ilevel, double dt) {
+  const int nv = m->nvector;
+  int64_t ncache = nactive(m, ilevel);
+  if (ncache == 0) return 0;
+  const int32_t *act = active_list(m, ilevel);
+  int64_t nbatch = (ncache + nv - 1) / nv;
+  int nth = 1;
+#ifdef _OPENMP
+  nth = m->nthreads > 0 ? m->nthreads : omp_get_max_threads();
+#endif
+  const int64_t chunk = 64 * (int64_t)nth;
+  const size_t fsz = (size_t)nv * 27 * NV * 3;
+  double *fbuf = (double *)malloc(sizeof(double) * fsz * (size_t)(chunk < nbatch ? chunk : nbatch));
+  if (!fbuf) return -4;
+  int err = 0;
+  for (int64_t b0 = 0; b0 < nbatch && !err; b0 += chunk) {
+    int64_t nb = (nbatch - b0) < chunk ? (nbatch - b0) : chunk;
+#pragma omp parallel num_threads(nth)
+    {
+      work w;
+      int lerr = work_init(&w, nv);
+      double *uloc = (double *)malloc(sizeof(double) * ST(nv) * NV);
+      double *gloc = (double *)calloc(ST(nv) * 3, sizeof(double));
+      unsigned char *ok = (unsigned char *)calloc(ST(nv), 1);
+      double *tmp = (double *)malloc(sizeof(double) * (size_t)nv * 27 * 2 * 3);
+      double *u1 = (double *)malloc(sizeof(double) * (size_t)nv * 7 * NV);
+      double *u2 = (double *)malloc(sizeof(double) * (size_t)nv * 8 * NV);
+      if (!uloc || !gloc || !ok || !tmp || !u1 || !u2) lerr = -4;
+#pragma omp for schedule(dynamic, 4)
+      for (int64_t b = 0; b < nb; b++) {
+        if (lerr) continue;
+        int64_t g0 = (b0 + b) * nv;
+        int n = (int)((ncache - g0) < nv ? (ncache - g0) : nv);
+        int rc = godfine1_flux(p, m, &w, act + g0, n, ilevel, dt, uloc, gloc, ok,
+                               fbuf + fsz * (size_t)b, tmp, u1, u2);
+        if (rc) lerr = rc;
+      }
+      if (lerr) {
+#pragma omp critical
+        err = lerr;
+      }
+      work_free(&w);
+      free(uloc); free(gloc); free(ok); free(tmp); free(u1); free(u2);
+    }
+    if (err) break;
+    for (int64_t b = 0; b < nb; b++) {
+      int64_t g0 = (b0 + b) * nv;
+      int n = (int)((ncache - g0) < nv ? (ncache - g0) : nv);
+      godfine1_update(m, act + g0, n, fbuf + fsz * (size_t)b);
+    }
+  }
+  free(fbuf);
+  return err;
+}
+
+/* ------------------------------------------------------------------------ */
+/* amr_step hydro sequence: amr/amr_step.f90:320-445, 571-576;               */
+/* pm/newdt_fine.f90:47-51,177; amr/update_time.f90:330-331                  */
+/* ------------------------------------------------------------------------ */
+static int64_t leaf_cells(const orc_mesh *m, int ilevel) {
+  const int32_t *act = active_list(m, ilevel);
+  int64_t n = nactive(m, ilevel), c = 0;
+  for (int64_t i = 0; i < n; i++)
+    for (int ind = 1; ind <= 8; ind++)
+      c += SON(m, m->ncoarse + (ind - 1) * m->ngridmax + act[i]) == 0;
+  return c;
+}
+
+static int amr_step(const orc_params *p, orc_mesh *m, int ilevel, int icount) {
+  if (nactive(m, ilevel) == 0) return 0;
+  int rc;
+  /* newdt_fine */
+  m->dtold[ilevel] = m->dtnew[ilevel];
+  m->dtnew[ilevel] = m->boxlen / p->smallc;
+  double dt_all = m->dtnew[ilevel], ma, ek, ei;
+  if ((rc = orc_courant_fine(p, m, ilevel, &dt_all, &ma, &ek, &ei))) return rc;
+  m->mass_tot += ma; m->ekin_tot += ek; m->eint_tot += ei;
+  m->dtnew[ilevel] = fmind(m->dtnew[ilevel], dt_all);
+  if (ilevel > m->levelmin)
+    m->dtnew[ilevel] = fmind(m->dtnew[ilevel - 1] / (double)(float)m->nsubcycle[ilevel - 1], m->dtnew[ilevel]);
+  orc_set_unew(p, m, ilevel);
+  if (ilevel < m->nlevelmax) {
+    if (nactive(m, ilevel + 1) > 0) {
+      if (m->nsubcycle[ilevel] == 2) {
+        if ((rc = amr_step(p, m, ilevel + 1, 1))) return rc;
+        if ((rc = amr_step(p, m, ilevel + 1, 2))) return rc;
+      } else {
+        if ((rc = amr_step(p, m, ilevel + 1, 1))) return rc;
+      }
+    } else {
+      m->dtold[ilevel + 1] = m->dtnew[ilevel] / (double)m->nsubcycle[ilevel];
+      m->dtnew[ilevel + 1] = m->dtnew[ilevel] / (double)m->nsubcycle[ilevel];
+      m->t += m->dtnew[ilevel]; m->nstep++;
+    }
+  } else {
+    m->t += m->dtnew[ilevel]; m->nstep++;
+  }
+  m->cell_updates += leaf_cells(m, ilevel);
+  if ((rc = orc_godunov_fine(p, m, ilevel, m->dtnew[ilevel]))) return rc;
+  orc_set_uold(p, m, ilevel);
+  orc_upload_fine(p, m, ilevel);
+  if (ilevel > m->levelmin) {
+    if (m->nsubcycle[ilevel - 1] == 1) m->dtnew[ilevel - 1] = m->dtnew[ilevel];
+    if (icount == 2) m->dtnew[ilevel - 1] = m->dtold[ilevel] + m->dtnew[ilevel];
+  }
+  return 0;
+}
+
+int orc_coarse_step(const orc_params *p, orc_mesh *m) {
+  m->mass_tot = 0; m->ekin_tot = 0; m->eint_tot = 0;
+  int rc = amr_step(p, m, m->levelmin, 1);
+  if (rc) return rc;
+  for (int il = m->levelmin - 1; il >= 1; il--) orc_upload_fine(p, m, il);
+  return 0;
+}

@@ -1,0 +1,99 @@
+/*
+ * ramses_oracle.h -- CPU restatement of RAMSES's unsplit MUSCL-Hancock hydro
+ * step (NDIM=3, NENER=0, nvar=5, real*8), used ONLY as test infrastructure:
+ * the parity checker for the CUDA library and the timed CPU baseline.
+ * Nothing in the product library links or calls this code.
+ *
+ * Parity status: the reference is Fortran and no Fortran compiler exists in
+ * the build image, so this restatement could not be compiled against the
+ * reference binary. It is pinned (a) line by line to the cited Fortran and
+ * (b) physically against the reference's own Sod known-answer file
+ * (tests/hydro/sod-tube/sod-tube-ana.dat); 3D bit-level parity with the
+ * Fortran binary is unpinned.
+ *
+ * Array conventions follow the Fortran ones exactly (column-major, 1-based
+ * cell / grid indices stored as int32):
+ *   uold/unew(1:ncell,1:nvar)      -> u[(ivar-1)*ncell + (icell-1)]
+ *   son(1:ncell)                   -> son[icell-1]
+ *   father(1:ngridmax)             -> father[igrid-1]
+ *   nbor(1:ngridmax,1:6)           -> nbor[(j-1)*ngridmax + (igrid-1)]
+ *   icell = ncoarse + (ind-1)*ngridmax + igrid   (ind = 1..8 child slot)
+ */
+#ifndef RAMSES_ORACLE_H
+#define RAMSES_ORACLE_H
+#include <stdint.h>
+
+#define ORC_NVAR 5
+#define ORC_MAXLEVEL 32
+
+enum { ORC_RIEMANN_LLF = 1, ORC_RIEMANN_HLL = 2, ORC_RIEMANN_HLLC = 3 };
+
+typedef struct orc_params {
+  double gamma, smallr, smallc, courant_factor, slope_theta;
+  int32_t riemann;       /* ORC_RIEMANN_* */
+  int32_t slope_type;    /* 0,1,2,3,7,8 */
+  int32_t interpol_var;  /* 0,1,2 */
+  int32_t interpol_type; /* 0..4 */
+} orc_params;
+
+typedef struct orc_mesh {
+  int32_t nx, ny, nz, ncoarse, ngridmax, nlevelmax, levelmin, nvector;
+  double boxlen;
+  int32_t *son, *father, *nbor;
+  int32_t *active;      /* concatenated active(ilevel)%igrid lists        */
+  int64_t *active_off;  /* [nlevelmax+2]; level l list = [off[l],off[l+1]) */
+  double *uold, *unew;
+  int32_t nsubcycle[ORC_MAXLEVEL + 1];
+  double dtnew[ORC_MAXLEVEL + 1], dtold[ORC_MAXLEVEL + 1];
+  double t;
+  int64_t nstep;
+  double mass_tot, ekin_tot, eint_tot;
+  int64_t cell_updates; /* leaf-cell updates accumulated by orc_coarse_step */
+  int32_t nthreads;     /* OpenMP threads for the flux phase (0 = default) */
+} orc_mesh;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* umuscl.f90:22-171 with Fortran-layout arrays:
+ * uin(nvector,-1:4,-1:4,-1:4,5), gravin(nvector,-1:4,-1:4,-1:4,3),
+ * flux(nvector,1:3,1:3,1:3,5,3), tmp(nvector,1:3,1:3,1:3,2,3). */
+int orc_unsplit(const orc_params *p, const double *uin, const double *gravin,
+                double *flux, double *tmp, double dx, double dy, double dz,
+                double dt, int ngrid, int nvector);
+
+/* godunov_utils.f90:5-120 (cmpdt) for ncell cells, uu(nvector,5) layout. */
+double orc_cmpdt(const orc_params *p, double *uu, const double *gg, double dx,
+                 int ncell, int nvector);
+
+/* Level operations on the mesh (godunov_fine.f90, courant_fine.f90,
+ * interpol_hydro.f90). */
+int orc_set_unew(const orc_params *p, orc_mesh *m, int ilevel);
+int orc_set_uold(const orc_params *p, orc_mesh *m, int ilevel);
+int orc_godunov_fine(const orc_params *p, orc_mesh *m, int ilevel, double dt);
+int orc_courant_fine(const orc_params *p, orc_mesh *m, int ilevel,
+                     double *dt_io, double *mass, double *ekin, double *eint);
+int orc_upload_fine(const orc_params *p, orc_mesh *m, int ilevel);
+
+/* amr_step.f90 hydro call sequence for one coarse step (levelmin .. finest),
+ * followed by the restriction of levels levelmin-1..1 (adaptive_loop.f90). */
+int orc_coarse_step(const orc_params *p, orc_mesh *m);
+
+/* nbors_utils.f90:5-194 for one father cell: the 27 neighbouring father
+ * cells (1-based cell indices) of cell ind_cell_father at level ilevel-1. */
+int orc_get3cubefather(const orc_mesh *m, int ind_cell_father, int ilevel,
+                       int32_t *nbors_father_cells27);
+
+/* nbors_utils.f90:404-525: cell + 6 neighbour (or neighbour-father) cells. */
+int orc_getnborfather(const orc_mesh *m, int ind_cell, int ilevel,
+                      int32_t *ind_father7);
+
+/* interpol_hydro.f90:268-444 for nn father stencils:
+ * u1(nn,0:6,5) -> u2(nn,1:8,5), column-major with leading dim nn. */
+int orc_interpol_hydro(const orc_params *p, double *u1, double *u2, int nn);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,341 @@
+// godunov_tile.cuh -- the level-wide godunov kernel (godunov_fine.f90:5-35,
+// godfine1 :486-911 and unsplit, umuscl.f90:22-171) as a tiled sm_100a stencil.
+//
+// A tile is an aligned box of TX x TY x TZ level-l cells (TX/2 x TY/2 x TZ/2
+// octs). One CTA owns one tile:
+//   A. gather the (TX+4)(TY+4)(TZ+4) stencil into shared memory as primitive
+//      variables. Each 2x2x2 block of the stencil is an existing level-l oct
+//      (read from uold), a prolongated coarse cell (interpol_hydro, computed
+//      beforehand into the interpolation buffer), or absent (no active oct
+//      reads it); plus the refinement flag son(cell)>0 of every cell;
+//   B. slopes + MUSCL-Hancock trace once per cell of the tile and of the
+//      one-cell face slabs around it;
+//   C. one Riemann problem per face, flux*dt/dx, zeroed where either side is
+//      refined (godunov_fine.f90:720-747);
+//   D. unew += (Fx_l - Fx_r) then y then z for the cells of active octs
+//      (godunov_fine.f90:751-792);
+//   E. the boundary-face fluxes of octs that border an unrefined coarser cell
+//      are stored for the deterministic fine-to-coarse correction.
+// Every quantity is a pure function of its stencil, so computing each cell
+// and face once per tile gives the values the reference computes (redundantly)
+// per oct.
+#pragma once
+#include <cstdint>
+
+#include "hydro_core.cuh"
+
+namespace rb {
+
+struct TileArgs {
+  const double* __restrict__ uold;      // [5][ncell], device cell layout
+  double* __restrict__ unew;            // [5][ncell]
+  const int32_t* __restrict__ son;      // [ncell], device cell layout
+  const double* __restrict__ interp;    // [5][ninterp*8] prolongated blocks
+  const int32_t* __restrict__ tile_blk; // [ntile][NBLK] block codes
+  const int32_t* __restrict__ corr_slot;// [ngridmax] slot or -1 (may be null)
+  double* __restrict__ corr_flux;       // [nslot][6][4][5]
+  int64_t ncell;
+  int64_t ninterp8;                     // ninterp*8 (stride of interp)
+  int32_t ncoarse;
+  int32_t ntile;
+  int32_t has_refined;                  // any son>0 among this level's cells
+  int32_t dx_pow2;                      // dx is an exact power of two
+  int32_t fused;                        // 1: unew = uold + fluxes (set_unew fused) and
+                                        //    CFL partials of the new state
+  double dt, dx, inv_dx;
+  const double* __restrict__ dt_dev;    // if non-null, dt is read here
+  double* __restrict__ partial;         // fused: [ntile][4] (min dt, mass, E, eint)
+  rb_hydro_params hp;
+};
+
+// block code: >= 0 oct index (igrid-1); -1 absent; <= -2 interpolation entry (-code-2)
+template <int TX, int TY, int TZ>
+struct TileGeom {
+  static constexpr int SX = TX + 4, SY = TY + 4, SZ = TZ + 4;
+  static constexpr int NS = SX * SY * SZ;
+  static constexpr int BX = TX / 2 + 2, BY = TY / 2 + 2, BZ = TZ / 2 + 2;
+  static constexpr int NBLK = BX * BY * BZ;
+  // face-state arrays (per variable)
+  static constexpr int NFX = (TX + 1) * TY * TZ;
+  static constexpr int NFY = TX * (TY + 1) * TZ;
+  static constexpr int NFZ = TX * TY * (TZ + 1);
+  static constexpr int NF = NFX + NFY + NFZ;
+  static constexpr int NCELL = TX * TY * TZ;
+  static constexpr int NTRACE = NCELL + 2 * (TY * TZ + TX * TZ + TX * TY);
+  static_assert(5 * NF <= 5 * NS, "flux must fit in the stencil buffer");
+};
+
+template <typename R, int TX, int TY, int TZ>
+constexpr size_t tile_smem_bytes() {
+  using G = TileGeom<TX, TY, TZ>;
+  // q/flux union + face states (M and P) + block codes + refinement flags
+  return sizeof(R) * (size_t)(5 * G::NS) + sizeof(R) * (size_t)(2 * 5 * G::NF) +
+         sizeof(int32_t) * (size_t)G::NBLK + (size_t)((G::NS + 15) & ~15);
+}
+
+template <typename R, int TX, int TY, int TZ, int NT>
+__global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
+  using G = TileGeom<TX, TY, TZ>;
+  constexpr int SX = G::SX, SY = G::SY, SZ = G::SZ, NS = G::NS;
+  constexpr int BX = G::BX, BY = G::BY, NBLK = G::NBLK;
+  constexpr int NFX = G::NFX, NFY = G::NFY, NF = G::NF;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* q = reinterpret_cast<R*>(smem_raw);                 // [5][NS]; reused as flux [5][NF]
+  R* qm = q + 5 * NS;                                    // [5][NF]
+  R* qp = qm + 5 * NF;                                   // [5][NF]
+  int32_t* blk = reinterpret_cast<int32_t*>(qp + 5 * NF);// [NBLK]
+  unsigned char* okf = reinterpret_cast<unsigned char*>(blk + NBLK);  // [NS]
+
+  const int tile = blockIdx.x;
+  if (tile >= a.ntile) return;
+  const int tid = threadIdx.x;
+  const Consts<R> c = make_consts<R>(a.hp);
+  const int64_t ncell = a.ncell;
+
+  for (int i = tid; i < NBLK; i += NT) blk[i] = a.tile_blk[(int64_t)tile * NBLK + i];
+  __syncthreads();
+
+  // ---- A. gather + ctoprim ------------------------------------------------
+  const bool slope27 = (a.hp.slope_type == 3);
+  for (int it = tid; it < NBLK * 8; it += NT) {
+    const int b = it >> 3, ch = it & 7;
+    const int bx = b % BX, by = (b / BX) % BY, bz = b / (BX * BY);
+    const int sx = 2 * bx + (ch & 1), sy = 2 * by + ((ch >> 1) & 1), sz = 2 * bz + (ch >> 2);
+    const int s = sx + SX * (sy + SY * sz);
+    const int code = blk[b];
+    double u[5];
+    unsigned char ok = 0;
+    bool have = true;
+    if (!slope27) {
+      // corner cells of the stencil are read by no slope of types 0,1,2,7,8
+      const int hx = (sx < 2) | (sx >= SX - 2), hy = (sy < 2) | (sy >= SY - 2), hz = (sz < 2) | (sz >= SZ - 2);
+      if (hx + hy + hz == 3) have = false;
+    }
+    if (have && code >= 0) {
+      const int64_t dc = (int64_t)a.ncoarse + (int64_t)code * 8 + ch;
+#pragma unroll
+      for (int v = 0; v < 5; v++) u[v] = __ldg(a.uold + v * ncell + dc);
+      if (a.has_refined) ok = __ldg(a.son + dc) > 0;
+    } else if (have && code <= -2) {
+      const int64_t e = (int64_t)(-code - 2) * 8 + ch;
+#pragma unroll
+      for (int v = 0; v < 5; v++) u[v] = __ldg(a.interp + v * a.ninterp8 + e);
+    } else {
+      u[0] = 1.0; u[1] = 0.0; u[2] = 0.0; u[3] = 0.0; u[4] = 1.0;
+    }
+    Prim<R> pq = ctoprim_cell<R>(u, a.hp);
+    q[0 * NS + s] = pq.r;
+    q[1 * NS + s] = pq.u;
+    q[2 * NS + s] = pq.v;
+    q[3 * NS + s] = pq.w;
+    q[4 * NS + s] = pq.p;
+    okf[s] = ok;
+  }
+  __syncthreads();
+
+  // ---- B. slopes + trace ----------------------------------------------------
+  const double dt = a.dt_dev ? *a.dt_dev : a.dt;
+  R dtd[3];
+  {
+    const double dtdx = dt / a.dx;  // trace3d.f90 dtdx = dt/dx (dx=dy=dz)
+    dtd[0] = dtd[1] = dtd[2] = (R)dtdx;
+  }
+  for (int it = tid; it < G::NTRACE; it += NT) {
+    int x, y, z;
+    unsigned mask;
+    if (it < G::NCELL) {
+      x = it % TX; y = (it / TX) % TY; z = it / (TX * TY); mask = 7u;
+    } else {
+      int r = it - G::NCELL;
+      if (r < 2 * TY * TZ) {           // x slabs: x = -1 (qm only) and x = TX (qp only)
+        const int side = r / (TY * TZ); r %= TY * TZ;
+        x = side ? TX : -1; y = r % TY; z = r / TY; mask = 1u;
+      } else if ((r -= 2 * TY * TZ) < 2 * TX * TZ) {
+        const int side = r / (TX * TZ); r %= TX * TZ;
+        y = side ? TY : -1; x = r % TX; z = r / TX; mask = 2u;
+      } else {
+        r -= 2 * TX * TZ;
+        const int side = r / (TX * TY); r %= TX * TY;
+        z = side ? TZ : -1; x = r % TX; y = r / TX; mask = 4u;
+      }
+    }
+    const int s = (x + 2) + SX * ((y + 2) + SY * (z + 2));
+    R dq[5][3];
+    Prim<R> q0;
+    q0.r = q[s]; q0.u = q[NS + s]; q0.v = q[2 * NS + s]; q0.w = q[3 * NS + s]; q0.p = q[4 * NS + s];
+    if (a.hp.slope_type == 0) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) { dq[v][0] = (R)0; dq[v][1] = (R)0; dq[v][2] = (R)0; }
+    } else if (!slope27) {
+      constexpr int st[3] = {1, SX, SX * SY};
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const R* qv = q + v * NS;
+        const R qc = qv[s];
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+          dq[v][d] = slope1<R>(qv[s - st[d]], qc, qv[s + st[d]], a.hp.slope_type, c.slope_theta);
+      }
+    } else {
+      // positivity-preserving multidimensional slope (umuscl.f90:1328-1392)
+      const R half = (R)0.5, one = (R)1, zero = (R)0;
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const R* qv = q + v * NS;
+        const R qc = qv[s];
+        R vmin = (R)0, vmax = (R)0;
+        bool first = true;
+        for (int kk = -1; kk <= 1; kk++)
+          for (int ii = -1; ii <= 1; ii++)
+            for (int jj = -1; jj <= 1; jj++) {
+              const R d = qv[s + ii + SX * (jj + SY * kk)] - qc;
+              if (first) { vmin = d; vmax = d; first = false; }
+              else { vmin = fmn(vmin, d); vmax = fmx(vmax, d); }
+            }
+        const R dfx = half * (qv[s + 1] - qv[s - 1]);
+        const R dfy = half * (qv[s + SX] - qv[s - SX]);
+        const R dfz = half * (qv[s + SX * SY] - qv[s - SX * SY]);
+        const R dff = half * ((R)fabs(dfx) + (R)fabs(dfy) + (R)fabs(dfz));
+        R slop;
+        if (dff > zero) slop = fmn(one, fmn((R)fabs(vmin), (R)fabs(vmax)) / dff);
+        else slop = one;
+        dq[v][0] = slop * dfx; dq[v][1] = slop * dfy; dq[v][2] = slop * dfz;
+      }
+    }
+    Prim<R> sp[3], sm[3];
+    trace_cell<R>(q0, dq, c.gamma, c.smallr, dtd, sp, sm, mask);
+    // store: qm of direction d at face index (coord+1), qp at face index coord
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (!(mask & (1u << d))) continue;
+      int off, fm, fp;
+      if (d == 0) { off = 0;         fm = (x + 1) + (TX + 1) * (y + TY * z); fp = x + (TX + 1) * (y + TY * z); }
+      else if (d == 1) { off = NFX;  fm = x + TX * ((y + 1) + (TY + 1) * z); fp = x + TX * (y + (TY + 1) * z); }
+      else { off = NFX + NFY;        fm = x + TX * (y + TY * (z + 1));       fp = x + TX * (y + TY * z); }
+      const bool wm = (d == 0) ? (x < TX) : (d == 1) ? (y < TY) : (z < TZ);
+      const bool wp = (d == 0) ? (x >= 0) : (d == 1) ? (y >= 0) : (z >= 0);
+      if (wm) {
+        qm[0 * NF + off + fm] = sm[d].r; qm[1 * NF + off + fm] = sm[d].u; qm[2 * NF + off + fm] = sm[d].v;
+        qm[3 * NF + off + fm] = sm[d].w; qm[4 * NF + off + fm] = sm[d].p;
+      }
+      if (wp) {
+        qp[0 * NF + off + fp] = sp[d].r; qp[1 * NF + off + fp] = sp[d].u; qp[2 * NF + off + fp] = sp[d].v;
+        qp[3 * NF + off + fp] = sp[d].w; qp[4 * NF + off + fp] = sp[d].p;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- C. Riemann fluxes (flux buffer aliases q) ------------------------------
+  R* F = q;
+  for (int f = tid; f < NF; f += NT) {
+    int d, x, y, z;
+    if (f < NFX) { d = 0; x = f % (TX + 1); y = (f / (TX + 1)) % TY; z = f / ((TX + 1) * TY); }
+    else if (f < NFX + NFY) { const int r = f - NFX; d = 1; x = r % TX; y = (r / TX) % (TY + 1); z = r / (TX * (TY + 1)); }
+    else { const int r = f - NFX - NFY; d = 2; x = r % TX; y = (r / TX) % TY; z = r / (TX * TY); }
+    Prim<R> L, Rr;
+    L.r = qm[f]; L.u = qm[NF + f]; L.v = qm[2 * NF + f]; L.w = qm[3 * NF + f]; L.p = qm[4 * NF + f];
+    Rr.r = qp[f]; Rr.u = qp[NF + f]; Rr.v = qp[2 * NF + f]; Rr.w = qp[3 * NF + f]; Rr.p = qp[4 * NF + f];
+    R ql[5], qr[5], fg[6], fo[5];
+    to_face(L, d, ql);
+    to_face(Rr, d, qr);
+    riemann<R>(ql, qr, c, fg);
+    from_face(fg, d, fo);
+    // refined interface: either neighbour cell refined -> zero flux
+    const int sr = (x + 2) + SX * ((y + 2) + SY * (z + 2));
+    const int sl = sr - (d == 0 ? 1 : d == 1 ? SX : SX * SY);
+    const bool zero_face = okf[sl] | okf[sr];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      R val;
+      if (sizeof(R) == 8) {
+        // flux = fx*dt/dx, evaluated as (fx*dt)/dx (umuscl.f90:101-163);
+        // division by an exact power of two equals the multiplication
+        const double t = (double)fo[v] * dt;
+        val = (R)(a.dx_pow2 ? t * a.inv_dx : t / a.dx);
+      } else {
+        val = fo[v] * dtd[0];
+      }
+      F[v * NF + f] = zero_face ? (R)0 : val;
+    }
+  }
+  __syncthreads();
+
+  // ---- D. conservative update of active octs ----------------------------------
+  double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
+  const double vol = a.dx * a.dx * a.dx;
+  for (int it = tid; it < G::NCELL; it += NT) {
+    // octs-major order: 8 consecutive threads update one oct (coalesced rows)
+    const int o = it >> 3, ch = it & 7;
+    const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
+    const int code = blk[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
+    if (code < 0) continue;
+    const int x = 2 * ox + (ch & 1), y = 2 * oy + ((ch >> 1) & 1), z = 2 * oz + (ch >> 2);
+    const int fxl = x + (TX + 1) * (y + TY * z);
+    const int fyl = NFX + x + TX * (y + (TY + 1) * z);
+    const int fzl = NFX + NFY + x + TX * (y + TY * z);
+    const int64_t dc = (int64_t)a.ncoarse + (int64_t)code * 8 + ch;
+    double unv[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      const R* Fv = F + v * NF;
+      double un = a.fused ? __ldg(a.uold + v * ncell + dc) : a.unew[v * ncell + dc];
+      un = un + ((double)Fv[fxl] - (double)Fv[fxl + 1]);
+      un = un + ((double)Fv[fyl] - (double)Fv[fyl + TX]);
+      un = un + ((double)Fv[fzl] - (double)Fv[fzl + TX * TY]);
+      a.unew[v * ncell + dc] = un;
+      unv[v] = un;
+    }
+    if (a.fused) {
+      // courant_fine on the updated state (the next step's CFL condition)
+      mass = mass + unv[0] * vol;
+      etot = etot + unv[4] * vol;
+      double ei = unv[4] * vol;
+      for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (unv[d] * unv[d]) / fmx(unv[0], a.hp.smallr) * vol;
+      eint = eint + ei;
+      dtm = fmn(dtm, cmpdt_cell(unv, a.dx, a.hp));
+    }
+  }
+  if (a.fused) {
+    __shared__ double red[4][NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      dtm = fmn(dtm, __shfl_xor_sync(0xffffffffu, dtm, o));
+      mass += __shfl_xor_sync(0xffffffffu, mass, o);
+      etot += __shfl_xor_sync(0xffffffffu, etot, o);
+      eint += __shfl_xor_sync(0xffffffffu, eint, o);
+    }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = dtm; red[1][tid >> 5] = mass; red[2][tid >> 5] = etot; red[3][tid >> 5] = eint; }
+    __syncthreads();
+    if (tid == 0) {
+      for (int k = 1; k < NT / 32; k++) { dtm = fmn(dtm, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k]; }
+      a.partial[(int64_t)tile * 4 + 0] = dtm;
+      a.partial[(int64_t)tile * 4 + 1] = mass;
+      a.partial[(int64_t)tile * 4 + 2] = etot;
+      a.partial[(int64_t)tile * 4 + 3] = eint;
+    }
+  }
+
+  // ---- E. boundary fluxes for the fine-to-coarse correction --------------------
+  if (a.corr_slot != nullptr) {
+    constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
+    for (int it = tid; it < NOCT * 120; it += NT) {
+      const int o = it / 120, r = it % 120;
+      const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
+      const int code = blk[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
+      if (code < 0) continue;
+      const int slot = __ldg(a.corr_slot + code);
+      if (slot < 0) continue;
+      const int face = r / 20, cc = (r / 5) % 4, v = r % 5;   // face 0..5 = -x,+x,-y,+y,-z,+z
+      const int d = face >> 1, side = face & 1;
+      const int t1 = cc & 1, t2 = cc >> 1;
+      int fidx;
+      if (d == 0) { const int fx = 2 * ox + 2 * side; fidx = fx + (TX + 1) * ((2 * oy + t1) + TY * (2 * oz + t2)); }
+      else if (d == 1) { const int fy = 2 * oy + 2 * side; fidx = NFX + (2 * ox + t1) + TX * (fy + (TY + 1) * (2 * oz + t2)); }
+      else { const int fz = 2 * oz + 2 * side; fidx = NFX + NFY + (2 * ox + t1) + TX * ((2 * oy + t2) + TY * fz); }
+      a.corr_flux[(int64_t)slot * 120 + r] = (double)F[v * NF + fidx];
+    }
+  }
+}
+
+}  // namespace rb

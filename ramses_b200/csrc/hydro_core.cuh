@@ -1,0 +1,434 @@
+// hydro_core.cuh -- per-cell and per-face arithmetic of RAMSES's unsplit
+// MUSCL-Hancock scheme (NDIM=3, nvar=5), as device functions templated on
+// the compute type R.
+//
+// R = double: the FP64 drop-in. Every expression keeps the operation order of
+// the reference Fortran, and the translation units that instantiate it are
+// compiled with --fmad=false so that no multiply-add is contracted; results
+// are then bit-identical to the FP64 CPU restatement.
+// R = float: the FP32-mixed path. Slopes, trace and Riemann fluxes run in
+// FP32; conservative->primitive (density floor, E - 1/2 rho v^2, pressure
+// floor) stays FP64 and is rounded to FP32 on output.
+#pragma once
+#include <cstdint>
+
+#include "rb_types.h"
+
+namespace rb {
+
+// Fortran MAX/MIN with a fixed tie rule (first argument wins on equality),
+// used identically by the CPU restatement so that signed zeros agree.
+template <typename R> __device__ __forceinline__ R fmx(R a, R b) { return a > b ? a : (b > a ? b : a); }
+template <typename R> __device__ __forceinline__ R fmn(R a, R b) { return a < b ? a : (b < a ? b : a); }
+
+template <typename R> struct Prim { R r, u, v, w, p; };
+
+// Hydro constants in compute precision.
+template <typename R> struct Consts {
+  R gamma, smallr, smallc, smallp, entho, half, slope_theta, courant;
+  int slope_type, riemann;
+};
+
+template <typename R>
+__device__ __forceinline__ Consts<R> make_consts(const rb_hydro_params& hp) {
+  Consts<R> c;
+  c.gamma = (R)hp.gamma;
+  c.smallr = (R)hp.smallr;
+  c.smallc = (R)hp.smallc;
+  // smallp = smallc**2/gamma ; entho = one/(gamma-one) (godunov_utils.f90:1019-1020)
+  c.smallp = (R)(hp.smallc * hp.smallc / hp.gamma);
+  c.entho = (R)(1.0 / (hp.gamma - 1.0));
+  c.half = (R)0.5;
+  c.slope_theta = (R)hp.slope_theta;
+  c.courant = (R)hp.courant_factor;
+  c.slope_type = hp.slope_type;
+  c.riemann = hp.riemann;
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// ctoprim for one cell (umuscl.f90:861-965), conservative FP64 input.
+// The sound speed of ctoprim is only used by the PLMDE trace and is not formed.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ Prim<R> ctoprim_cell(const double u[5], const rb_hydro_params& hp) {
+  const double gamma = hp.gamma;
+  const double smalle = hp.smallc * hp.smallc / gamma / (gamma - 1.0);
+  double q1 = fmx(u[0], hp.smallr);
+  double oneoverrho = 1.0 / q1;
+  double q2 = u[1] * oneoverrho;
+  double q3 = u[2] * oneoverrho;
+  double q4 = u[3] * oneoverrho;
+  double eken = 0.5 * q2 * q2;
+  eken = eken + 0.5 * q3 * q3;
+  eken = eken + 0.5 * q4 * q4;
+  const double erad = 0.0;
+  double eint = fmx(u[4] * oneoverrho - eken - erad, smalle);
+  double q5 = (gamma - 1.0) * q1 * eint;
+  // gravity predictor with the zero gravity field of a pure-hydro run:
+  // q + 0*dt/2 == q + 0.0 (turns a negative zero positive, as the reference)
+  q2 = __dadd_rn(q2, 0.0);
+  q3 = __dadd_rn(q3, 0.0);
+  q4 = __dadd_rn(q4, 0.0);
+  Prim<R> q;
+  q.r = (R)q1; q.u = (R)q2; q.v = (R)q3; q.w = (R)q4; q.p = (R)q5;
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// One-direction limited slope (uslope, umuscl.f90:1241-1473) for slope types
+// 1 (minmod), 2 (moncen), 7 (van Leer), 8 (generalised moncen).
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ R slope1(R qm1, R q0, R qp1, int st, R theta) {
+  const R zero = (R)0, half = (R)0.5, one = (R)1;
+  if (st == 1) {
+    R dlft = q0 - qm1;
+    R drgt = qp1 - q0;
+    if ((dlft * drgt) <= zero) return zero;
+    if (dlft > 0) return fmn(dlft, drgt);
+    return fmx(dlft, drgt);
+  } else if (st == 2) {
+    const R two = (R)2;
+    R dlft = two * (q0 - qm1);
+    R drgt = two * (qp1 - q0);
+    R dcen = half * (dlft + drgt) / two;
+    R dsgn = copysign(one, dcen);
+    R slop = fmn(fabs(dlft), fabs(drgt));
+    R dlim = slop;
+    if ((dlft * drgt) <= zero) dlim = zero;
+    return dsgn * fmn(dlim, (R)fabs(dcen));
+  } else if (st == 7) {
+    R dlft = (q0 - qm1);
+    R drgt = (qp1 - q0);
+    if ((dlft * drgt) <= zero) return zero;
+    return ((R)2 * dlft * drgt / (dlft + drgt));
+  } else if (st == 8) {
+    R dlft = (q0 - qm1);
+    R drgt = (qp1 - q0);
+    R dcen = half * (dlft + drgt);
+    R dsgn = copysign(one, dcen);
+    R slop = fmn(theta * (R)fabs(dlft), theta * (R)fabs(drgt));
+    R dlim = slop;
+    if ((dlft * drgt) <= zero) dlim = zero;
+    return dsgn * fmn(dlim, (R)fabs(dcen));
+  }
+  return zero;  // slope_type 0
+}
+
+// MUSCL-Hancock predictor for one cell (trace3d, umuscl.f90:483-708):
+// given the cell state q and its 15 slopes dq[var][dir], produce the face
+// states qp[dir] (right state at the left interface) and qm[dir] (left state
+// at the right interface). Variables are ordered (r, u, v, w, p).
+template <typename R>
+__device__ __forceinline__ void trace_cell(const Prim<R>& q, const R dq[5][3], R gamma, R smallr,
+                                           const R dtd[3], Prim<R> qp[3], Prim<R> qm[3],
+                                           unsigned dirmask = 7u) {
+  const R half = (R)0.5;
+  const R r = q.r, u = q.u, v = q.v, w = q.w, p = q.p;
+  const R drx = dq[0][0], dry = dq[0][1], drz = dq[0][2];
+  const R dux = dq[1][0], duy = dq[1][1], duz = dq[1][2];
+  const R dvx = dq[2][0], dvy = dq[2][1], dvz = dq[2][2];
+  const R dwx = dq[3][0], dwy = dq[3][1], dwz = dq[3][2];
+  const R dpx = dq[4][0], dpy = dq[4][1], dpz = dq[4][2];
+  // source terms (:576-580)
+  const R sr0 = -(u * drx) - v * dry - w * drz - (dux + dvy + dwz) * r;
+  const R sp0 = -(u * dpx) - v * dpy - w * dpz - (dux + dvy + dwz) * gamma * p;
+  const R su0 = -(u * dux) - v * duy - w * duz - (dpx) / r;
+  const R sv0 = -(u * dvx) - v * dvy - w * dvz - (dpy) / r;
+  const R sw0 = -(u * dwx) - v * dwy - w * dwz - (dpz) / r;
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (!(dirmask & (1u << d))) continue;
+    const R t = dtd[d];
+    const R dr = dq[0][d], du = dq[1][d], dv = dq[2][d], dw = dq[3][d], dp = dq[4][d];
+    Prim<R> P, M;
+    P.r = r - half * dr + sr0 * t * half;
+    P.p = p - half * dp + sp0 * t * half;
+    P.u = u - half * du + su0 * t * half;
+    P.v = v - half * dv + sv0 * t * half;
+    P.w = w - half * dw + sw0 * t * half;
+    if (P.r < smallr) P.r = r;
+    M.r = r + half * dr + sr0 * t * half;
+    M.p = p + half * dp + sp0 * t * half;
+    M.u = u + half * du + su0 * t * half;
+    M.v = v + half * dv + sv0 * t * half;
+    M.w = w + half * dw + sw0 * t * half;
+    if (M.r < smallr) M.r = r;
+    qp[d] = P;
+    qm[d] = M;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers (godunov_utils.f90). Inputs in the face frame:
+// (rho, u_normal, P, u_t1, u_t2). Output f[0..4] = (mass, normal momentum,
+// energy, t1 momentum, t2 momentum) and f[5] = thermal-energy flux.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void riemann_llf(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  // :660-820
+  const R half = c.half;
+  R rl = fmx(ql[0], c.smallr), ul = ql[1], pl = fmx(ql[2], rl * c.smallp);
+  R cl = c.gamma * pl;
+  cl = sqrt(cl / rl);
+  R rr = fmx(qr[0], c.smallr), ur = qr[1], pr = fmx(qr[2], rr * c.smallp);
+  R cr = c.gamma * pr;
+  cr = sqrt(cr / rr);
+  R cmax = fmx((R)fabs(ul) + cl, (R)fabs(ur) + cr);
+  R uL[6], uR[6], fL[6], fR[6];
+  uL[0] = ql[0]; uR[0] = qr[0];
+  uL[1] = ql[0] * ql[1]; uR[1] = qr[0] * qr[1];
+  uL[2] = ql[2] * c.entho + half * ql[0] * (ql[1] * ql[1]);
+  uR[2] = qr[2] * c.entho + half * qr[0] * (qr[1] * qr[1]);
+  uL[2] = uL[2] + half * ql[0] * (ql[3] * ql[3]);
+  uR[2] = uR[2] + half * qr[0] * (qr[3] * qr[3]);
+  uL[2] = uL[2] + half * ql[0] * (ql[4] * ql[4]);
+  uR[2] = uR[2] + half * qr[0] * (qr[4] * qr[4]);
+  uL[3] = ql[0] * ql[3]; uR[3] = qr[0] * qr[3];
+  uL[4] = ql[0] * ql[4]; uR[4] = qr[0] * qr[4];
+  uL[5] = ql[2] * c.entho; uR[5] = qr[2] * c.entho;
+  fL[0] = ql[1] * uL[0]; fR[0] = qr[1] * uR[0];
+  fL[1] = ql[1] * uL[1] + ql[2]; fR[1] = qr[1] * uR[1] + qr[2];
+  fL[2] = ql[1] * (uL[2] + ql[2]); fR[2] = qr[1] * (uR[2] + qr[2]);
+#pragma unroll
+  for (int n = 3; n < 6; n++) { fL[n] = ql[1] * uL[n]; fR[n] = qr[1] * uR[n]; }
+#pragma unroll
+  for (int n = 0; n < 6; n++) f[n] = half * (fL[n] + fR[n] - cmax * (uR[n] - uL[n]));
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann_hll(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  // :825-983
+  const R half = c.half, zero = (R)0;
+  R rl = fmx(ql[0], c.smallr), ul = ql[1], pl = fmx(ql[2], rl * c.smallp);
+  R cl = c.gamma * pl;
+  cl = sqrt(cl / rl);
+  R rr = fmx(qr[0], c.smallr), ur = qr[1], pr = fmx(qr[2], rr * c.smallp);
+  R cr = c.gamma * pr;
+  cr = sqrt(cr / rr);
+  R SL = fmn(fmn(ul, ur) - fmx(cl, cr), zero);
+  R SR = fmx(fmx(ul, ur) + fmx(cl, cr), zero);
+  R uL[6], uR[6], fL[6], fR[6];
+  uL[0] = ql[0]; uR[0] = qr[0];
+  uL[1] = ql[0] * ql[1]; uR[1] = qr[0] * qr[1];
+  uL[2] = ql[2] * c.entho + half * ql[0] * (ql[1] * ql[1]);
+  uR[2] = qr[2] * c.entho + half * qr[0] * (qr[1] * qr[1]);
+  uL[2] = uL[2] + half * ql[0] * (ql[3] * ql[3]);
+  uR[2] = uR[2] + half * qr[0] * (qr[3] * qr[3]);
+  uL[2] = uL[2] + half * ql[0] * (ql[4] * ql[4]);
+  uR[2] = uR[2] + half * qr[0] * (qr[4] * qr[4]);
+  uL[3] = ql[0] * ql[3]; uR[3] = qr[0] * qr[3];
+  uL[4] = ql[0] * ql[4]; uR[4] = qr[0] * qr[4];
+  uL[5] = ql[2] * c.entho; uR[5] = qr[2] * c.entho;
+  fL[0] = uL[1]; fR[0] = uR[1];
+  fL[1] = ql[2] + uL[1] * ql[1]; fR[1] = qr[2] + uR[1] * qr[1];
+  fL[2] = ql[1] * (uL[2] + ql[2]); fR[2] = qr[1] * (uR[2] + qr[2]);
+#pragma unroll
+  for (int n = 3; n < 6; n++) { fL[n] = ql[1] * uL[n]; fR[n] = qr[1] * uR[n]; }
+#pragma unroll
+  for (int n = 0; n < 6; n++) f[n] = (SR * fL[n] - SL * fR[n] + SR * SL * (uR[n] - uL[n])) / (SR - SL);
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann_hllc(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  // :988-1209 (only the sampled star state is formed; the others are dead)
+  const R half = c.half;
+  R rl = fmx(ql[0], c.smallr);
+  R Pl = fmx(ql[2], rl * c.smallp);
+  R ul = ql[1];
+  R el = Pl * c.entho;
+  R ecinl = half * rl * ul * ul;
+  ecinl = ecinl + half * rl * (ql[3] * ql[3]);
+  ecinl = ecinl + half * rl * (ql[4] * ql[4]);
+  R etotl = el + ecinl;
+  R Ptotl = Pl;
+  R rr = fmx(qr[0], c.smallr);
+  R Pr = fmx(qr[2], rr * c.smallp);
+  R ur = qr[1];
+  R er = Pr * c.entho;
+  R ecinr = half * rr * ur * ur;
+  ecinr = ecinr + half * rr * (qr[3] * qr[3]);
+  ecinr = ecinr + half * rr * (qr[4] * qr[4]);
+  R etotr = er + ecinr;
+  R Ptotr = Pr;
+  const R smallc2 = c.smallc * c.smallc;
+  R cfastl = c.gamma * Pl;
+  cfastl = sqrt(fmx(cfastl / rl, smallc2));
+  R cfastr = c.gamma * Pr;
+  cfastr = sqrt(fmx(cfastr / rr, smallc2));
+  R SL = fmn(ul, ur) - fmx(cfastl, cfastr);
+  R SR = fmx(ul, ur) + fmx(cfastl, cfastr);
+  R rcl = rl * (ul - SL);
+  R rcr = rr * (SR - ur);
+  R ustar = (rcr * ur + rcl * ul + (Ptotl - Ptotr)) / (rcr + rcl);
+  R Ptotstar = (rcr * Ptotl + rcl * Ptotr + rcl * rcr * (ul - ur)) / (rcr + rcl);
+  R ro, uo, Ptoto, etoto, eo;
+  if (SL > (R)0) {
+    ro = rl; uo = ul; Ptoto = Ptotl; etoto = etotl; eo = el;
+  } else if (ustar > (R)0) {
+    ro = rl * (SL - ul) / (SL - ustar);
+    uo = ustar; Ptoto = Ptotstar;
+    etoto = ((SL - ul) * etotl - Ptotl * ul + Ptotstar * ustar) / (SL - ustar);
+    eo = el * (SL - ul) / (SL - ustar);
+  } else if (SR > (R)0) {
+    ro = rr * (SR - ur) / (SR - ustar);
+    uo = ustar; Ptoto = Ptotstar;
+    etoto = ((SR - ur) * etotr - Ptotr * ur + Ptotstar * ustar) / (SR - ustar);
+    eo = er * (SR - ur) / (SR - ustar);
+  } else {
+    ro = rr; uo = ur; Ptoto = Ptotr; etoto = etotr; eo = er;
+  }
+  f[0] = ro * uo;
+  f[1] = ro * uo * uo + Ptoto;
+  f[2] = (etoto + Ptoto) * uo;
+  if (ustar > (R)0) { f[3] = ro * uo * ql[3]; f[4] = ro * uo * ql[4]; }
+  else { f[3] = ro * uo * qr[3]; f[4] = ro * uo * qr[4]; }
+  f[5] = uo * eo;
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  if (c.riemann == RB_RIEMANN_HLLC) riemann_hllc(ql, qr, c, f);
+  else if (c.riemann == RB_RIEMANN_HLL) riemann_hll(ql, qr, c, f);
+  else riemann_llf(ql, qr, c, f);
+}
+
+// Face frame permutation of cmpflxm (umuscl.f90:745-790): normal velocity of
+// direction d is variable 1+d; the tangential ones are the remaining two in
+// ascending order.
+template <typename R>
+__device__ __forceinline__ void to_face(const Prim<R>& s, int d, R out[5]) {
+  out[0] = s.r;
+  out[2] = s.p;
+  if (d == 0) { out[1] = s.u; out[3] = s.v; out[4] = s.w; }
+  else if (d == 1) { out[1] = s.v; out[3] = s.u; out[4] = s.w; }
+  else { out[1] = s.w; out[3] = s.u; out[4] = s.v; }
+}
+
+// Godunov flux back in (rho, mx, my, mz, E) order.
+template <typename R>
+__device__ __forceinline__ void from_face(const R f[6], int d, R out[5]) {
+  out[0] = f[0];
+  out[4] = f[2];
+  if (d == 0) { out[1] = f[1]; out[2] = f[3]; out[3] = f[4]; }
+  else if (d == 1) { out[2] = f[1]; out[1] = f[3]; out[3] = f[4]; }
+  else { out[3] = f[1]; out[1] = f[3]; out[2] = f[4]; }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-to-fine prolongation of one child (interpol_hydro,
+// interpol_hydro.f90:268-637). u7[j][v]: father cell (j=0) and its 6
+// neighbours (-x,+x,-y,+y,-z,+z), conservative FP64. Produces the 8
+// children; called per child by the gather, results identical per child.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void interp_children(double u1[7][5], const rb_hydro_params& hp,
+                                                double u2[8][5]) {
+  const int ivar_ = hp.interpol_var, itype = hp.interpol_type;
+  const double smallr = hp.smallr;
+  if (ivar_ == 1 || ivar_ == 2) {
+    for (int j = 0; j <= 6; j++) {
+      double ekin = 0.0;
+      for (int idim = 1; idim <= 3; idim++)
+        ekin = ekin + 0.5 * (u1[j][idim] * u1[j][idim]) / fmx(u1[j][0], smallr);
+      const double erad = 0.0;
+      u1[j][4] = u1[j][4] - ekin - erad;
+      if (ivar_ == 2)
+        for (int idim = 1; idim <= 3; idim++) u1[j][idim] = u1[j][idim] / fmx(u1[j][0], smallr);
+    }
+  }
+  for (int iv = 0; iv < 5; iv++) {
+    double a[7], w[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j <= 6; j++) a[j] = u1[j][iv];
+    int t = itype;
+    if (itype == 4) t = (iv >= 1 && iv <= 3) ? 3 : 2;
+    if (t == 1) {  // compute_limiter_minmod :449-476
+      for (int idim = 1; idim <= 3; idim++) {
+        double dl = 0.5 * (a[2 * idim] - a[0]);
+        double dr = 0.5 * (a[0] - a[2 * idim - 1]);
+        double mm;
+        if (dl * dr <= 0.0) mm = 0;
+        else mm = fmn(fabs(dl), fabs(dr)) * dl / fabs(dl);
+        w[idim - 1] = mm;
+      }
+    } else if (t == 3) {  // compute_central :618-637
+      for (int idim = 1; idim <= 3; idim++) w[idim - 1] = 0.25 * (a[2 * idim] - a[2 * idim - 1]);
+    } else if (t == 2) {  // compute_limiter_central :481-613
+      for (int idim = 1; idim <= 3; idim++) w[idim - 1] = 0.25 * (a[2 * idim] - a[2 * idim - 1]);
+      double ac[8];
+      for (int ind = 0; ind < 8; ind++) ac[ind] = a[0];
+      for (int idim = 0; idim < 3; idim++)
+        for (int ind = 0; ind < 8; ind++) {
+          double xc = (double)((ind >> idim) & 1) - 0.5;
+          ac[ind] = ac[ind] + 2.0 * w[idim] * xc;
+        }
+      double corner = ac[0];
+      for (int j = 1; j < 8; j++) corner = fmx(corner, ac[j]);
+      double kernel = a[1];
+      for (int j = 2; j <= 6; j++) kernel = fmx(kernel, a[j]);
+      double dk = a[0] - kernel, dc = a[0] - corner;
+      double max_lim = 0.0;
+      if (dk * dc > 0.0) max_lim = fmn(1.0, dk / dc);
+      corner = ac[0];
+      for (int j = 1; j < 8; j++) corner = fmn(corner, ac[j]);
+      kernel = a[1];
+      for (int j = 2; j <= 6; j++) kernel = fmn(kernel, a[j]);
+      dk = a[0] - kernel;
+      dc = a[0] - corner;
+      double min_lim = 0.0;
+      if (dk * dc > 0.0) min_lim = fmn(1.0, dk / dc);
+      double lim = fmn(min_lim, max_lim);
+      for (int idim = 0; idim < 3; idim++) w[idim] = w[idim] * lim;
+    }
+    for (int ind = 0; ind < 8; ind++) {
+      double v = a[0];
+      for (int idim = 0; idim < 3; idim++) v = v + w[idim] * ((double)((ind >> idim) & 1) - 0.5);
+      u2[ind][iv] = v;
+    }
+  }
+  if (ivar_ == 1 || ivar_ == 2) {
+    if (ivar_ == 2) {
+      for (int ind = 0; ind < 8; ind++)
+        for (int idim = 1; idim <= 3; idim++) u2[ind][idim] = u2[ind][idim] * u2[ind][0];
+      for (int idim = 1; idim <= 3; idim++) {
+        double mom = 0;
+        for (int ind = 0; ind < 8; ind++) mom = mom + u2[ind][idim] * 0.125;
+        mom = mom - u1[0][idim] * u1[0][0];
+        for (int ind = 0; ind < 8; ind++) u2[ind][idim] = u2[ind][idim] - mom;
+      }
+    }
+    for (int ind = 0; ind < 8; ind++) {
+      double ekin = 0.0;
+      for (int idim = 1; idim <= 3; idim++)
+        ekin = ekin + 0.5 * (u2[ind][idim] * u2[ind][idim]) / fmx(u2[ind][0], smallr);
+      const double erad = 0.0;
+      u2[ind][4] = u2[ind][4] + ekin + erad;
+    }
+  }
+}
+
+// Per-cell CFL time step (cmpdt, godunov_utils.f90:5-120) with zero gravity.
+__device__ __forceinline__ double cmpdt_cell(const double uu_in[5], double dx, const rb_hydro_params& hp) {
+  const double gamma = hp.gamma, smallc = hp.smallc, C = hp.courant_factor;
+  const double smallp = smallc * smallc / gamma;
+  double u1 = fmx(uu_in[0], hp.smallr);
+  double v1 = uu_in[1] / u1, v2 = uu_in[2] / u1, v3 = uu_in[3] / u1;
+  double e = uu_in[4];
+  e = e - 0.5 * u1 * (v1 * v1);
+  e = e - 0.5 * u1 * (v2 * v2);
+  e = e - 0.5 * u1 * (v3 * v3);
+  e = fmx((gamma - 1.0) * e, u1 * smallp);
+  e = gamma * e;
+  e = sqrt(e / u1);
+  e = 3.0 * e;
+  e = e + fabs(v1);
+  e = e + fabs(v2);
+  e = e + fabs(v3);
+  double g = 0.0;
+  g = g + 0.0; g = g + 0.0; g = g + 0.0;  // sum of |gravity| over 3 directions
+  g = g * dx / (e * e);
+  g = fmx(g, 0.0001);
+  return dx / e * (sqrt(1.0 + 2.0 * C * g) - 1.0) / g;
+}
+
+}  // namespace rb

@@ -1,0 +1,351 @@
+// rb_aux.cuh -- FP64 kernels around the godunov tile kernel: coarse-to-fine
+// prolongation, deterministic fine-to-coarse flux correction, the CFL
+// reduction, set_unew/set_uold, restriction, and layout permutations between
+// the Fortran arrays and the device layout.
+//
+// Device layout: variable-major, then oct-major: u[v*ncell + dc] with
+// dc = icell-1 for the ncoarse coarse cells and dc = ncoarse + 8*(igrid-1) +
+// (ind-1) for child slot ind of oct igrid, so an oct's 8 cells of one
+// variable are one 64-byte row.
+#pragma once
+#include <cstdint>
+
+#include "hydro_core.cuh"
+
+namespace rb {
+
+__device__ __forceinline__ int64_t dev_cell_of_fortran(int64_t icell /*1-based*/, int32_t ncoarse,
+                                                       int32_t ngridmax) {
+  if (icell <= ncoarse) return icell - 1;
+  const int64_t r = icell - 1 - ncoarse;
+  const int64_t ind = r / ngridmax, ig = r % ngridmax;  // ig = igrid-1
+  return ncoarse + ig * 8 + ind;
+}
+
+// Fortran uold(ncell,5) -> device layout (and back).
+__global__ void permute_f2d_kernel(const double* __restrict__ f, double* __restrict__ d, int64_t ncell,
+                                   int32_t ncoarse, int32_t ngridmax, int nvar) {
+  const int64_t n = ncell * nvar;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ncell, icell = i % ncell + 1;
+    d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)] = f[i];
+  }
+}
+__global__ void permute_d2f_kernel(const double* __restrict__ d, double* __restrict__ f, int64_t ncell,
+                                   int32_t ncoarse, int32_t ngridmax, int nvar) {
+  const int64_t n = ncell * nvar;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ncell, icell = i % ncell + 1;
+    f[i] = d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)];
+  }
+}
+__global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t* __restrict__ d, int64_t ncell,
+                                   int32_t ncoarse, int32_t ngridmax) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += (int64_t)gridDim.x * blockDim.x)
+    d[dev_cell_of_fortran(i + 1, ncoarse, ngridmax)] = f[i];
+}
+
+// set_unew / set_uold (godunov_fine.f90:40-130, 135-232): copy the 8x5
+// values of every active oct. active[] holds igrid-1.
+__global__ void copy_octs_kernel(const double* __restrict__ src, double* __restrict__ dst,
+                                 const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
+                                 int32_t ncoarse) {
+  const int64_t n = (int64_t)noct * 8 * 5;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+    const int64_t dc = ncoarse + (int64_t)active[r >> 3] * 8 + (r & 7);
+    dst[v * ncell + dc] = src[v * ncell + dc];
+  }
+}
+
+// coarse-to-fine prolongation of the level's missing neighbour blocks
+// (interpol_hydro, called from godunov_fine.f90:584-592). cells7[e*7+j]: device
+// cell of the father cell (j=0) and of its 6 neighbour (or neighbour-father)
+// cells, as getnborfather (nbors_utils.f90:404-525) returns them.
+__global__ void interp_blocks_kernel(const double* __restrict__ uold, const int32_t* __restrict__ cells7,
+                                     int32_t nentry, int64_t ncell, double* __restrict__ out,
+                                     rb_hydro_params hp) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nentry) return;
+  double u1[7][5], u2[8][5];
+  for (int j = 0; j < 7; j++) {
+    const int64_t dc = cells7[(int64_t)e * 7 + j];
+    for (int v = 0; v < 5; v++) u1[j][v] = uold[v * ncell + dc];
+  }
+  interp_children(u1, hp, u2);
+  const int64_t stride = (int64_t)nentry * 8;
+  for (int ind = 0; ind < 8; ind++)
+    for (int v = 0; v < 5; v++) out[v * stride + (int64_t)e * 8 + ind] = u2[ind][v];
+}
+
+// Fine-to-coarse correction (godunov_fine.f90:798-908), applied target by
+// target with the contributions in the reference's sweep order: by vector
+// batch of the contributing oct, then direction, then left before right, and
+// within one face its 4 fine cells in (k3,j3,i3) order.
+// contrib[k] = slot*6 + face (face 0..5 = -x,+x,-y,+y,-z,+z).
+__global__ void apply_corrections_kernel(double* __restrict__ unew, const int32_t* __restrict__ tgt,
+                                         const int32_t* __restrict__ off, const int32_t* __restrict__ contrib,
+                                         int32_t ntgt, const double* __restrict__ corr_flux, int64_t ncell) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntgt) return;
+  const int64_t dc = tgt[t];
+  const double oneontwotondim = 1.0 / 8.0;
+  for (int v = 0; v < 5; v++) {
+    double u = unew[v * ncell + dc];
+    for (int k = off[t]; k < off[t + 1]; k++) {
+      const int slot = contrib[k] / 6, face = contrib[k] % 6;
+      const double* fl = corr_flux + (int64_t)slot * 120 + face * 20;
+      if ((face & 1) == 0) {
+        for (int c = 0; c < 4; c++) u = u - fl[c * 5 + v] * oneontwotondim;
+      } else {
+        for (int c = 0; c < 4; c++) u = u + fl[c * 5 + v] * oneontwotondim;
+      }
+    }
+    unew[v * ncell + dc] = u;
+  }
+}
+
+// courant_fine (courant_fine.f90:1-159): per-block partial (min dt, mass,
+// total energy, internal energy) over the leaf cells of the level's octs.
+// A second single-block pass reduces the partials in a fixed order.
+template <int NT>
+__global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __restrict__ uold,
+                                                             const int32_t* __restrict__ son,
+                                                             const int32_t* __restrict__ active, int32_t noct,
+                                                             int64_t ncell, int32_t ncoarse, double dx,
+                                                             rb_hydro_params hp, double* __restrict__ partial) {
+  const double vol = dx * dx * dx;
+  double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    if (son[dc] != 0) continue;
+    double u[5];
+    for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    mass = mass + u[0] * vol;
+    etot = etot + u[4] * vol;
+    double ei = u[4] * vol;
+    for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (u[d] * u[d]) / fmx(u[0], hp.smallr) * vol;
+    eint = eint + ei;
+    dtm = fmn(dtm, cmpdt_cell(u, dx, hp));
+  }
+  __shared__ double red[4][NT / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    dtm = fmn(dtm, __shfl_xor_sync(0xffffffffu, dtm, o));
+    mass += __shfl_xor_sync(0xffffffffu, mass, o);
+    etot += __shfl_xor_sync(0xffffffffu, etot, o);
+    eint += __shfl_xor_sync(0xffffffffu, eint, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { red[0][w] = dtm; red[1][w] = mass; red[2][w] = etot; red[3][w] = eint; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < NT / 32; k++) {
+      dtm = fmn(dtm, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k];
+    }
+    partial[blockIdx.x * 4 + 0] = dtm;
+    partial[blockIdx.x * 4 + 1] = mass;
+    partial[blockIdx.x * 4 + 2] = etot;
+    partial[blockIdx.x * 4 + 3] = eint;
+  }
+}
+
+// Deterministic reduction of per-block partials (min dt, mass, E, eint) by
+// one CTA of RB_RED_NT threads in a fixed order.
+// mode 0 (courant_fine, courant_fine.f90:33,123-127,154): out[0] = dt_in if the
+//   level has no leaf cell, else min(dt_in, min(courant_factor*dx/smallc,
+//   min cell dt)); out[1..3] = mass, E, eint.
+// mode 1 (device clock of the uniform stepper): out[1] += out[0] (time
+//   advanced by the step just taken), out[0] = the next step's dt as
+//   newdt_fine + courant_fine give it, out[2..4] = totals, out[5] += 1.
+#define RB_RED_NT 1024
+__global__ void __launch_bounds__(RB_RED_NT) reduce_partials_kernel(const double* __restrict__ partial, int n,
+                                                                    double dt_in, double dt_cmpdt0, int any_leaf,
+                                                                    double* __restrict__ out, int mode) {
+  __shared__ double red[4][RB_RED_NT];
+  double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
+  for (int k = threadIdx.x; k < n; k += RB_RED_NT) {
+    dtm = fmn(dtm, partial[k * 4 + 0]);
+    mass += partial[k * 4 + 1];
+    etot += partial[k * 4 + 2];
+    eint += partial[k * 4 + 3];
+  }
+  red[0][threadIdx.x] = dtm; red[1][threadIdx.x] = mass; red[2][threadIdx.x] = etot; red[3][threadIdx.x] = eint;
+  __syncthreads();
+  for (int h = RB_RED_NT / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      red[0][threadIdx.x] = fmn(red[0][threadIdx.x], red[0][threadIdx.x + h]);
+      red[1][threadIdx.x] += red[1][threadIdx.x + h];
+      red[2][threadIdx.x] += red[2][threadIdx.x + h];
+      red[3][threadIdx.x] += red[3][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double dt_lev = fmn(dt_cmpdt0, red[0][0]);
+    if (mode == 0) {
+      out[0] = any_leaf ? fmn(dt_in, dt_lev) : dt_in;
+      out[1] = red[1][0]; out[2] = red[2][0]; out[3] = red[3][0];
+    } else {
+      out[1] = out[1] + out[0];
+      out[0] = fmn(dt_in, dt_lev);
+      out[2] = red[1][0]; out[3] = red[2][0]; out[4] = red[3][0];
+      out[5] = out[5] + 1.0;
+    }
+  }
+}
+
+// upload_fine / upl (interpol_hydro.f90:5-263): restriction of every split
+// cell of the level's active octs from its 8 children.
+__global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,
+                                   const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
+                                   int32_t ncoarse, rb_hydro_params hp) {
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    const int gs = son[dc];
+    if (gs <= 0) continue;
+    const int64_t c0 = ncoarse + (int64_t)(gs - 1) * 8;
+    double getx = 0.0;
+    for (int is = 0; is < 8; is++) getx = getx + fmx(uold[c0 + is], hp.smallr);
+    uold[dc] = getx / 8.0;
+    for (int v = 1; v < 5; v++) {
+      getx = 0.0;
+      for (int is = 0; is < 8; is++) getx = getx + uold[v * ncell + c0 + is];
+      uold[v * ncell + dc] = getx / 8.0;
+    }
+    if (hp.interpol_var == 1 || hp.interpol_var == 2) {
+      getx = 0.0;
+      for (int is = 0; is < 8; is++) {
+        const int64_t sc = c0 + is;
+        double ekin = 0.0;
+        for (int d = 1; d <= 3; d++)
+          ekin = ekin + 0.5 * (uold[d * ncell + sc] * uold[d * ncell + sc]) / fmx(uold[sc], hp.smallr);
+        const double erad = 0.0;
+        getx = getx + uold[4 * ncell + sc] - ekin - erad;
+      }
+      double ekin = 0.0;
+      for (int d = 1; d <= 3; d++)
+        ekin = ekin + 0.5 * (uold[d * ncell + dc] * uold[d * ncell + dc]) / fmx(uold[dc], hp.smallr);
+      const double erad = 0.0;
+      uold[4 * ncell + dc] = getx / 8.0 + ekin + erad;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// unsplit with the reference's own Fortran array layout (umuscl.f90:22-38):
+// uin(nvector,-1:4,-1:4,-1:4,5), gravin(nvector,-1:4,-1:4,-1:4,3),
+// flux(nvector,1:3,1:3,1:3,5,3), tmp(nvector,1:3,1:3,1:3,2,3).
+// One CTA per oct (grid index l); the 32 traced cells and 36 faces the
+// fluxes depend on are computed from the 6x6x6 stencil in shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double* __restrict__ uin,
+                                                             const double* __restrict__ gravin,
+                                                             double* __restrict__ flux, double* __restrict__ tmp,
+                                                             double dx, double dy, double dz, double dt,
+                                                             int ngrid, int nvector, rb_hydro_params hp) {
+  const int l = blockIdx.x;
+  if (l >= ngrid) return;
+  __shared__ double q[5][216];
+  __shared__ double qm[5][3][64], qp[5][3][64];  // indexed [v][dir][cell 4x4x4 over 0..3]
+  const Consts<double> c = make_consts<double>(hp);
+  const int64_t nv = nvector;
+  auto S6 = [&](int i, int j, int k) { return (int64_t)l + nv * ((i + 1) + 6 * ((j + 1) + 6 * (k + 1))); };
+  const int64_t st = nv * 216;
+  const double dtxhalf = dt * 0.5;
+  for (int s = threadIdx.x; s < 216; s += 64) {
+    const int i = s % 6 - 1, j = (s / 6) % 6 - 1, k = s / 36 - 1;
+    double u[5];
+    for (int v = 0; v < 5; v++) u[v] = uin[S6(i, j, k) + st * v];
+    // ctoprim including the gravity predictor with the caller's gravin
+    const double gamma = hp.gamma;
+    const double smalle = hp.smallc * hp.smallc / gamma / (gamma - 1.0);
+    double q1 = fmx(u[0], hp.smallr);
+    double oneoverrho = 1.0 / q1;
+    double q2 = u[1] * oneoverrho, q3 = u[2] * oneoverrho, q4 = u[3] * oneoverrho;
+    double eken = 0.5 * q2 * q2;
+    eken = eken + 0.5 * q3 * q3;
+    eken = eken + 0.5 * q4 * q4;
+    const double erad = 0.0;
+    double eint = fmx(u[4] * oneoverrho - eken - erad, smalle);
+    double q5 = (gamma - 1.0) * q1 * eint;
+    q2 = q2 + gravin[S6(i, j, k)] * dtxhalf;
+    q3 = q3 + gravin[S6(i, j, k) + st] * dtxhalf;
+    q4 = q4 + gravin[S6(i, j, k) + 2 * st] * dtxhalf;
+    q[0][s] = q1; q[1][s] = q2; q[2][s] = q3; q[3][s] = q4; q[4][s] = q5;
+  }
+  __syncthreads();
+  const double dtd[3] = {dt / dx, dt / dy, dt / dz};
+  for (int cidx = threadIdx.x; cidx < 64; cidx += 64) {
+    const int i = cidx % 4, j = (cidx / 4) % 4, k = cidx / 16;  // cells 0..3
+    const int s = (i + 1) + 6 * ((j + 1) + 6 * (k + 1));
+    double dq[5][3];
+    Prim<double> q0;
+    q0.r = q[0][s]; q0.u = q[1][s]; q0.v = q[2][s]; q0.w = q[3][s]; q0.p = q[4][s];
+    if (hp.slope_type == 0) {
+      for (int v = 0; v < 5; v++) dq[v][0] = dq[v][1] = dq[v][2] = 0.0;
+    } else if (hp.slope_type != 3) {
+      const int stp[3] = {1, 6, 36};
+      for (int v = 0; v < 5; v++)
+        for (int d = 0; d < 3; d++)
+          dq[v][d] = slope1<double>(q[v][s - stp[d]], q[v][s], q[v][s + stp[d]], hp.slope_type, hp.slope_theta);
+    } else {
+      for (int v = 0; v < 5; v++) {
+        const double qc = q[v][s];
+        double vmin = 0, vmax = 0;
+        bool first = true;
+        for (int kk = -1; kk <= 1; kk++)
+          for (int ii = -1; ii <= 1; ii++)
+            for (int jj = -1; jj <= 1; jj++) {
+              const double d = q[v][s + ii + 6 * jj + 36 * kk] - qc;
+              if (first) { vmin = d; vmax = d; first = false; }
+              else { vmin = fmn(vmin, d); vmax = fmx(vmax, d); }
+            }
+        const double dfx = 0.5 * (q[v][s + 1] - q[v][s - 1]);
+        const double dfy = 0.5 * (q[v][s + 6] - q[v][s - 6]);
+        const double dfz = 0.5 * (q[v][s + 36] - q[v][s - 36]);
+        const double dff = 0.5 * (fabs(dfx) + fabs(dfy) + fabs(dfz));
+        double slop;
+        if (dff > 0.0) slop = fmn(1.0, fmn(fabs(vmin), fabs(vmax)) / dff);
+        else slop = 1.0;
+        dq[v][0] = slop * dfx; dq[v][1] = slop * dfy; dq[v][2] = slop * dfz;
+      }
+    }
+    Prim<double> sp[3], sm[3];
+    trace_cell<double>(q0, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
+    for (int d = 0; d < 3; d++) {
+      qm[0][d][cidx] = sm[d].r; qm[1][d][cidx] = sm[d].u; qm[2][d][cidx] = sm[d].v;
+      qm[3][d][cidx] = sm[d].w; qm[4][d][cidx] = sm[d].p;
+      qp[0][d][cidx] = sp[d].r; qp[1][d][cidx] = sp[d].u; qp[2][d][cidx] = sp[d].v;
+      qp[3][d][cidx] = sp[d].w; qp[4][d][cidx] = sp[d].p;
+    }
+  }
+  __syncthreads();
+  const double ddd[3] = {dx, dy, dz};
+  for (int f = threadIdx.x; f < 36; f += 64) {
+    const int d = f / 12, r = f % 12;
+    // face (i,j,k) in 1..3 along d, 1..2 across; left cell = face - e_d
+    int i, j, k;
+    if (d == 0) { i = 1 + r % 3; j = 1 + (r / 3) % 2; k = 1 + r / 6; }
+    else if (d == 1) { i = 1 + r % 2; j = 1 + (r / 2) % 3; k = 1 + r / 6; }
+    else { i = 1 + r % 2; j = 1 + (r / 2) % 2; k = 1 + r / 4; }
+    const int cr = i + 4 * (j + 4 * k);
+    const int cl = cr - (d == 0 ? 1 : d == 1 ? 4 : 16);
+    Prim<double> L, Rr;
+    L.r = qm[0][d][cl]; L.u = qm[1][d][cl]; L.v = qm[2][d][cl]; L.w = qm[3][d][cl]; L.p = qm[4][d][cl];
+    Rr.r = qp[0][d][cr]; Rr.u = qp[1][d][cr]; Rr.v = qp[2][d][cr]; Rr.w = qp[3][d][cr]; Rr.p = qp[4][d][cr];
+    double ql[5], qr[5], fg[6], fo[5];
+    to_face(L, d, ql);
+    to_face(Rr, d, qr);
+    riemann<double>(ql, qr, c, fg);
+    from_face(fg, d, fo);
+    const int64_t base = (int64_t)l + nv * ((i - 1) + 3 * ((j - 1) + 3 * (k - 1)));
+    const int64_t s3 = nv * 27;
+    for (int v = 0; v < 5; v++) flux[base + s3 * (v + 5 * d)] = fo[v] * dt / ddd[d];
+    tmp[base + s3 * (0 + 2 * d)] = 0.5 * (ql[1] + qr[1]) * dt / ddd[d];
+    tmp[base + s3 * (1 + 2 * d)] = fg[5] * dt / ddd[d];
+  }
+}
+
+}  // namespace rb

@@ -1,0 +1,1114 @@
+// rb_runtime.cu -- host runtime and C ABI of the B200 hydro step.
+//
+// Owns one problem per rb_context: device mirrors of uold/unew/son in the
+// device layout (variable-major, oct-major), per-level tables derived from the
+// octree (active lists, godunov tiles, prolongation entries, fine-to-coarse
+// correction lists), and the amr_step hydro scheduler
+// (amr/amr_step.f90:320-445) that drives the level kernels on one stream.
+// Compiled with --fmad=false (FP64 kernels bit-identical to the reference
+// operation order).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ramses_b200.h"
+#include "godunov_tile.cuh"
+#include "rb_aux.cuh"
+#include "tile_launch.h"
+
+namespace {
+
+// host-side Fortran MIN with the same tie rule as the device and the oracle
+inline double rb_min_host(double a, double b) { return a < b ? a : (b < a ? b : a); }
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define RB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(RB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                                 \
+  } while (0)
+
+#define RB_TRY(expr)       \
+  do {                     \
+    int rc_ = (expr);      \
+    if (rc_) return rc_;   \
+  } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) return RB_OK;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(RB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  return RB_OK;
+}
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+inline int grid_for(int64_t n, int nt, int cap = 148 * 32) {
+  int64_t g = (n + nt - 1) / nt;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+struct Level {
+  int noct = 0;
+  std::vector<int32_t> h_active;  // igrid (1-based), host order
+  int32_t* d_active = nullptr;    // igrid-1
+  int shape = -1;
+  int ntile = 0;
+  int32_t* d_tile_blk = nullptr;
+  int ninterp = 0;
+  int32_t* d_interp7 = nullptr;
+  double* d_interp_buf = nullptr;
+  int has_refined = 0;
+  int nslot = 0;
+  double* d_corr_flux = nullptr;
+  int ntgt = 0;
+  int32_t* d_tgt = nullptr;
+  int32_t* d_tgt_off = nullptr;
+  int32_t* d_contrib = nullptr;
+  int64_t leaf_cells = 0;
+  double dx = 0.0;
+  bool complete = false;
+  bool tables_built = false;
+};
+
+// sorted (key, igrid) lookup of one level's octs
+struct OctIndex {
+  std::vector<std::pair<int64_t, int32_t>> v;
+  int64_t nx = 1, ny = 1, nz = 1;  // octs per dimension at this level
+  int64_t key(int64_t x, int64_t y, int64_t z) const {
+    x = ((x % nx) + nx) % nx;
+    y = ((y % ny) + ny) % ny;
+    z = ((z % nz) + nz) % nz;
+    return x + nx * (y + ny * z);
+  }
+  int32_t find(int64_t x, int64_t y, int64_t z) const {
+    const int64_t k = key(x, y, z);
+    auto it = std::lower_bound(v.begin(), v.end(), std::make_pair(k, (int32_t)INT32_MIN));
+    if (it != v.end() && it->first == k) return it->second;
+    return 0;
+  }
+};
+
+}  // namespace
+
+struct rb_context {
+  rb_hydro_params hp;
+  rb_mesh_params mp;
+  int precision = RB_PREC_FP64;
+  int device = 0;
+  int64_t ncell = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  double* d_uold = nullptr;
+  double* d_unew = nullptr;
+  int32_t* d_son = nullptr;
+  int32_t* d_corr_slot = nullptr;   // [ngridmax]
+  double* d_stage = nullptr;        // Fortran-layout staging [5*ncell]
+  double* d_partial = nullptr;      // CFL partials
+  int64_t partial_cap = 0;
+  double* d_red = nullptr;          // [8] reduction output
+  double* d_clock = nullptr;        // [8] device clock of the uniform stepper
+  double* h_red = nullptr;          // pinned [8]
+  bool have_tree = false;
+  bool have_state = false;
+  bool clock_valid = false;
+  // host copies of the tree (Fortran layout)
+  std::vector<int32_t> son, father, nbor;
+  std::vector<int64_t> coords;      // [ngridmax*3] oct coordinates at its level
+  std::vector<int8_t> level_of;     // [ngridmax] level of each oct (0 = unused)
+  Level lv[RB_MAXLEVEL + 2];
+  std::vector<OctIndex> idx;        // per-level position -> igrid lookup
+  int finest = 0;                   // finest level holding octs
+  std::vector<cudaEvent_t> evpool;  // per-step kernel timing events
+  float kernel_ms_avg = 0.f;        // mean tile-kernel time of the last timed run
+  cudaGraphExec_t graph = nullptr;  // cached uniform-run graph
+  int graph_steps = 0;
+  double* graph_cur = nullptr;
+  // scheduler state (amr_commons dtnew/dtold, t, nstep)
+  double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
+  double t = 0.0;
+  int64_t nstep = 0;
+  int64_t cell_updates = 0;
+  double mass_tot = 0, ekin_tot = 0, eint_tot = 0;
+};
+
+namespace {
+
+int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
+  if (!hp || !mp) return fail(RB_ERR_INVALID, "null parameter struct");
+  if (hp->riemann != RB_RIEMANN_LLF && hp->riemann != RB_RIEMANN_HLL && hp->riemann != RB_RIEMANN_HLLC)
+    return fail(RB_ERR_INVALID, "unknown Riemann solver code %d (llf=1, hll=2, hllc=3)", hp->riemann);
+  const int st = hp->slope_type;
+  if (!(st == 0 || st == 1 || st == 2 || st == 3 || st == 7 || st == 8))
+    return fail(RB_ERR_INVALID, "Unknown slope type %d", st);
+  if (hp->scheme != 0) return fail(RB_ERR_INVALID, "scheme %d not supported (muscl only)", hp->scheme);
+  if (hp->pressure_fix) return fail(RB_ERR_INVALID, "pressure_fix is not supported");
+  if (hp->difmag != 0.0) return fail(RB_ERR_INVALID, "difmag>0 is not supported");
+  if (hp->interpol_var < 0 || hp->interpol_var > 2 || hp->interpol_type < 0 || hp->interpol_type > 4)
+    return fail(RB_ERR_INVALID, "bad interpol_var/interpol_type");
+  if (hp->interpol_type == 4 && hp->interpol_var != 2)
+    return fail(RB_ERR_INVALID, "interpol_type=4 is designed for interpol_var=2");
+  if (!(hp->gamma > 1.0) || !(hp->smallr > 0.0) || !(hp->smallc > 0.0) || !(hp->courant_factor > 0.0))
+    return fail(RB_ERR_INVALID, "gamma must exceed 1 and smallr, smallc, courant_factor be positive");
+  if (mp->nx < 1 || mp->ny < 1 || mp->nz < 1 || mp->ncoarse != mp->nx * mp->ny * mp->nz)
+    return fail(RB_ERR_INVALID, "bad coarse grid");
+  if (mp->ngridmax < 1 || mp->nlevelmax < 1 || mp->nlevelmax > RB_MAXLEVEL || mp->levelmin < 1 ||
+      mp->levelmin > mp->nlevelmax)
+    return fail(RB_ERR_INVALID, "bad ngridmax/levelmin/nlevelmax");
+  if (mp->nvector < 1) return fail(RB_ERR_INVALID, "nvector must be positive");
+  if (!(mp->boxlen > 0.0)) return fail(RB_ERR_INVALID, "boxlen must be positive");
+  return RB_OK;
+}
+
+inline int64_t fcell(const rb_context* c, int ind /*1..8*/, int igrid /*1-based*/) {
+  return (int64_t)c->mp.ncoarse + (int64_t)(ind - 1) * c->mp.ngridmax + igrid;
+}
+inline int64_t dev_of_fortran(const rb_context* c, int64_t icell) {
+  if (icell <= c->mp.ncoarse) return icell - 1;
+  const int64_t r = icell - 1 - c->mp.ncoarse;
+  return c->mp.ncoarse + (r % c->mp.ngridmax) * 8 + r / c->mp.ngridmax;
+}
+
+inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
+  auto spread = [](uint64_t a) {
+    a &= 0x1fffff;
+    a = (a | a << 32) & 0x1f00000000ffffULL;
+    a = (a | a << 16) & 0x1f0000ff0000ffULL;
+    a = (a | a << 8) & 0x100f00f00f00f00fULL;
+    a = (a | a << 4) & 0x10c30c30c30c30c3ULL;
+    a = (a | a << 2) & 0x1249249249249249ULL;
+    return a;
+  };
+  return spread(x) | spread(y) << 1 | spread(z) << 2;
+}
+
+void free_level_tables(Level& L) {
+  dfree(L.d_tile_blk);
+  dfree(L.d_interp7);
+  dfree(L.d_interp_buf);
+  dfree(L.d_corr_flux);
+  dfree(L.d_tgt);
+  dfree(L.d_tgt_off);
+  dfree(L.d_contrib);
+  L.ntile = L.ninterp = L.nslot = L.ntgt = 0;
+  L.tables_built = false;
+}
+
+void drop_graph(rb_context* c) {
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->graph = nullptr;
+  c->graph_steps = 0;
+  c->graph_cur = nullptr;
+}
+
+void free_tree(rb_context* c) {
+  drop_graph(c);
+  for (int l = 0; l <= RB_MAXLEVEL + 1; l++) {
+    free_level_tables(c->lv[l]);
+    dfree(c->lv[l].d_active);
+    c->lv[l].noct = 0;
+    c->lv[l].h_active.clear();
+  }
+  c->have_tree = false;
+}
+
+int default_shape(const rb_context* c, const Level& L) {
+  (void)c;
+  if (L.complete && L.noct >= 64 * 148) return 4;   // 8x8x8 cells
+  if (L.noct >= 8 * 64) return 1;                   // 4x4x4 cells
+  return 0;                                         // single oct
+}
+
+// Build the godunov tile / prolongation / correction tables of level l.
+int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
+  Level& L = c->lv[l];
+  free_level_tables(L);
+  if (L.noct == 0) return RB_OK;
+  if (L.shape < 0) L.shape = default_shape(c, L);
+  const rb::TileShape sh = rb::kTileShapes[L.shape];
+  const int TOX = sh.tx / 2, TOY = sh.ty / 2, TOZ = sh.tz / 2;
+  const int BX = TOX + 2, BY = TOY + 2, BZ = TOZ + 2, NBLK = BX * BY * BZ;
+  const OctIndex& I = idx[l];
+  // --- tiles: unique tile coordinates of the level's octs, Morton ordered
+  std::vector<std::pair<uint64_t, std::array<int64_t, 3>>> tiles;
+  {
+    std::vector<uint64_t> seen;
+    seen.reserve(L.noct);
+    std::unordered_map<uint64_t, int> tmap;
+    tmap.reserve(L.noct * 2 / (TOX * TOY * TOZ) + 16);
+    for (int32_t g : L.h_active) {
+      const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+      const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
+      const uint64_t m = morton3(tx, ty, tz);
+      if (tmap.emplace(m, 0).second) tiles.push_back({m, {tx, ty, tz}});
+    }
+    std::sort(tiles.begin(), tiles.end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+  }
+  L.ntile = (int)tiles.size();
+  std::vector<int32_t> blk((size_t)L.ntile * NBLK, -1);
+  std::unordered_map<int64_t, int32_t> interp_of;  // father Fortran cell -> entry
+  std::vector<int32_t> interp7;
+  const OctIndex* P = l >= 2 ? &idx[l - 1] : nullptr;
+  // level l-1 cells per dimension
+  const int64_t cnx = I.nx, cny = I.ny, cnz = I.nz;
+  auto father_cell_of_pos = [&](int64_t x, int64_t y, int64_t z, int64_t* fc) -> int {
+    // level-(l-1) cell at coordinates (x,y,z) (a level-l oct position)
+    x = ((x % cnx) + cnx) % cnx;
+    y = ((y % cny) + cny) % cny;
+    z = ((z % cnz) + cnz) % cnz;
+    if (l == 1) {
+      *fc = 1 + x + c->mp.nx * (y + (int64_t)c->mp.ny * z);
+      return RB_OK;
+    }
+    const int32_t pg = P->find(x >> 1, y >> 1, z >> 1);
+    if (pg <= 0)
+      return fail(RB_ERR_TREE, "level %d: father cell (%lld,%lld,%lld) of a needed neighbour block does not exist "
+                  "(refinement rule violated)", l, (long long)x, (long long)y, (long long)z);
+    const int ind = 1 + (int)(x & 1) + 2 * (int)(y & 1) + 4 * (int)(z & 1);
+    *fc = fcell(c, ind, pg);
+    return RB_OK;
+  };
+  auto make_interp = [&](int64_t x, int64_t y, int64_t z, int32_t* code) -> int {
+    int64_t f;
+    RB_TRY(father_cell_of_pos(x, y, z, &f));
+    auto it = interp_of.find(f);
+    if (it != interp_of.end()) { *code = -2 - it->second; return RB_OK; }
+    const int32_t e = (int32_t)interp_of.size();
+    interp_of.emplace(f, e);
+    int64_t cells[7];
+    cells[0] = f;
+    // getnborfather (nbors_utils.f90:404-525)
+    if (l == 1) {
+      const int64_t nx = c->mp.nx, ny = c->mp.ny, nz = c->mp.nz, nxny = nx * ny;
+      const int64_t ib[3] = {nx - 1, ny - 1, nz - 1};
+      const int64_t s1[3] = {1, nx, nxny};
+      const int64_t s2[3] = {nx - 1, (ny - 1) * nx, (nz - 1) * nxny};
+      int64_t ix[3];
+      ix[2] = (f - 1) / nxny;
+      ix[1] = (f - 1 - ix[2] * nxny) / nx;
+      ix[0] = (f - 1 - ix[1] * nx - ix[2] * nxny);
+      for (int d = 0; d < 3; d++) {
+        cells[2 * d + 1] = ix[d] > 0 ? f - s1[d] : f + s2[d];
+        cells[2 * d + 2] = ix[d] < ib[d] ? f + s1[d] : f - s2[d];
+      }
+    } else {
+      const int64_t r = f - 1 - c->mp.ncoarse;
+      const int32_t pg = (int32_t)(r % c->mp.ngridmax) + 1;
+      const int pos = (int)(r / c->mp.ngridmax);
+      const int cc[3] = {pos & 1, (pos >> 1) & 1, (pos >> 2) & 1};
+      const int64_t* pc = &c->coords[(size_t)(pg - 1) * 3];
+      for (int j = 1; j <= 6; j++) {
+        const int d = (j - 1) / 2, plus = (j - 1) & 1;
+        int64_t q[3] = {2 * pc[0] + cc[0], 2 * pc[1] + cc[1], 2 * pc[2] + cc[2]};
+        q[d] += plus ? 1 : -1;
+        const int32_t g = P->find(q[0] >> 1, q[1] >> 1, q[2] >> 1);
+        if (g > 0) {
+          const int64_t cx = ((q[0] % cnx) + cnx) % cnx, cy = ((q[1] % cny) + cny) % cny, cz = ((q[2] % cnz) + cnz) % cnz;
+          const int ind = 1 + (int)(cx & 1) + 2 * (int)(cy & 1) + 4 * (int)(cz & 1);
+          cells[j] = fcell(c, ind, g);
+        } else {
+          cells[j] = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (pg - 1)];
+        }
+      }
+    }
+    for (int j = 0; j < 7; j++) interp7.push_back((int32_t)dev_of_fortran(c, cells[j]));
+    *code = -2 - e;
+    return RB_OK;
+  };
+  std::vector<char> inner((size_t)TOX * TOY * TOZ);
+  for (int t = 0; t < L.ntile; t++) {
+    const int64_t ox0 = tiles[t].second[0] * TOX, oy0 = tiles[t].second[1] * TOY, oz0 = tiles[t].second[2] * TOZ;
+    int32_t* B = &blk[(size_t)t * NBLK];
+    for (int bz = 0; bz < BZ; bz++)
+      for (int by = 0; by < BY; by++)
+        for (int bx = 0; bx < BX; bx++) {
+          const int32_t g = I.find(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
+          B[bx + BX * (by + BY * bz)] = g > 0 ? g - 1 : -1;
+        }
+    for (int z = 0; z < TOZ; z++)
+      for (int y = 0; y < TOY; y++)
+        for (int x = 0; x < TOX; x++) inner[x + TOX * (y + TOY * z)] = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))] >= 0;
+    for (int bz = 0; bz < BZ; bz++)
+      for (int by = 0; by < BY; by++)
+        for (int bx = 0; bx < BX; bx++) {
+          int32_t& code = B[bx + BX * (by + BY * bz)];
+          if (code >= 0) continue;
+          bool needed = false;
+          for (int dz = -1; dz <= 1 && !needed; dz++)
+            for (int dy = -1; dy <= 1 && !needed; dy++)
+              for (int dx = -1; dx <= 1 && !needed; dx++) {
+                const int ix = bx - 1 + dx, iy = by - 1 + dy, iz = bz - 1 + dz;
+                if (ix < 0 || iy < 0 || iz < 0 || ix >= TOX || iy >= TOY || iz >= TOZ) continue;
+                needed = inner[ix + TOX * (iy + TOY * iz)];
+              }
+          if (needed) RB_TRY(make_interp(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz, &code));
+        }
+  }
+  L.ninterp = (int)interp_of.size();
+  RB_TRY(dalloc(&L.d_tile_blk, blk.size()));
+  RB_CUDA(cudaMemcpy(L.d_tile_blk, blk.data(), blk.size() * 4, cudaMemcpyHostToDevice));
+  if (L.ninterp) {
+    RB_TRY(dalloc(&L.d_interp7, interp7.size()));
+    RB_CUDA(cudaMemcpy(L.d_interp7, interp7.data(), interp7.size() * 4, cudaMemcpyHostToDevice));
+    RB_TRY(dalloc(&L.d_interp_buf, (size_t)L.ninterp * 8 * 5));
+  }
+  // --- fine-to-coarse corrections (godunov_fine.f90:798-908)
+  struct Contrib { int64_t tgt; int64_t batch; int face; int slot; };
+  std::vector<Contrib> cons;
+  std::vector<int32_t> slot_of((size_t)L.noct, -1);
+  int nslot = 0;
+  std::vector<int32_t> h_slot_upd;  // (igrid-1, slot) pairs
+  for (int p = 0; p < L.noct; p++) {
+    const int32_t g = L.h_active[p];
+    int slot = -1;
+    for (int j = 1; j <= 6; j++) {
+      const int64_t nc = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (g - 1)];
+      if (nc < 1 || nc > c->ncell) return fail(RB_ERR_TREE, "nbor(%d,%d)=%lld out of range", g, j, (long long)nc);
+      if (c->son[nc - 1] == 0) {
+        if (slot < 0) slot = nslot++;
+        cons.push_back({dev_of_fortran(c, nc), p / c->mp.nvector, j - 1, slot});
+      }
+    }
+    if (slot >= 0) { h_slot_upd.push_back(g - 1); h_slot_upd.push_back(slot); }
+  }
+  L.nslot = nslot;
+  if (nslot) {
+    std::stable_sort(cons.begin(), cons.end(), [](const Contrib& a, const Contrib& b) {
+      if (a.tgt != b.tgt) return a.tgt < b.tgt;
+      if (a.batch != b.batch) return a.batch < b.batch;
+      return a.face < b.face;  // direction, then left (even) before right (odd)
+    });
+    std::vector<int32_t> tgt, off, contrib;
+    for (size_t i = 0; i < cons.size(); i++) {
+      if (i == 0 || cons[i].tgt != cons[i - 1].tgt) {
+        tgt.push_back((int32_t)cons[i].tgt);
+        off.push_back((int32_t)i);
+      }
+      contrib.push_back(cons[i].slot * 6 + cons[i].face);
+    }
+    off.push_back((int32_t)cons.size());
+    L.ntgt = (int)tgt.size();
+    RB_TRY(dalloc(&L.d_tgt, tgt.size()));
+    RB_TRY(dalloc(&L.d_tgt_off, off.size()));
+    RB_TRY(dalloc(&L.d_contrib, contrib.size()));
+    RB_TRY(dalloc(&L.d_corr_flux, (size_t)nslot * 120));
+    RB_CUDA(cudaMemcpy(L.d_tgt, tgt.data(), tgt.size() * 4, cudaMemcpyHostToDevice));
+    RB_CUDA(cudaMemcpy(L.d_tgt_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+    RB_CUDA(cudaMemcpy(L.d_contrib, contrib.data(), contrib.size() * 4, cudaMemcpyHostToDevice));
+    // scatter slots into the global per-oct slot table
+    std::vector<int32_t> tmp(h_slot_upd);
+    for (size_t i = 0; i + 1 < tmp.size(); i += 2)
+      RB_CUDA(cudaMemcpy(c->d_corr_slot + tmp[i], &tmp[i + 1], 4, cudaMemcpyHostToDevice));
+  }
+  L.tables_built = true;
+  return RB_OK;
+}
+
+int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
+                   const int32_t* numbl, const int32_t* active) {
+  if (!son || !father || !nbor || !numbl || !active) return fail(RB_ERR_INVALID, "null tree array");
+  free_tree(c);
+  const int64_t ncell = c->ncell;
+  const int ngm = c->mp.ngridmax;
+  c->son.assign(son, son + ncell);
+  c->father.assign(father, father + ngm);
+  c->nbor.assign(nbor, nbor + (size_t)6 * ngm);
+  c->coords.assign((size_t)ngm * 3, 0);
+  c->level_of.assign((size_t)ngm, 0);
+  c->idx.assign(RB_MAXLEVEL + 2, OctIndex());
+  std::vector<OctIndex>& idx = c->idx;
+  int64_t off = 0;
+  c->finest = 0;
+  for (int l = 1; l <= c->mp.nlevelmax; l++) {
+    Level& L = c->lv[l];
+    const int n = numbl[l - 1];
+    if (n < 0 || n > ngm) return fail(RB_ERR_INVALID, "numbl(%d)=%d out of range", l, n);
+    L.h_active.assign(active + off, active + off + n);
+    off += n;
+    L.noct = n;
+    if (n) c->finest = l;
+    L.dx = std::pow(0.5, l) * (c->mp.boxlen / (double)c->mp.nx);
+    OctIndex& I = idx[l];
+    I.nx = (int64_t)c->mp.nx << (l - 1);
+    I.ny = (int64_t)c->mp.ny << (l - 1);
+    I.nz = (int64_t)c->mp.nz << (l - 1);
+    I.v.reserve(n);
+    for (int32_t g : L.h_active) {
+      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "active grid %d out of range", g);
+      const int64_t fc = father[g - 1];
+      int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+      if (l == 1) {
+        if (fc < 1 || fc > c->mp.ncoarse) return fail(RB_ERR_TREE, "level-1 grid %d father %lld is not coarse", g, (long long)fc);
+        x[0] = (fc - 1) % c->mp.nx;
+        x[1] = ((fc - 1) / c->mp.nx) % c->mp.ny;
+        x[2] = (fc - 1) / ((int64_t)c->mp.nx * c->mp.ny);
+      } else {
+        const int64_t r = fc - 1 - c->mp.ncoarse;
+        if (r < 0 || r >= (int64_t)8 * ngm) return fail(RB_ERR_TREE, "grid %d father %lld out of range", g, (long long)fc);
+        const int32_t pg = (int32_t)(r % ngm) + 1;
+        const int pos = (int)(r / ngm);
+        if (c->level_of[pg - 1] != l - 1) return fail(RB_ERR_TREE, "grid %d: father grid %d is not at level %d", g, pg, l - 1);
+        const int64_t* px = &c->coords[(size_t)(pg - 1) * 3];
+        x[0] = 2 * px[0] + (pos & 1);
+        x[1] = 2 * px[1] + ((pos >> 1) & 1);
+        x[2] = 2 * px[2] + ((pos >> 2) & 1);
+      }
+      c->level_of[g - 1] = (int8_t)l;
+      I.v.push_back({I.key(x[0], x[1], x[2]), g});
+    }
+    std::sort(I.v.begin(), I.v.end());
+    for (size_t i = 1; i < I.v.size(); i++)
+      if (I.v[i].first == I.v[i - 1].first) return fail(RB_ERR_TREE, "level %d: two octs at one position", l);
+    L.complete = (int64_t)n == I.nx * I.ny * I.nz;
+    int64_t leaf = 0;
+    int refined = 0;
+    for (int32_t g : L.h_active)
+      for (int ind = 1; ind <= 8; ind++) {
+        const int32_t s = son[fcell(c, ind, g) - 1];
+        leaf += (s == 0);
+        refined |= (s > 0);
+      }
+    L.leaf_cells = leaf;
+    L.has_refined = refined;
+    if (n) {
+      std::vector<int32_t> a0(n);
+      for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
+      RB_TRY(dalloc(&L.d_active, (size_t)n));
+      RB_CUDA(cudaMemcpy(L.d_active, a0.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  // son mirror (device layout) and the per-oct correction slot table
+  RB_CUDA(cudaMemcpy(c->d_stage, son, ncell * 4, cudaMemcpyHostToDevice));
+  rb::permute_son_kernel<<<grid_for(ncell, 256), 256, 0, c->stream>>>((const int32_t*)c->d_stage, c->d_son, ncell,
+                                                                      c->mp.ncoarse, ngm);
+  RB_CUDA(cudaGetLastError());
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  RB_CUDA(cudaMemset(c->d_corr_slot, 0xff, (size_t)ngm * 4));
+  for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(build_level_tables(c, l, idx));
+  c->have_tree = true;
+  c->clock_valid = false;
+  return RB_OK;
+}
+
+int ensure_partial(rb_context* c, int64_t n) {
+  if (n <= c->partial_cap) return RB_OK;
+  drop_graph(c);
+  dfree(c->d_partial);
+  RB_TRY(dalloc(&c->d_partial, (size_t)n * 4));
+  c->partial_cap = n;
+  return RB_OK;
+}
+
+int check_level(rb_context* c, int l) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree) return fail(RB_ERR_STATE, "rb_sync_tree has not been called");
+  if (l < 1 || l > c->mp.nlevelmax) return fail(RB_ERR_INVALID, "level %d out of range", l);
+  return RB_OK;
+}
+
+int set_unew_impl(rb_context* c, int l) {
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+      c->d_uold, c->d_unew, L.d_active, L.noct, c->ncell, c->mp.ncoarse);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+int set_uold_impl(rb_context* c, int l) {
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+      c->d_unew, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+int upload_fine_impl(rb_context* c, int l) {
+  if (l == c->mp.nlevelmax) return RB_OK;  // interpol_hydro.f90:16
+  Level& L = c->lv[l];
+  if (!L.noct || !L.has_refined) return RB_OK;
+  rb::upload_fine_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
+  rb::TileArgs a;
+  memset(&a, 0, sizeof a);
+  a.uold = c->d_uold;
+  a.unew = c->d_unew;
+  a.son = c->d_son;
+  a.interp = L.d_interp_buf;
+  a.tile_blk = L.d_tile_blk;
+  a.corr_slot = L.nslot ? c->d_corr_slot : nullptr;
+  a.corr_flux = L.d_corr_flux;
+  a.ncell = c->ncell;
+  a.ninterp8 = (int64_t)L.ninterp * 8;
+  a.ncoarse = c->mp.ncoarse;
+  a.ntile = L.ntile;
+  a.has_refined = L.has_refined;
+  int e2;
+  const double m = std::frexp(L.dx, &e2);
+  a.dx_pow2 = (m == 0.5);
+  a.fused = 0;
+  a.dt = dt;
+  a.dx = L.dx;
+  a.inv_dx = 1.0 / L.dx;
+  a.dt_dev = nullptr;
+  a.partial = nullptr;
+  a.hp = c->hp;
+  return a;
+}
+
+int launch_tile(rb_context* c, int shape, const rb::TileArgs& a, int grid) {
+  cudaError_t e = c->precision == RB_PREC_MIXED ? rb::launch_tile_mixed(shape, a, grid, c->stream)
+                                                : rb::launch_tile_f64(shape, a, grid, c->stream);
+  if (e != cudaSuccess) return fail(RB_ERR_CUDA, "godunov tile kernel launch failed: %s", cudaGetErrorString(e));
+  return RB_OK;
+}
+
+int godunov_impl(rb_context* c, int l, double dt, bool timed) {
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(RB_ERR_INVALID, "dt=%g must be positive and finite", dt);
+  if (L.ninterp) {
+    rb::interp_blocks_kernel<<<(L.ninterp + 127) / 128, 128, 0, c->stream>>>(c->d_uold, L.d_interp7, L.ninterp,
+                                                                             c->ncell, L.d_interp_buf, c->hp);
+    RB_CUDA(cudaGetLastError());
+  }
+  rb::TileArgs a = tile_args(c, L, dt);
+  if (timed) RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+  RB_TRY(launch_tile(c, L.shape, a, L.ntile));
+  if (timed) RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+  if (L.ntgt) {
+    rb::apply_corrections_kernel<<<(L.ntgt + 127) / 128, 128, 0, c->stream>>>(
+        c->d_unew, L.d_tgt, L.d_tgt_off, L.d_contrib, L.ntgt, L.d_corr_flux, c->ncell);
+    RB_CUDA(cudaGetLastError());
+  }
+  return RB_OK;
+}
+
+int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin, double* eint) {
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  const int nt = 256;
+  const int nblk = grid_for((int64_t)L.noct * 8, nt, 148 * 8);
+  RB_TRY(ensure_partial(c, nblk));
+  rb::courant_partial_kernel<256><<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
+                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+  RB_CUDA(cudaGetLastError());
+  const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
+  rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, *dt_io, dt0,
+                                                            L.leaf_cells > 0 ? 1 : 0, c->d_red, 0);
+  RB_CUDA(cudaGetLastError());
+  RB_CUDA(cudaMemcpyAsync(c->h_red, c->d_red, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  *dt_io = c->h_red[0];
+  if (mass) *mass = c->h_red[1];
+  if (ekin) *ekin = c->h_red[2];
+  if (eint) *eint = c->h_red[3];
+  return RB_OK;
+}
+
+// amr_step hydro call sequence (amr/amr_step.f90:320-445, 571-576;
+// pm/newdt_fine.f90:47-51,177; amr/update_time.f90:330-331).
+int amr_step_impl(rb_context* c, int l, int icount) {
+  if (c->lv[l].noct == 0) return RB_OK;
+  c->dtold[l] = c->dtnew[l];
+  c->dtnew[l] = c->mp.boxlen / c->hp.smallc;
+  double dt_all = c->dtnew[l], ma = 0, ek = 0, ei = 0;
+  RB_TRY(courant_impl(c, l, &dt_all, &ma, &ek, &ei));
+  c->mass_tot += ma; c->ekin_tot += ek; c->eint_tot += ei;
+  c->dtnew[l] = rb_min_host(c->dtnew[l], dt_all);
+  if (l > c->mp.levelmin)
+    c->dtnew[l] = rb_min_host(c->dtnew[l - 1] / (double)(float)c->mp.nsubcycle[l - 1], c->dtnew[l]);
+  RB_TRY(set_unew_impl(c, l));
+  if (l < c->mp.nlevelmax) {
+    if (c->lv[l + 1].noct > 0) {
+      if (c->mp.nsubcycle[l] == 2) {
+        RB_TRY(amr_step_impl(c, l + 1, 1));
+        RB_TRY(amr_step_impl(c, l + 1, 2));
+      } else {
+        RB_TRY(amr_step_impl(c, l + 1, 1));
+      }
+    } else {
+      c->dtold[l + 1] = c->dtnew[l] / (double)c->mp.nsubcycle[l];
+      c->dtnew[l + 1] = c->dtnew[l] / (double)c->mp.nsubcycle[l];
+      c->t += c->dtnew[l];
+      c->nstep++;
+    }
+  } else {
+    c->t += c->dtnew[l];
+    c->nstep++;
+  }
+  RB_TRY(godunov_impl(c, l, c->dtnew[l], false));
+  c->cell_updates += c->lv[l].leaf_cells;
+  RB_TRY(set_uold_impl(c, l));
+  RB_TRY(upload_fine_impl(c, l));
+  if (l > c->mp.levelmin) {
+    if (c->mp.nsubcycle[l - 1] == 1) c->dtnew[l - 1] = c->dtnew[l];
+    if (icount == 2) c->dtnew[l - 1] = c->dtold[l] + c->dtnew[l];
+  }
+  return RB_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* rb_version(void) { return "ramses_b200 0.1 (sm_100a)"; }
+
+const char* rb_status_string(int s) {
+  switch (s) {
+    case RB_OK: return "ok";
+    case RB_ERR_INVALID: return "invalid argument or unsupported parameter";
+    case RB_ERR_STATE: return "call out of order";
+    case RB_ERR_CUDA: return "CUDA error";
+    case RB_ERR_NOMEM: return "out of memory";
+    case RB_ERR_TREE: return "octree violates the refinement rules";
+    case RB_ERR_NUMERIC: return "non-physical state";
+    case RB_ERR_NO_DEVICE: return "no usable CUDA device";
+    case RB_ERR_CAPACITY: return "request above a fixed capacity";
+  }
+  return "unknown status";
+}
+
+const char* rb_last_error(void) { return g_last_error.c_str(); }
+
+int rb_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int rb_select_device(int device) {
+  const int n = rb_device_count();
+  if (device < 0 || device >= n) return fail(RB_ERR_NO_DEVICE, "device %d not visible (%d devices)", device, n);
+  RB_CUDA(cudaSetDevice(device));
+  return RB_OK;
+}
+
+int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision, rb_context** out) {
+  if (!out) return fail(RB_ERR_INVALID, "null output pointer");
+  *out = nullptr;
+  RB_TRY(check_params(hp, mp));
+  if (precision != RB_PREC_FP64 && precision != RB_PREC_MIXED)
+    return fail(RB_ERR_INVALID, "precision must be RB_PREC_FP64 or RB_PREC_MIXED");
+  if (rb_device_count() == 0) return fail(RB_ERR_NO_DEVICE, "no CUDA device visible");
+  rb_context* c = new rb_context();
+  c->hp = *hp;
+  c->mp = *mp;
+  c->precision = precision;
+  c->ncell = (int64_t)mp->ncoarse + 8 * (int64_t)mp->ngridmax;
+  auto bail = [&](int rc) { rb_destroy(c); return rc; };
+  if (cudaGetDevice(&c->device) != cudaSuccess) return bail(fail(RB_ERR_NO_DEVICE, "cudaGetDevice failed"));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
+    return bail(fail(RB_ERR_CUDA, "stream/event creation failed"));
+  int rc;
+  if ((rc = dalloc(&c->d_uold, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_unew, (size_t)c->ncell * 5)) ||
+      (rc = dalloc(&c->d_son, (size_t)c->ncell)) || (rc = dalloc(&c->d_corr_slot, (size_t)mp->ngridmax)) ||
+      (rc = dalloc(&c->d_stage, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_red, 8)) ||
+      (rc = dalloc(&c->d_clock, 8)))
+    return bail(rc);
+  if (cudaMallocHost((void**)&c->h_red, 8 * sizeof(double)) != cudaSuccess)
+    return bail(fail(RB_ERR_NOMEM, "pinned allocation failed"));
+  cudaMemset(c->d_uold, 0, (size_t)c->ncell * 5 * sizeof(double));
+  cudaMemset(c->d_unew, 0, (size_t)c->ncell * 5 * sizeof(double));
+  cudaMemset(c->d_clock, 0, 8 * sizeof(double));
+  // make sure the kernel image for this GPU is present
+  cudaError_t e = rb::launch_tile_f64(0, rb::TileArgs{}, 0, c->stream);
+  if (e != cudaSuccess) return bail(fail(RB_ERR_NO_DEVICE, "tile kernel unavailable on this device: %s", cudaGetErrorString(e)));
+  *out = c;
+  return RB_OK;
+}
+
+int rb_destroy(rb_context* c) {
+  if (!c) return RB_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_tree(c);
+  dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son); dfree(c->d_corr_slot);
+  dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock);
+  if (c->h_red) cudaFreeHost(c->h_red);
+  for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+  c->evpool.clear();
+  drop_graph(c);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return RB_OK;
+}
+
+int rb_sync_tree(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
+                 const int32_t* numbl, const int32_t* active_igrid) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  int rc = sync_tree_impl(c, son, father, nbor, numbl, active_igrid);
+  if (rc) free_tree(c);
+  return rc;
+}
+
+static int upload_impl(rb_context* c, const double* h, double* d) {
+  if (!c || !h) return fail(RB_ERR_INVALID, "null argument");
+  RB_CUDA(cudaMemcpyAsync(c->d_stage, h, (size_t)c->ncell * 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  rb::permute_f2d_kernel<<<grid_for(c->ncell * 5, 256), 256, 0, c->stream>>>(c->d_stage, d, c->ncell, c->mp.ncoarse,
+                                                                            c->mp.ngridmax, 5);
+  RB_CUDA(cudaGetLastError());
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  return RB_OK;
+}
+static int download_impl(rb_context* c, const double* d, double* h) {
+  if (!c || !h) return fail(RB_ERR_INVALID, "null argument");
+  rb::permute_d2f_kernel<<<grid_for(c->ncell * 5, 256), 256, 0, c->stream>>>(d, c->d_stage, c->ncell, c->mp.ncoarse,
+                                                                            c->mp.ngridmax, 5);
+  RB_CUDA(cudaGetLastError());
+  RB_CUDA(cudaMemcpyAsync(h, c->d_stage, (size_t)c->ncell * 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  return RB_OK;
+}
+
+int rb_upload_state(rb_context* c, const double* uold) {
+  RB_TRY(upload_impl(c, uold, c ? c->d_uold : nullptr));
+  c->have_state = true;
+  c->clock_valid = false;
+  return RB_OK;
+}
+int rb_download_state(rb_context* c, double* uold) { return download_impl(c, c ? c->d_uold : nullptr, uold); }
+int rb_upload_unew(rb_context* c, const double* unew) { return upload_impl(c, unew, c ? c->d_unew : nullptr); }
+int rb_download_unew(rb_context* c, double* unew) { return download_impl(c, c ? c->d_unew : nullptr, unew); }
+
+int rb_set_unew(rb_context* c, int l) { RB_TRY(check_level(c, l)); return set_unew_impl(c, l); }
+int rb_set_uold(rb_context* c, int l) { RB_TRY(check_level(c, l)); return set_uold_impl(c, l); }
+int rb_upload_fine(rb_context* c, int l) { RB_TRY(check_level(c, l)); return upload_fine_impl(c, l); }
+
+int rb_godunov_fine(rb_context* c, int l, double dt) {
+  RB_TRY(check_level(c, l));
+  RB_TRY(godunov_impl(c, l, dt, true));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+  c->kernel_ms_avg = c->last_ms;
+  return RB_OK;
+}
+
+int rb_courant_fine(rb_context* c, int l, double* dt_io, double* mass, double* ekin, double* eint) {
+  RB_TRY(check_level(c, l));
+  if (!dt_io) return fail(RB_ERR_INVALID, "null dt");
+  return courant_impl(c, l, dt_io, mass, ekin, eint);
+}
+
+int rb_coarse_step(rb_context* c, double* t_io, double* dtnew_out) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  if (t_io) c->t = *t_io;
+  c->mass_tot = c->ekin_tot = c->eint_tot = 0.0;
+  RB_TRY(amr_step_impl(c, c->mp.levelmin, 1));
+  for (int l = c->mp.levelmin - 1; l >= 1; l--) RB_TRY(upload_fine_impl(c, l));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  if (t_io) *t_io = c->t;
+  if (dtnew_out)
+    for (int l = 1; l <= c->mp.nlevelmax; l++) dtnew_out[l - 1] = c->dtnew[l];
+  c->clock_valid = false;
+  return RB_OK;
+}
+
+int rb_cell_updates(rb_context* c, int64_t* out) {
+  if (!c || !out) return fail(RB_ERR_INVALID, "null argument");
+  *out = c->cell_updates;
+  return RB_OK;
+}
+
+int rb_tile_shape_info(int shape, int* tx, int* ty, int* tz, int* nthreads) {
+  if (shape < 0 || shape >= rb::kNumTileShapes) return fail(RB_ERR_INVALID, "tile shape %d out of range", shape);
+  if (tx) *tx = rb::kTileShapes[shape].tx;
+  if (ty) *ty = rb::kTileShapes[shape].ty;
+  if (tz) *tz = rb::kTileShapes[shape].tz;
+  if (nthreads) *nthreads = rb::kTileShapes[shape].nthreads;
+  return RB_OK;
+}
+
+int rb_get_tile_shape(rb_context* c, int l, int* shape) {
+  RB_TRY(check_level(c, l));
+  if (!shape) return fail(RB_ERR_INVALID, "null argument");
+  *shape = c->lv[l].shape;
+  return RB_OK;
+}
+
+int rb_synchronize(rb_context* c) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  return RB_OK;
+}
+
+int rb_get_stream(rb_context* c, void** s) {
+  if (!c || !s) return fail(RB_ERR_INVALID, "null argument");
+  *s = (void*)c->stream;
+  return RB_OK;
+}
+
+int rb_last_kernel_ms(rb_context* c, float* ms) {
+  if (!c || !ms) return fail(RB_ERR_INVALID, "null argument");
+  *ms = c->kernel_ms_avg;
+  return RB_OK;
+}
+
+int rb_last_run_ms(rb_context* c, float* ms) {
+  if (!c || !ms) return fail(RB_ERR_INVALID, "null argument");
+  *ms = c->last_ms;
+  return RB_OK;
+}
+
+int rb_unsplit(const rb_hydro_params* hp, const double* uin, const double* gravin, const double* pin, double* flux,
+               double* tmp, double dx, double dy, double dz, double dt, int ngrid, int nvector) {
+  (void)pin;
+  rb_mesh_params mp;
+  memset(&mp, 0, sizeof mp);
+  mp.nx = mp.ny = mp.nz = mp.ncoarse = 1;
+  mp.ngridmax = 1; mp.nlevelmax = 1; mp.levelmin = 1; mp.nvector = 1; mp.boxlen = 1.0;
+  RB_TRY(check_params(hp, &mp));
+  if (!uin || !flux || !tmp) return fail(RB_ERR_INVALID, "null array");
+  if (nvector < 1 || ngrid < 0 || ngrid > nvector) return fail(RB_ERR_INVALID, "bad ngrid/nvector");
+  if (ngrid == 0) return RB_OK;
+  if (rb_device_count() == 0) return fail(RB_ERR_NO_DEVICE, "no CUDA device visible");
+  const size_t nin = (size_t)nvector * 216, nfl = (size_t)nvector * 27;
+  double *d_uin = nullptr, *d_g = nullptr, *d_flux = nullptr, *d_tmp = nullptr;
+  int rc = RB_OK;
+  if ((rc = dalloc(&d_uin, nin * 5)) || (rc = dalloc(&d_g, nin * 3)) || (rc = dalloc(&d_flux, nfl * 15)) ||
+      (rc = dalloc(&d_tmp, nfl * 6))) {
+    dfree(d_uin); dfree(d_g); dfree(d_flux); dfree(d_tmp);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpy(d_uin, uin, nin * 5 * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = gravin ? cudaMemcpy(d_g, gravin, nin * 3 * sizeof(double), cudaMemcpyHostToDevice)
+               : cudaMemset(d_g, 0, nin * 3 * sizeof(double));
+  // outputs keep the caller's values outside the computed ranges
+  if (e == cudaSuccess) e = cudaMemcpy(d_flux, flux, nfl * 15 * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_tmp, tmp, nfl * 6 * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rb::unsplit_fortran_kernel<<<ngrid, 64>>>(d_uin, d_g, d_flux, d_tmp, dx, dy, dz, dt, ngrid, nvector, *hp);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(flux, d_flux, nfl * 15 * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(tmp, d_tmp, nfl * 6 * sizeof(double), cudaMemcpyDeviceToHost);
+  dfree(d_uin); dfree(d_g); dfree(d_flux); dfree(d_tmp);
+  if (e != cudaSuccess) return fail(RB_ERR_CUDA, "rb_unsplit: %s", cudaGetErrorString(e));
+  return RB_OK;
+}
+
+int rb_set_tile_shape(rb_context* c, int l, int shape) {
+  RB_TRY(check_level(c, l));
+  Level& L = c->lv[l];
+  if (shape >= rb::kNumTileShapes) return fail(RB_ERR_INVALID, "tile shape %d out of range", shape);
+  drop_graph(c);
+  if (shape >= 0 || L.noct == 0) {
+    L.shape = shape >= 0 ? shape : L.shape;
+    return build_level_tables(c, l, c->idx);
+  }
+  // time every shape on the current state against a scratch copy of unew
+  int best = -1;
+  float best_ms = 1e30f;
+  double* keep_unew = c->d_unew;
+  for (int s = 0; s < rb::kNumTileShapes; s++) {
+    const size_t smem = c->precision == RB_PREC_MIXED ? rb::tile_smem_mixed(s) : rb::tile_smem_f64(s);
+    if (smem > 227 * 1024) continue;
+    L.shape = s;
+    RB_TRY(build_level_tables(c, l, c->idx));
+    if (L.ninterp) {
+      rb::interp_blocks_kernel<<<(L.ninterp + 127) / 128, 128, 0, c->stream>>>(c->d_uold, L.d_interp7, L.ninterp,
+                                                                               c->ncell, L.d_interp_buf, c->hp);
+      RB_CUDA(cudaGetLastError());
+    }
+    RB_CUDA(cudaMemcpyAsync(c->d_stage, keep_unew, (size_t)c->ncell * 5 * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->stream));
+    c->d_unew = c->d_stage;
+    rb::TileArgs a = tile_args(c, L, 1e-30);
+    c->d_unew = keep_unew;
+    float ms = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+      RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+      int rc = launch_tile(c, s, a, L.ntile);
+      if (rc) return rc;
+      RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+      RB_CUDA(cudaEventSynchronize(c->ev1));
+      float t = 0.f;
+      RB_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+      if (rep > 0) ms = std::min(ms, t);
+    }
+    if (ms < best_ms) { best_ms = ms; best = s; }
+  }
+  if (best < 0) return fail(RB_ERR_INVALID, "no tile shape fits on this device");
+  L.shape = best;
+  return build_level_tables(c, l, c->idx);
+}
+
+// Device-resident uniform-grid stepper: one complete finest level, every
+// coarser level fully refined (no leaf cell). Per step: the fused tile kernel
+// (unew = uold + fluxes, CFL partials of the new state) and the device clock
+// update; the two state buffers alternate; optionally captured as one graph.
+int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, double* dt_last_out) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  if (nsteps < 0) return fail(RB_ERR_INVALID, "nsteps must be >= 0");
+  const int lf = c->finest;
+  Level& L = c->lv[lf];
+  if (lf < 1 || !L.complete || L.leaf_cells != (int64_t)L.noct * 8)
+    return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
+  for (int l = 1; l < lf; l++)
+    if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
+  if (L.ninterp || L.nslot) return fail(RB_ERR_STATE, "uniform level unexpectedly needs prolongation/corrections");
+  RB_TRY(ensure_partial(c, std::max<int64_t>(L.ntile, 1)));
+  const double dt_max = c->mp.boxlen / c->hp.smallc;
+  const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
+  if (t_io) c->t = *t_io;
+  if (!c->clock_valid) {
+    // newdt_fine + courant_fine on the starting state
+    const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
+    RB_TRY(ensure_partial(c, nblk));
+    rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+    RB_CUDA(cudaGetLastError());
+    rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, dt_max, dt0, 1, c->d_red, 0);
+    RB_CUDA(cudaGetLastError());
+    c->h_red[0] = c->t;
+    RB_CUDA(cudaMemcpyAsync(c->d_clock, c->d_red, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    RB_CUDA(cudaMemcpyAsync(c->d_clock + 1, c->h_red, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+    c->clock_valid = true;
+  } else if (t_io) {
+    c->h_red[0] = c->t;
+    RB_CUDA(cudaMemcpyAsync(c->d_clock + 1, c->h_red, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  auto enqueue = [&](double* cur, double* nxt) -> int {
+    rb::TileArgs a = tile_args(c, L, 0.0);
+    a.uold = cur;
+    a.unew = nxt;
+    a.fused = 1;
+    a.dt_dev = c->d_clock;
+    a.partial = c->d_partial;
+    RB_TRY(launch_tile(c, L.shape, a, L.ntile));
+    rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, L.ntile, dt_max, dt0, 1, c->d_clock, 1);
+    RB_CUDA(cudaGetLastError());
+    return RB_OK;
+  };
+  if (nsteps > 0) {
+    if (use_graph) {
+      if (!(c->graph && c->graph_steps == nsteps && c->graph_cur == c->d_uold)) {
+        drop_graph(c);
+        cudaGraph_t g;
+        RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        double *cur = c->d_uold, *nxt = c->d_unew;
+        int rc = RB_OK;
+        for (int s = 0; s < nsteps && rc == RB_OK; s++) {
+          rc = enqueue(cur, nxt);
+          std::swap(cur, nxt);
+        }
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (rc) return rc;
+        if (ce != cudaSuccess) return fail(RB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { c->graph = nullptr; return fail(RB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce)); }
+        c->graph_steps = nsteps;
+        c->graph_cur = c->d_uold;
+      }
+      RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+      RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+      RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+    } else {
+      // per-step events around the tile kernel only (kernel-time roofline)
+      const int ntimed = std::min(nsteps, 4096);
+      while ((int)c->evpool.size() < 2 * ntimed) {
+        cudaEvent_t e;
+        RB_CUDA(cudaEventCreate(&e));
+        c->evpool.push_back(e);
+      }
+      RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+      double *cur = c->d_uold, *nxt = c->d_unew;
+      for (int s = 0; s < nsteps; s++) {
+        if (s < ntimed) RB_CUDA(cudaEventRecord(c->evpool[2 * s], c->stream));
+        rb::TileArgs a = tile_args(c, L, 0.0);
+        a.uold = cur;
+        a.unew = nxt;
+        a.fused = 1;
+        a.dt_dev = c->d_clock;
+        a.partial = c->d_partial;
+        RB_TRY(launch_tile(c, L.shape, a, L.ntile));
+        if (s < ntimed) RB_CUDA(cudaEventRecord(c->evpool[2 * s + 1], c->stream));
+        rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, L.ntile, dt_max, dt0, 1,
+                                                                  c->d_clock, 1);
+        RB_CUDA(cudaGetLastError());
+        std::swap(cur, nxt);
+      }
+      RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+      RB_CUDA(cudaEventSynchronize(c->ev1));
+      double tot = 0.0;
+      for (int s = 0; s < ntimed; s++) {
+        float ms = 0.f;
+        RB_CUDA(cudaEventElapsedTime(&ms, c->evpool[2 * s], c->evpool[2 * s + 1]));
+        tot += ms;
+      }
+      c->kernel_ms_avg = ntimed ? (float)(tot / ntimed) : 0.f;
+    }
+    if (nsteps & 1) {
+      std::swap(c->d_uold, c->d_unew);  // a cached odd-length graph is recaptured on the next call
+    }
+  }
+  // coarser levels: restriction of the final state (adaptive_loop.f90 + amr_step.f90:442)
+  for (int l = lf - 1; l >= 1; l--) RB_TRY(upload_fine_impl(c, l));
+  RB_CUDA(cudaMemcpyAsync(c->h_red, c->d_clock, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  if (nsteps > 0) RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+  c->t = c->h_red[1];
+  c->nstep += nsteps;
+  c->cell_updates += (int64_t)nsteps * L.leaf_cells;
+  c->dtnew[lf] = c->h_red[0];
+  c->mass_tot = c->h_red[2];
+  c->ekin_tot = c->h_red[3];
+  c->eint_tot = c->h_red[4];
+  if (t_io) *t_io = c->t;
+  if (dt_last_out) *dt_last_out = c->h_red[0];
+  return RB_OK;
+}
+
+}  // extern "C"

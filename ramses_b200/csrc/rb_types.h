@@ -1,0 +1,57 @@
+/* rb_types.h -- plain-C parameter structs shared by the C ABI, the host
+ * runtime and the device kernels. The public header include/ramses_b200.h
+ * includes this file. */
+#ifndef RB_TYPES_H
+#define RB_TYPES_H
+#include <stdint.h>
+
+#define RB_NVAR 5
+#define RB_MAXLEVEL 32
+
+enum { RB_RIEMANN_LLF = 1, RB_RIEMANN_HLL = 2, RB_RIEMANN_HLLC = 3 };
+enum { RB_PREC_FP64 = 0, RB_PREC_MIXED = 1 };
+
+/* Status codes returned by every C-ABI entry point (0 = success). */
+enum {
+  RB_OK = 0,
+  RB_ERR_INVALID = 1,     /* bad argument / unsupported namelist value     */
+  RB_ERR_STATE = 2,       /* call out of order (no init, no tree, ...)     */
+  RB_ERR_CUDA = 3,        /* CUDA runtime error                             */
+  RB_ERR_NOMEM = 4,       /* device or host allocation failed               */
+  RB_ERR_TREE = 5,        /* octree violates the nesting rule               */
+  RB_ERR_NUMERIC = 6,     /* non-finite or non-positive state detected      */
+  RB_ERR_NO_DEVICE = 7,   /* no CUDA device / kernel image for this GPU     */
+  RB_ERR_CAPACITY = 8     /* request above a fixed capacity                 */
+};
+
+/* &HYDRO_PARAMS values consumed by the hydro step
+ * (hydro/hydro_parameters.f90:74-89). Strings are passed as codes. */
+typedef struct rb_hydro_params {
+  double gamma;
+  double smallr;
+  double smallc;
+  double courant_factor;
+  double slope_theta;
+  int32_t riemann;       /* RB_RIEMANN_*; 'exact'/'acoustic' are rejected  */
+  int32_t slope_type;    /* 0,1,2,3,7,8                                    */
+  int32_t scheme;        /* 0 = 'muscl' ('plmde' is rejected)              */
+  int32_t interpol_var;  /* 0,1,2                                          */
+  int32_t interpol_type; /* 0..4                                           */
+  int32_t pressure_fix;  /* must be 0                                      */
+  double difmag;         /* must be 0                                      */
+} rb_hydro_params;
+
+/* &AMR_PARAMS / &RUN_PARAMS values and the tree dimensions
+ * (amr/amr_parameters.f90, amr/amr_commons.f90). */
+typedef struct rb_mesh_params {
+  int32_t nx, ny, nz;          /* coarse grid                              */
+  int32_t ncoarse;             /* nx*ny*nz                                 */
+  int32_t ngridmax;            /* oct capacity                             */
+  int32_t nlevelmax;
+  int32_t levelmin;
+  int32_t nvector;             /* host vector-sweep width (batch order)    */
+  double boxlen;
+  int32_t nsubcycle[RB_MAXLEVEL + 1]; /* index = level (1-based)          */
+} rb_mesh_params;
+
+#endif

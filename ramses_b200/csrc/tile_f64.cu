@@ -1,0 +1,7 @@
+// FP64 drop-in instances of the godunov tile kernel. Compiled with
+// --fmad=false: no multiply-add is contracted, so every flux and update is
+// bit-identical to the reference's operation order.
+#define RB_TILE_REAL double
+#define RB_TILE_LAUNCH launch_tile_f64
+#define RB_TILE_SMEM tile_smem_f64
+#include "tile_instances.inc"

@@ -1,0 +1,33 @@
+// tile_launch.h -- host-side launch interface of the godunov tile kernel for
+// the two compute precisions (separate translation units so that the FP64
+// unit is compiled without multiply-add contraction).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace rb {
+
+struct TileArgs;
+
+struct TileShape {
+  int tx, ty, tz;   // tile size in cells (even)
+  int nthreads;     // CTA size
+};
+
+// Supported tile shapes, indexed by shape id.
+constexpr int kNumTileShapes = 5;
+constexpr TileShape kTileShapes[kNumTileShapes] = {
+    {2, 2, 2, 64},    // one oct: the reference's per-oct stencil
+    {4, 4, 4, 128},
+    {8, 4, 4, 256},
+    {8, 8, 4, 256},
+    {8, 8, 8, 256},
+};
+
+size_t tile_smem_f64(int shape);
+size_t tile_smem_mixed(int shape);
+cudaError_t launch_tile_f64(int shape, const TileArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_tile_mixed(int shape, const TileArgs& a, int grid, cudaStream_t s);
+
+}  // namespace rb

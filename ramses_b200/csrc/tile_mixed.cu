@@ -1,0 +1,7 @@
+// FP32-mixed instances of the godunov tile kernel: slopes, trace and Riemann
+// fluxes in FP32 (contracted, fast division); conservative->primitive and the
+// conservative accumulation into unew stay FP64.
+#define RB_TILE_REAL float
+#define RB_TILE_LAUNCH launch_tile_mixed
+#define RB_TILE_SMEM tile_smem_mixed
+#include "tile_instances.inc"

@@ -1,0 +1,304 @@
+"""Octree construction in RAMSES's own index conventions.
+
+The hydro path consumes the tree arrays exactly as RAMSES lays them out
+(``amr/amr_commons.f90:67-75``, ``amr/init_amr.f90:37-54,227-233``):
+
+* ``ncoarse = nx*ny*nz`` coarse cells, then ``8*ngridmax`` oct cells;
+  the cell of child slot ``ind`` (1..8) of oct ``igrid`` (1-based) is
+  ``ncoarse + (ind-1)*ngridmax + igrid``; ``ind = 1 + ix + 2*iy + 4*iz``;
+* ``son(icell)`` = the oct refining that cell, or 0;
+* ``father(igrid)`` = the cell the oct refines;
+* ``nbor(igrid, j)``, j = 1..6 for -x,+x,-y,+y,-z,+z = the cell adjacent
+  to ``father(igrid)`` at the father's level (periodic box);
+* ``active(ilevel)%igrid`` = the octs of level ``ilevel``.
+
+Levels 1..levelmin are complete; finer levels follow a refinement map that is
+closed under RAMSES's nesting rule (every refined cell's 3x3x3 neighbourhood
+exists at its level), which is what ``get3cubefather``
+(``amr/nbors_utils.f90:5-194``) relies on. Octs of each level are numbered in
+creation order (parents in order, children in slot order), which for a
+single-cell coarse grid is Morton order.
+
+This module builds inputs; it performs no hydro arithmetic.
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+MAXLEVEL = 32
+
+
+@dataclasses.dataclass
+class Octree:
+    nx: int
+    ny: int
+    nz: int
+    ncoarse: int
+    ngridmax: int
+    nlevelmax: int
+    levelmin: int
+    boxlen: float
+    son: np.ndarray          # int32 [ncell]
+    father: np.ndarray       # int32 [ngridmax]
+    nbor: np.ndarray         # int32 [6, ngridmax]  (Fortran nbor(ngridmax,6))
+    active: list             # active[l] = int32 array of 1-based igrids, l=1..nlevelmax
+    coords: list             # coords[l] = int64 (n,3) oct coordinates at level l
+
+    @property
+    def ncell(self) -> int:
+        return self.ncoarse + 8 * self.ngridmax
+
+    def noct(self, level: int) -> int:
+        return len(self.active[level]) if level < len(self.active) else 0
+
+    def active_concat(self):
+        """(concatenated int32 list, int64 offsets[nlevelmax+2]) with level l's
+        list at [off[l], off[l+1])."""
+        off = np.zeros(self.nlevelmax + 2, dtype=np.int64)
+        for l in range(1, self.nlevelmax + 1):
+            off[l + 1] = off[l] + self.noct(l)
+        cat = np.concatenate([self.active[l] for l in range(1, self.nlevelmax + 1)
+                              if self.noct(l) > 0] or [np.zeros(0, np.int32)])
+        return cat.astype(np.int32), off
+
+    def leaf_cells(self, level: int) -> int:
+        a = self.active[level]
+        if len(a) == 0:
+            return 0
+        cells = self.ncoarse + np.arange(8)[:, None] * self.ngridmax + a[None, :]
+        return int(np.count_nonzero(self.son[cells - 1] == 0))
+
+    def cell_index(self, level: int, order: str = "C") -> np.ndarray:
+        """1-based cell indices of level ``level`` arranged as a dense cube
+        [z, y, x] (only valid for a complete level)."""
+        n = 2 ** level
+        a = self.active[level]
+        c = self.coords[level]
+        if len(a) != (n // 2) ** 3:
+            raise ValueError("level %d is not complete" % level)
+        out = np.zeros((n, n, n), dtype=np.int64)
+        for ind in range(8):
+            ix, iy, iz = ind & 1, (ind >> 1) & 1, (ind >> 2) & 1
+            cell = self.ncoarse + ind * self.ngridmax + a.astype(np.int64)
+            out[2 * c[:, 2] + iz, 2 * c[:, 1] + iy, 2 * c[:, 0] + ix] = cell
+        return out
+
+    def cell_centres(self, level: int):
+        """(cells[1-based], x[n,3]) for every cell of the octs of ``level``."""
+        a = self.active[level].astype(np.int64)
+        c = self.coords[level]
+        dx = self.boxlen / self.nx * 0.5 ** level
+        cells, xs = [], []
+        for ind in range(8):
+            off = np.array([ind & 1, (ind >> 1) & 1, (ind >> 2) & 1])
+            cells.append(self.ncoarse + ind * self.ngridmax + a)
+            xs.append((2 * c + off + 0.5) * dx)
+        return np.concatenate(cells), np.concatenate(xs)
+
+
+def _keys(c: np.ndarray, n: int) -> np.ndarray:
+    return c[:, 0] + n * (c[:, 1] + n * c[:, 2])
+
+
+def _neighbourhood(cells: np.ndarray) -> np.ndarray:
+    offs = np.array([[i, j, k] for k in (-1, 0, 1) for j in (-1, 0, 1) for i in (-1, 0, 1)])
+    return (cells[:, None, :] + offs[None, :, :]).reshape(-1, 3)
+
+
+def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
+               refine: Optional[Callable[[int, np.ndarray], np.ndarray]] = None,
+               boxlen: float = 1.0, nexpand: int = 1) -> Octree:
+    """Build a periodic single-coarse-cell (nx=ny=nz=1) octree.
+
+    ``refine(level, cell_coords[n,3]) -> bool[n]`` flags level-``level``
+    cells (level >= levelmin) for refinement; flags are expanded by
+    ``nexpand`` cells and closed under the nesting rule.
+    """
+    if nlevelmax is None:
+        nlevelmax = levelmin
+    if not (1 <= levelmin <= nlevelmax <= MAXLEVEL - 1):
+        raise ValueError("bad level range")
+    # -- 1. refined cell sets per level, as integer coords (level-l units) --
+    refined = {}
+    cur_octs = np.zeros((1, 3), dtype=np.int64)   # level-1 oct(s)
+    oct_coords = {1: cur_octs}
+    for l in range(1, nlevelmax):
+        n = 2 ** l
+        octs = oct_coords[l]
+        cells = (2 * octs[:, None, :] + np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1]
+                                                   for i in range(8)])[None]).reshape(-1, 3)
+        if l < levelmin:
+            flag = np.ones(len(cells), dtype=bool)
+        elif refine is None:
+            flag = np.zeros(len(cells), dtype=bool)
+        else:
+            flag = np.asarray(refine(l, cells), dtype=bool)
+        fc = cells[flag]
+        for _ in range(nexpand if l >= levelmin else 0):
+            if len(fc) == 0:
+                break
+            nb = _neighbourhood(fc) % n
+            k = np.unique(_keys(nb, n))
+            ck = _keys(cells, n)
+            fc = cells[np.isin(ck, k)]
+        refined[l] = fc
+        oct_coords[l + 1] = fc.copy()
+        if len(fc) == 0:
+            for ll in range(l + 1, nlevelmax + 1):
+                oct_coords.setdefault(ll, np.zeros((0, 3), np.int64))
+            break
+    for l in range(1, nlevelmax + 1):
+        oct_coords.setdefault(l, np.zeros((0, 3), np.int64))
+    # -- 2. closure under the nesting rule, finest to coarsest --
+    for l in range(nlevelmax - 1, levelmin, -1):
+        fc = refined.get(l, np.zeros((0, 3), np.int64))
+        if len(fc) == 0:
+            continue
+        n = 2 ** l
+        need = np.unique(_keys((_neighbourhood(fc) % n) // 2, n // 2))
+        have = _keys(refined[l - 1], n // 2)
+        missing = np.setdiff1d(need, have)
+        if len(missing):
+            nn = n // 2
+            mc = np.stack([missing % nn, (missing // nn) % nn, missing // (nn * nn)], 1)
+            refined[l - 1] = np.concatenate([refined[l - 1], mc])
+    # recompute oct sets from the closed refinement sets, keeping only cells
+    # whose own oct exists (parents refined)
+    oct_coords = {1: np.zeros((1, 3), dtype=np.int64)}
+    for l in range(1, nlevelmax):
+        n = 2 ** l
+        fc = refined.get(l, np.zeros((0, 3), np.int64))
+        if len(fc) == 0:
+            oct_coords[l + 1] = np.zeros((0, 3), np.int64)
+            continue
+        parent_keys = _keys(oct_coords[l], n // 2)
+        fc = fc[np.isin(_keys(fc // 2, n // 2), parent_keys)]
+        refined[l] = fc
+        oct_coords[l + 1] = fc
+    return _assemble(oct_coords, levelmin, nlevelmax, boxlen)
+
+
+def _assemble(oct_coords, levelmin, nlevelmax, boxlen) -> Octree:
+    ncoarse = 1
+    counts = [len(oct_coords.get(l, ())) for l in range(1, nlevelmax + 1)]
+    ngridmax = int(sum(counts))
+    ncell = ncoarse + 8 * ngridmax
+    son = np.zeros(ncell, dtype=np.int32)
+    father = np.zeros(ngridmax, dtype=np.int32)
+    nbor = np.zeros((6, ngridmax), dtype=np.int32)
+    active = [np.zeros(0, np.int32) for _ in range(nlevelmax + 1)]
+    coords = [np.zeros((0, 3), np.int64) for _ in range(nlevelmax + 1)]
+    # order: level by level; within a level, by (parent igrid, child slot)
+    g0 = 0
+    parent_lookup = None   # (sorted keys, igrid) for level l-1 octs
+    for l in range(1, nlevelmax + 1):
+        oc = oct_coords.get(l, np.zeros((0, 3), np.int64))
+        n_oct = len(oc)
+        if n_oct == 0:
+            break
+        if l == 1:
+            order = np.arange(n_oct)
+        else:
+            # parent oct at level l-1 and slot of the father cell
+            pk = _keys(oc // 2, 2 ** (l - 2))
+            keys_sorted, igr = parent_lookup
+            pos = np.searchsorted(keys_sorted, pk)
+            pg = igr[pos]
+            slot = (oc[:, 0] & 1) + 2 * (oc[:, 1] & 1) + 4 * (oc[:, 2] & 1)
+            order = np.lexsort((slot, pg))
+        oc = oc[order]
+        ig = np.arange(g0 + 1, g0 + 1 + n_oct, dtype=np.int64)
+        active[l] = ig.astype(np.int32)
+        coords[l] = oc
+        # father cells and neighbour father cells
+        if l == 1:
+            father[ig - 1] = 1
+            nbor[:, ig - 1] = 1
+            son[0] = int(ig[0])
+        else:
+            keys_sorted, igr = parent_lookup
+            nl = 2 ** (l - 1)  # cells per dim at level l-1
+
+            def cell_of(cc):
+                cc = cc % nl
+                k = _keys(cc // 2, nl // 2)
+                pos = np.searchsorted(keys_sorted, k)
+                if np.any(pos >= len(keys_sorted)) or np.any(keys_sorted[np.minimum(pos, len(keys_sorted) - 1)] != k):
+                    raise ValueError("refinement map violates the nesting rule at level %d" % l)
+                slot = (cc[:, 0] & 1) + 2 * (cc[:, 1] & 1) + 4 * (cc[:, 2] & 1)
+                return ncoarse + slot * ngridmax + igr[pos]
+
+            fcell = cell_of(oc)
+            father[ig - 1] = fcell
+            son[fcell - 1] = ig
+            for j in range(6):
+                d = j // 2
+                step = np.zeros(3, np.int64)
+                step[d] = 1 if (j % 2) else -1
+                nbor[j, ig - 1] = cell_of(oc + step)
+        k = _keys(oc, 2 ** (l - 1))
+        srt = np.argsort(k)
+        parent_lookup = (k[srt], ig[srt])
+        g0 += n_oct
+    return Octree(nx=1, ny=1, nz=1, ncoarse=ncoarse, ngridmax=ngridmax,
+                  nlevelmax=nlevelmax, levelmin=levelmin, boxlen=float(boxlen),
+                  son=son, father=father, nbor=nbor, active=active, coords=coords)
+
+
+def uniform_tree(level: int, boxlen: float = 1.0) -> Octree:
+    """Complete periodic grid of (2**level)^3 leaf cells (levelmin=levelmax)."""
+    return build_tree(level, level, None, boxlen)
+
+
+def gradient_refine(field_fn: Callable[[np.ndarray], Sequence[np.ndarray]],
+                    thresholds: Sequence[float], boxlen: float = 1.0,
+                    floor: float = 1e-10) -> Callable[[int, np.ndarray], np.ndarray]:
+    """Refinement flags from RAMSES's relative-gradient criterion
+    (``hydro/godunov_utils.f90:125-263``, ``err_grad_*``) evaluated on an
+    analytic field at level-``l`` cell centres: a cell is flagged when
+    ``|f(i+1)-f(i-1)| / (|f(i+1)|+|f(i)|+|f(i-1)|+floor)`` exceeds the
+    threshold in any direction for any field."""
+    def refine(level: int, cells: np.ndarray) -> np.ndarray:
+        dx = boxlen * 0.5 ** level
+        x0 = (cells + 0.5) * dx
+        flag = np.zeros(len(cells), dtype=bool)
+        f0 = field_fn(x0 % boxlen)
+        for d in range(3):
+            e = np.zeros(3)
+            e[d] = dx
+            fp = field_fn((x0 + e) % boxlen)
+            fm = field_fn((x0 - e) % boxlen)
+            for a, b, c, thr in zip(fm, f0, fp, thresholds):
+                if thr <= 0:
+                    continue
+                err = np.abs(c - a) / (np.abs(c) + np.abs(b) + np.abs(a) + floor)
+                flag |= err > thr
+        return flag
+    return refine
+
+
+def sphere_refine(centre, radius: float, boxlen: float = 1.0, pad_cells: float = 2.0
+                  ) -> Callable[[int, np.ndarray], np.ndarray]:
+    """Geometric refinement: flag level-``l`` cells whose centre lies within
+    ``radius + pad_cells*dx_l`` of ``centre`` (periodic distance)."""
+    c = np.asarray(centre, dtype=np.float64) * boxlen
+
+    def refine(level: int, cells: np.ndarray) -> np.ndarray:
+        dx = boxlen * 0.5 ** level
+        x = (cells + 0.5) * dx
+        d = np.abs(x - c)
+        d = np.minimum(d, boxlen - d)
+        return np.sqrt(np.sum(d * d, axis=1)) < radius + pad_cells * dx
+    return refine
+
+
+def union_refine(*fns) -> Callable[[int, np.ndarray], np.ndarray]:
+    def refine(level: int, cells: np.ndarray) -> np.ndarray:
+        out = np.zeros(len(cells), dtype=bool)
+        for f in fns:
+            out |= f(level, cells)
+        return out
+    return refine

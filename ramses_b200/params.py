@@ -1,0 +1,116 @@
+"""Host-side mirror of RAMSES's ``&HYDRO_PARAMS`` / ``&AMR_PARAMS`` knobs that the
+hydro step reads (``hydro/hydro_parameters.f90:74-89``, read by
+``hydro/read_hydro_params.f90:43-54,138``; ``amr/amr_parameters.f90``).
+
+Defaults are the reference's defaults. Values outside what the CUDA path
+implements are rejected when the library is initialised (there is no CPU
+fallback), mirroring the reference's ``stop`` on an unknown Riemann solver
+(``hydro/umuscl.f90:801-803``) or slope type (``:1474-1476``).
+"""
+from __future__ import annotations
+
+import dataclasses
+import re
+from typing import Dict, List
+
+RIEMANN_CODES = {"llf": 1, "hll": 2, "hllc": 3}
+SLOPE_TYPES = (0, 1, 2, 3, 7, 8)
+
+
+@dataclasses.dataclass
+class HydroParams:
+    gamma: float = 1.4
+    courant_factor: float = 0.5
+    smallr: float = 1e-10
+    smallc: float = 1e-10
+    slope_type: int = 1
+    slope_theta: float = 1.5
+    riemann: str = "llf"
+    scheme: str = "muscl"
+    interpol_var: int = 0
+    interpol_type: int = 1
+    pressure_fix: bool = False
+    difmag: float = 0.0
+
+    @property
+    def riemann_code(self) -> int:
+        try:
+            return RIEMANN_CODES[self.riemann.strip().lower()]
+        except KeyError:
+            raise ValueError("unknown Riemann solver %r (supported: llf, hll, hllc)" % self.riemann)
+
+    def validate(self) -> None:
+        self.riemann_code  # noqa: B018 - raises on unknown solver
+        if self.slope_type not in SLOPE_TYPES:
+            raise ValueError("Unknown slope type %r" % self.slope_type)
+        if self.scheme.strip().lower() != "muscl":
+            raise ValueError("scheme %r not supported (muscl only)" % self.scheme)
+        if self.pressure_fix:
+            raise ValueError("pressure_fix is not supported")
+        if self.difmag != 0.0:
+            raise ValueError("difmag>0 is not supported")
+        if self.interpol_var not in (0, 1, 2) or self.interpol_type not in (0, 1, 2, 3, 4):
+            raise ValueError("bad interpol_var/interpol_type")
+        if self.interpol_type == 4 and self.interpol_var != 2:
+            raise ValueError("interpol_type=4 is designed for interpol_var=2")
+
+
+def parse_namelist(text: str) -> Dict[str, Dict[str, str]]:
+    """Minimal Fortran namelist reader: {group: {name: raw value}}."""
+    groups: Dict[str, Dict[str, str]] = {}
+    for m in re.finditer(r"&(\w+)(.*?)\n\s*/", text, flags=re.S):
+        g = m.group(1).upper()
+        body = re.sub(r"!.*", "", m.group(2))
+        entries: Dict[str, str] = {}
+        for line in re.split(r"[\n,](?=\s*[A-Za-z_][\w()]*\s*=)", body):
+            if "=" in line:
+                k, v = line.split("=", 1)
+                entries[k.strip().lower()] = v.strip().rstrip(",")
+        groups[g] = entries
+    return groups
+
+
+def _fortran_value(v: str):
+    v = v.strip()
+    if v.lower() in (".true.", "t"):
+        return True
+    if v.lower() in (".false.", "f"):
+        return False
+    if v[:1] in "'\"":
+        return v.strip("'\"")
+    try:
+        return int(v)
+    except ValueError:
+        return float(v.lower().replace("d", "e"))
+
+
+def hydro_params_from_namelist(text: str) -> HydroParams:
+    g = parse_namelist(text).get("HYDRO_PARAMS", {})
+    hp = HydroParams()
+    fields = {f.name for f in dataclasses.fields(HydroParams)}
+    for k, v in g.items():
+        if k in fields:
+            setattr(hp, k, _fortran_value(v))
+    for k, v in parse_namelist(text).get("REFINE_PARAMS", {}).items():
+        if k in ("interpol_var", "interpol_type"):
+            setattr(hp, k, _fortran_value(v))
+    return hp
+
+
+def nsubcycle_from_namelist(text: str, nlevelmax: int) -> List[int]:
+    """``nsubcycle`` of ``&RUN_PARAMS`` (default 2 for every level), with
+    Fortran repeat counts (``3*1,2``)."""
+    out = [2] * (nlevelmax + 1)
+    raw = parse_namelist(text).get("RUN_PARAMS", {}).get("nsubcycle")
+    if raw:
+        vals: List[int] = []
+        for tok in raw.replace(" ", "").split(","):
+            if "*" in tok:
+                r, v = tok.split("*")
+                vals += [int(v)] * int(r)
+            elif tok:
+                vals.append(int(tok))
+        for i, v in enumerate(vals):
+            if i + 1 <= nlevelmax:
+                out[i + 1] = v
+    return out

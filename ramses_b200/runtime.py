@@ -1,0 +1,305 @@
+"""ctypes binding of the C ABI (``include/ramses_b200.h``) and a small host-side
+driver that mirrors the reference's hydro call sites.
+
+The library is the in-tree ``ramses_b200/lib/libramses_b200.so``; there is no
+CPU fallback: if it cannot be loaded, or no CUDA device is visible, every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .mesh import Octree
+from .params import HydroParams
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libramses_b200.so"
+
+RB_PREC_FP64 = 0
+RB_PREC_MIXED = 1
+MAXLEVEL = 32
+
+_P32 = ctypes.POINTER(ctypes.c_int32)
+_P64 = ctypes.POINTER(ctypes.c_int64)
+_PD = ctypes.POINTER(ctypes.c_double)
+
+
+class HydroParamsC(ctypes.Structure):
+    _fields_ = [("gamma", ctypes.c_double), ("smallr", ctypes.c_double), ("smallc", ctypes.c_double),
+                ("courant_factor", ctypes.c_double), ("slope_theta", ctypes.c_double),
+                ("riemann", ctypes.c_int32), ("slope_type", ctypes.c_int32), ("scheme", ctypes.c_int32),
+                ("interpol_var", ctypes.c_int32), ("interpol_type", ctypes.c_int32),
+                ("pressure_fix", ctypes.c_int32), ("difmag", ctypes.c_double)]
+
+
+class MeshParamsC(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("ncoarse", ctypes.c_int32), ("ngridmax", ctypes.c_int32), ("nlevelmax", ctypes.c_int32),
+                ("levelmin", ctypes.c_int32), ("nvector", ctypes.c_int32), ("boxlen", ctypes.c_double),
+                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1))]
+
+
+class RBError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        super().__init__("%s: status %d (%s): %s" % (where, status, status_string(status), detail))
+        self.status = status
+
+
+_lib = None
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "rb_version": (ctypes.c_char_p, []),
+    "rb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "rb_last_error": (ctypes.c_char_p, []),
+    "rb_device_count": (ctypes.c_int, []),
+    "rb_select_device": (ctypes.c_int, [ctypes.c_int]),
+    "rb_create": (ctypes.c_int, [ctypes.POINTER(HydroParamsC), ctypes.POINTER(MeshParamsC), ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_void_p)]),
+    "rb_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_sync_tree": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32, _P32]),
+    "rb_upload_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_download_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_upload_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_download_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_set_unew": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rb_set_uold": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rb_godunov_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]),
+    "rb_upload_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rb_courant_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _PD, _PD, _PD, _PD]),
+    "rb_coarse_step": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
+    "rb_cell_updates": (ctypes.c_int, [ctypes.c_void_p, _P64]),
+    "rb_set_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "rb_get_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P32]),
+    "rb_tile_shape_info": (ctypes.c_int, [ctypes.c_int, _P32, _P32, _P32, _P32]),
+    "rb_unsplit": (ctypes.c_int, [ctypes.POINTER(HydroParamsC), _PD, _PD, _PD, _PD, _PD, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
+    "rb_uniform_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _PD, _PD]),
+    "rb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    "rb_last_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "rb_last_run_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+}
+
+
+def load(path: Optional[os.PathLike] = None):
+    """Load the CUDA library (build it first with ``ramses_b200.build``)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError("CUDA library %s not built (run python -m ramses_b200.build)" % p)
+    L = ctypes.CDLL(str(p))
+    for name, (res, args) in _PROTOS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    if path is None:
+        _lib = L
+    return L
+
+
+def status_string(s: int) -> str:
+    try:
+        return load().rb_status_string(s).decode()
+    except Exception:  # pragma: no cover - message formatting only
+        return "?"
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        raise RBError(rc, where, load().rb_last_error().decode())
+
+
+def hydro_params_c(hp: HydroParams) -> HydroParamsC:
+    hp.validate()
+    return HydroParamsC(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta, hp.riemann_code,
+                        hp.slope_type, 0, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix), hp.difmag)
+
+
+def mesh_params_c(tree: Octree, nsubcycle: Optional[Sequence[int]] = None, nvector: int = 32) -> MeshParamsC:
+    m = MeshParamsC()
+    m.nx, m.ny, m.nz = tree.nx, tree.ny, tree.nz
+    m.ncoarse, m.ngridmax = tree.ncoarse, tree.ngridmax
+    m.nlevelmax, m.levelmin, m.nvector = tree.nlevelmax, tree.levelmin, nvector
+    m.boxlen = tree.boxlen
+    ns = list(nsubcycle) if nsubcycle is not None else [2] * (MAXLEVEL + 1)
+    for i in range(MAXLEVEL + 1):
+        m.nsubcycle[i] = ns[i] if i < len(ns) else 2
+    return m
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+def device_count() -> int:
+    return load().rb_device_count()
+
+
+def select_device(device: int) -> None:
+    _check(load().rb_select_device(device), "rb_select_device")
+
+
+class Solver:
+    """One device-resident hydro problem (a ``rb_context``)."""
+
+    def __init__(self, tree: Octree, hp: HydroParams, precision: str = "fp64",
+                 nsubcycle: Optional[Sequence[int]] = None, nvector: int = 32, uold: Optional[np.ndarray] = None):
+        L = load()
+        self.tree = tree
+        self.hp = hp
+        self.precision = precision
+        prec = {"fp64": RB_PREC_FP64, "mixed": RB_PREC_MIXED}[precision]
+        self._hpc = hydro_params_c(hp)
+        self._mpc = mesh_params_c(tree, nsubcycle, nvector)
+        h = ctypes.c_void_p()
+        _check(L.rb_create(ctypes.byref(self._hpc), ctypes.byref(self._mpc), prec, ctypes.byref(h)), "rb_create")
+        self._h = h
+        self.t = 0.0
+        self.sync_tree()
+        if uold is not None:
+            self.upload_state(uold)
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            load().rb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- tree / state -----------------------------------------------------
+    def sync_tree(self, tree: Optional[Octree] = None):
+        if tree is not None:
+            self.tree = tree
+        t = self.tree
+        son = np.ascontiguousarray(t.son, np.int32)
+        father = np.ascontiguousarray(t.father, np.int32)
+        nbor = np.ascontiguousarray(t.nbor, np.int32)
+        numbl = np.array([t.noct(l) for l in range(1, t.nlevelmax + 1)], np.int32)
+        act, _ = t.active_concat()
+        _check(load().rb_sync_tree(self._h, _ptr(son, _P32), _ptr(father, _P32), _ptr(nbor, _P32),
+                                   _ptr(numbl, _P32), _ptr(act, _P32)), "rb_sync_tree")
+
+    def upload_state(self, uold: np.ndarray):
+        u = np.ascontiguousarray(uold, np.float64)
+        assert u.shape == (5, self.tree.ncell)
+        _check(load().rb_upload_state(self._h, _ptr(u, _PD)), "rb_upload_state")
+
+    def download_state(self) -> np.ndarray:
+        u = np.empty((5, self.tree.ncell))
+        _check(load().rb_download_state(self._h, _ptr(u, _PD)), "rb_download_state")
+        return u
+
+    def upload_unew(self, unew: np.ndarray):
+        u = np.ascontiguousarray(unew, np.float64)
+        _check(load().rb_upload_unew(self._h, _ptr(u, _PD)), "rb_upload_unew")
+
+    def download_unew(self) -> np.ndarray:
+        u = np.empty((5, self.tree.ncell))
+        _check(load().rb_download_unew(self._h, _ptr(u, _PD)), "rb_download_unew")
+        return u
+
+    # -- level operations (reference names) ------------------------------
+    def set_unew(self, ilevel: int):
+        _check(load().rb_set_unew(self._h, ilevel), "rb_set_unew")
+
+    def set_uold(self, ilevel: int):
+        _check(load().rb_set_uold(self._h, ilevel), "rb_set_uold")
+
+    def godunov_fine(self, ilevel: int, dt: float):
+        _check(load().rb_godunov_fine(self._h, ilevel, dt), "rb_godunov_fine")
+
+    def upload_fine(self, ilevel: int):
+        _check(load().rb_upload_fine(self._h, ilevel), "rb_upload_fine")
+
+    def courant_fine(self, ilevel: int, dt_in: Optional[float] = None):
+        dt = ctypes.c_double(self.tree.boxlen / self.hp.smallc if dt_in is None else dt_in)
+        ma, ek, ei = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(load().rb_courant_fine(self._h, ilevel, ctypes.byref(dt), ctypes.byref(ma), ctypes.byref(ek),
+                                      ctypes.byref(ei)), "rb_courant_fine")
+        return dt.value, ma.value, ek.value, ei.value
+
+    def coarse_step(self) -> float:
+        t = ctypes.c_double(self.t)
+        dts = (ctypes.c_double * MAXLEVEL)()
+        _check(load().rb_coarse_step(self._h, ctypes.byref(t), dts), "rb_coarse_step")
+        self.t = t.value
+        self.last_dtnew = list(dts)
+        return self.t
+
+    def uniform_run(self, nsteps: int, graph: bool = True) -> float:
+        t = ctypes.c_double(self.t)
+        dt = ctypes.c_double()
+        _check(load().rb_uniform_run(self._h, nsteps, 1 if graph else 0, ctypes.byref(t), ctypes.byref(dt)),
+               "rb_uniform_run")
+        self.t = t.value
+        self.next_dt = dt.value
+        return self.t
+
+    @property
+    def cell_updates(self) -> int:
+        n = ctypes.c_int64()
+        _check(load().rb_cell_updates(self._h, ctypes.byref(n)), "rb_cell_updates")
+        return n.value
+
+    def set_tile_shape(self, ilevel: int, shape: int):
+        _check(load().rb_set_tile_shape(self._h, ilevel, shape), "rb_set_tile_shape")
+
+    def tile_shape(self, ilevel: int) -> int:
+        s = ctypes.c_int32()
+        _check(load().rb_get_tile_shape(self._h, ilevel, ctypes.byref(s)), "rb_get_tile_shape")
+        return s.value
+
+    def synchronize(self):
+        _check(load().rb_synchronize(self._h), "rb_synchronize")
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(load().rb_get_stream(self._h, ctypes.byref(s)), "rb_get_stream")
+        return s.value or 0
+
+    def last_kernel_ms(self) -> float:
+        f = ctypes.c_float()
+        _check(load().rb_last_kernel_ms(self._h, ctypes.byref(f)), "rb_last_kernel_ms")
+        return f.value
+
+    def last_run_ms(self) -> float:
+        f = ctypes.c_float()
+        _check(load().rb_last_run_ms(self._h, ctypes.byref(f)), "rb_last_run_ms")
+        return f.value
+
+
+def unsplit(hp: HydroParams, uin: np.ndarray, gravin: Optional[np.ndarray], dx: float, dt: float,
+            ngrid: Optional[int] = None):
+    """GPU ``unsplit`` with the reference's Fortran layouts: uin (5,6,6,6,nvector)
+    C-order == Fortran uin(nvector,-1:4,-1:4,-1:4,5). Returns (flux, tmp) with
+    shapes (3,5,3,3,3,nv) and (3,2,3,3,3,nv)."""
+    L = load()
+    uin = np.ascontiguousarray(uin, np.float64)
+    nv = uin.shape[-1]
+    g = None if gravin is None else np.ascontiguousarray(gravin, np.float64)
+    flux = np.zeros((3, 5, 3, 3, 3, nv))
+    tmp = np.zeros((3, 2, 3, 3, 3, nv))
+    hpc = hydro_params_c(hp)
+    _check(L.rb_unsplit(ctypes.byref(hpc), _ptr(uin, _PD), None if g is None else _ptr(g, _PD), None,
+                        _ptr(flux, _PD), _ptr(tmp, _PD), dx, dx, dx, dt, nv if ngrid is None else ngrid, nv),
+           "rb_unsplit")
+    return flux, tmp

@@ -1,0 +1,64 @@
+"""Shared problem builders for the tests (seeded synthetic inputs)."""
+import numpy as np
+
+from ramses_b200 import ics, mesh
+from ramses_b200.params import HydroParams
+
+
+def sedov_uniform(level, riemann="hllc", slope_type=1, courant=0.8):
+    hp = HydroParams(gamma=1.4, riemann=riemann, slope_type=slope_type, courant_factor=courant)
+    tree = mesh.uniform_tree(level)
+    u = ics.fill_all_levels(tree, ics.sedov_prim(level), hp.gamma)
+    return tree, hp, u
+
+
+def sedov_amr(lmin, lmax, riemann="hllc", slope_type=1, courant=0.8, interpol_var=0, interpol_type=1):
+    hp = HydroParams(gamma=1.4, riemann=riemann, slope_type=slope_type, courant_factor=courant,
+                     interpol_var=interpol_var, interpol_type=interpol_type)
+    prim = ics.sedov_prim(lmax)
+
+    def fields(x):
+        q = prim(x)
+        return [q[0], q[4]]
+    ref = mesh.union_refine(mesh.gradient_refine(fields, [0.1, 0.1]),
+                            mesh.sphere_refine((0.5, 0.5, 0.5), 2.5 * 0.5 ** lmax))
+    tree = mesh.build_tree(lmin, lmax, ref)
+    u = ics.fill_all_levels(tree, prim, hp.gamma)
+    return tree, hp, u
+
+
+def turbulent_uniform(level, seed=2024, slope_type=2, riemann="hllc"):
+    hp = HydroParams(gamma=1.001, riemann=riemann, slope_type=slope_type, courant_factor=0.8)
+    tree = mesh.uniform_tree(level)
+    q = ics.turbulent_box_prim_grid(2 ** level, seed=seed, gamma=hp.gamma)
+    u = ics.fill_uniform_level_from_grid(tree, level, q, hp.gamma)
+    return tree, hp, u
+
+
+def random_blocks(nv, seed=0, amp=0.3):
+    """Random positive states in the Fortran unsplit layout uin(nv,-1:4,-1:4,-1:4,5)
+    (C array (5,6,6,6,nv))."""
+    rng = np.random.default_rng(seed)
+    rho = np.exp(amp * rng.standard_normal((6, 6, 6, nv)))
+    vel = amp * rng.standard_normal((3, 6, 6, 6, nv))
+    p = np.exp(amp * rng.standard_normal((6, 6, 6, nv)))
+    q = np.concatenate([rho[None], vel, p[None]])
+    from ramses_b200.ics import prim_to_cons
+    return prim_to_cons(q.reshape(5, -1), 1.4).reshape(5, 6, 6, 6, nv)
+
+
+def leaf_values(tree, u):
+    """(cells, values[5,n]) of every leaf cell."""
+    cells = []
+    for l in range(1, tree.nlevelmax + 1):
+        a = tree.active[l]
+        if len(a) == 0:
+            continue
+        c = (tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + a[None, :]).reshape(-1)
+        cells.append(c[tree.son[c - 1] == 0])
+    cells = np.concatenate(cells)
+    return cells, u[:, cells - 1]
+
+
+def max_rel(a, b, floor=1e-300):
+    return float(np.max(np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), floor)))

@@ -1,0 +1,171 @@
+"""CPU checks of the oracle (the FP64 restatement of RAMSES's hydro step)
+against the reference's known-answer data and against properties the scheme
+must have. No GPU."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from ramses_b200 import ics, mesh
+from ramses_b200.params import HydroParams
+
+import exact_riemann
+from helpers import leaf_values, random_blocks, sedov_amr, sedov_uniform
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def sod_table():
+    return np.loadtxt(GOLDEN / "sod_tube_ana.csv", delimiter=",")
+
+
+def test_exact_riemann_reproduces_reference_sod_table():
+    d = sod_table()
+    s = exact_riemann.sample(d[:, 0], 0.245, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
+    # the reference table is printed with 4 significant digits
+    assert np.abs(s[0] - d[:, 2]).max() < 5e-4
+    assert np.abs(s[1] - d[:, 1]).max() < 5e-4
+    assert np.abs(s[2] - d[:, 3]).max() < 5e-4
+
+
+def _sod_run(level, slope_type):
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=slope_type, courant_factor=0.8)
+    tree = mesh.build_tree(level, level, None, boxlen=2.0)
+    prim = ics.shock_tube_prim(1.0, 1.0, 0.0, 0.125, 0.1, 0.0, x0=1.0, boxlen=2.0)
+    u = ics.fill_all_levels(tree, prim, hp.gamma)
+    run = oracle.OracleRun(tree, hp, u)
+    while run.t < 0.245:
+        run.coarse_step()
+    idx = tree.cell_index(level)
+    x = (np.arange(2 ** level) + 0.5) * (2.0 / 2 ** level) - 0.5
+    return run, tree, idx, x
+
+
+def test_oracle_sod_known_answer():
+    """Planar Sod tube (the reference's tests/hydro/sod-tube setup: hllc,
+    slope 2, C=0.8) on a periodic 64^3 box of length 2, tube = [0.5,1.5):
+    L1 density error against the exact solution at the final time, whose
+    solver is itself pinned to the reference table above."""
+    errs = {}
+    for st in (2, 0):
+        run, tree, idx, x = _sod_run(6, st)
+        rho = run.uold[0][idx - 1]
+        assert np.array_equal(rho, np.broadcast_to(rho[0, 0], rho.shape))  # planar symmetry kept
+        m = (x > 0) & (x < 1)
+        ana = exact_riemann.sample(x[m], run.t, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
+        errs[st] = np.abs(rho[0, 0][m] - ana[0]).sum() / np.abs(ana[0]).sum()
+    assert errs[2] < 0.03, errs
+    assert errs[2] < 0.7 * errs[0], errs
+
+
+def test_oracle_conserves_and_keeps_mirror_symmetry():
+    tree, hp, u = sedov_uniform(4)
+    run = oracle.OracleRun(tree, hp, u)
+    _, a0 = leaf_values(tree, u)
+    for _ in range(5):
+        run.coarse_step()
+    cells, a1 = leaf_values(tree, run.uold)
+    assert abs(a1[0].sum() - a0[0].sum()) <= 1e-14 * a0[0].sum()
+    assert abs(a1[4].sum() - a0[4].sum()) <= 1e-13 * a0[4].sum()
+    idx = tree.cell_index(4)
+    rho = run.uold[0][idx - 1]
+    np.testing.assert_array_equal(rho, rho[:, :, ::-1])
+    np.testing.assert_array_equal(rho, rho[::-1])
+
+
+def test_oracle_amr_conserves_mass_energy():
+    tree, hp, u = sedov_amr(3, 5)
+    run = oracle.OracleRun(tree, hp, u)
+
+    def totals(uu):
+        tot = np.zeros(5)
+        for l in range(1, tree.nlevelmax + 1):
+            a = tree.active[l]
+            if len(a) == 0:
+                continue
+            c = tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + a[None, :]
+            leaf = tree.son[c - 1] == 0
+            tot += (uu[:, c - 1] * leaf).sum(axis=(1, 2)) * (0.5 ** l) ** 3
+        return tot
+    t0 = totals(u)
+    for _ in range(3):
+        run.coarse_step()
+    t1 = totals(run.uold)
+    assert abs(t1[0] - t0[0]) <= 1e-14 * t0[0]
+    assert abs(t1[4] - t0[4]) <= 1e-13 * t0[4]
+
+
+def test_get3cubefather_matches_geometry():
+    tree, hp, u = sedov_amr(3, 5)
+    run = oracle.OracleRun(tree, hp, u)
+    rng = np.random.default_rng(1)
+    for level in (2, 4, 5):
+        a = tree.active[level]
+        for g in rng.choice(a, size=min(20, len(a)), replace=False):
+            fc = int(tree.father[g - 1])
+            got = run.get3cubefather(fc, level)
+            oc = tree.coords[level][np.searchsorted(a, g)]   # oct coords = father cell coords
+            n = 2 ** (level - 1)
+            for k in range(27):
+                off = np.array([k % 3 - 1, (k // 3) % 3 - 1, k // 9 - 1])
+                want = (oc + off) % n
+                cell = got[k]
+                assert cell > tree.ncoarse or level == 1
+                r = cell - 1 - tree.ncoarse
+                pg, ind = r % tree.ngridmax + 1, r // tree.ngridmax
+                pc = tree.coords[level - 1][np.searchsorted(tree.active[level - 1], pg)]
+                cc = 2 * pc + np.array([ind & 1, (ind >> 1) & 1, (ind >> 2) & 1])
+                np.testing.assert_array_equal(cc, want)
+
+
+def test_unsplit_uniform_state_gives_equal_fluxes():
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=2)
+    nv = 4
+    q = np.zeros((5, 6, 6, 6, nv))
+    q[0] = 1.3; q[1] = 0.2; q[2] = -0.1; q[3] = 0.05; q[4] = 0.7
+    u = ics.prim_to_cons(q.reshape(5, -1), hp.gamma).reshape(q.shape)
+    flux, _ = oracle.unsplit(hp, u, None, dx=0.1, dt=0.01)
+    fx = flux[0][:, 0:2, 0:2, 0:3, :]
+    assert np.all(fx == fx[:, :, :, :1, :])   # same flux on every x face
+
+
+def test_interpolation_is_conservative_for_density():
+    hp = HydroParams(interpol_var=0, interpol_type=2)
+    import ctypes
+    rng = np.random.default_rng(5)
+    nn = 16
+    u1 = np.ascontiguousarray(np.abs(rng.standard_normal((5, 7, nn))) + 0.5)
+    u2 = np.zeros((5, 8, nn))
+    p = oracle.params_struct(hp)
+    rc = oracle.lib().orc_interpol_hydro(ctypes.byref(p), u1.ctypes.data_as(oracle._PD),
+                                         u2.ctypes.data_as(oracle._PD), nn)
+    assert rc == 0
+    np.testing.assert_allclose(u2.mean(axis=1), u1[:, 0, :], rtol=1e-14)
+
+
+def test_cmpdt_formula():
+    hp = HydroParams(gamma=1.4, courant_factor=0.8)
+    nv = 8
+    rng = np.random.default_rng(2)
+    rho = rng.uniform(0.5, 2, nv); v = rng.standard_normal((3, nv)); p = rng.uniform(0.1, 1, nv)
+    q = np.concatenate([rho[None], v, p[None]])
+    uu = np.ascontiguousarray(ics.prim_to_cons(q, hp.gamma))
+    gg = np.zeros((3, nv))
+    import ctypes
+    dt = oracle.lib().orc_cmpdt(ctypes.byref(oracle.params_struct(hp)), uu.ctypes.data_as(oracle._PD),
+                                gg.ctypes.data_as(oracle._PD), 0.01, nv, nv)
+    c = np.sqrt(1.4 * p / rho)
+    speed = 3 * c + np.abs(v).sum(axis=0)
+    r = 1e-4
+    want = np.min(0.01 / speed * (np.sqrt(1 + 2 * 0.8 * r) - 1) / r)
+    assert abs(dt - want) <= 1e-12 * want
+
+
+def test_unsplit_batch_independence():
+    """Results of one oct do not depend on the other octs of the batch."""
+    hp = HydroParams(gamma=1.4, riemann="llf", slope_type=1)
+    u = random_blocks(8, seed=9)
+    f8, _ = oracle.unsplit(hp, u, None, dx=0.05, dt=1e-3)
+    f1, _ = oracle.unsplit(hp, np.ascontiguousarray(u[..., 3:4]), None, dx=0.05, dt=1e-3)
+    np.testing.assert_array_equal(f8[..., 3], f1[..., 0])
