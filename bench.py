@@ -52,6 +52,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-octs", type=int, default=32768)
+    ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
+                    help="run only one precision's timed steps (for profiling)")
+    ap.add_argument("--tile-shape", type=int, default=-1,
+                    help="force a godunov tile shape (default: autotuned on the workload)")
     return ap.parse_args()
 
 
@@ -125,6 +129,16 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def tile_dims(shape):
+    import ctypes
+
+    from ramses_b200 import runtime
+    v = [ctypes.c_int32() for _ in range(4)]
+    if runtime.load().rb_tile_shape_info(shape, *[ctypes.byref(x) for x in v]):
+        return "?"
+    return "%dx%dx%d cells/%d threads" % tuple(x.value for x in v)
 
 
 def hbm_peak():
@@ -231,8 +245,21 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.only:
+        # one precision's timed steps only (profiling runs: one solver resident)
+        s = runtime.Solver(tree, hp, precision=args.only, uold=u)
+        s.set_tile_shape(level, args.tile_shape)
+        s.uniform_run(args.warmup, graph=False)
+        s.uniform_run(args.steps, graph=False)
+        print(json.dumps({"only": args.only, "cells": cells, "ms_per_step": s.last_run_ms() / args.steps,
+                          "kernel_ms": s.last_kernel_ms(), "tile_shape": s.tile_shape(level),
+                          "value": cells * args.steps / (s.last_run_ms() / 1e3)}), flush=True)
+        s.close()
+        return
+
     # ---- FP32-mixed, device resident (headline) -------------------------
     mixed = runtime.Solver(tree, hp, precision="mixed", uold=u)
+    mixed.set_tile_shape(level, args.tile_shape)
     mixed.uniform_run(args.warmup, graph=False)
     barrier()
     mixed.synchronize()
@@ -242,11 +269,14 @@ def main():
     barrier()
     run_ms = max_over_ranks(mixed.last_run_ms())
     kern_ms = mixed.last_kernel_ms()
+    mixed_shape = mixed.tile_shape(level)
     value = cells * args.steps * world / (run_ms / 1e3)
     u_mixed = mixed.download_state()
 
     # ---- FP64 drop-in path on the same steps ----------------------------
     f64 = runtime.Solver(tree, hp, precision="fp64", uold=u)
+    f64.set_tile_shape(level, args.tile_shape)
+    f64_shape = f64.tile_shape(level)
     f64.uniform_run(args.warmup, graph=False)
     barrier()
     f64.uniform_run(args.steps, graph=False)
@@ -282,7 +312,7 @@ def main():
     for _ in range(args.e2e_steps):
         mixed.upload_state(host)
         mixed.uniform_run(1, graph=False)
-        host[:] = mixed.download_state()
+        mixed.download_state(out=host)
     mixed.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = cells * args.e2e_steps * world / e2e_s
@@ -308,13 +338,15 @@ def main():
                     "path": "rb_upload_state + rb_uniform_run(1) + rb_download_state, pinned host buffers"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "godunov_tile_kernel<float,8,8,8> (fused update + CFL partials)",
+                         "kernel": "godunov_tile_kernel<float> tile shape %d %s (fused update + CFL partials)"
+                                   % (mixed_shape, tile_dims(mixed_shape)),
                          "bytes_per_cell_update": BYTES_PER_CELL_UPDATE, "kernel_ms": kern_ms,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": 2 * args.steps,
             "fp64": {"value": f64_value, "ms_per_step": f64_ms / args.steps, "kernel_ms": f64_kern,
+                     "tile_shape": "%d %s" % (f64_shape, tile_dims(f64_shape)),
                      "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak},
             "mixed_over_fp64": value / f64_value,
             "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,

@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   __syncthreads();
 
   // ---- D. conservative update of active octs ----------------------------------
-  double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
+  double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
   const double vol = a.dx * a.dx * a.dx;
   for (int it = tid; it < G::NCELL; it += NT) {
     // octs-major order: 8 consecutive threads update one oct (coalesced rows)
@@ -287,29 +287,29 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       unv[v] = un;
     }
     if (a.fused) {
-      // courant_fine on the updated state (the next step's CFL condition)
+      // courant_fine on the updated state (the next step's CFL condition);
+      // the level minimum of dt_cell is dt_cell(maximum wave speed)
+      const double ir = 1.0 / fmx(unv[0], a.hp.smallr);
       mass = mass + unv[0] * vol;
       etot = etot + unv[4] * vol;
-      double ei = unv[4] * vol;
-      for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (unv[d] * unv[d]) / fmx(unv[0], a.hp.smallr) * vol;
-      eint = eint + ei;
-      dtm = fmn(dtm, cmpdt_cell(unv, a.dx, a.hp));
+      eint = eint + (unv[4] - 0.5 * (unv[1] * unv[1] + unv[2] * unv[2] + unv[3] * unv[3]) * ir) * vol;
+      smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(unv, a.hp) : cfl_speed_fast(unv, a.hp));
     }
   }
   if (a.fused) {
     __shared__ double red[4][NT / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-      dtm = fmn(dtm, __shfl_xor_sync(0xffffffffu, dtm, o));
+      smax = fmx(smax, __shfl_xor_sync(0xffffffffu, smax, o));
       mass += __shfl_xor_sync(0xffffffffu, mass, o);
       etot += __shfl_xor_sync(0xffffffffu, etot, o);
       eint += __shfl_xor_sync(0xffffffffu, eint, o);
     }
-    if ((tid & 31) == 0) { red[0][tid >> 5] = dtm; red[1][tid >> 5] = mass; red[2][tid >> 5] = etot; red[3][tid >> 5] = eint; }
+    if ((tid & 31) == 0) { red[0][tid >> 5] = smax; red[1][tid >> 5] = mass; red[2][tid >> 5] = etot; red[3][tid >> 5] = eint; }
     __syncthreads();
     if (tid == 0) {
-      for (int k = 1; k < NT / 32; k++) { dtm = fmn(dtm, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k]; }
-      a.partial[(int64_t)tile * 4 + 0] = dtm;
+      for (int k = 1; k < NT / 32; k++) { smax = fmx(smax, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k]; }
+      a.partial[(int64_t)tile * 4 + 0] = smax > 0.0 ? cfl_dt_from_speed(smax, a.dx, a.hp.courant_factor) : 1.0e300;
       a.partial[(int64_t)tile * 4 + 1] = mass;
       a.partial[(int64_t)tile * 4 + 2] = etot;
       a.partial[(int64_t)tile * 4 + 3] = eint;

@@ -408,8 +408,9 @@ __device__ __forceinline__ void interp_children(double u1[7][5], const rb_hydro_
 }
 
 // Per-cell CFL time step (cmpdt, godunov_utils.f90:5-120) with zero gravity.
-__device__ __forceinline__ double cmpdt_cell(const double uu_in[5], double dx, const rb_hydro_params& hp) {
-  const double gamma = hp.gamma, smallc = hp.smallc, C = hp.courant_factor;
+// CFL wave speed ndim*c + sum|v| of one cell in cmpdt's operation order.
+__device__ __forceinline__ double cfl_speed(const double uu_in[5], const rb_hydro_params& hp) {
+  const double gamma = hp.gamma, smallc = hp.smallc;
   const double smallp = smallc * smallc / gamma;
   double u1 = fmx(uu_in[0], hp.smallr);
   double v1 = uu_in[1] / u1, v2 = uu_in[2] / u1, v3 = uu_in[3] / u1;
@@ -424,11 +425,28 @@ __device__ __forceinline__ double cmpdt_cell(const double uu_in[5], double dx, c
   e = e + fabs(v1);
   e = e + fabs(v2);
   e = e + fabs(v3);
-  double g = 0.0;
-  g = g + 0.0; g = g + 0.0; g = g + 0.0;  // sum of |gravity| over 3 directions
-  g = g * dx / (e * e);
-  g = fmx(g, 0.0001);
-  return dx / e * (sqrt(1.0 + 2.0 * C * g) - 1.0) / g;
+  return e;
+}
+
+// Same speed with one reciprocal instead of four divisions (FP32-mixed path;
+// differs from cfl_speed in the last bits only).
+__device__ __forceinline__ double cfl_speed_fast(const double u[5], const rb_hydro_params& hp) {
+  const double gamma = hp.gamma;
+  const double rho = fmx(u[0], hp.smallr);
+  const double ir = 1.0 / rho;
+  const double v1 = u[1] * ir, v2 = u[2] * ir, v3 = u[3] * ir;
+  double e = u[4] - 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
+  e = fmx((gamma - 1.0) * e, rho * (hp.smallc * hp.smallc / gamma));
+  return 3.0 * sqrt(gamma * e * ir) + fabs(v1) + fabs(v2) + fabs(v3);
+}
+
+// With zero gravity the gravity-strength ratio of cmpdt is its floor 1e-4 in
+// every cell, so dt_cell = ((dx/speed)*(sqrt(1+2*C*1e-4)-1))/1e-4 is a
+// monotone function of the speed: the minimum over cells is exactly
+// dt_cell(maximum speed). (godunov_utils.f90:100-118)
+__device__ __forceinline__ double cfl_dt_from_speed(double s, double dx, double C) {
+  const double g = 0.0001;
+  return dx / s * (sqrt(1.0 + 2.0 * C * g) - 1.0) / g;
 }
 
 }  // namespace rb

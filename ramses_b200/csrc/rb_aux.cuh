@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __res
                                                              int64_t ncell, int32_t ncoarse, double dx,
                                                              rb_hydro_params hp, double* __restrict__ partial) {
   const double vol = dx * dx * dx;
-  double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
+  double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
   const int64_t n = (int64_t)noct * 8;
   for (int64_t i = blockIdx.x * (int64_t)NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
     const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
@@ -127,23 +127,23 @@ __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __res
     double ei = u[4] * vol;
     for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (u[d] * u[d]) / fmx(u[0], hp.smallr) * vol;
     eint = eint + ei;
-    dtm = fmn(dtm, cmpdt_cell(u, dx, hp));
+    smax = fmx(smax, cfl_speed(u, hp));
   }
   __shared__ double red[4][NT / 32];
   for (int o = 16; o > 0; o >>= 1) {
-    dtm = fmn(dtm, __shfl_xor_sync(0xffffffffu, dtm, o));
+    smax = fmx(smax, __shfl_xor_sync(0xffffffffu, smax, o));
     mass += __shfl_xor_sync(0xffffffffu, mass, o);
     etot += __shfl_xor_sync(0xffffffffu, etot, o);
     eint += __shfl_xor_sync(0xffffffffu, eint, o);
   }
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) { red[0][w] = dtm; red[1][w] = mass; red[2][w] = etot; red[3][w] = eint; }
+  if (l == 0) { red[0][w] = smax; red[1][w] = mass; red[2][w] = etot; red[3][w] = eint; }
   __syncthreads();
   if (threadIdx.x == 0) {
     for (int k = 1; k < NT / 32; k++) {
-      dtm = fmn(dtm, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k];
+      smax = fmx(smax, red[0][k]); mass += red[1][k]; etot += red[2][k]; eint += red[3][k];
     }
-    partial[blockIdx.x * 4 + 0] = dtm;
+    partial[blockIdx.x * 4 + 0] = smax > 0.0 ? cfl_dt_from_speed(smax, dx, hp.courant_factor) : 1.0e300;
     partial[blockIdx.x * 4 + 1] = mass;
     partial[blockIdx.x * 4 + 2] = etot;
     partial[blockIdx.x * 4 + 3] = eint;

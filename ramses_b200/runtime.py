@@ -203,8 +203,11 @@ class Solver:
         assert u.shape == (5, self.tree.ncell)
         _check(load().rb_upload_state(self._h, _ptr(u, _PD)), "rb_upload_state")
 
-    def download_state(self) -> np.ndarray:
-        u = np.empty((5, self.tree.ncell))
+    def download_state(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Fortran-layout uold (5, ncell); ``out`` (e.g. pinned memory) is
+        filled in place when given."""
+        u = np.empty((5, self.tree.ncell)) if out is None else out
+        assert u.shape == (5, self.tree.ncell) and u.dtype == np.float64 and u.flags.c_contiguous
         _check(load().rb_download_state(self._h, _ptr(u, _PD)), "rb_download_state")
         return u
 
