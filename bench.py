@@ -44,8 +44,8 @@ BYTES_PER_CELL_UPDATE = 80  # read uold (5 x 8 B) + write unew (5 x 8 B) per lea
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--level", type=int, default=8)
     ap.add_argument("--seed", type=int, default=2024)
@@ -55,8 +55,18 @@ def parse():
     ap.add_argument("--only", choices=["mixed", "fp64"], default=None,
                     help="run only one precision's timed steps (for profiling)")
     ap.add_argument("--tile-shape", type=int, default=-1,
-                    help="force a godunov tile shape (default: autotuned on the workload)")
+                    help="oct-tile method: force a godunov tile shape (default: autotuned on the workload)")
+    ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
+                    help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
+
+
+def make_solver(runtime, tree, hp, precision, u, args):
+    s = runtime.Solver(tree, hp, precision=precision, uold=u)
+    s.set_uniform_method(args.method)
+    if args.method == "tiles":
+        s.set_tile_shape(tree.nlevelmax, args.tile_shape)
+    return s
 
 
 def workload(level, seed):
@@ -92,7 +102,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -148,10 +158,12 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the mixed tile kernel from the committed ncu
-    summary (line 'traffic_bytes_per_launch: N'), scaled to this workload."""
-    f = ROOT / "profiles" / "godunov_tile_mixed_turb256.md"
+def ncu_traffic(method):
+    """DRAM bytes per launch of the dominant FP32-mixed kernel on this
+    workload, from the committed ncu summary (line
+    'traffic_bytes_per_launch: N')."""
+    name = "stream_step_mixed_turb256.md" if method == "stream" else "godunov_tile_mixed_turb256.md"
+    f = ROOT / "profiles" / name
     if not f.exists():
         return None
     for ln in f.read_text().splitlines():
@@ -247,37 +259,35 @@ def main():
 
     if args.only:
         # one precision's timed steps only (profiling runs: one solver resident)
-        s = runtime.Solver(tree, hp, precision=args.only, uold=u)
-        s.set_tile_shape(level, args.tile_shape)
+        s = make_solver(runtime, tree, hp, args.only, u, args)
         s.uniform_run(args.warmup, graph=False)
         s.uniform_run(args.steps, graph=False)
         print(json.dumps({"only": args.only, "cells": cells, "ms_per_step": s.last_run_ms() / args.steps,
-                          "kernel_ms": s.last_kernel_ms(), "tile_shape": s.tile_shape(level),
+                          "kernel_ms": s.last_kernel_ms(), "kernel": s.uniform_info()["kernel"],
                           "value": cells * args.steps / (s.last_run_ms() / 1e3)}), flush=True)
         s.close()
         return
 
     # ---- FP32-mixed, device resident (headline) -------------------------
-    mixed = runtime.Solver(tree, hp, precision="mixed", uold=u)
-    mixed.set_tile_shape(level, args.tile_shape)
+    mixed = make_solver(runtime, tree, hp, "mixed", u, args)
     mixed.uniform_run(args.warmup, graph=False)
     barrier()
     mixed.synchronize()
     with ClockSampler(local) as clk:
+        time.sleep(0.3)  # let the sampler start before the timed region
         mixed.uniform_run(args.steps, graph=False)
         mixed.synchronize()
     barrier()
     run_ms = max_over_ranks(mixed.last_run_ms())
     kern_ms = mixed.last_kernel_ms()
-    mixed_shape = mixed.tile_shape(level)
+    mixed_kernel = mixed.uniform_info()["kernel"]
     value = cells * args.steps * world / (run_ms / 1e3)
     u_mixed = mixed.download_state()
 
     # ---- FP64 drop-in path on the same steps ----------------------------
-    f64 = runtime.Solver(tree, hp, precision="fp64", uold=u)
-    f64.set_tile_shape(level, args.tile_shape)
-    f64_shape = f64.tile_shape(level)
+    f64 = make_solver(runtime, tree, hp, "fp64", u, args)
     f64.uniform_run(args.warmup, graph=False)
+    f64_kernel = f64.uniform_info()["kernel"]
     barrier()
     f64.uniform_run(args.steps, graph=False)
     barrier()
@@ -320,7 +330,7 @@ def main():
 
     peak, peak_kind = hbm_peak()
     achieved = BYTES_PER_CELL_UPDATE * cells / (kern_ms / 1e3) / 1e9
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(args.method)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nocts = min(args.cpu_sample_octs, tree.noct(level))
@@ -338,15 +348,14 @@ def main():
                     "path": "rb_upload_state + rb_uniform_run(1) + rb_download_state, pinned host buffers"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "godunov_tile_kernel<float> tile shape %d %s (fused update + CFL partials)"
-                                   % (mixed_shape, tile_dims(mixed_shape)),
+                         "kernel": mixed_kernel + " (fused godunov + update + CFL partials)",
                          "bytes_per_cell_update": BYTES_PER_CELL_UPDATE, "kernel_ms": kern_ms,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": 2 * args.steps,
             "fp64": {"value": f64_value, "ms_per_step": f64_ms / args.steps, "kernel_ms": f64_kern,
-                     "tile_shape": "%d %s" % (f64_shape, tile_dims(f64_shape)),
+                     "kernel": f64_kernel,
                      "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak},
             "mixed_over_fp64": value / f64_value,
             "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,

@@ -109,6 +109,15 @@ int rb_unsplit(const rb_hydro_params *hp, const double *uin, const double *gravi
  * as newdt_fine/courant_fine give it. t_io advanced; dt_last_out may be NULL. */
 int rb_uniform_run(rb_context *ctx, int nsteps, int use_graph, double *t_io, double *dt_last_out);
 
+/* Kernel used by rb_uniform_run: 0 = z-streaming stencil over a dense
+ * Cartesian mirror of the level (default), 1 = the godunov_fine oct tiles.
+ * Both give identical results. */
+int rb_set_uniform_method(rb_context *ctx, int method);
+/* Kernel configuration of the last rb_uniform_run: method, shape (z-streaming
+ * column shape 0: 8x8, 1: 16x8, 2: 16x16 cells, or oct-tile shape), z extent
+ * of a work item and number of work items (CTAs) per step. */
+int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *items);
+
 /* Wait for all work queued on the context's stream. */
 int rb_synchronize(rb_context *ctx);
 /* The context's CUDA stream (cudaStream_t) for callers that order their own work. */

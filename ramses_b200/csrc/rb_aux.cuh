@@ -348,4 +348,33 @@ __global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double* __res
   }
 }
 
+// Oct layout <-> dense Cartesian array of one complete level.
+// cbase[i]: dense index of child 0 of the level's i-th active oct.
+__global__ void oct_to_dense_kernel(const double* __restrict__ u, double* __restrict__ d,
+                                    const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
+                                    int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
+                                    int64_t vstr) {
+  const int64_t n = (int64_t)noct * 8 * 5;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+    const int64_t o = r >> 3;
+    const int ch = (int)(r & 7);
+    const int64_t di = cbase[o] + (ch & 1) + (int64_t)nx * (((ch >> 1) & 1) + (int64_t)ny * (ch >> 2));
+    d[v * vstr + di] = u[v * ncell + oct0 + (int64_t)active[o] * 8 + ch];
+  }
+}
+__global__ void dense_to_oct_kernel(const double* __restrict__ d, double* __restrict__ u,
+                                    const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
+                                    int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
+                                    int64_t vstr) {
+  const int64_t n = (int64_t)noct * 8 * 5;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+    const int64_t o = r >> 3;
+    const int ch = (int)(r & 7);
+    const int64_t di = cbase[o] + (ch & 1) + (int64_t)nx * (((ch >> 1) & 1) + (int64_t)ny * (ch >> 2));
+    u[v * ncell + oct0 + (int64_t)active[o] * 8 + ch] = d[v * vstr + di];
+  }
+}
+
 }  // namespace rb

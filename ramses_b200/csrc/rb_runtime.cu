@@ -22,6 +22,7 @@
 #include "../../include/ramses_b200.h"
 #include "godunov_tile.cuh"
 #include "rb_aux.cuh"
+#include "stream_kernel.cuh"
 #include "tile_launch.h"
 
 namespace {
@@ -156,6 +157,15 @@ struct rb_context {
   cudaGraphExec_t graph = nullptr;  // cached uniform-run graph
   int graph_steps = 0;
   double* graph_cur = nullptr;
+  // dense Cartesian mirror of the finest (complete) level for the z-streaming path
+  int uniform_method = 0;           // 0: z-streaming over the dense mirror, 1: oct tiles
+  double* d_dense[2] = {nullptr, nullptr};
+  int dense_cur = 0;
+  int64_t* d_cbase = nullptr;
+  int32_t dnx = 0, dny = 0, dnz = 0;
+  bool dense_valid = false;         // the dense mirror holds the newest state of `finest`
+  bool oct_stale = false;           // the oct layout of `finest` lags the dense mirror
+  int stream_shape = -1, stream_hz = 0, stream_items = 0;
   // scheduler state (amr_commons dtnew/dtold, t, nstep)
   double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
   double t = 0.0;
@@ -233,8 +243,18 @@ void drop_graph(rb_context* c) {
   c->graph_cur = nullptr;
 }
 
+void free_dense(rb_context* c) {
+  dfree(c->d_dense[0]);
+  dfree(c->d_dense[1]);
+  dfree(c->d_cbase);
+  c->dense_valid = false;
+  c->oct_stale = false;
+  c->stream_shape = -1;
+}
+
 void free_tree(rb_context* c) {
   drop_graph(c);
+  free_dense(c);
   for (int l = 0; l <= RB_MAXLEVEL + 1; l++) {
     free_level_tables(c->lv[l]);
     dfree(c->lv[l].d_active);
@@ -567,6 +587,65 @@ int upload_fine_impl(rb_context* c, int l) {
   return RB_OK;
 }
 
+// Write the dense mirror of the finest level back into the oct layout and
+// restrict it to the coarser levels (amr_step.f90:442, adaptive_loop.f90),
+// when the dense mirror is ahead.
+int sync_oct(rb_context* c) {
+  if (!c->oct_stale) return RB_OK;
+  Level& L = c->lv[c->finest];
+  const int64_t vstr = (int64_t)c->dnx * c->dny * c->dnz;
+  rb::dense_to_oct_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+      c->d_dense[c->dense_cur], c->d_uold, L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
+      c->dny, vstr);
+  RB_CUDA(cudaGetLastError());
+  for (int l = c->finest - 1; l >= 1; l--) RB_TRY(upload_fine_impl(c, l));
+  c->oct_stale = false;
+  return RB_OK;
+}
+
+// Any change of the oct-layout state makes the dense mirror stale.
+inline void oct_changed(rb_context* c) {
+  c->dense_valid = false;
+  c->clock_valid = false;
+}
+
+// Allocate the dense mirror of the finest level (complete by construction of
+// the callers) and the per-oct dense base offsets; pick the column shape.
+int dense_prepare(rb_context* c) {
+  const int lf = c->finest;
+  Level& L = c->lv[lf];
+  const int32_t nx = c->mp.nx << lf, ny = c->mp.ny << lf, nz = c->mp.nz << lf;
+  if (c->d_dense[0] && c->dnx == nx && c->dny == ny && c->dnz == nz) return RB_OK;
+  free_dense(c);
+  c->dnx = nx; c->dny = ny; c->dnz = nz;
+  const int64_t ncells = (int64_t)nx * ny * nz;
+  RB_TRY(dalloc(&c->d_dense[0], (size_t)ncells * 5));
+  RB_TRY(dalloc(&c->d_dense[1], (size_t)ncells * 5));
+  std::vector<int64_t> cb(L.noct);
+  for (int i = 0; i < L.noct; i++) {
+    const int64_t* x = &c->coords[(size_t)(L.h_active[i] - 1) * 3];
+    cb[i] = 2 * x[0] + (int64_t)nx * (2 * x[1] + (int64_t)ny * 2 * x[2]);
+  }
+  RB_TRY(dalloc(&c->d_cbase, cb.size()));
+  RB_CUDA(cudaMemcpy(c->d_cbase, cb.data(), cb.size() * 8, cudaMemcpyHostToDevice));
+  // column shape: the largest that divides the grid; z extent: items >= 4 per SM
+  int shape = -1;
+  for (int s = rb::kNumStreamShapes - 1; s >= 0; s--)
+    if (nx % rb::kStreamShapes[s][0] == 0 && ny % rb::kStreamShapes[s][1] == 0 &&
+        nx >= rb::kStreamShapes[s][0] && ny >= rb::kStreamShapes[s][1]) { shape = s; break; }
+  c->stream_shape = shape;
+  if (shape >= 0) {
+    const int64_t cols = (int64_t)(nx / rb::kStreamShapes[shape][0]) * (ny / rb::kStreamShapes[shape][1]);
+    int hz = 64;
+    while (hz > 2 && (nz % hz != 0 || cols * (nz / hz) < 4 * 148)) hz >>= 1;
+    if (nz % hz != 0) hz = 2;
+    c->stream_hz = hz;
+    c->stream_items = (int)(cols * (nz / hz));
+  }
+  c->dense_valid = false;
+  return RB_OK;
+}
+
 rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
   rb::TileArgs a;
   memset(&a, 0, sizeof a);
@@ -811,19 +890,39 @@ static int download_impl(rb_context* c, const double* d, double* h) {
 int rb_upload_state(rb_context* c, const double* uold) {
   RB_TRY(upload_impl(c, uold, c ? c->d_uold : nullptr));
   c->have_state = true;
-  c->clock_valid = false;
+  c->oct_stale = false;  // overwritten entirely
+  oct_changed(c);
   return RB_OK;
 }
-int rb_download_state(rb_context* c, double* uold) { return download_impl(c, c ? c->d_uold : nullptr, uold); }
+int rb_download_state(rb_context* c, double* uold) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  RB_TRY(sync_oct(c));
+  return download_impl(c, c->d_uold, uold);
+}
 int rb_upload_unew(rb_context* c, const double* unew) { return upload_impl(c, unew, c ? c->d_unew : nullptr); }
 int rb_download_unew(rb_context* c, double* unew) { return download_impl(c, c ? c->d_unew : nullptr, unew); }
 
-int rb_set_unew(rb_context* c, int l) { RB_TRY(check_level(c, l)); return set_unew_impl(c, l); }
-int rb_set_uold(rb_context* c, int l) { RB_TRY(check_level(c, l)); return set_uold_impl(c, l); }
-int rb_upload_fine(rb_context* c, int l) { RB_TRY(check_level(c, l)); return upload_fine_impl(c, l); }
+int rb_set_unew(rb_context* c, int l) {
+  RB_TRY(check_level(c, l));
+  RB_TRY(sync_oct(c));
+  return set_unew_impl(c, l);
+}
+int rb_set_uold(rb_context* c, int l) {
+  RB_TRY(check_level(c, l));
+  RB_TRY(sync_oct(c));
+  oct_changed(c);
+  return set_uold_impl(c, l);
+}
+int rb_upload_fine(rb_context* c, int l) {
+  RB_TRY(check_level(c, l));
+  RB_TRY(sync_oct(c));
+  oct_changed(c);
+  return upload_fine_impl(c, l);
+}
 
 int rb_godunov_fine(rb_context* c, int l, double dt) {
   RB_TRY(check_level(c, l));
+  RB_TRY(sync_oct(c));
   RB_TRY(godunov_impl(c, l, dt, true));
   RB_CUDA(cudaStreamSynchronize(c->stream));
   RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
@@ -834,12 +933,15 @@ int rb_godunov_fine(rb_context* c, int l, double dt) {
 int rb_courant_fine(rb_context* c, int l, double* dt_io, double* mass, double* ekin, double* eint) {
   RB_TRY(check_level(c, l));
   if (!dt_io) return fail(RB_ERR_INVALID, "null dt");
+  RB_TRY(sync_oct(c));
   return courant_impl(c, l, dt_io, mass, ekin, eint);
 }
 
 int rb_coarse_step(rb_context* c, double* t_io, double* dtnew_out) {
   if (!c) return fail(RB_ERR_INVALID, "null context");
   if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  RB_TRY(sync_oct(c));
+  oct_changed(c);
   if (t_io) c->t = *t_io;
   c->mass_tot = c->ekin_tot = c->eint_tot = 0.0;
   RB_TRY(amr_step_impl(c, c->mp.levelmin, 1));
@@ -941,6 +1043,7 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
   Level& L = c->lv[l];
   if (shape >= rb::kNumTileShapes) return fail(RB_ERR_INVALID, "tile shape %d out of range", shape);
   drop_graph(c);
+  RB_TRY(sync_oct(c));
   if (shape >= 0 || L.noct == 0) {
     L.shape = shape >= 0 ? shape : L.shape;
     return build_level_tables(c, l, c->idx);
@@ -986,10 +1089,9 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
 // coarser level fully refined (no leaf cell). Per step: the fused tile kernel
 // (unew = uold + fluxes, CFL partials of the new state) and the device clock
 // update; the two state buffers alternate; optionally captured as one graph.
-int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, double* dt_last_out) {
-  if (!c) return fail(RB_ERR_INVALID, "null context");
-  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
-  if (nsteps < 0) return fail(RB_ERR_INVALID, "nsteps must be >= 0");
+static int uniform_run_tiles(rb_context* c, int nsteps, int use_graph, double* t_io, double* dt_last_out) {
+  RB_TRY(sync_oct(c));
+  c->dense_valid = false;
   const int lf = c->finest;
   Level& L = c->lv[lf];
   if (lf < 1 || !L.complete || L.leaf_cells != (int64_t)L.noct * 8)
@@ -1108,6 +1210,159 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
   c->eint_tot = c->h_red[4];
   if (t_io) *t_io = c->t;
   if (dt_last_out) *dt_last_out = c->h_red[0];
+  return RB_OK;
+}
+
+// z-streaming stepper over the dense mirror of the finest level.
+static int uniform_run_dense(rb_context* c, int nsteps, int use_graph, double* t_io, double* dt_last_out) {
+  const int lf = c->finest;
+  Level& L = c->lv[lf];
+  RB_TRY(dense_prepare(c));
+  if (c->stream_shape < 0) return uniform_run_tiles(c, nsteps, use_graph, t_io, dt_last_out);
+  const double dt_max = c->mp.boxlen / c->hp.smallc;
+  const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
+  const int64_t vstr = (int64_t)c->dnx * c->dny * c->dnz;
+  if (t_io) c->t = *t_io;
+  if (!c->dense_valid) {
+    RB_TRY(sync_oct(c));
+    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+        c->d_uold, c->d_dense[c->dense_cur], L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
+        c->dny, vstr);
+    RB_CUDA(cudaGetLastError());
+    c->dense_valid = true;
+    drop_graph(c);
+  }
+  RB_TRY(ensure_partial(c, std::max<int64_t>(c->stream_items, grid_for((int64_t)L.noct * 8, 256, 148 * 8))));
+  if (!c->clock_valid) {
+    const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
+    rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+    RB_CUDA(cudaGetLastError());
+    rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, dt_max, dt0, 1, c->d_red, 0);
+    RB_CUDA(cudaGetLastError());
+    c->h_red[0] = c->t;
+    RB_CUDA(cudaMemcpyAsync(c->d_clock, c->d_red, sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    RB_CUDA(cudaMemcpyAsync(c->d_clock + 1, c->h_red, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+    c->clock_valid = true;
+  } else if (t_io) {
+    c->h_red[0] = c->t;
+    RB_CUDA(cudaMemcpyAsync(c->d_clock + 1, c->h_red, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  rb::StreamArgs sa;
+  memset(&sa, 0, sizeof sa);
+  sa.partial = c->d_partial;
+  sa.dt_dev = c->d_clock;
+  sa.nx = c->dnx; sa.ny = c->dny; sa.nz = c->dnz;
+  sa.hz = c->stream_hz;
+  int e2;
+  sa.dx_pow2 = std::frexp(L.dx, &e2) == 0.5;
+  sa.dx = L.dx;
+  sa.inv_dx = 1.0 / L.dx;
+  sa.hp = c->hp;
+  auto step = [&](int s_idx, bool timed) -> int {
+    sa.uin = c->d_dense[(c->dense_cur + s_idx) & 1];
+    sa.uout = c->d_dense[(c->dense_cur + s_idx + 1) & 1];
+    if (timed) RB_CUDA(cudaEventRecord(c->evpool[2 * s_idx], c->stream));
+    cudaError_t e = c->precision == RB_PREC_MIXED
+                        ? rb::launch_stream_mixed(c->stream_shape, sa, c->stream_items, c->stream)
+                        : rb::launch_stream_f64(c->stream_shape, sa, c->stream_items, c->stream);
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, "stream kernel launch failed: %s", cudaGetErrorString(e));
+    if (timed) RB_CUDA(cudaEventRecord(c->evpool[2 * s_idx + 1], c->stream));
+    rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, c->stream_items, dt_max, dt0, 1,
+                                                              c->d_clock, 1);
+    RB_CUDA(cudaGetLastError());
+    return RB_OK;
+  };
+  if (nsteps > 0) {
+    if (use_graph) {
+      if (!(c->graph && c->graph_steps == nsteps && c->graph_cur == c->d_dense[c->dense_cur])) {
+        drop_graph(c);
+        cudaGraph_t g;
+        RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = RB_OK;
+        for (int s = 0; s < nsteps && rc == RB_OK; s++) rc = step(s, false);
+        cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        if (rc) return rc;
+        if (ce != cudaSuccess) return fail(RB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { c->graph = nullptr; return fail(RB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce)); }
+        c->graph_steps = nsteps;
+        c->graph_cur = c->d_dense[c->dense_cur];
+      }
+      RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+      RB_CUDA(cudaGraphLaunch(c->graph, c->stream));
+      RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+    } else {
+      const int ntimed = std::min(nsteps, 4096);
+      while ((int)c->evpool.size() < 2 * ntimed) {
+        cudaEvent_t e;
+        RB_CUDA(cudaEventCreate(&e));
+        c->evpool.push_back(e);
+      }
+      RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+      for (int s = 0; s < nsteps; s++) RB_TRY(step(s, s < ntimed));
+      RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+      RB_CUDA(cudaEventSynchronize(c->ev1));
+      double tot = 0.0;
+      for (int s = 0; s < ntimed; s++) {
+        float ms = 0.f;
+        RB_CUDA(cudaEventElapsedTime(&ms, c->evpool[2 * s], c->evpool[2 * s + 1]));
+        tot += ms;
+      }
+      c->kernel_ms_avg = ntimed ? (float)(tot / ntimed) : 0.f;
+    }
+    c->dense_cur = (c->dense_cur + nsteps) & 1;
+    c->oct_stale = true;
+  }
+  RB_CUDA(cudaMemcpyAsync(c->h_red, c->d_clock, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  if (nsteps > 0) RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));
+  c->t = c->h_red[1];
+  c->nstep += nsteps;
+  c->cell_updates += (int64_t)nsteps * L.leaf_cells;
+  c->dtnew[lf] = c->h_red[0];
+  c->mass_tot = c->h_red[2];
+  c->ekin_tot = c->h_red[3];
+  c->eint_tot = c->h_red[4];
+  if (t_io) *t_io = c->t;
+  if (dt_last_out) *dt_last_out = c->h_red[0];
+  return RB_OK;
+}
+
+int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, double* dt_last_out) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  if (nsteps < 0) return fail(RB_ERR_INVALID, "nsteps must be >= 0");
+  const int lf = c->finest;
+  Level& L = c->lv[lf];
+  if (lf < 1 || !L.complete || L.leaf_cells != (int64_t)L.noct * 8)
+    return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
+  for (int l = 1; l < lf; l++)
+    if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
+  if (c->uniform_method == 0) return uniform_run_dense(c, nsteps, use_graph, t_io, dt_last_out);
+  return uniform_run_tiles(c, nsteps, use_graph, t_io, dt_last_out);
+}
+
+int rb_get_uniform_info(rb_context* c, int* method, int* shape, int* hz, int* items) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (method) *method = c->uniform_method;
+  if (shape) *shape = c->uniform_method == 0 ? c->stream_shape : (c->finest ? c->lv[c->finest].shape : -1);
+  if (hz) *hz = c->stream_hz;
+  if (items) *items = c->uniform_method == 0 ? c->stream_items : (c->finest ? c->lv[c->finest].ntile : 0);
+  return RB_OK;
+}
+
+int rb_set_uniform_method(rb_context* c, int method) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (method != 0 && method != 1) return fail(RB_ERR_INVALID, "method must be 0 (z-streaming) or 1 (oct tiles)");
+  if (method != c->uniform_method) {
+    RB_TRY(sync_oct(c));
+    c->dense_valid = false;
+    drop_graph(c);
+  }
+  c->uniform_method = method;
   return RB_OK;
 }
 

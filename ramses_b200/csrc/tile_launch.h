@@ -30,4 +30,11 @@ size_t tile_smem_mixed(int shape);
 cudaError_t launch_tile_f64(int shape, const TileArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_tile_mixed(int shape, const TileArgs& a, int grid, cudaStream_t s);
 
+// z-streaming kernel of complete levels; column shapes (TX x TY cells)
+struct StreamArgs;
+constexpr int kNumStreamShapes = 3;
+constexpr int kStreamShapes[kNumStreamShapes][2] = {{8, 8}, {16, 8}, {16, 16}};
+cudaError_t launch_stream_f64(int shape, const StreamArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_stream_mixed(int shape, const StreamArgs& a, int grid, cudaStream_t s);
+
 }  // namespace rb

@@ -4,4 +4,5 @@
 #define RB_TILE_REAL float
 #define RB_TILE_LAUNCH launch_tile_mixed
 #define RB_TILE_SMEM tile_smem_mixed
+#define RB_STREAM_LAUNCH launch_stream_mixed
 #include "tile_instances.inc"

@@ -1,0 +1,60 @@
+!###########################################################
+! B200 replacement of hydro/godunov_fine.f90 for the PATCH mechanism:
+! godunov_fine, set_unew and set_uold run on the GPU through rb_b200.
+! Same call sites and semantics as the reference (pure hydro: no Poisson
+! source terms, no pressure_fix, no momentum feedback, one MPI rank).
+!###########################################################
+subroutine godunov_fine(ilevel)
+  use amr_commons
+  use hydro_commons
+  use rb_b200
+  implicit none
+  integer::ilevel
+  if(numbtot(1,ilevel)==0)return
+  if(static)return
+  call rb_b200_push
+  call rb_b200_check(rb_godunov_fine(rb_ctx, int(ilevel, c_int), real(dtnew(ilevel), c_double)), 'godunov_fine')
+end subroutine godunov_fine
+!###########################################################
+subroutine set_unew(ilevel)
+  use amr_commons
+  use hydro_commons
+  use rb_b200
+  implicit none
+  integer::ilevel
+  if(numbtot(1,ilevel)==0)return
+  call rb_b200_init
+  call rb_b200_check(rb_set_unew(rb_ctx, int(ilevel, c_int)), 'set_unew')
+end subroutine set_unew
+!###########################################################
+subroutine set_uold(ilevel)
+  use amr_commons
+  use hydro_commons
+  use rb_b200
+  implicit none
+  integer::ilevel
+  if(numbtot(1,ilevel)==0)return
+  if(poisson .or. pressure_fix .or. nener>0)then
+     write(*,*)'rb_b200: gravity and pdV source terms are not supported'
+     call clean_stop
+  end if
+  call rb_b200_check(rb_set_uold(rb_ctx, int(ilevel, c_int)), 'set_uold')
+  ! restriction to the coarser level on the device; the host's own
+  ! upload_fine, called next by amr_step, recomputes the same values
+  call rb_b200_check(rb_upload_fine(rb_ctx, int(ilevel, c_int)), 'upload_fine')
+  call rb_b200_pull
+end subroutine set_uold
+!###########################################################
+subroutine add_gravity_source_terms(ilevel)
+  implicit none
+  integer::ilevel
+  write(*,*)'rb_b200: add_gravity_source_terms is not supported', ilevel
+  call clean_stop
+end subroutine add_gravity_source_terms
+!###########################################################
+subroutine add_pdv_source_terms(ilevel)
+  implicit none
+  integer::ilevel
+  write(*,*)'rb_b200: add_pdv_source_terms is not supported', ilevel
+  call clean_stop
+end subroutine add_pdv_source_terms

@@ -1,0 +1,176 @@
+!###########################################################
+! rb_b200: ISO_C_BINDING layer between RAMSES's hydro call sites and the
+! B200 library (include/ramses_b200.h). The Fortran host keeps its arrays
+! (son, father, nbor, active, uold) and its &HYDRO_PARAMS namelist; this
+! module mirrors them on the GPU and converts the namelist strings to codes.
+!
+! Synchronisation protocol (correct whatever the host does between calls):
+!   rb_b200_push : host -> device (tree if it changed, then uold); called at
+!                  the start of courant_fine and godunov_fine;
+!   rb_b200_pull : device -> host uold; called at the end of set_uold.
+! unew lives on the device only between set_unew and set_uold.
+!###########################################################
+module rb_b200
+  use iso_c_binding
+  implicit none
+
+  type, bind(c) :: rb_hydro_params_t
+     real(c_double) :: gamma, smallr, smallc, courant_factor, slope_theta
+     integer(c_int32_t) :: riemann, slope_type, scheme, interpol_var, interpol_type, pressure_fix
+     real(c_double) :: difmag
+  end type rb_hydro_params_t
+
+  type, bind(c) :: rb_mesh_params_t
+     integer(c_int32_t) :: nx, ny, nz, ncoarse, ngridmax, nlevelmax, levelmin, nvector
+     real(c_double) :: boxlen
+     integer(c_int32_t) :: nsubcycle(0:32)
+  end type rb_mesh_params_t
+
+  type(c_ptr), save :: rb_ctx = c_null_ptr
+  integer(c_int64_t), save :: rb_tree_stamp = -1
+
+  interface
+     integer(c_int) function rb_create(hp, mp, precision, ctx) bind(c, name='rb_create')
+       import :: c_int, c_ptr, rb_hydro_params_t, rb_mesh_params_t
+       type(rb_hydro_params_t), intent(in) :: hp
+       type(rb_mesh_params_t), intent(in) :: mp
+       integer(c_int), value :: precision
+       type(c_ptr), intent(out) :: ctx
+     end function rb_create
+     integer(c_int) function rb_sync_tree(ctx, son, father, nbor, numbl, active) bind(c, name='rb_sync_tree')
+       import :: c_int, c_ptr, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), intent(in) :: son(*), father(*), nbor(*), numbl(*), active(*)
+     end function rb_sync_tree
+     integer(c_int) function rb_upload_state(ctx, uold) bind(c, name='rb_upload_state')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       real(c_double), intent(in) :: uold(*)
+     end function rb_upload_state
+     integer(c_int) function rb_download_state(ctx, uold) bind(c, name='rb_download_state')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       real(c_double), intent(inout) :: uold(*)
+     end function rb_download_state
+     integer(c_int) function rb_set_unew(ctx, ilevel) bind(c, name='rb_set_unew')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+     end function rb_set_unew
+     integer(c_int) function rb_set_uold(ctx, ilevel) bind(c, name='rb_set_uold')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+     end function rb_set_uold
+     integer(c_int) function rb_upload_fine(ctx, ilevel) bind(c, name='rb_upload_fine')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+     end function rb_upload_fine
+     integer(c_int) function rb_godunov_fine(ctx, ilevel, dt) bind(c, name='rb_godunov_fine')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+       real(c_double), value :: dt
+     end function rb_godunov_fine
+     integer(c_int) function rb_courant_fine(ctx, ilevel, dt, mass, ekin, eint) bind(c, name='rb_courant_fine')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+       real(c_double), intent(inout) :: dt
+       real(c_double), intent(out) :: mass, ekin, eint
+     end function rb_courant_fine
+     type(c_ptr) function rb_last_error() bind(c, name='rb_last_error')
+       import :: c_ptr
+     end function rb_last_error
+  end interface
+
+contains
+
+  subroutine rb_b200_check(rc, where)
+    integer(c_int), intent(in) :: rc
+    character(len=*), intent(in) :: where
+    character(kind=c_char), pointer :: msg(:)
+    integer :: n
+    if (rc == 0) return
+    call c_f_pointer(rb_last_error(), msg, [1024])
+    n = 0
+    do while (n < 1024)
+       if (msg(n+1) == c_null_char) exit
+       n = n + 1
+    end do
+    write(*,*) 'rb_b200: ', where, ' failed with status ', rc, ': ', msg(1:n)
+    call clean_stop
+  end subroutine rb_b200_check
+
+  subroutine rb_b200_init
+    use amr_commons
+    use hydro_commons
+    type(rb_hydro_params_t) :: hp
+    type(rb_mesh_params_t) :: mp
+    integer :: l
+    if (c_associated(rb_ctx)) return
+    hp%gamma = gamma; hp%smallr = smallr; hp%smallc = smallc
+    hp%courant_factor = courant_factor; hp%slope_theta = slope_theta
+    hp%slope_type = slope_type; hp%scheme = 0; hp%pressure_fix = 0
+    hp%interpol_var = interpol_var; hp%interpol_type = interpol_type; hp%difmag = difmag
+    if (scheme /= 'muscl') hp%scheme = 1
+    if (pressure_fix) hp%pressure_fix = 1
+    hp%riemann = 0
+    if (riemann == 'llf') hp%riemann = 1
+    if (riemann == 'hll') hp%riemann = 2
+    if (riemann == 'hllc') hp%riemann = 3
+    mp%nx = nx; mp%ny = ny; mp%nz = nz; mp%ncoarse = ncoarse; mp%ngridmax = ngridmax
+    mp%nlevelmax = nlevelmax; mp%levelmin = levelmin; mp%nvector = nvector
+    mp%boxlen = boxlen
+    mp%nsubcycle = 2
+    do l = 1, min(nlevelmax, 32)
+       mp%nsubcycle(l) = nsubcycle(l)
+    end do
+    call rb_b200_check(rb_create(hp, mp, 0_c_int, rb_ctx), 'rb_create')
+  end subroutine rb_b200_init
+
+  ! host -> device: the tree (when any level's oct count or the son array
+  ! changed) and the whole uold
+  subroutine rb_b200_push
+    use amr_commons
+    use hydro_commons
+    integer(c_int32_t), allocatable :: numbl(:), act(:)
+    integer(c_int64_t) :: stamp
+    integer :: l, i, n
+    call rb_b200_init
+    stamp = 0
+    do l = 1, nlevelmax
+       stamp = stamp * 31 + active(l)%ngrid
+    end do
+    do i = 1, ncoarse + twotondim * ngridmax, 97
+       stamp = stamp * 7 + son(i)
+    end do
+    if (stamp /= rb_tree_stamp) then
+       allocate(numbl(nlevelmax))
+       n = 0
+       do l = 1, nlevelmax
+          numbl(l) = active(l)%ngrid
+          n = n + active(l)%ngrid
+       end do
+       allocate(act(max(n, 1)))
+       n = 0
+       do l = 1, nlevelmax
+          do i = 1, active(l)%ngrid
+             n = n + 1
+             act(n) = active(l)%igrid(i)
+          end do
+       end do
+       call rb_b200_check(rb_sync_tree(rb_ctx, son, father, nbor, numbl, act), 'rb_sync_tree')
+       deallocate(numbl, act)
+       rb_tree_stamp = stamp
+    end if
+    call rb_b200_check(rb_upload_state(rb_ctx, uold), 'rb_upload_state')
+  end subroutine rb_b200_push
+
+  subroutine rb_b200_pull
+    use hydro_commons
+    call rb_b200_check(rb_download_state(rb_ctx, uold), 'rb_download_state')
+  end subroutine rb_b200_pull
+
+end module rb_b200

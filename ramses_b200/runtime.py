@@ -81,6 +81,8 @@ _PROTOS = {
                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int]),
     "rb_uniform_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _PD, _PD]),
     "rb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_set_uniform_method": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rb_get_uniform_info": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32]),
     "rb_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "rb_last_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "rb_last_run_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
@@ -262,6 +264,24 @@ class Solver:
         n = ctypes.c_int64()
         _check(load().rb_cell_updates(self._h, ctypes.byref(n)), "rb_cell_updates")
         return n.value
+
+    def set_uniform_method(self, method: str):
+        """'stream' (z-streaming over a dense mirror) or 'tiles' (oct tiles)."""
+        _check(load().rb_set_uniform_method(self._h, {"stream": 0, "tiles": 1}[method]), "rb_set_uniform_method")
+
+    def uniform_info(self) -> dict:
+        v = [ctypes.c_int32() for _ in range(4)]
+        _check(load().rb_get_uniform_info(self._h, *[ctypes.byref(x) for x in v]), "rb_get_uniform_info")
+        method, shape, hz, items = (x.value for x in v)
+        if method == 0:
+            dims = [(8, 8), (16, 8), (16, 16)][shape] if 0 <= shape < 3 else (0, 0)
+            kern = "stream_step_kernel<%s,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
+                "float" if self.precision == "mixed" else "double", dims[0], dims[1], hz, items)
+        else:
+            kern = "godunov_tile_kernel<%s> shape %d (%d tiles)" % (
+                "float" if self.precision == "mixed" else "double", shape, items)
+        return {"method": "stream" if method == 0 else "tiles", "shape": shape, "hz": hz, "items": items,
+                "kernel": kern}
 
     def set_tile_shape(self, ilevel: int, shape: int):
         _check(load().rb_set_tile_shape(self._h, ilevel, shape), "rb_set_tile_shape")
