@@ -56,6 +56,8 @@ def parse():
                     help="run only one precision's timed steps (for profiling)")
     ap.add_argument("--tile-shape", type=int, default=-1,
                     help="oct-tile method: force a godunov tile shape (default: autotuned on the workload)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="z-streaming method: keep the default configuration instead of autotuning")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
                     help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
@@ -66,6 +68,8 @@ def make_solver(runtime, tree, hp, precision, u, args):
     s.set_uniform_method(args.method)
     if args.method == "tiles":
         s.set_tile_shape(tree.nlevelmax, args.tile_shape)
+    elif not args.no_autotune:
+        s.autotune_uniform()
     return s
 
 

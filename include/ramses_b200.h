@@ -117,6 +117,11 @@ int rb_set_uniform_method(rb_context *ctx, int method);
  * column shape 0: 8x8, 1: 16x8, 2: 16x16 cells, or oct-tile shape), z extent
  * of a work item and number of work items (CTAs) per step. */
 int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *items);
+/* Autotune the z-streaming step on the live state: every column shape and
+ * register budget (0: 8x8, 1: 16x8, 2: 16x16, 3: 16x8 at 2 CTAs/SM, 4: 8x8 at
+ * 4 CTAs/SM) and z extent 4..64 is timed; the fastest is kept. The state,
+ * the time and the next dt are unchanged. Outputs may be NULL. */
+int rb_autotune_uniform(rb_context *ctx, int *shape, int *hz, float *ms);
 
 /* Wait for all work queued on the context's stream. */
 int rb_synchronize(rb_context *ctx);

@@ -55,7 +55,8 @@ __device__ __forceinline__ Prim<R> ctoprim_cell(const double u[5], const rb_hydr
   const double gamma = hp.gamma;
   const double smalle = hp.smallc * hp.smallc / gamma / (gamma - 1.0);
   double q1 = fmx(u[0], hp.smallr);
-  double oneoverrho = 1.0 / q1;
+  // FP64 path: IEEE division as the reference; FP32-mixed: IEEE reciprocal
+  double oneoverrho = sizeof(R) == 8 ? 1.0 / q1 : __drcp_rn(q1);
   double q2 = u[1] * oneoverrho;
   double q3 = u[2] * oneoverrho;
   double q4 = u[3] * oneoverrho;
@@ -433,7 +434,7 @@ __device__ __forceinline__ double cfl_speed(const double uu_in[5], const rb_hydr
 __device__ __forceinline__ double cfl_speed_fast(const double u[5], const rb_hydro_params& hp) {
   const double gamma = hp.gamma;
   const double rho = fmx(u[0], hp.smallr);
-  const double ir = 1.0 / rho;
+  const double ir = __drcp_rn(rho);
   const double v1 = u[1] * ir, v2 = u[2] * ir, v3 = u[3] * ir;
   double e = u[4] - 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
   e = fmx((gamma - 1.0) * e, rho * (hp.smallc * hp.smallc / gamma));

@@ -152,6 +152,7 @@ struct rb_context {
   Level lv[RB_MAXLEVEL + 2];
   std::vector<OctIndex> idx;        // per-level position -> igrid lookup
   int finest = 0;                   // finest level holding octs
+  std::vector<int32_t> h_corr_slot; // host copy of d_corr_slot
   std::vector<cudaEvent_t> evpool;  // per-step kernel timing events
   float kernel_ms_avg = 0.f;        // mean tile-kernel time of the last timed run
   cudaGraphExec_t graph = nullptr;  // cached uniform-run graph
@@ -175,6 +176,17 @@ struct rb_context {
 };
 
 namespace {
+
+// Host->device copy ordered on the context's stream. A plain cudaMemcpy from
+// pageable memory may return before its DMA has landed and runs on the legacy
+// default stream, which does not order with the context's non-blocking
+// stream; kernels on the context's stream could then read stale device data.
+int h2d(rb_context* c, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return RB_OK;
+  RB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));  // the caller may free src next
+  return RB_OK;
+}
 
 int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
   if (!hp || !mp) return fail(RB_ERR_INVALID, "null parameter struct");
@@ -399,10 +411,10 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   }
   L.ninterp = (int)interp_of.size();
   RB_TRY(dalloc(&L.d_tile_blk, blk.size()));
-  RB_CUDA(cudaMemcpy(L.d_tile_blk, blk.data(), blk.size() * 4, cudaMemcpyHostToDevice));
+  RB_TRY(h2d(c, L.d_tile_blk, blk.data(), blk.size() * 4));
   if (L.ninterp) {
     RB_TRY(dalloc(&L.d_interp7, interp7.size()));
-    RB_CUDA(cudaMemcpy(L.d_interp7, interp7.data(), interp7.size() * 4, cudaMemcpyHostToDevice));
+    RB_TRY(h2d(c, L.d_interp7, interp7.data(), interp7.size() * 4));
     RB_TRY(dalloc(&L.d_interp_buf, (size_t)L.ninterp * 8 * 5));
   }
   // --- fine-to-coarse corrections (godunov_fine.f90:798-908)
@@ -445,14 +457,14 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(dalloc(&L.d_tgt_off, off.size()));
     RB_TRY(dalloc(&L.d_contrib, contrib.size()));
     RB_TRY(dalloc(&L.d_corr_flux, (size_t)nslot * 120));
-    RB_CUDA(cudaMemcpy(L.d_tgt, tgt.data(), tgt.size() * 4, cudaMemcpyHostToDevice));
-    RB_CUDA(cudaMemcpy(L.d_tgt_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
-    RB_CUDA(cudaMemcpy(L.d_contrib, contrib.data(), contrib.size() * 4, cudaMemcpyHostToDevice));
-    // scatter slots into the global per-oct slot table
-    std::vector<int32_t> tmp(h_slot_upd);
-    for (size_t i = 0; i + 1 < tmp.size(); i += 2)
-      RB_CUDA(cudaMemcpy(c->d_corr_slot + tmp[i], &tmp[i + 1], 4, cudaMemcpyHostToDevice));
+    RB_TRY(h2d(c, L.d_tgt, tgt.data(), tgt.size() * 4));
+    RB_TRY(h2d(c, L.d_tgt_off, off.data(), off.size() * 4));
+    RB_TRY(h2d(c, L.d_contrib, contrib.data(), contrib.size() * 4));
   }
+  // this level's entries of the per-oct correction slot table
+  for (int32_t g : L.h_active) c->h_corr_slot[g - 1] = -1;
+  for (size_t i = 0; i + 1 < h_slot_upd.size(); i += 2) c->h_corr_slot[h_slot_upd[i]] = h_slot_upd[i + 1];
+  RB_TRY(h2d(c, c->d_corr_slot, c->h_corr_slot.data(), c->h_corr_slot.size() * 4));
   L.tables_built = true;
   return RB_OK;
 }
@@ -527,16 +539,16 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
       std::vector<int32_t> a0(n);
       for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
       RB_TRY(dalloc(&L.d_active, (size_t)n));
-      RB_CUDA(cudaMemcpy(L.d_active, a0.data(), (size_t)n * 4, cudaMemcpyHostToDevice));
+      RB_TRY(h2d(c, L.d_active, a0.data(), (size_t)n * 4));
     }
   }
   // son mirror (device layout) and the per-oct correction slot table
-  RB_CUDA(cudaMemcpy(c->d_stage, son, ncell * 4, cudaMemcpyHostToDevice));
+  RB_TRY(h2d(c, c->d_stage, son, ncell * 4));
   rb::permute_son_kernel<<<grid_for(ncell, 256), 256, 0, c->stream>>>((const int32_t*)c->d_stage, c->d_son, ncell,
                                                                       c->mp.ncoarse, ngm);
   RB_CUDA(cudaGetLastError());
   RB_CUDA(cudaStreamSynchronize(c->stream));
-  RB_CUDA(cudaMemset(c->d_corr_slot, 0xff, (size_t)ngm * 4));
+  c->h_corr_slot.assign((size_t)ngm, -1);
   for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(build_level_tables(c, l, idx));
   c->have_tree = true;
   c->clock_valid = false;
@@ -609,6 +621,22 @@ inline void oct_changed(rb_context* c) {
   c->clock_valid = false;
 }
 
+bool stream_shape_fits(const rb_context* c, int s) {
+  const int tx = rb::kStreamShapes[s][0], ty = rb::kStreamShapes[s][1];
+  return c->dnx % tx == 0 && c->dny % ty == 0 && c->dnx >= tx && c->dny >= ty;
+}
+int stream_items_of(const rb_context* c, int s, int hz) {
+  return (c->dnx / rb::kStreamShapes[s][0]) * (c->dny / rb::kStreamShapes[s][1]) * (c->dnz / hz);
+}
+// z extent of a work item: the longest power of two <= 64 dividing nz that
+// still gives >= 4 work items per SM
+int default_stream_hz(const rb_context* c, int s) {
+  int hz = 64;
+  while (hz > 2 && (c->dnz % hz != 0 || stream_items_of(c, s, hz) < 4 * 148)) hz >>= 1;
+  if (c->dnz % hz != 0) hz = 2;
+  return hz;
+}
+
 // Allocate the dense mirror of the finest level (complete by construction of
 // the callers) and the per-oct dense base offsets; pick the column shape.
 int dense_prepare(rb_context* c) {
@@ -627,20 +655,15 @@ int dense_prepare(rb_context* c) {
     cb[i] = 2 * x[0] + (int64_t)nx * (2 * x[1] + (int64_t)ny * 2 * x[2]);
   }
   RB_TRY(dalloc(&c->d_cbase, cb.size()));
-  RB_CUDA(cudaMemcpy(c->d_cbase, cb.data(), cb.size() * 8, cudaMemcpyHostToDevice));
-  // column shape: the largest that divides the grid; z extent: items >= 4 per SM
+  RB_TRY(h2d(c, c->d_cbase, cb.data(), cb.size() * 8));
+  // default column shape: the widest of 16x16, 16x8, 8x8 that divides the grid
   int shape = -1;
-  for (int s = rb::kNumStreamShapes - 1; s >= 0; s--)
-    if (nx % rb::kStreamShapes[s][0] == 0 && ny % rb::kStreamShapes[s][1] == 0 &&
-        nx >= rb::kStreamShapes[s][0] && ny >= rb::kStreamShapes[s][1]) { shape = s; break; }
+  for (int s : {2, 1, 0})
+    if (stream_shape_fits(c, s)) { shape = s; break; }
   c->stream_shape = shape;
   if (shape >= 0) {
-    const int64_t cols = (int64_t)(nx / rb::kStreamShapes[shape][0]) * (ny / rb::kStreamShapes[shape][1]);
-    int hz = 64;
-    while (hz > 2 && (nz % hz != 0 || cols * (nz / hz) < 4 * 148)) hz >>= 1;
-    if (nz % hz != 0) hz = 2;
-    c->stream_hz = hz;
-    c->stream_items = (int)(cols * (nz / hz));
+    c->stream_hz = default_stream_hz(c, shape);
+    c->stream_items = stream_items_of(c, shape, c->stream_hz);
   }
   c->dense_valid = false;
   return RB_OK;
@@ -833,9 +856,11 @@ int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision
     return bail(rc);
   if (cudaMallocHost((void**)&c->h_red, 8 * sizeof(double)) != cudaSuccess)
     return bail(fail(RB_ERR_NOMEM, "pinned allocation failed"));
-  cudaMemset(c->d_uold, 0, (size_t)c->ncell * 5 * sizeof(double));
-  cudaMemset(c->d_unew, 0, (size_t)c->ncell * 5 * sizeof(double));
-  cudaMemset(c->d_clock, 0, 8 * sizeof(double));
+  if (cudaMemsetAsync(c->d_uold, 0, (size_t)c->ncell * 5 * sizeof(double), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_unew, 0, (size_t)c->ncell * 5 * sizeof(double), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(c->d_clock, 0, 8 * sizeof(double), c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return bail(fail(RB_ERR_CUDA, "initialising device buffers failed"));
   // make sure the kernel image for this GPU is present
   cudaError_t e = rb::launch_tile_f64(0, rb::TileArgs{}, 0, c->stream);
   if (e != cudaSuccess) return bail(fail(RB_ERR_NO_DEVICE, "tile kernel unavailable on this device: %s", cudaGetErrorString(e)));
@@ -1328,6 +1353,93 @@ static int uniform_run_dense(rb_context* c, int nsteps, int use_graph, double* t
   c->eint_tot = c->h_red[4];
   if (t_io) *t_io = c->t;
   if (dt_last_out) *dt_last_out = c->h_red[0];
+  return RB_OK;
+}
+
+// Autotuner of the z-streaming step: times every column shape / register
+// budget (kStreamShapes) and z extent (4..64) on the live state, reading the
+// current dense buffer and writing the other one (the state, the clock and t
+// are left unchanged), and keeps the fastest.
+int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_out) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  const int lf = c->finest;
+  if (!c->have_tree || !c->have_state || lf < 1 || !c->lv[lf].complete)
+    return fail(RB_ERR_STATE, "autotuning needs a uniform grid with its state uploaded");
+  Level& L = c->lv[lf];
+  RB_TRY(dense_prepare(c));
+  if (c->stream_shape < 0) return fail(RB_ERR_STATE, "grid too small for the z-streaming kernel");
+  if (!c->dense_valid) {
+    RB_TRY(sync_oct(c));
+    const int64_t vstr = (int64_t)c->dnx * c->dny * c->dnz;
+    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+        c->d_uold, c->d_dense[c->dense_cur], L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
+        c->dny, vstr);
+    RB_CUDA(cudaGetLastError());
+    c->dense_valid = true;
+  }
+  // a representative dt in a scratch slot of the reduction buffer
+  double dt_probe = 0.0;
+  {
+    double d = c->mp.boxlen / c->hp.smallc;
+    const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
+    RB_TRY(ensure_partial(c, nblk));
+    rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+    RB_CUDA(cudaGetLastError());
+    rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, d, c->hp.courant_factor * L.dx / c->hp.smallc, 1, c->d_red + 4, 0);
+    RB_CUDA(cudaGetLastError());
+    RB_CUDA(cudaMemcpyAsync(c->h_red, c->d_red + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+    dt_probe = c->h_red[0];
+  }
+  (void)dt_probe;
+  int best_s = -1, best_hz = 0;
+  float best_ms = 1e30f;
+  for (int s = 0; s < rb::kNumStreamShapes; s++) {
+    if (!stream_shape_fits(c, s)) continue;
+    const size_t smem = c->precision == RB_PREC_MIXED ? rb::stream_smem_mixed(s) : rb::stream_smem_f64(s);
+    if (smem > 227 * 1024) continue;
+    for (int hz = 4; hz <= 64; hz *= 2) {
+      if (c->dnz % hz != 0) continue;
+      const int items = stream_items_of(c, s, hz);
+      if (items < 148 && hz != 4) continue;
+      RB_TRY(ensure_partial(c, items));
+      rb::StreamArgs sa;
+      memset(&sa, 0, sizeof sa);
+      sa.uin = c->d_dense[c->dense_cur];
+      sa.uout = c->d_dense[c->dense_cur ^ 1];
+      sa.partial = c->d_partial;
+      sa.dt_dev = c->d_red + 4;
+      sa.nx = c->dnx; sa.ny = c->dny; sa.nz = c->dnz;
+      sa.hz = hz;
+      int e2;
+      sa.dx_pow2 = std::frexp(L.dx, &e2) == 0.5;
+      sa.dx = L.dx;
+      sa.inv_dx = 1.0 / L.dx;
+      sa.hp = c->hp;
+      float ms = 1e30f;
+      for (int rep = 0; rep < 4; rep++) {
+        RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+        cudaError_t e = c->precision == RB_PREC_MIXED ? rb::launch_stream_mixed(s, sa, items, c->stream)
+                                                      : rb::launch_stream_f64(s, sa, items, c->stream);
+        if (e != cudaSuccess) return fail(RB_ERR_CUDA, "stream kernel launch failed: %s", cudaGetErrorString(e));
+        RB_CUDA(cudaEventRecord(c->ev1, c->stream));
+        RB_CUDA(cudaEventSynchronize(c->ev1));
+        float t = 0.f;
+        RB_CUDA(cudaEventElapsedTime(&t, c->ev0, c->ev1));
+        if (rep > 0) ms = std::min(ms, t);
+      }
+      if (ms < best_ms) { best_ms = ms; best_s = s; best_hz = hz; }
+    }
+  }
+  if (best_s < 0) return fail(RB_ERR_STATE, "no z-streaming configuration fits this grid");
+  c->stream_shape = best_s;
+  c->stream_hz = best_hz;
+  c->stream_items = stream_items_of(c, best_s, best_hz);
+  drop_graph(c);
+  if (shape_out) *shape_out = best_s;
+  if (hz_out) *hz_out = best_hz;
+  if (ms_out) *ms_out = best_ms;
   return RB_OK;
 }
 

@@ -1,18 +1,22 @@
 // stream_kernel.cuh -- godunov_fine + set_uold + courant_fine for one complete
 // (uniform) level held as a dense Cartesian array, as a z-streaming stencil.
 //
-// A CTA owns a TX x TY column of cells and a z range [z0, z0+HZ). One thread
+// A CTA owns a TX x TY column of cells and a z range [z0, z0+hz). One thread
 // owns one column (cx, cy) of the trace region (TX+2) x (TY+2) and marches in
-// z: the conservative state of the planes ahead is prefetched with 16-byte
-// cp.async into a 4-plane shared ring; the primitive state of planes k-1, k,
-// k+1 of its column lives in registers, so the z slopes, the z face states
+// z. The conservative state of the planes ahead is prefetched with 16-byte
+// cp.async into a 5-plane shared ring. The primitive state of planes k-1..k+2
+// of its own column lives in registers, so the z slopes, the z face states
 // and the z Riemann problems need no shared memory; the x and y neighbours
-// are exchanged through one plane of shared memory. Per trace plane k:
-//   1. ctoprim of plane k+1 (own column -> registers, every stencil column ->
-//      shared plane buffer), prefetch of plane k+3;
-//   2. slopes + MUSCL-Hancock trace of plane k; publish the x/y left states;
-//   3. Riemann: x face left of the column, y face below, z face k-1/2;
-//   4. unew(k-1) = ((uold + dFx) + dFy) + dFz, CFL speed of the new state.
+// read a 3-plane shared buffer of primitive planes. Per trace plane k
+// (two CTA barriers):
+//   A. ctoprim of plane k+2 (own column -> registers, every stencil column ->
+//      shared buffer);
+//   B. slopes + MUSCL-Hancock trace of plane k; publish the x/y left states;
+//      -- barrier --; prefetch plane k+4;
+//   C. Riemann: x face left of the column, y face below, z face k-1/2;
+//      publish Fx, Fy; wait for plane k+3; -- barrier --
+//   D. unew(k-1) = ((uold + dFx) + dFy) + dFz and the CFL wave speed of the
+//      new state; partial update of plane k.
 // Every face flux and cell update is the same function of the same stencil as
 // in godunov_fine/unsplit, so with R = double (no FMA contraction) the result
 // is bit-identical to the reference operation order.
@@ -26,7 +30,7 @@ namespace rb {
 struct StreamArgs {
   const double* __restrict__ uin;   // [5][Nz][Ny][Nx] state at t
   double* __restrict__ uout;        // [5][Nz][Ny][Nx] state at t+dt
-  double* __restrict__ partial;     // [nitems][4] (CFL dt, mass, E, eint)
+  double* __restrict__ partial;     // [nitems][4] (CFL dt, 0, 0, 0)
   const double* __restrict__ dt_dev;
   int32_t nx, ny, nz;               // cells per dimension (multiples of TX, TY, hz; even)
   int32_t hz;                       // z extent of one work item
@@ -51,27 +55,33 @@ struct StreamGeom {
   static constexpr int NT = (NC + 31) / 32 * 32;        // launched threads (whole warps)
   static constexpr int NS = SX * SY;
   static constexpr int NEXTRA = NS - NC;                // q-only outer ring columns
+  static constexpr int NRAW = 5;                        // raw planes in flight
+  static constexpr int NQ = 3;                          // primitive planes in shared memory
   static constexpr int CHUNKS = 5 * SY * (SX / 2);      // 16-byte chunks per raw plane
-  static constexpr size_t RAW_BYTES = sizeof(double) * 4 * 5 * NS;
-  static constexpr size_t Q_BYTES = sizeof(R) * 2 * 5 * NS;
+  static constexpr size_t RAW_BYTES = sizeof(double) * NRAW * 5 * NS;
+  static constexpr size_t Q_BYTES = sizeof(R) * NQ * 5 * NS;
   static constexpr size_t X_BYTES = sizeof(R) * 4 * 5 * NC;   // qm_x, qm_y, Fx, Fy
   static constexpr size_t SMEM = RAW_BYTES + Q_BYTES + X_BYTES;
   static_assert(NEXTRA <= NC, "one extra column per thread at most");
   static_assert(TX % 2 == 0 && TY % 2 == 0, "even tile");
 };
 
-template <typename R, int TX, int TY>
-__global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(StreamArgs a) {
+__device__ __forceinline__ int pmod(int a, int m) { return ((a % m) + m) % m; }
+
+// MINB: CTAs per SM the register allocation must allow (the register budget
+// knob of the autotuner).
+template <typename R, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_kernel(StreamArgs a) {
   using G = StreamGeom<R, TX, TY>;
   constexpr int SX = G::SX, SY = G::SY, CX = G::CX, NS = G::NS, NC = G::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* raw = reinterpret_cast<double*>(smem_raw);                      // [4][5][NS]
-  R* qb = reinterpret_cast<R*>(smem_raw + G::RAW_BYTES);                  // [2][5][NS]
-  R* xm = qb + 2 * 5 * NS;                                                // [5][NC] qm_x
+  double* raw = reinterpret_cast<double*>(smem_raw);                      // [NRAW][5][NS]
+  R* qb = reinterpret_cast<R*>(smem_raw + G::RAW_BYTES);                  // [NQ][5][NS]
+  R* xm = qb + G::NQ * 5 * NS;                                            // [5][NC] qm_x
   R* ym = xm + 5 * NC;                                                    // [5][NC] qm_y
   R* fxs = ym + 5 * NC;                                                   // [5][NC] Fx (left face)
   R* fys = fxs + 5 * NC;                                                  // [5][NC] Fy (lower face)
-  __shared__ double red[4][G::NT / 32];
+  __shared__ double red[G::NT / 32];
 
   const int tid = threadIdx.x;
   const bool valid = tid < NC;                       // padding threads own no column
@@ -80,7 +90,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(
   const int nxt = a.nx / TX, nyt = a.ny / TY;
   const int item = blockIdx.x;
   const int tx0 = (item % nxt) * TX, ty0 = ((item / nxt) % nyt) * TY, z0 = (item / (nxt * nyt)) * a.hz;
-  const int hz = a.hz;
+  const int zend = z0 + a.hz;                        // planes [z0, zend) are updated
   const int64_t plane = (int64_t)a.nx * a.ny;
   const int64_t vstr = plane * a.nz;
   const Consts<R> c = make_consts<R>(a.hp);
@@ -102,18 +112,17 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(
   const int s_ext = ex + SX * ey;
 
   auto issue_plane = [&](int zp) {
-    const int slot = zp & 3;
-    const int zg = ((zp % a.nz) + a.nz) % a.nz;
+    double* dst = raw + pmod(zp, G::NRAW) * 5 * NS;
+    const int zg = pmod(zp, a.nz);
     for (int ch = tid; ch < G::CHUNKS; ch += G::NT) {
       const int j = ch % (SX / 2), r = ch / (SX / 2), row = r % SY, v = r / SY;
-      const int xg = ((tx0 - 2 + 2 * j) % a.nx + a.nx) % a.nx;
-      const int yg = ((ty0 - 2 + row) % a.ny + a.ny) % a.ny;
-      const double* src = a.uin + v * vstr + zg * plane + (int64_t)yg * a.nx + xg;
-      cp_async16(raw + ((slot * 5 + v) * NS + row * SX + 2 * j), src);
+      const int xg = pmod(tx0 - 2 + 2 * j, a.nx);
+      const int yg = pmod(ty0 - 2 + row, a.ny);
+      cp_async16(dst + v * NS + row * SX + 2 * j, a.uin + v * vstr + zg * plane + (int64_t)yg * a.nx + xg);
     }
   };
   auto load_u = [&](int zp, int s, double u[5]) {
-    const double* p = raw + (zp & 3) * 5 * NS + s;
+    const double* p = raw + pmod(zp, G::NRAW) * 5 * NS + s;
 #pragma unroll
     for (int v = 0; v < 5; v++) u[v] = p[v * NS];
   };
@@ -122,70 +131,67 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(
     load_u(zp, s, u);
     return ctoprim_cell<R>(u, a.hp);
   };
-  auto put_q = [&](int buf, int s, const Prim<R>& q) {
-    R* p = qb + buf * 5 * NS + s;
+  auto put_q = [&](int zp, int s, const Prim<R>& q) {
+    R* p = qb + pmod(zp, G::NQ) * 5 * NS + s;
     p[0] = q.r; p[NS] = q.u; p[2 * NS] = q.v; p[3 * NS] = q.w; p[4 * NS] = q.p;
   };
 
-  // ---- prologue: raw planes z0-2 .. z0+1; q(z0-2) (own), q(z0-1) (all) ----
-  for (int zp = z0 - 2; zp <= z0 + 1; zp++) { issue_plane(zp); cp_async_commit(); }
-  Prim<R> qprev, qcur, qnext;
-  cp_async_wait<3>();
+  // ---- prologue: planes z0-2 .. z0+2 in flight; q(z0-2..z0) converted ----
+  for (int zp = z0 - 2; zp <= z0 + 2; zp++) { issue_plane(zp); cp_async_commit(); }
+  cp_async_wait<1>();
   __syncthreads();
-  qprev = to_q(z0 - 2, s_own);
-  cp_async_wait<2>();
+  Prim<R> q_m1 = to_q(z0 - 2, s_own);
+  Prim<R> q_0 = to_q(z0 - 1, s_own);
+  Prim<R> q_p1 = to_q(z0, s_own);
+  Prim<R> q_p2 = q_p1;
+  if (valid) { put_q(z0 - 1, s_own, q_0); put_q(z0, s_own, q_p1); }
+  if (has_extra) { put_q(z0 - 1, s_ext, to_q(z0 - 1, s_ext)); put_q(z0, s_ext, to_q(z0, s_ext)); }
+  cp_async_wait<0>();
   __syncthreads();
-  qcur = to_q(z0 - 1, s_own);
-  if (valid) put_q((z0 - 1) & 1, s_own, qcur);
-  if (has_extra) put_q((z0 - 1) & 1, s_ext, to_q(z0 - 1, s_ext));
 
   Prim<R> qmz_prev;                  // qm_z of the plane below (left state of face k-1/2)
   qmz_prev.r = qmz_prev.u = qmz_prev.v = qmz_prev.w = qmz_prev.p = (R)0;
   double upd[5] = {0, 0, 0, 0, 0};   // uold + dFx + dFy of the pending plane
   R fzb[5] = {0, 0, 0, 0, 0};        // flux through the pending plane's lower face
-  double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
-  const double vol = a.dx * a.dx * a.dx;
+  double smax = 0.0;
   const int64_t col = inner ? (int64_t)(ty0 + cy) * a.nx + (tx0 + cx) : 0;
 
-  for (int k = z0 - 1; k <= z0 + hz; k++) {
-    const bool upd_plane = (k >= z0) && (k < z0 + hz);   // x/y fluxes and partial update at k
-    // 0. raw plane k+1 has landed
-    cp_async_wait<1>();
-    __syncthreads();
-    // 1. ctoprim of plane k+1, prefetch plane k+3
-    qnext = to_q(k + 1, s_own);
-    if (valid) put_q((k + 1) & 1, s_own, qnext);
-    if (has_extra) put_q((k + 1) & 1, s_ext, to_q(k + 1, s_ext));
-    double uo[5] = {0, 0, 0, 0, 0};
-    if (upd_plane && inner) load_u(k, s_own, uo);
-    if (k + 3 <= z0 + hz + 1) issue_plane(k + 3);
-    cp_async_commit();
-    __syncthreads();
-    // 2. slopes and trace of plane k
-    const R* qk = qb + (k & 1) * 5 * NS;
+  for (int k = z0 - 1; k <= zend; k++) {
+    const bool upd_plane = (k >= z0) && (k < zend);  // x/y fluxes and partial update at k
+    // A. ctoprim of plane k+2
+    if (k + 2 <= zend + 1) {
+      q_p2 = to_q(k + 2, s_own);
+      if (valid) put_q(k + 2, s_own, q_p2);
+      if (has_extra) put_q(k + 2, s_ext, to_q(k + 2, s_ext));
+    }
+    // B. slopes and trace of plane k
+    const R* qk = qb + pmod(k, G::NQ) * 5 * NS;
     R dq[5][3];
     {
-      const R own[5] = {qcur.r, qcur.u, qcur.v, qcur.w, qcur.p};
-      const R zm[5] = {qprev.r, qprev.u, qprev.v, qprev.w, qprev.p};
-      const R zp[5] = {qnext.r, qnext.u, qnext.v, qnext.w, qnext.p};
+      const R own[5] = {q_0.r, q_0.u, q_0.v, q_0.w, q_0.p};
+      const R zm[5] = {q_m1.r, q_m1.u, q_m1.v, q_m1.w, q_m1.p};
+      const R zp[5] = {q_p1.r, q_p1.u, q_p1.v, q_p1.w, q_p1.p};
+      const int sxm = valid ? s_own - 1 : 0, sxp = valid ? s_own + 1 : 0;
+      const int sym = valid ? s_own - SX : 0, syp = valid ? s_own + SX : 0;
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const R* qv = qk + v * NS;
-        dq[v][0] = slope1<R>(qv[s_own - 1 + (valid ? 0 : 1)], own[v], qv[s_own + 1], a.hp.slope_type, c.slope_theta);
-        dq[v][1] = slope1<R>(qv[valid ? s_own - SX : 0], own[v], qv[valid ? s_own + SX : 0], a.hp.slope_type,
-                             c.slope_theta);
+        dq[v][0] = slope1<R>(qv[sxm], own[v], qv[sxp], a.hp.slope_type, c.slope_theta);
+        dq[v][1] = slope1<R>(qv[sym], own[v], qv[syp], a.hp.slope_type, c.slope_theta);
         dq[v][2] = slope1<R>(zm[v], own[v], zp[v], a.hp.slope_type, c.slope_theta);
       }
     }
     Prim<R> sp[3], sm[3];
-    trace_cell<R>(qcur, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
+    trace_cell<R>(q_0, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
     if (valid) {
       const int o = tid;
       xm[o] = sm[0].r; xm[NC + o] = sm[0].u; xm[2 * NC + o] = sm[0].v; xm[3 * NC + o] = sm[0].w; xm[4 * NC + o] = sm[0].p;
       ym[o] = sm[1].r; ym[NC + o] = sm[1].u; ym[2 * NC + o] = sm[1].v; ym[3 * NC + o] = sm[1].w; ym[4 * NC + o] = sm[1].p;
     }
     __syncthreads();
-    // 3. Riemann problems
+    if (k + 4 <= zend + 1) issue_plane(k + 4);
+    cp_async_commit();
+    // C. Riemann problems
     R fx[5] = {0, 0, 0, 0, 0}, fy[5] = {0, 0, 0, 0, 0}, fz[5] = {0, 0, 0, 0, 0};
     if (upd_plane && valid && cx >= 0 && cy >= 0 && cy < TY) {
       const int o = tid - 1;  // column (cx-1, cy)
@@ -237,24 +243,23 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(
 #pragma unroll
       for (int v = 0; v < 5; v++) fz[v] = scale(fz[v]);
     }
+    cp_async_wait<1>();  // plane k+3 (converted at the next A) has landed
     __syncthreads();
-    // 4. finish plane k-1, partial update of plane k
+    // D. finish plane k-1, partial update of plane k
     if (inner) {
       if (k - 1 >= z0) {
         double un[5];
-        const int64_t zo = (int64_t)(k - 1) * plane;   // k-1 in [z0, z0+hz) lies inside the box
+        const int64_t zo = (int64_t)(k - 1) * plane;  // k-1 in [z0, zend) lies inside the box
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           un[v] = upd[v] + ((double)fzb[v] - (double)fz[v]);
           a.uout[v * vstr + zo + col] = un[v];
         }
-        const double ir = 1.0 / fmx(un[0], a.hp.smallr);
-        mass = mass + un[0] * vol;
-        etot = etot + un[4] * vol;
-        eint = eint + (un[4] - 0.5 * (un[1] * un[1] + un[2] * un[2] + un[3] * un[3]) * ir) * vol;
         smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(un, a.hp) : cfl_speed_fast(un, a.hp));
       }
       if (upd_plane) {
+        double uo[5];
+        load_u(k, s_own, uo);
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
@@ -265,29 +270,23 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT) stream_step_kernel(
         }
       }
     }
-    qprev = qcur;
-    qcur = qnext;
+    q_m1 = q_0;
+    q_0 = q_p1;
+    q_p1 = q_p2;
   }
   cp_async_wait<0>();
 
-  // ---- CFL partial of this work item ----
+  // ---- CFL partial of this work item (max wave speed -> min dt) ----
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    smax = fmx(smax, __shfl_xor_sync(0xffffffffu, smax, o));
-    mass += __shfl_xor_sync(0xffffffffu, mass, o);
-    etot += __shfl_xor_sync(0xffffffffu, etot, o);
-    eint += __shfl_xor_sync(0xffffffffu, eint, o);
-  }
-  if ((tid & 31) == 0) { red[0][tid >> 5] = smax; red[1][tid >> 5] = mass; red[2][tid >> 5] = etot; red[3][tid >> 5] = eint; }
+  for (int o = 16; o > 0; o >>= 1) smax = fmx(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+  if ((tid & 31) == 0) red[tid >> 5] = smax;
   __syncthreads();
   if (tid == 0) {
-    for (int w = 1; w < G::NT / 32; w++) {
-      smax = fmx(smax, red[0][w]); mass += red[1][w]; etot += red[2][w]; eint += red[3][w];
-    }
+    for (int w = 1; w < G::NT / 32; w++) smax = fmx(smax, red[w]);
     a.partial[(int64_t)item * 4 + 0] = smax > 0.0 ? cfl_dt_from_speed(smax, a.dx, a.hp.courant_factor) : 1.0e300;
-    a.partial[(int64_t)item * 4 + 1] = mass;
-    a.partial[(int64_t)item * 4 + 2] = etot;
-    a.partial[(int64_t)item * 4 + 3] = eint;
+    a.partial[(int64_t)item * 4 + 1] = 0.0;
+    a.partial[(int64_t)item * 4 + 2] = 0.0;
+    a.partial[(int64_t)item * 4 + 3] = 0.0;
   }
 }
 

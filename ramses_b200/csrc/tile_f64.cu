@@ -5,4 +5,5 @@
 #define RB_TILE_LAUNCH launch_tile_f64
 #define RB_TILE_SMEM tile_smem_f64
 #define RB_STREAM_LAUNCH launch_stream_f64
+#define RB_STREAM_SMEM stream_smem_f64
 #include "tile_instances.inc"

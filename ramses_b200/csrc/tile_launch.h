@@ -30,11 +30,14 @@ size_t tile_smem_mixed(int shape);
 cudaError_t launch_tile_f64(int shape, const TileArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_tile_mixed(int shape, const TileArgs& a, int grid, cudaStream_t s);
 
-// z-streaming kernel of complete levels; column shapes (TX x TY cells)
+// z-streaming kernel of complete levels: column shape (TX x TY cells) and the
+// number of CTAs per SM the register allocation is bounded for
 struct StreamArgs;
-constexpr int kNumStreamShapes = 3;
-constexpr int kStreamShapes[kNumStreamShapes][2] = {{8, 8}, {16, 8}, {16, 16}};
+constexpr int kNumStreamShapes = 5;
+constexpr int kStreamShapes[kNumStreamShapes][3] = {{8, 8, 1}, {16, 8, 1}, {16, 16, 1}, {16, 8, 2}, {8, 8, 4}};
 cudaError_t launch_stream_f64(int shape, const StreamArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_stream_mixed(int shape, const StreamArgs& a, int grid, cudaStream_t s);
+size_t stream_smem_f64(int shape);
+size_t stream_smem_mixed(int shape);
 
 }  // namespace rb

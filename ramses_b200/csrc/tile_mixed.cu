@@ -5,4 +5,5 @@
 #define RB_TILE_LAUNCH launch_tile_mixed
 #define RB_TILE_SMEM tile_smem_mixed
 #define RB_STREAM_LAUNCH launch_stream_mixed
+#define RB_STREAM_SMEM stream_smem_mixed
 #include "tile_instances.inc"

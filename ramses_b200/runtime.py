@@ -83,6 +83,7 @@ _PROTOS = {
     "rb_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "rb_set_uniform_method": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_get_uniform_info": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32]),
+    "rb_autotune_uniform": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, ctypes.POINTER(ctypes.c_float)]),
     "rb_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "rb_last_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "rb_last_run_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
@@ -269,14 +270,21 @@ class Solver:
         """'stream' (z-streaming over a dense mirror) or 'tiles' (oct tiles)."""
         _check(load().rb_set_uniform_method(self._h, {"stream": 0, "tiles": 1}[method]), "rb_set_uniform_method")
 
+    def autotune_uniform(self) -> dict:
+        """Time every z-streaming configuration on the live state; keep the best."""
+        s, hz, ms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_float()
+        _check(load().rb_autotune_uniform(self._h, ctypes.byref(s), ctypes.byref(hz), ctypes.byref(ms)),
+               "rb_autotune_uniform")
+        return {"shape": s.value, "hz": hz.value, "ms": ms.value}
+
     def uniform_info(self) -> dict:
         v = [ctypes.c_int32() for _ in range(4)]
         _check(load().rb_get_uniform_info(self._h, *[ctypes.byref(x) for x in v]), "rb_get_uniform_info")
         method, shape, hz, items = (x.value for x in v)
         if method == 0:
-            dims = [(8, 8), (16, 8), (16, 16)][shape] if 0 <= shape < 3 else (0, 0)
-            kern = "stream_step_kernel<%s,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
-                "float" if self.precision == "mixed" else "double", dims[0], dims[1], hz, items)
+            dims = [(8, 8, 1), (16, 8, 1), (16, 16, 1), (16, 8, 2), (8, 8, 4)][shape] if 0 <= shape < 5 else (0, 0, 0)
+            kern = "stream_step_kernel<%s,%d,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
+                "float" if self.precision == "mixed" else "double", dims[0], dims[1], dims[2], hz, items)
         else:
             kern = "godunov_tile_kernel<%s> shape %d (%d tiles)" % (
                 "float" if self.precision == "mixed" else "double", shape, items)
