@@ -123,6 +123,25 @@ int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *
  * the time and the next dt are unchanged. Outputs may be NULL. */
 int rb_autotune_uniform(rb_context *ctx, int *shape, int *hz, float *ms);
 
+/* CFL reduction over plain device arrays that allocates nothing.
+ * No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc/cudaFree mid-run (those calls wait for the whole device to go
+ * idle), e.g. a host loop keeping several problems in flight on one stream or
+ * a host with its own fixed device-memory pool. Its scratch is a fixed
+ * 2 MiB device array inside the library, shared by all calls.
+ * d_u: device array of conservative variables, variable v of cell i at
+ * d_u[v*stride + i], i < ncell, all treated as leaf cells of cell size dx.
+ * d_out: 4 device doubles receiving (dt, mass, total energy, internal energy)
+ * with dt = min(dt_in, courant_factor*dx/smallc, min over cells of the cmpdt
+ * time step) as courant_fine gives it. Runs on `stream` (a cudaStream_t, NULL
+ * for the default stream) without synchronising.
+ * Limit: ncell <= RB_NOALLOC_MAX_CELLS, else RB_ERR_CAPACITY. Calls that
+ * overlap on the GPU race on the shared scratch. The first call on each device
+ * resolves the scratch address and should come before any stream capture. */
+#define RB_NOALLOC_MAX_CELLS 16777216LL
+int rb_courant_cells_noalloc(const rb_hydro_params *hp, const double *d_u, int64_t ncell, int64_t stride,
+                             double dx, double dt_in, double *d_out, void *stream);
+
 /* Wait for all work queued on the context's stream. */
 int rb_synchronize(rb_context *ctx);
 /* The context's CUDA stream (cudaStream_t) for callers that order their own work. */

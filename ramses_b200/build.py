@@ -25,6 +25,7 @@ UNITS = {
     "rb_runtime.cu": ["--fmad=false"],
     "tile_f64.cu": ["--fmad=false"],
     "tile_mixed.cu": ["-use_fast_math"],
+    "rb_noalloc.cu": ["--fmad=false"],
 }
 HEADERS = sorted(list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc"))
                  + [PKG.parent / "include" / "ramses_b200.h"])

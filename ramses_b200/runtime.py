@@ -87,6 +87,9 @@ _PROTOS = {
     "rb_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "rb_last_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "rb_last_run_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "rb_courant_cells_noalloc": (ctypes.c_int, [ctypes.POINTER(HydroParamsC), ctypes.c_void_p, ctypes.c_int64,
+                                                ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
 }
 
 
