@@ -111,18 +111,22 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
   const int s_own = valid ? (cx + 2) + SX * (cy + 2) : 0;
   const int s_ext = ex + SX * ey;
 
+  // every plane index used below is >= z0-2, so ring slots come from a
+  // non-negative offset and constant moduli; periodic wraps need one step
+  const int zbase = z0 - 2;
+  auto wrap = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
   auto issue_plane = [&](int zp) {
-    double* dst = raw + pmod(zp, G::NRAW) * 5 * NS;
-    const int zg = pmod(zp, a.nz);
+    double* dst = raw + ((zp - zbase) % G::NRAW) * 5 * NS;
+    const double* src = a.uin + (int64_t)wrap(zp, a.nz) * plane;
     for (int ch = tid; ch < G::CHUNKS; ch += G::NT) {
       const int j = ch % (SX / 2), r = ch / (SX / 2), row = r % SY, v = r / SY;
-      const int xg = pmod(tx0 - 2 + 2 * j, a.nx);
-      const int yg = pmod(ty0 - 2 + row, a.ny);
-      cp_async16(dst + v * NS + row * SX + 2 * j, a.uin + v * vstr + zg * plane + (int64_t)yg * a.nx + xg);
+      const int xg = wrap(tx0 - 2 + 2 * j, a.nx);
+      const int yg = wrap(ty0 - 2 + row, a.ny);
+      cp_async16(dst + v * NS + row * SX + 2 * j, src + v * vstr + (int64_t)yg * a.nx + xg);
     }
   };
   auto load_u = [&](int zp, int s, double u[5]) {
-    const double* p = raw + pmod(zp, G::NRAW) * 5 * NS + s;
+    const double* p = raw + ((zp - zbase) % G::NRAW) * 5 * NS + s;
 #pragma unroll
     for (int v = 0; v < 5; v++) u[v] = p[v * NS];
   };
@@ -132,7 +136,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
     return ctoprim_cell<R>(u, a.hp);
   };
   auto put_q = [&](int zp, int s, const Prim<R>& q) {
-    R* p = qb + pmod(zp, G::NQ) * 5 * NS + s;
+    R* p = qb + ((zp - zbase) % G::NQ) * 5 * NS + s;
     p[0] = q.r; p[NS] = q.u; p[2 * NS] = q.v; p[3 * NS] = q.w; p[4 * NS] = q.p;
   };
 
@@ -165,7 +169,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
       if (has_extra) put_q(k + 2, s_ext, to_q(k + 2, s_ext));
     }
     // B. slopes and trace of plane k
-    const R* qk = qb + pmod(k, G::NQ) * 5 * NS;
+    const R* qk = qb + ((k - zbase) % G::NQ) * 5 * NS;
     R dq[5][3];
     {
       const R own[5] = {q_0.r, q_0.u, q_0.v, q_0.w, q_0.p};
@@ -252,7 +256,9 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
         const int64_t zo = (int64_t)(k - 1) * plane;  // k-1 in [z0, zend) lies inside the box
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          un[v] = upd[v] + ((double)fzb[v] - (double)fz[v]);
+          // FP64 path: difference of the FP64 fluxes (reference order); FP32-mixed:
+          // the FP32 flux difference, accumulated in FP64
+          un[v] = upd[v] + (sizeof(R) == 8 ? ((double)fzb[v] - (double)fz[v]) : (double)(fzb[v] - fz[v]));
           a.uout[v * vstr + zo + col] = un[v];
         }
         smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(un, a.hp) : cfl_speed_fast(un, a.hp));
@@ -263,8 +269,13 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
-          u = u + ((double)fx[v] - (double)fxs[v * NC + tid + 1]);
-          u = u + ((double)fy[v] - (double)fys[v * NC + tid + CX]);
+          if (sizeof(R) == 8) {
+            u = u + ((double)fx[v] - (double)fxs[v * NC + tid + 1]);
+            u = u + ((double)fy[v] - (double)fys[v * NC + tid + CX]);
+          } else {
+            u = u + (double)(fx[v] - fxs[v * NC + tid + 1]);
+            u = u + (double)(fy[v] - fys[v * NC + tid + CX]);
+          }
           upd[v] = u;
           fzb[v] = fz[v];
         }
