@@ -20,6 +20,9 @@ namespace rb {
 // used identically by the CPU restatement so that signed zeros agree.
 template <typename R> __device__ __forceinline__ R fmx(R a, R b) { return a > b ? a : (b > a ? b : a); }
 template <typename R> __device__ __forceinline__ R fmn(R a, R b) { return a < b ? a : (b < a ? b : a); }
+// The FP32-mixed path needs no signed-zero tie rule: one native min/max.
+template <> __device__ __forceinline__ float fmx<float>(float a, float b) { return fmaxf(a, b); }
+template <> __device__ __forceinline__ float fmn<float>(float a, float b) { return fminf(a, b); }
 
 template <typename R> struct Prim { R r, u, v, w, p; };
 

@@ -60,7 +60,7 @@ struct StreamGeom {
   static constexpr int CHUNKS = 5 * SY * (SX / 2);      // 16-byte chunks per raw plane
   static constexpr size_t RAW_BYTES = sizeof(double) * NRAW * 5 * NS;
   static constexpr size_t Q_BYTES = sizeof(R) * NQ * 5 * NS;
-  static constexpr size_t X_BYTES = sizeof(R) * 4 * 5 * NC;   // qm_x, qm_y, Fx, Fy
+  static constexpr size_t X_BYTES = sizeof(double) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;  // Fx, Fy; qm_x, qm_y
   static constexpr size_t SMEM = RAW_BYTES + Q_BYTES + X_BYTES;
   static_assert(NEXTRA <= NC, "one extra column per thread at most");
   static_assert(TX % 2 == 0 && TY % 2 == 0, "even tile");
@@ -77,10 +77,10 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* raw = reinterpret_cast<double*>(smem_raw);                      // [NRAW][5][NS]
   R* qb = reinterpret_cast<R*>(smem_raw + G::RAW_BYTES);                  // [NQ][5][NS]
-  R* xm = qb + G::NQ * 5 * NS;                                            // [5][NC] qm_x
+  double* fxs = reinterpret_cast<double*>(qb + G::NQ * 5 * NS);           // [5][NC] Fx (left face)
+  double* fys = fxs + 5 * NC;                                             // [5][NC] Fy (lower face)
+  R* xm = reinterpret_cast<R*>(fys + 5 * NC);                             // [5][NC] qm_x
   R* ym = xm + 5 * NC;                                                    // [5][NC] qm_y
-  R* fxs = ym + 5 * NC;                                                   // [5][NC] Fx (left face)
-  R* fys = fxs + 5 * NC;                                                  // [5][NC] Fy (lower face)
   __shared__ double red[G::NT / 32];
 
   const int tid = threadIdx.x;
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
   Prim<R> qmz_prev;                  // qm_z of the plane below (left state of face k-1/2)
   qmz_prev.r = qmz_prev.u = qmz_prev.v = qmz_prev.w = qmz_prev.p = (R)0;
   double upd[5] = {0, 0, 0, 0, 0};   // uold + dFx + dFy of the pending plane
-  R fzb[5] = {0, 0, 0, 0, 0};        // flux through the pending plane's lower face
+  double fzb[5] = {0, 0, 0, 0, 0};   // flux through the pending plane's lower face
   double smax = 0.0;
   const int64_t col = inner ? (int64_t)(ty0 + cy) * a.nx + (tx0 + cx) : 0;
 
@@ -227,25 +227,27 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
     qmz_prev = sm[2];
     // flux*dt/dx evaluated as (fx*dt)/dx (umuscl.f90:101-163); dividing by an
     // exact power-of-two dx equals multiplying by its reciprocal
-    auto scale = [&](R f) -> R {
+    // Each face flux is rounded to FP64 once, by the face's owner, so that the
+    // FP64 accumulation below telescopes exactly (conservation to FP64
+    // roundoff in both precisions).
+    auto scale = [&](R f) -> double {
       if (sizeof(R) == 8) {
         const double t = (double)f * dt;
-        return (R)(a.dx_pow2 ? t * a.inv_dx : t / a.dx);
+        return a.dx_pow2 ? t * a.inv_dx : t / a.dx;
       }
-      return f * dtdx;
+      return (double)(f * dtdx);
     };
+    double fzd[5];
     if (upd_plane && valid) {
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        fx[v] = scale(fx[v]);
-        fy[v] = scale(fy[v]);
-        fxs[v * NC + tid] = fx[v];
-        fys[v * NC + tid] = fy[v];
+        fxs[v * NC + tid] = scale(fx[v]);
+        fys[v * NC + tid] = scale(fy[v]);
       }
     }
     if (inner && k >= z0) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) fz[v] = scale(fz[v]);
+      for (int v = 0; v < 5; v++) fzd[v] = scale(fz[v]);
     }
     cp_async_wait<1>();  // plane k+3 (converted at the next A) has landed
     __syncthreads();
@@ -256,9 +258,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
         const int64_t zo = (int64_t)(k - 1) * plane;  // k-1 in [z0, zend) lies inside the box
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          // FP64 path: difference of the FP64 fluxes (reference order); FP32-mixed:
-          // the FP32 flux difference, accumulated in FP64
-          un[v] = upd[v] + (sizeof(R) == 8 ? ((double)fzb[v] - (double)fz[v]) : (double)(fzb[v] - fz[v]));
+          un[v] = upd[v] + (fzb[v] - fzd[v]);
           a.uout[v * vstr + zo + col] = un[v];
         }
         smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(un, a.hp) : cfl_speed_fast(un, a.hp));
@@ -269,15 +269,10 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
-          if (sizeof(R) == 8) {
-            u = u + ((double)fx[v] - (double)fxs[v * NC + tid + 1]);
-            u = u + ((double)fy[v] - (double)fys[v * NC + tid + CX]);
-          } else {
-            u = u + (double)(fx[v] - fxs[v * NC + tid + 1]);
-            u = u + (double)(fy[v] - fys[v * NC + tid + CX]);
-          }
+          u = u + (fxs[v * NC + tid] - fxs[v * NC + tid + 1]);
+          u = u + (fys[v * NC + tid] - fys[v * NC + tid + CX]);
           upd[v] = u;
-          fzb[v] = fz[v];
+          fzb[v] = fzd[v];
         }
       }
     }
