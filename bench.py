@@ -58,6 +58,9 @@ def parse():
                     help="oct-tile method: force a godunov tile shape (default: autotuned on the workload)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="z-streaming method: keep the default configuration instead of autotuning")
+    ap.add_argument("--stream-config", default=None, metavar="SHAPE,HZ",
+                    help="z-streaming method: use this column shape and z extent instead of autotuning "
+                         "(profiling runs replay the autotuned choice without its probe launches)")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
                     help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
@@ -68,6 +71,9 @@ def make_solver(runtime, tree, hp, precision, u, args):
     s.set_uniform_method(args.method)
     if args.method == "tiles":
         s.set_tile_shape(tree.nlevelmax, args.tile_shape)
+    elif args.stream_config:
+        shape, hz = (int(x) for x in args.stream_config.split(","))
+        s.set_stream_shape(shape, hz)
     elif not args.no_autotune:
         s.autotune_uniform()
     return s

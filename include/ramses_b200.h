@@ -82,6 +82,14 @@ int rb_courant_fine(rb_context *ctx, int ilevel, double *dt_io, double *mass, do
  * subcycling, followed by the restriction of levels levelmin-1..1. t_io is
  * advanced by the step; dtnew_out (may be NULL) receives dtnew(1..nlevelmax). */
 int rb_coarse_step(rb_context *ctx, double *t_io, double *dtnew_out);
+/* Coarse steps until t >= t_end or max_steps steps have run, the loop of
+ * adaptive_loop (amr/adaptive_loop.f90:118-205) over amr_step (same results
+ * as repeated rb_coarse_step calls). The scheduler state (dtnew, dtold, t,
+ * nstep, amr/amr_step.f90:320-331,571-576) stays on the device, so the steps
+ * run without host round trips; with use_graph the steps run from a cached
+ * CUDA graph of 8 coarse steps whose launches become no-ops past the stop
+ * rule. steps_done (may be NULL) receives the coarse steps taken. */
+int rb_run(rb_context *ctx, int max_steps, double t_end, int use_graph, double *t_io, int *steps_done);
 /* Leaf-cell updates done by this context so far (one per leaf cell per step of its level). */
 int rb_cell_updates(rb_context *ctx, int64_t *out);
 
@@ -122,6 +130,9 @@ int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *
  * 4 CTAs/SM) and z extent 4..64 is timed; the fastest is kept. The state,
  * the time and the next dt are unchanged. Outputs may be NULL. */
 int rb_autotune_uniform(rb_context *ctx, int *shape, int *hz, float *ms);
+/* Set the z-streaming configuration by hand (shape as above; hz even and
+ * dividing the grid's nz), e.g. to replay an autotuned choice. */
+int rb_set_stream_shape(rb_context *ctx, int shape, int hz);
 
 /* CFL reduction over plain device arrays that allocates nothing.
  * No counterpart in the reference: it exists for callers that cannot call
@@ -152,6 +163,49 @@ int rb_get_stream(rb_context *ctx, void **stream);
 int rb_last_kernel_ms(rb_context *ctx, float *ms);
 /* Device milliseconds of the whole last rb_uniform_run (all steps). */
 int rb_last_run_ms(rb_context *ctx, float *ms);
+
+/* ---- serving engine: many independent problems on one GPU ----------------
+ * No counterpart in the reference (one RAMSES run is one problem). Problems
+ * are admitted first-come first-served while their device memory fits in the
+ * budget, stay resident until t >= t_end or max_steps steps, and their result
+ * is then copied into the caller's `result` buffer. The caller keeps every
+ * array it passes (input, tree, result) valid until the request completes or
+ * is cancelled. A problem's result is bitwise the same whatever other
+ * problems share the GPU with it: no reduction or atomic spans problems.
+ * Single-threaded: one host thread drives a server. */
+typedef struct rb_server rb_server;
+#define RB_REQ_QUEUED 0
+#define RB_REQ_ACTIVE 1
+#define RB_REQ_DONE 2
+#define RB_REQ_FAILED 3
+#define RB_REQ_CANCELLED 4
+/* hbm_budget_bytes <= 0: 85% of the free device memory. steps_per_round:
+ * batched steps enqueued per rb_server_progress call (1..1024). */
+int rb_server_create(const rb_hydro_params *hp, int precision, int64_t hbm_budget_bytes, int steps_per_round,
+                     rb_server **out);
+int rb_server_destroy(rb_server *srv);
+/* A periodic uniform problem as a dense grid: u[v][z][y][x] conservative
+ * (rho, rho*u, rho*v, rho*w, E), nx = ny = nz, nx a multiple of 16. Every
+ * step is a time step of the complete level (the z-streaming kernel, batched
+ * with every other active dense problem); result has the layout of u. */
+int rb_server_submit_dense(rb_server *srv, int32_t nx, int32_t ny, int32_t nz, double boxlen, const double *u,
+                           double t_end, int64_t max_steps, double *result, int64_t *id);
+/* An AMR problem in the rb_sync_tree / rb_upload_state form; stepped by
+ * coarse steps as rb_run does; result is uold(ncell,5). */
+int rb_server_submit_octree(rb_server *srv, const rb_mesh_params *mp, const int32_t *son, const int32_t *father,
+                            const int32_t *nbor, const int32_t *numbl, const int32_t *active_igrid,
+                            const double *uold, double t_end, int64_t max_steps, double *result, int64_t *id);
+/* Admit, enqueue one round of steps, retire finished problems. Up to max_ids
+ * completed request ids are written to done_ids (the rest on later calls). */
+int rb_server_progress(rb_server *srv, int64_t *done_ids, int max_ids, int *ndone);
+/* State (RB_REQ_*), time reached, steps, leaf-cell updates and seconds from
+ * submission to completion (or to now). Returns the request's error status. */
+int rb_server_request_info(rb_server *srv, int64_t id, int *state, double *t, int64_t *steps,
+                           int64_t *cell_updates, double *seconds_in_system);
+/* Cancel a queued or active request (it completes as RB_REQ_CANCELLED). */
+int rb_server_cancel(rb_server *srv, int64_t id);
+int rb_server_stats(rb_server *srv, int *queued, int *active, int64_t *bytes_in_use, int64_t *budget,
+                    int64_t *cell_updates, int64_t *batch_launches);
 
 #ifdef __cplusplus
 }

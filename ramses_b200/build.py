@@ -26,6 +26,7 @@ UNITS = {
     "tile_f64.cu": ["--fmad=false"],
     "tile_mixed.cu": ["-use_fast_math"],
     "rb_noalloc.cu": ["--fmad=false"],
+    "rb_server.cu": ["--fmad=false"],
 }
 HEADERS = sorted(list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc"))
                  + [PKG.parent / "include" / "ramses_b200.h"])

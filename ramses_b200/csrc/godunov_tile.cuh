@@ -45,6 +45,7 @@ struct TileArgs {
   double dt, dx, inv_dx;
   const double* __restrict__ dt_dev;    // if non-null, dt is read here
   double* __restrict__ partial;         // fused: [ntile][4] (min dt, mass, E, eint)
+  const double* __restrict__ gate;      // if non-null and *gate != 0 the launch is a no-op
   rb_hydro_params hp;
 };
 
@@ -75,6 +76,7 @@ constexpr size_t tile_smem_bytes() {
 
 template <typename R, int TX, int TY, int TZ, int NT>
 __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
+  if (a.gate != nullptr && *a.gate != 0.0) return;
   using G = TileGeom<TX, TY, TZ>;
   constexpr int SX = G::SX, SY = G::SY, SZ = G::SZ, NS = G::NS;
   constexpr int BX = G::BX, BY = G::BY, NBLK = G::NBLK;

@@ -14,6 +14,12 @@
 
 namespace rb {
 
+// early exit of a level kernel when the device clock says the run is over
+#define RB_GATE(g)                                \
+  do {                                            \
+    if ((g) != nullptr && *(g) != 0.0) return;    \
+  } while (0)
+
 __device__ __forceinline__ int64_t dev_cell_of_fortran(int64_t icell /*1-based*/, int32_t ncoarse,
                                                        int32_t ngridmax) {
   if (icell <= ncoarse) return icell - 1;
@@ -23,7 +29,7 @@ __device__ __forceinline__ int64_t dev_cell_of_fortran(int64_t icell /*1-based*/
 }
 
 // Fortran uold(ncell,5) -> device layout (and back).
-__global__ void permute_f2d_kernel(const double* __restrict__ f, double* __restrict__ d, int64_t ncell,
+static __global__ void permute_f2d_kernel(const double* __restrict__ f, double* __restrict__ d, int64_t ncell,
                                    int32_t ncoarse, int32_t ngridmax, int nvar) {
   const int64_t n = ncell * nvar;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -31,7 +37,7 @@ __global__ void permute_f2d_kernel(const double* __restrict__ f, double* __restr
     d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)] = f[i];
   }
 }
-__global__ void permute_d2f_kernel(const double* __restrict__ d, double* __restrict__ f, int64_t ncell,
+static __global__ void permute_d2f_kernel(const double* __restrict__ d, double* __restrict__ f, int64_t ncell,
                                    int32_t ncoarse, int32_t ngridmax, int nvar) {
   const int64_t n = ncell * nvar;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -39,7 +45,7 @@ __global__ void permute_d2f_kernel(const double* __restrict__ d, double* __restr
     f[i] = d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)];
   }
 }
-__global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t* __restrict__ d, int64_t ncell,
+static __global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t* __restrict__ d, int64_t ncell,
                                    int32_t ncoarse, int32_t ngridmax) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += (int64_t)gridDim.x * blockDim.x)
     d[dev_cell_of_fortran(i + 1, ncoarse, ngridmax)] = f[i];
@@ -47,9 +53,10 @@ __global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t* __res
 
 // set_unew / set_uold (godunov_fine.f90:40-130, 135-232): copy the 8x5
 // values of every active oct. active[] holds igrid-1.
-__global__ void copy_octs_kernel(const double* __restrict__ src, double* __restrict__ dst,
+static __global__ void copy_octs_kernel(const double* __restrict__ src, double* __restrict__ dst,
                                  const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
-                                 int32_t ncoarse) {
+                                 int32_t ncoarse, const double* __restrict__ gate) {
+  RB_GATE(gate);
   const int64_t n = (int64_t)noct * 8 * 5;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
@@ -62,9 +69,10 @@ __global__ void copy_octs_kernel(const double* __restrict__ src, double* __restr
 // (interpol_hydro, called from godunov_fine.f90:584-592). cells7[e*7+j]: device
 // cell of the father cell (j=0) and of its 6 neighbour (or neighbour-father)
 // cells, as getnborfather (nbors_utils.f90:404-525) returns them.
-__global__ void interp_blocks_kernel(const double* __restrict__ uold, const int32_t* __restrict__ cells7,
+static __global__ void interp_blocks_kernel(const double* __restrict__ uold, const int32_t* __restrict__ cells7,
                                      int32_t nentry, int64_t ncell, double* __restrict__ out,
-                                     rb_hydro_params hp) {
+                                     rb_hydro_params hp, const double* __restrict__ gate) {
+  RB_GATE(gate);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nentry) return;
   double u1[7][5], u2[8][5];
@@ -83,9 +91,11 @@ __global__ void interp_blocks_kernel(const double* __restrict__ uold, const int3
 // batch of the contributing oct, then direction, then left before right, and
 // within one face its 4 fine cells in (k3,j3,i3) order.
 // contrib[k] = slot*6 + face (face 0..5 = -x,+x,-y,+y,-z,+z).
-__global__ void apply_corrections_kernel(double* __restrict__ unew, const int32_t* __restrict__ tgt,
+static __global__ void apply_corrections_kernel(double* __restrict__ unew, const int32_t* __restrict__ tgt,
                                          const int32_t* __restrict__ off, const int32_t* __restrict__ contrib,
-                                         int32_t ntgt, const double* __restrict__ corr_flux, int64_t ncell) {
+                                         int32_t ntgt, const double* __restrict__ corr_flux, int64_t ncell,
+                                         const double* __restrict__ gate) {
+  RB_GATE(gate);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntgt) return;
   const int64_t dc = tgt[t];
@@ -109,11 +119,13 @@ __global__ void apply_corrections_kernel(double* __restrict__ unew, const int32_
 // total energy, internal energy) over the leaf cells of the level's octs.
 // A second single-block pass reduces the partials in a fixed order.
 template <int NT>
-__global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __restrict__ uold,
+static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __restrict__ uold,
                                                              const int32_t* __restrict__ son,
                                                              const int32_t* __restrict__ active, int32_t noct,
                                                              int64_t ncell, int32_t ncoarse, double dx,
-                                                             rb_hydro_params hp, double* __restrict__ partial) {
+                                                             rb_hydro_params hp, double* __restrict__ partial,
+                                                             const double* __restrict__ gate) {
+  RB_GATE(gate);
   const double vol = dx * dx * dx;
   double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
   const int64_t n = (int64_t)noct * 8;
@@ -159,10 +171,10 @@ __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __res
 //   advanced by the step just taken), out[0] = the next step's dt as
 //   newdt_fine + courant_fine give it, out[2..4] = totals, out[5] += 1.
 #define RB_RED_NT 1024
-__global__ void __launch_bounds__(RB_RED_NT) reduce_partials_kernel(const double* __restrict__ partial, int n,
-                                                                    double dt_in, double dt_cmpdt0, int any_leaf,
-                                                                    double* __restrict__ out, int mode) {
-  __shared__ double red[4][RB_RED_NT];
+// Fixed-order reduction of n partials [n][4] (min dt, sums of mass, E, eint)
+// by one CTA of RB_RED_NT threads; the totals end up in red[0..3][0].
+__device__ __forceinline__ void reduce4_block(const double* __restrict__ partial, int n,
+                                              double (*red)[RB_RED_NT]) {
   double dtm = 1.0e300, mass = 0.0, etot = 0.0, eint = 0.0;
   for (int k = threadIdx.x; k < n; k += RB_RED_NT) {
     dtm = fmn(dtm, partial[k * 4 + 0]);
@@ -181,6 +193,13 @@ __global__ void __launch_bounds__(RB_RED_NT) reduce_partials_kernel(const double
     }
     __syncthreads();
   }
+}
+
+static __global__ void __launch_bounds__(RB_RED_NT) reduce_partials_kernel(const double* __restrict__ partial, int n,
+                                                                    double dt_in, double dt_cmpdt0, int any_leaf,
+                                                                    double* __restrict__ out, int mode) {
+  __shared__ double red[4][RB_RED_NT];
+  reduce4_block(partial, n, red);
   if (threadIdx.x == 0) {
     const double dt_lev = fmn(dt_cmpdt0, red[0][0]);
     if (mode == 0) {
@@ -195,11 +214,89 @@ __global__ void __launch_bounds__(RB_RED_NT) reduce_partials_kernel(const double
   }
 }
 
+// ---- device-resident amr_step clock ----------------------------------------
+// The scalar bookkeeping of amr_step (amr/amr_step.f90:320-331,571-576),
+// newdt_fine (pm/newdt_fine.f90:47-51,173) and update_time's t/nstep advance
+// (amr/update_time.f90:330-331) runs in single-thread kernels on one array
+// `s`, so a sequence of coarse steps needs no host round trip and can be
+// captured into a CUDA graph. Every level kernel of a coarse step takes
+// gate = s + RB_S_DONE and returns at once when the run is over (t >= t_end or
+// the requested number of coarse steps done), so a graph of K coarse steps
+// stops exactly where a host loop would.
+#define RB_NLV (RB_MAXLEVEL + 2)
+#define RB_S_DTNEW 0
+#define RB_S_DTOLD RB_NLV
+#define RB_S_T (2 * RB_NLV)
+#define RB_S_NSTEP (2 * RB_NLV + 1)
+#define RB_S_MASS (2 * RB_NLV + 2)
+#define RB_S_EKIN (2 * RB_NLV + 3)
+#define RB_S_EINT (2 * RB_NLV + 4)
+#define RB_S_DONE (2 * RB_NLV + 5)
+#define RB_S_TEND (2 * RB_NLV + 6)
+#define RB_S_MAXC (2 * RB_NLV + 7)
+#define RB_S_COARSE (2 * RB_NLV + 8)
+#define RB_S_SIZE (2 * RB_NLV + 16)
+
+// start of a coarse step: decide whether it runs; reset the level totals
+static __global__ void sched_gate_kernel(double* __restrict__ s) {
+  const bool done = !(s[RB_S_T] < s[RB_S_TEND]) || !(s[RB_S_COARSE] < s[RB_S_MAXC]);
+  s[RB_S_DONE] = done ? 1.0 : 0.0;
+  if (!done) s[RB_S_MASS] = s[RB_S_EKIN] = s[RB_S_EINT] = 0.0;
+}
+
+// newdt_fine + courant_fine of level l from the level's CFL partials:
+// dtold(l)=dtnew(l); dtnew(l)=min(boxlen/smallc, courant); for l>levelmin
+// dtnew(l)=min(dtnew(l-1)/nsubcycle(l-1), dtnew(l)); level totals accumulated.
+static __global__ void __launch_bounds__(RB_RED_NT) sched_courant_kernel(const double* __restrict__ partial, int n, int l,
+                                                                  int levelmin, double dt_cmpdt0, int any_leaf,
+                                                                  double dt_max, double nsub_prev,
+                                                                  double* __restrict__ s) {
+  if (s[RB_S_DONE] != 0.0) return;
+  __shared__ double red[4][RB_RED_NT];
+  reduce4_block(partial, n, red);
+  if (threadIdx.x == 0) {
+    s[RB_S_DTOLD + l] = s[RB_S_DTNEW + l];
+    const double dt_lev = fmn(dt_cmpdt0, red[0][0]);
+    const double dt_all = any_leaf ? fmn(dt_max, dt_lev) : dt_max;
+    s[RB_S_MASS] = s[RB_S_MASS] + red[1][0];
+    s[RB_S_EKIN] = s[RB_S_EKIN] + red[2][0];
+    s[RB_S_EINT] = s[RB_S_EINT] + red[3][0];
+    double dtn = fmn(dt_max, dt_all);
+    if (l > levelmin) dtn = fmn(s[RB_S_DTNEW + l - 1] / nsub_prev, dtn);
+    s[RB_S_DTNEW + l] = dtn;
+  }
+}
+
+// the finest level of this step is l: advance t and nstep; when the next
+// level exists but holds no oct (mode 1) also set its dtold/dtnew
+static __global__ void sched_advance_kernel(double* __restrict__ s, int l, int mode, double nsub_l) {
+  if (s[RB_S_DONE] != 0.0) return;
+  if (mode == 1) {
+    s[RB_S_DTOLD + l + 1] = s[RB_S_DTNEW + l] / nsub_l;
+    s[RB_S_DTNEW + l + 1] = s[RB_S_DTNEW + l] / nsub_l;
+  }
+  s[RB_S_T] = s[RB_S_T] + s[RB_S_DTNEW + l];
+  s[RB_S_NSTEP] = s[RB_S_NSTEP] + 1.0;
+}
+
+// end of amr_step(l, icount) for l > levelmin (amr_step.f90:571-576)
+static __global__ void sched_end_kernel(double* __restrict__ s, int l, int nsub_prev_is_one, int icount) {
+  if (s[RB_S_DONE] != 0.0) return;
+  if (nsub_prev_is_one) s[RB_S_DTNEW + l - 1] = s[RB_S_DTNEW + l];
+  if (icount == 2) s[RB_S_DTNEW + l - 1] = s[RB_S_DTOLD + l] + s[RB_S_DTNEW + l];
+}
+
+static __global__ void sched_finish_kernel(double* __restrict__ s) {
+  if (s[RB_S_DONE] != 0.0) return;
+  s[RB_S_COARSE] = s[RB_S_COARSE] + 1.0;
+}
+
 // upload_fine / upl (interpol_hydro.f90:5-263): restriction of every split
 // cell of the level's active octs from its 8 children.
-__global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,
+static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,
                                    const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
-                                   int32_t ncoarse, rb_hydro_params hp) {
+                                   int32_t ncoarse, rb_hydro_params hp, const double* __restrict__ gate) {
+  RB_GATE(gate);
   const int64_t n = (int64_t)noct * 8;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
@@ -240,7 +337,7 @@ __global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __r
 // One CTA per oct (grid index l); the 32 traced cells and 36 faces the
 // fluxes depend on are computed from the 6x6x6 stencil in shared memory.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double* __restrict__ uin,
+static __global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double* __restrict__ uin,
                                                              const double* __restrict__ gravin,
                                                              double* __restrict__ flux, double* __restrict__ tmp,
                                                              double dx, double dy, double dz, double dt,
@@ -350,7 +447,7 @@ __global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double* __res
 
 // Oct layout <-> dense Cartesian array of one complete level.
 // cbase[i]: dense index of child 0 of the level's i-th active oct.
-__global__ void oct_to_dense_kernel(const double* __restrict__ u, double* __restrict__ d,
+static __global__ void oct_to_dense_kernel(const double* __restrict__ u, double* __restrict__ d,
                                     const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
                                     int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
                                     int64_t vstr) {
@@ -363,7 +460,7 @@ __global__ void oct_to_dense_kernel(const double* __restrict__ u, double* __rest
     d[v * vstr + di] = u[v * ncell + oct0 + (int64_t)active[o] * 8 + ch];
   }
 }
-__global__ void dense_to_oct_kernel(const double* __restrict__ d, double* __restrict__ u,
+static __global__ void dense_to_oct_kernel(const double* __restrict__ d, double* __restrict__ u,
                                     const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
                                     int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
                                     int64_t vstr) {

@@ -1,0 +1,185 @@
+// rb_context.h -- internal to the library: the per-problem context of the
+// host runtime, its per-level tables, and the helpers shared by the runtime
+// and the serving engine (error reporting, device allocation).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/ramses_b200.h"
+#include "godunov_tile.cuh"
+#include "rb_aux.cuh"
+#include "stream_kernel.cuh"
+#include "tile_launch.h"
+
+namespace rbi {
+
+// host-side Fortran MIN with the same tie rule as the device and the oracle
+inline double rb_min_host(double a, double b) { return a < b ? a : (b < a ? b : a); }
+
+inline thread_local std::string g_last_error;
+
+inline int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define RB_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(RB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                  __LINE__);                                                                 \
+  } while (0)
+
+#define RB_TRY(expr)       \
+  do {                     \
+    int rc_ = (expr);      \
+    if (rc_) return rc_;   \
+  } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) return RB_OK;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(RB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+  }
+  return RB_OK;
+}
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+inline int grid_for(int64_t n, int nt, int cap = 148 * 32) {
+  int64_t g = (n + nt - 1) / nt;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+struct Level {
+  int noct = 0;
+  std::vector<int32_t> h_active;  // igrid (1-based), host order
+  int32_t* d_active = nullptr;    // igrid-1
+  int shape = -1;
+  int ntile = 0;
+  int32_t* d_tile_blk = nullptr;
+  int ninterp = 0;
+  int32_t* d_interp7 = nullptr;
+  double* d_interp_buf = nullptr;
+  int has_refined = 0;
+  int nslot = 0;
+  double* d_corr_flux = nullptr;
+  int ntgt = 0;
+  int32_t* d_tgt = nullptr;
+  int32_t* d_tgt_off = nullptr;
+  int32_t* d_contrib = nullptr;
+  int64_t leaf_cells = 0;
+  double dx = 0.0;
+  bool complete = false;
+  bool tables_built = false;
+};
+
+// sorted (key, igrid) lookup of one level's octs
+struct OctIndex {
+  std::vector<std::pair<int64_t, int32_t>> v;
+  int64_t nx = 1, ny = 1, nz = 1;  // octs per dimension at this level
+  int64_t key(int64_t x, int64_t y, int64_t z) const {
+    x = ((x % nx) + nx) % nx;
+    y = ((y % ny) + ny) % ny;
+    z = ((z % nz) + nz) % nz;
+    return x + nx * (y + ny * z);
+  }
+  int32_t find(int64_t x, int64_t y, int64_t z) const {
+    const int64_t k = key(x, y, z);
+    auto it = std::lower_bound(v.begin(), v.end(), std::make_pair(k, (int32_t)INT32_MIN));
+    if (it != v.end() && it->first == k) return it->second;
+    return 0;
+  }
+};
+
+}  // namespace rbi
+
+struct rb_context {
+  rb_hydro_params hp;
+  rb_mesh_params mp;
+  int precision = RB_PREC_FP64;
+  int device = 0;
+  int64_t ncell = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+  double* d_uold = nullptr;
+  double* d_unew = nullptr;
+  int32_t* d_son = nullptr;
+  int32_t* d_corr_slot = nullptr;   // [ngridmax]
+  double* d_stage = nullptr;        // Fortran-layout staging [5*ncell]
+  double* d_partial = nullptr;      // CFL partials
+  int64_t partial_cap = 0;
+  double* d_red = nullptr;          // [8] reduction output
+  double* d_clock = nullptr;        // [8] device clock of the uniform stepper
+  double* h_red = nullptr;          // pinned [8]
+  double* d_sched = nullptr;        // [RB_S_SIZE] device-resident amr_step clock
+  double* h_sched = nullptr;        // pinned [RB_S_SIZE]
+  const double* gate = nullptr;     // level kernels return early when *gate != 0
+  cudaGraphExec_t amr_graph = nullptr;  // cached graph of amr_chunk coarse steps
+  int amr_chunk = 0;
+  bool have_tree = false;
+  bool have_state = false;
+  bool clock_valid = false;
+  // host copies of the tree (Fortran layout)
+  std::vector<int32_t> son, father, nbor;
+  std::vector<int64_t> coords;      // [ngridmax*3] oct coordinates at its level
+  std::vector<int8_t> level_of;     // [ngridmax] level of each oct (0 = unused)
+  rbi::Level lv[RB_MAXLEVEL + 2];
+  std::vector<rbi::OctIndex> idx;        // per-level position -> igrid lookup
+  int finest = 0;                   // finest level holding octs
+  std::vector<int32_t> h_corr_slot; // host copy of d_corr_slot
+  std::vector<cudaEvent_t> evpool;  // per-step kernel timing events
+  float kernel_ms_avg = 0.f;        // mean tile-kernel time of the last timed run
+  cudaGraphExec_t graph = nullptr;  // cached uniform-run graph
+  int graph_steps = 0;
+  double* graph_cur = nullptr;
+  // dense Cartesian mirror of the finest (complete) level for the z-streaming path
+  int uniform_method = 0;           // 0: z-streaming over the dense mirror, 1: oct tiles
+  double* d_dense[2] = {nullptr, nullptr};
+  int dense_cur = 0;
+  int64_t* d_cbase = nullptr;
+  int32_t dnx = 0, dny = 0, dnz = 0;
+  bool dense_valid = false;         // the dense mirror holds the newest state of `finest`
+  bool oct_stale = false;           // the oct layout of `finest` lags the dense mirror
+  int stream_shape = -1, stream_hz = 0, stream_items = 0;
+  // scheduler state (amr_commons dtnew/dtold, t, nstep)
+  double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
+  double t = 0.0;
+  int64_t nstep = 0;
+  int64_t cell_updates = 0;
+  double mass_tot = 0, ekin_tot = 0, eint_tot = 0;
+};
+
+namespace rbi {
+// parameter rules of rb_create (rb_runtime.cu)
+int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp);
+// device-scheduled coarse steps without waiting (rb_runtime.cu)
+int run_async_begin(rb_context* c, double t_end, int64_t max_coarse);
+int run_async_chunk(rb_context* c, int chunk, bool use_graph);
+int run_async_end(rb_context* c, int64_t* coarse_out);
+}  // namespace rbi

@@ -7,175 +7,11 @@
 // (amr/amr_step.f90:320-445) that drives the level kernels on one stream.
 // Compiled with --fmad=false (FP64 kernels bit-identical to the reference
 // operation order).
-#include <cuda_runtime.h>
+#include "rb_context.h"
 
-#include <algorithm>
-#include <array>
-#include <cmath>
-#include <cstdarg>
-#include <cstdio>
-#include <cstring>
-#include <string>
-#include <unordered_map>
-#include <vector>
+using namespace rbi;
 
-#include "../../include/ramses_b200.h"
-#include "godunov_tile.cuh"
-#include "rb_aux.cuh"
-#include "stream_kernel.cuh"
-#include "tile_launch.h"
-
-namespace {
-
-// host-side Fortran MIN with the same tie rule as the device and the oracle
-inline double rb_min_host(double a, double b) { return a < b ? a : (b < a ? b : a); }
-
-thread_local std::string g_last_error;
-
-int fail(int code, const char* fmt, ...) {
-  char buf[1024];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  g_last_error = buf;
-  return code;
-}
-
-#define RB_CUDA(call)                                                                        \
-  do {                                                                                       \
-    cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
-      return fail(RB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
-                  __LINE__);                                                                 \
-  } while (0)
-
-#define RB_TRY(expr)       \
-  do {                     \
-    int rc_ = (expr);      \
-    if (rc_) return rc_;   \
-  } while (0)
-
-template <typename T>
-int dalloc(T** p, size_t n) {
-  *p = nullptr;
-  if (n == 0) return RB_OK;
-  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(RB_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
-  }
-  return RB_OK;
-}
-template <typename T>
-void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
-  p = nullptr;
-}
-
-inline int grid_for(int64_t n, int nt, int cap = 148 * 32) {
-  int64_t g = (n + nt - 1) / nt;
-  if (g < 1) g = 1;
-  if (g > cap) g = cap;
-  return (int)g;
-}
-
-struct Level {
-  int noct = 0;
-  std::vector<int32_t> h_active;  // igrid (1-based), host order
-  int32_t* d_active = nullptr;    // igrid-1
-  int shape = -1;
-  int ntile = 0;
-  int32_t* d_tile_blk = nullptr;
-  int ninterp = 0;
-  int32_t* d_interp7 = nullptr;
-  double* d_interp_buf = nullptr;
-  int has_refined = 0;
-  int nslot = 0;
-  double* d_corr_flux = nullptr;
-  int ntgt = 0;
-  int32_t* d_tgt = nullptr;
-  int32_t* d_tgt_off = nullptr;
-  int32_t* d_contrib = nullptr;
-  int64_t leaf_cells = 0;
-  double dx = 0.0;
-  bool complete = false;
-  bool tables_built = false;
-};
-
-// sorted (key, igrid) lookup of one level's octs
-struct OctIndex {
-  std::vector<std::pair<int64_t, int32_t>> v;
-  int64_t nx = 1, ny = 1, nz = 1;  // octs per dimension at this level
-  int64_t key(int64_t x, int64_t y, int64_t z) const {
-    x = ((x % nx) + nx) % nx;
-    y = ((y % ny) + ny) % ny;
-    z = ((z % nz) + nz) % nz;
-    return x + nx * (y + ny * z);
-  }
-  int32_t find(int64_t x, int64_t y, int64_t z) const {
-    const int64_t k = key(x, y, z);
-    auto it = std::lower_bound(v.begin(), v.end(), std::make_pair(k, (int32_t)INT32_MIN));
-    if (it != v.end() && it->first == k) return it->second;
-    return 0;
-  }
-};
-
-}  // namespace
-
-struct rb_context {
-  rb_hydro_params hp;
-  rb_mesh_params mp;
-  int precision = RB_PREC_FP64;
-  int device = 0;
-  int64_t ncell = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  float last_ms = 0.f;
-  double* d_uold = nullptr;
-  double* d_unew = nullptr;
-  int32_t* d_son = nullptr;
-  int32_t* d_corr_slot = nullptr;   // [ngridmax]
-  double* d_stage = nullptr;        // Fortran-layout staging [5*ncell]
-  double* d_partial = nullptr;      // CFL partials
-  int64_t partial_cap = 0;
-  double* d_red = nullptr;          // [8] reduction output
-  double* d_clock = nullptr;        // [8] device clock of the uniform stepper
-  double* h_red = nullptr;          // pinned [8]
-  bool have_tree = false;
-  bool have_state = false;
-  bool clock_valid = false;
-  // host copies of the tree (Fortran layout)
-  std::vector<int32_t> son, father, nbor;
-  std::vector<int64_t> coords;      // [ngridmax*3] oct coordinates at its level
-  std::vector<int8_t> level_of;     // [ngridmax] level of each oct (0 = unused)
-  Level lv[RB_MAXLEVEL + 2];
-  std::vector<OctIndex> idx;        // per-level position -> igrid lookup
-  int finest = 0;                   // finest level holding octs
-  std::vector<int32_t> h_corr_slot; // host copy of d_corr_slot
-  std::vector<cudaEvent_t> evpool;  // per-step kernel timing events
-  float kernel_ms_avg = 0.f;        // mean tile-kernel time of the last timed run
-  cudaGraphExec_t graph = nullptr;  // cached uniform-run graph
-  int graph_steps = 0;
-  double* graph_cur = nullptr;
-  // dense Cartesian mirror of the finest (complete) level for the z-streaming path
-  int uniform_method = 0;           // 0: z-streaming over the dense mirror, 1: oct tiles
-  double* d_dense[2] = {nullptr, nullptr};
-  int dense_cur = 0;
-  int64_t* d_cbase = nullptr;
-  int32_t dnx = 0, dny = 0, dnz = 0;
-  bool dense_valid = false;         // the dense mirror holds the newest state of `finest`
-  bool oct_stale = false;           // the oct layout of `finest` lags the dense mirror
-  int stream_shape = -1, stream_hz = 0, stream_items = 0;
-  // scheduler state (amr_commons dtnew/dtold, t, nstep)
-  double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
-  double t = 0.0;
-  int64_t nstep = 0;
-  int64_t cell_updates = 0;
-  double mass_tot = 0, ekin_tot = 0, eint_tot = 0;
-};
-
-namespace {
+namespace rbi {
 
 // Host->device copy ordered on the context's stream. A plain cudaMemcpy from
 // pageable memory may return before its DMA has landed and runs on the legacy
@@ -253,6 +89,9 @@ void drop_graph(rb_context* c) {
   c->graph = nullptr;
   c->graph_steps = 0;
   c->graph_cur = nullptr;
+  if (c->amr_graph) cudaGraphExecDestroy(c->amr_graph);
+  c->amr_graph = nullptr;
+  c->amr_chunk = 0;
 }
 
 void free_dense(rb_context* c) {
@@ -575,7 +414,7 @@ int set_unew_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
-      c->d_uold, c->d_unew, L.d_active, L.noct, c->ncell, c->mp.ncoarse);
+      c->d_uold, c->d_unew, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
   return RB_OK;
 }
@@ -584,7 +423,7 @@ int set_uold_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
-      c->d_unew, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse);
+      c->d_unew, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
   return RB_OK;
 }
@@ -594,7 +433,7 @@ int upload_fine_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct || !L.has_refined) return RB_OK;
   rb::upload_fine_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
-      c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp);
+      c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, c->gate);
   RB_CUDA(cudaGetLastError());
   return RB_OK;
 }
@@ -693,6 +532,7 @@ rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
   a.inv_dx = 1.0 / L.dx;
   a.dt_dev = nullptr;
   a.partial = nullptr;
+  a.gate = c->gate;
   a.hp = c->hp;
   return a;
 }
@@ -704,22 +544,25 @@ int launch_tile(rb_context* c, int shape, const rb::TileArgs& a, int grid) {
   return RB_OK;
 }
 
-int godunov_impl(rb_context* c, int l, double dt, bool timed) {
+int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_dev = nullptr) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
-  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(RB_ERR_INVALID, "dt=%g must be positive and finite", dt);
+  if (!dt_dev && (!(dt > 0.0) || !std::isfinite(dt)))
+    return fail(RB_ERR_INVALID, "dt=%g must be positive and finite", dt);
   if (L.ninterp) {
     rb::interp_blocks_kernel<<<(L.ninterp + 127) / 128, 128, 0, c->stream>>>(c->d_uold, L.d_interp7, L.ninterp,
-                                                                             c->ncell, L.d_interp_buf, c->hp);
+                                                                             c->ncell, L.d_interp_buf, c->hp,
+                                                                             c->gate);
     RB_CUDA(cudaGetLastError());
   }
   rb::TileArgs a = tile_args(c, L, dt);
+  a.dt_dev = dt_dev;
   if (timed) RB_CUDA(cudaEventRecord(c->ev0, c->stream));
   RB_TRY(launch_tile(c, L.shape, a, L.ntile));
   if (timed) RB_CUDA(cudaEventRecord(c->ev1, c->stream));
   if (L.ntgt) {
     rb::apply_corrections_kernel<<<(L.ntgt + 127) / 128, 128, 0, c->stream>>>(
-        c->d_unew, L.d_tgt, L.d_tgt_off, L.d_contrib, L.ntgt, L.d_corr_flux, c->ncell);
+        c->d_unew, L.d_tgt, L.d_tgt_off, L.d_contrib, L.ntgt, L.d_corr_flux, c->ncell, c->gate);
     RB_CUDA(cudaGetLastError());
   }
   return RB_OK;
@@ -732,7 +575,7 @@ int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin
   const int nblk = grid_for((int64_t)L.noct * 8, nt, 148 * 8);
   RB_TRY(ensure_partial(c, nblk));
   rb::courant_partial_kernel<256><<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate);
   RB_CUDA(cudaGetLastError());
   const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
   rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, *dt_io, dt0,
@@ -789,7 +632,156 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   return RB_OK;
 }
 
-}  // namespace
+// ---- device-scheduled coarse steps ----------------------------------------
+// Twin of amr_step_impl with the same launches, in the same order, on the same
+// stream; the scalar scheduler state lives in c->d_sched (sched_* kernels)
+// and every level kernel is gated on c->d_sched[RB_S_DONE].
+int courant_blocks(const rb_context* c, int l) { return grid_for((int64_t)c->lv[l].noct * 8, 256, 148 * 8); }
+
+int amr_step_dev(rb_context* c, int l, int icount) {
+  Level& L = c->lv[l];
+  if (L.noct == 0) return RB_OK;
+  double* s = c->d_sched;
+  const int nblk = courant_blocks(c, l);
+  rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
+                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate);
+  RB_CUDA(cudaGetLastError());
+  const double nsub_prev = l > c->mp.levelmin ? (double)(float)c->mp.nsubcycle[l - 1] : 1.0;
+  rb::sched_courant_kernel<<<1, RB_RED_NT, 0, c->stream>>>(
+      c->d_partial, nblk, l, c->mp.levelmin, c->hp.courant_factor * L.dx / c->hp.smallc, L.leaf_cells > 0 ? 1 : 0,
+      c->mp.boxlen / c->hp.smallc, nsub_prev, s);
+  RB_CUDA(cudaGetLastError());
+  RB_TRY(set_unew_impl(c, l));
+  if (l < c->mp.nlevelmax) {
+    if (c->lv[l + 1].noct > 0) {
+      RB_TRY(amr_step_dev(c, l + 1, 1));
+      if (c->mp.nsubcycle[l] == 2) RB_TRY(amr_step_dev(c, l + 1, 2));
+    } else {
+      rb::sched_advance_kernel<<<1, 1, 0, c->stream>>>(s, l, 1, (double)c->mp.nsubcycle[l]);
+    }
+  } else {
+    rb::sched_advance_kernel<<<1, 1, 0, c->stream>>>(s, l, 2, 1.0);
+  }
+  RB_CUDA(cudaGetLastError());
+  RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l));
+  RB_TRY(set_uold_impl(c, l));
+  RB_TRY(upload_fine_impl(c, l));
+  if (l > c->mp.levelmin && (c->mp.nsubcycle[l - 1] == 1 || icount == 2)) {
+    rb::sched_end_kernel<<<1, 1, 0, c->stream>>>(s, l, c->mp.nsubcycle[l - 1] == 1 ? 1 : 0, icount);
+    RB_CUDA(cudaGetLastError());
+  }
+  return RB_OK;
+}
+
+int coarse_step_dev(rb_context* c) {
+  rb::sched_gate_kernel<<<1, 1, 0, c->stream>>>(c->d_sched);
+  RB_CUDA(cudaGetLastError());
+  RB_TRY(amr_step_dev(c, c->mp.levelmin, 1));
+  for (int l = c->mp.levelmin - 1; l >= 1; l--) RB_TRY(upload_fine_impl(c, l));
+  rb::sched_finish_kernel<<<1, 1, 0, c->stream>>>(c->d_sched);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+// leaf-cell updates of one coarse step: every amr_step(l) call adds the
+// level's leaf cells (adaptive_loop.f90:204-207 counts the same cell-steps)
+int64_t updates_per_coarse(const rb_context* c, int l) {
+  if (l > c->mp.nlevelmax || c->lv[l].noct == 0) return 0;
+  int64_t n = c->lv[l].leaf_cells;
+  if (l < c->mp.nlevelmax && c->lv[l + 1].noct > 0) n += c->mp.nsubcycle[l] * updates_per_coarse(c, l + 1);
+  return n;
+}
+
+// Enqueue `chunk` gated coarse steps, from a cached CUDA graph if asked.
+int enqueue_chunk(rb_context* c, int chunk, bool use_graph) {
+  if (!use_graph) {
+    for (int k = 0; k < chunk; k++) RB_TRY(coarse_step_dev(c));
+    return RB_OK;
+  }
+  if (!c->amr_graph || c->amr_chunk != chunk) {
+    if (c->amr_graph) cudaGraphExecDestroy(c->amr_graph);
+    c->amr_graph = nullptr;
+    cudaGraph_t g;
+    RB_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = RB_OK;
+    for (int k = 0; k < chunk && rc == RB_OK; k++) rc = coarse_step_dev(c);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return fail(RB_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&c->amr_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      c->amr_graph = nullptr;
+      return fail(RB_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+    }
+    c->amr_chunk = chunk;
+  }
+  RB_CUDA(cudaGraphLaunch(c->amr_graph, c->stream));
+  return RB_OK;
+}
+
+// Load the host scheduler state into the device clock; set the stop rule.
+int sched_upload(rb_context* c, int64_t max_coarse, double t_end) {
+  double* h = c->h_sched;
+  for (int i = 0; i < RB_S_SIZE; i++) h[i] = 0.0;
+  for (int l = 0; l < RB_NLV; l++) {
+    h[RB_S_DTNEW + l] = c->dtnew[l];
+    h[RB_S_DTOLD + l] = c->dtold[l];
+  }
+  h[RB_S_T] = c->t;
+  h[RB_S_NSTEP] = (double)c->nstep;
+  h[RB_S_TEND] = t_end;
+  h[RB_S_MAXC] = (double)max_coarse;
+  RB_CUDA(cudaMemcpyAsync(c->d_sched, h, RB_S_SIZE * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return RB_OK;
+}
+
+// Read the device clock back into the host scheduler state.
+int sched_download(rb_context* c, int64_t* coarse_out) {
+  RB_CUDA(cudaMemcpyAsync(c->h_sched, c->d_sched, RB_S_SIZE * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  const double* h = c->h_sched;
+  for (int l = 0; l < RB_NLV; l++) {
+    c->dtnew[l] = h[RB_S_DTNEW + l];
+    c->dtold[l] = h[RB_S_DTOLD + l];
+  }
+  c->t = h[RB_S_T];
+  c->nstep = (int64_t)h[RB_S_NSTEP];
+  c->mass_tot = h[RB_S_MASS];
+  c->ekin_tot = h[RB_S_EKIN];
+  c->eint_tot = h[RB_S_EINT];
+  if (coarse_out) *coarse_out = (int64_t)h[RB_S_COARSE];
+  return RB_OK;
+}
+
+// Asynchronous device-scheduled run (rb_run and the serving engine): begin
+// loads the stop rule and the scheduler state, each chunk enqueues up to
+// `chunk` coarse steps without waiting, end brings the state back.
+int run_async_begin(rb_context* c, double t_end, int64_t max_coarse) {
+  RB_TRY(sync_oct(c));
+  oct_changed(c);
+  int nblk = 1;
+  for (int l = 1; l <= c->mp.nlevelmax; l++)
+    if (c->lv[l].noct) nblk = std::max(nblk, courant_blocks(c, l));
+  RB_TRY(ensure_partial(c, nblk));
+  RB_TRY(sched_upload(c, max_coarse, t_end));
+  c->gate = c->d_sched + RB_S_DONE;
+  return RB_OK;
+}
+
+int run_async_chunk(rb_context* c, int chunk, bool use_graph) { return enqueue_chunk(c, chunk, use_graph); }
+
+int run_async_end(rb_context* c, int64_t* coarse_out) {
+  c->gate = nullptr;
+  int64_t coarse = 0;
+  RB_TRY(sched_download(c, &coarse));
+  c->cell_updates += coarse * updates_per_coarse(c, c->mp.levelmin);
+  c->clock_valid = false;
+  if (coarse_out) *coarse_out = coarse;
+  return RB_OK;
+}
+
+}  // namespace rbi
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -852,9 +844,10 @@ int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision
   if ((rc = dalloc(&c->d_uold, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_unew, (size_t)c->ncell * 5)) ||
       (rc = dalloc(&c->d_son, (size_t)c->ncell)) || (rc = dalloc(&c->d_corr_slot, (size_t)mp->ngridmax)) ||
       (rc = dalloc(&c->d_stage, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_red, 8)) ||
-      (rc = dalloc(&c->d_clock, 8)))
+      (rc = dalloc(&c->d_clock, 8)) || (rc = dalloc(&c->d_sched, RB_S_SIZE)))
     return bail(rc);
-  if (cudaMallocHost((void**)&c->h_red, 8 * sizeof(double)) != cudaSuccess)
+  if (cudaMallocHost((void**)&c->h_red, 8 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void**)&c->h_sched, RB_S_SIZE * sizeof(double)) != cudaSuccess)
     return bail(fail(RB_ERR_NOMEM, "pinned allocation failed"));
   if (cudaMemsetAsync(c->d_uold, 0, (size_t)c->ncell * 5 * sizeof(double), c->stream) != cudaSuccess ||
       cudaMemsetAsync(c->d_unew, 0, (size_t)c->ncell * 5 * sizeof(double), c->stream) != cudaSuccess ||
@@ -873,8 +866,9 @@ int rb_destroy(rb_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_tree(c);
   dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son); dfree(c->d_corr_slot);
-  dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock);
+  dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
   if (c->h_red) cudaFreeHost(c->h_red);
+  if (c->h_sched) cudaFreeHost(c->h_sched);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
   c->evpool.clear();
   drop_graph(c);
@@ -976,6 +970,34 @@ int rb_coarse_step(rb_context* c, double* t_io, double* dtnew_out) {
   if (dtnew_out)
     for (int l = 1; l <= c->mp.nlevelmax; l++) dtnew_out[l - 1] = c->dtnew[l];
   c->clock_valid = false;
+  return RB_OK;
+}
+
+int rb_run(rb_context* c, int max_steps, double t_end, int use_graph, double* t_io, int* steps_done) {
+  if (steps_done) *steps_done = 0;
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  if (max_steps < 0) return fail(RB_ERR_INVALID, "max_steps=%d must be non-negative", max_steps);
+  if (std::isnan(t_end)) return fail(RB_ERR_INVALID, "t_end is NaN");
+  if (t_io) c->t = *t_io;
+  struct GateScope {
+    rb_context* c;
+    ~GateScope() { c->gate = nullptr; }
+  } scope{c};
+  RB_TRY(run_async_begin(c, t_end, max_steps));
+  const int chunk = std::max(1, std::min(max_steps, 8));
+  for (int64_t launched = 0; launched < max_steps;) {
+    RB_TRY(run_async_chunk(c, chunk, use_graph != 0));
+    launched += chunk;
+    RB_CUDA(cudaMemcpyAsync(c->h_sched, c->d_sched, RB_S_SIZE * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+    const double* h = c->h_sched;
+    if (!(h[RB_S_T] < h[RB_S_TEND]) || !(h[RB_S_COARSE] < h[RB_S_MAXC])) break;
+  }
+  int64_t coarse = 0;
+  RB_TRY(run_async_end(c, &coarse));
+  if (t_io) *t_io = c->t;
+  if (steps_done) *steps_done = (int)coarse;
   return RB_OK;
 }
 
@@ -1084,7 +1106,8 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
     RB_TRY(build_level_tables(c, l, c->idx));
     if (L.ninterp) {
       rb::interp_blocks_kernel<<<(L.ninterp + 127) / 128, 128, 0, c->stream>>>(c->d_uold, L.d_interp7, L.ninterp,
-                                                                               c->ncell, L.d_interp_buf, c->hp);
+                                                                               c->ncell, L.d_interp_buf, c->hp,
+                                                                               nullptr);
       RB_CUDA(cudaGetLastError());
     }
     RB_CUDA(cudaMemcpyAsync(c->d_stage, keep_unew, (size_t)c->ncell * 5 * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -1133,7 +1156,7 @@ static int uniform_run_tiles(rb_context* c, int nsteps, int use_graph, double* t
     const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
     RB_TRY(ensure_partial(c, nblk));
     rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial, nullptr);
     RB_CUDA(cudaGetLastError());
     rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, dt_max, dt0, 1, c->d_red, 0);
     RB_CUDA(cudaGetLastError());
@@ -1261,7 +1284,7 @@ static int uniform_run_dense(rb_context* c, int nsteps, int use_graph, double* t
   if (!c->clock_valid) {
     const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
     rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial, nullptr);
     RB_CUDA(cudaGetLastError());
     rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, dt_max, dt0, 1, c->d_red, 0);
     RB_CUDA(cudaGetLastError());
@@ -1384,7 +1407,7 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
     const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
     RB_TRY(ensure_partial(c, nblk));
     rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial);
+                                                                c->mp.ncoarse, L.dx, c->hp, c->d_partial, nullptr);
     RB_CUDA(cudaGetLastError());
     rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, d, c->hp.courant_factor * L.dx / c->hp.smallc, 1, c->d_red + 4, 0);
     RB_CUDA(cudaGetLastError());
@@ -1440,6 +1463,23 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
   if (shape_out) *shape_out = best_s;
   if (hz_out) *hz_out = best_hz;
   if (ms_out) *ms_out = best_ms;
+  return RB_OK;
+}
+
+int rb_set_stream_shape(rb_context* c, int shape, int hz) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  const int lf = c->finest;
+  if (!c->have_tree || lf < 1 || !c->lv[lf].complete)
+    return fail(RB_ERR_STATE, "the z-streaming kernel needs a uniform grid");
+  if (shape < 0 || shape >= rb::kNumStreamShapes) return fail(RB_ERR_INVALID, "stream shape %d out of range", shape);
+  RB_TRY(dense_prepare(c));
+  if (!stream_shape_fits(c, shape)) return fail(RB_ERR_INVALID, "stream shape %d does not tile the grid", shape);
+  if (hz < 2 || hz % 2 != 0 || c->dnz % hz != 0)
+    return fail(RB_ERR_INVALID, "hz=%d must be even and divide nz=%d", hz, c->dnz);
+  c->stream_shape = shape;
+  c->stream_hz = hz;
+  c->stream_items = stream_items_of(c, shape, hz);
+  drop_graph(c);
   return RB_OK;
 }
 

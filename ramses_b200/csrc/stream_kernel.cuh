@@ -68,10 +68,9 @@ struct StreamGeom {
 
 __device__ __forceinline__ int pmod(int a, int m) { return ((a % m) + m) % m; }
 
-// MINB: CTAs per SM the register allocation must allow (the register budget
-// knob of the autotuner).
-template <typename R, int TX, int TY, int MINB>
-__global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_kernel(StreamArgs a) {
+// One work item (TX x TY column, z range) of one problem.
+template <typename R, int TX, int TY>
+__device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int item) {
   using G = StreamGeom<R, TX, TY>;
   constexpr int SX = G::SX, SY = G::SY, CX = G::CX, NS = G::NS, NC = G::NC;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -88,7 +87,6 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
   const int cx = valid ? tid % CX - 1 : -1, cy = valid ? tid / CX - 1 : -1;
   const bool inner = valid && cx >= 0 && cx < TX && cy >= 0 && cy < TY;
   const int nxt = a.nx / TX, nyt = a.ny / TY;
-  const int item = blockIdx.x;
   const int tx0 = (item % nxt) * TX, ty0 = ((item / nxt) % nyt) * TY, z0 = (item / (nxt * nyt)) * a.hz;
   const int zend = z0 + a.hz;                        // planes [z0, zend) are updated
   const int64_t plane = (int64_t)a.nx * a.ny;
@@ -294,6 +292,49 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_k
     a.partial[(int64_t)item * 4 + 2] = 0.0;
     a.partial[(int64_t)item * 4 + 3] = 0.0;
   }
+}
+
+// One step of one problem: one CTA per work item.
+// MINB: CTAs per SM the register allocation must allow (the register budget
+// knob of the autotuner).
+template <typename R, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_kernel(StreamArgs a) {
+  stream_step_body<R, TX, TY>(a, blockIdx.x);
+}
+
+// Problem descriptor of the batched (serving) step. The problem's device
+// clock holds (dt, t, -, -, -, steps, done, -): the kernel reads dt from it,
+// picks the current buffer from the step parity and skips finished problems.
+struct BatchDesc {
+  StreamArgs a;          // geometry, partial slice and parameters of the problem
+  double* dense[2];      // the two state buffers
+  double* clock;         // [8]
+  double t_end;          // stop rule: t >= t_end or steps >= max_steps
+  double max_steps;
+  double dt_max, dt0;    // boxlen/smallc and courant_factor*dx/smallc
+  int32_t parity0;       // buffer holding the state when the clock read 0 steps
+  int32_t nitems;
+};
+
+// One round of the serving engine: the work items of every active problem in
+// one launch. item_off[p] .. item_off[p+1]-1 are problem p's items.
+template <typename R, int TX, int TY, int MINB>
+__global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB)
+    stream_batch_kernel(const BatchDesc* __restrict__ desc, const int32_t* __restrict__ item_off, int nprob) {
+  const int b = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {  // last p with item_off[p] <= b
+    const int mid = (lo + hi + 1) >> 1;
+    if (item_off[mid] <= b) lo = mid; else hi = mid - 1;
+  }
+  const BatchDesc& d = desc[lo];
+  if (d.clock[6] != 0.0) return;  // finished: the state stays where it is
+  StreamArgs a = d.a;
+  const int cur = (d.parity0 + (int)d.clock[5]) & 1;
+  a.uin = d.dense[cur];
+  a.uout = d.dense[cur ^ 1];
+  a.dt_dev = d.clock;
+  stream_step_body<R, TX, TY>(a, b - item_off[lo]);
 }
 
 }  // namespace rb

@@ -6,4 +6,5 @@
 #define RB_TILE_SMEM tile_smem_f64
 #define RB_STREAM_LAUNCH launch_stream_f64
 #define RB_STREAM_SMEM stream_smem_f64
+#define RB_BATCH_LAUNCH launch_batch_f64
 #include "tile_instances.inc"

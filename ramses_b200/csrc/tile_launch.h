@@ -39,5 +39,11 @@ cudaError_t launch_stream_f64(int shape, const StreamArgs& a, int grid, cudaStre
 cudaError_t launch_stream_mixed(int shape, const StreamArgs& a, int grid, cudaStream_t s);
 size_t stream_smem_f64(int shape);
 size_t stream_smem_mixed(int shape);
+// batched z-streaming step over many problems (serving)
+struct BatchDesc;
+cudaError_t launch_batch_f64(int shape, const BatchDesc* desc, const int32_t* item_off, int nprob, int grid,
+                             cudaStream_t s);
+cudaError_t launch_batch_mixed(int shape, const BatchDesc* desc, const int32_t* item_off, int nprob, int grid,
+                               cudaStream_t s);
 
 }  // namespace rb

@@ -6,4 +6,5 @@
 #define RB_TILE_SMEM tile_smem_mixed
 #define RB_STREAM_LAUNCH launch_stream_mixed
 #define RB_STREAM_SMEM stream_smem_mixed
+#define RB_BATCH_LAUNCH launch_batch_mixed
 #include "tile_instances.inc"

@@ -73,6 +73,7 @@ _PROTOS = {
     "rb_upload_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_courant_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _PD, _PD, _PD, _PD]),
     "rb_coarse_step": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
+    "rb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _PD, _P32]),
     "rb_cell_updates": (ctypes.c_int, [ctypes.c_void_p, _P64]),
     "rb_set_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "rb_get_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P32]),
@@ -84,6 +85,18 @@ _PROTOS = {
     "rb_set_uniform_method": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_get_uniform_info": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32]),
     "rb_autotune_uniform": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, ctypes.POINTER(ctypes.c_float)]),
+    "rb_set_stream_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "rb_server_create": (ctypes.c_int, [ctypes.POINTER(HydroParamsC), ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "rb_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_server_submit_dense": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_double, _PD, ctypes.c_double, ctypes.c_int64, _PD, _P64]),
+    "rb_server_submit_octree": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MeshParamsC), _P32, _P32, _P32,
+                                               _P32, _P32, _PD, ctypes.c_double, ctypes.c_int64, _PD, _P64]),
+    "rb_server_progress": (ctypes.c_int, [ctypes.c_void_p, _P64, ctypes.c_int, _P32]),
+    "rb_server_request_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, _P32, _PD, _P64, _P64, _PD]),
+    "rb_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    "rb_server_stats": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P64, _P64, _P64, _P64]),
     "rb_get_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     "rb_last_kernel_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "rb_last_run_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
@@ -254,6 +267,16 @@ class Solver:
         self.last_dtnew = list(dts)
         return self.t
 
+    def run(self, t_end: float = float("inf"), max_steps: int = 1 << 30, graph: bool = True) -> int:
+        """Coarse steps until t >= t_end or max_steps steps (adaptive_loop over
+        amr_step) with the scheduler state on the device; returns the steps taken."""
+        t = ctypes.c_double(self.t)
+        n = ctypes.c_int32()
+        _check(load().rb_run(self._h, int(max_steps), float(t_end), 1 if graph else 0, ctypes.byref(t),
+                             ctypes.byref(n)), "rb_run")
+        self.t = t.value
+        return n.value
+
     def uniform_run(self, nsteps: int, graph: bool = True) -> float:
         t = ctypes.c_double(self.t)
         dt = ctypes.c_double()
@@ -279,6 +302,10 @@ class Solver:
         _check(load().rb_autotune_uniform(self._h, ctypes.byref(s), ctypes.byref(hz), ctypes.byref(ms)),
                "rb_autotune_uniform")
         return {"shape": s.value, "hz": hz.value, "ms": ms.value}
+
+    def set_stream_shape(self, shape: int, hz: int):
+        """Fix the z-streaming column shape and z extent (no autotuning)."""
+        _check(load().rb_set_stream_shape(self._h, int(shape), int(hz)), "rb_set_stream_shape")
 
     def uniform_info(self) -> dict:
         v = [ctypes.c_int32() for _ in range(4)]
