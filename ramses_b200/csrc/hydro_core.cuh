@@ -298,6 +298,16 @@ __device__ __forceinline__ void riemann(const R ql[5], const R qr[5], const Cons
   else riemann_llf(ql, qr, c, f);
 }
 
+// Riemann solver fixed at compile time (RS = RB_RIEMANN_*), or chosen at run
+// time from c.riemann when RS == 0.
+template <typename R, int RS>
+__device__ __forceinline__ void riemann_sel(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  if (RS == RB_RIEMANN_HLLC) riemann_hllc(ql, qr, c, f);
+  else if (RS == RB_RIEMANN_HLL) riemann_hll(ql, qr, c, f);
+  else if (RS == RB_RIEMANN_LLF) riemann_llf(ql, qr, c, f);
+  else riemann(ql, qr, c, f);
+}
+
 // Face frame permutation of cmpflxm (umuscl.f90:745-790): normal velocity of
 // direction d is variable 1+d; the tangential ones are the remaining two in
 // ascending order.

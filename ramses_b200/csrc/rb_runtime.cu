@@ -1388,6 +1388,7 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
   const int lf = c->finest;
   if (!c->have_tree || !c->have_state || lf < 1 || !c->lv[lf].complete)
     return fail(RB_ERR_STATE, "autotuning needs a uniform grid with its state uploaded");
+  if (c->hp.slope_type == 3) return fail(RB_ERR_STATE, "slope_type 3 runs on the oct tiles only");
   Level& L = c->lv[lf];
   RB_TRY(dense_prepare(c));
   if (c->stream_shape < 0) return fail(RB_ERR_STATE, "grid too small for the z-streaming kernel");
@@ -1471,6 +1472,7 @@ int rb_set_stream_shape(rb_context* c, int shape, int hz) {
   const int lf = c->finest;
   if (!c->have_tree || lf < 1 || !c->lv[lf].complete)
     return fail(RB_ERR_STATE, "the z-streaming kernel needs a uniform grid");
+  if (c->hp.slope_type == 3) return fail(RB_ERR_STATE, "slope_type 3 runs on the oct tiles only");
   if (shape < 0 || shape >= rb::kNumStreamShapes) return fail(RB_ERR_INVALID, "stream shape %d out of range", shape);
   RB_TRY(dense_prepare(c));
   if (!stream_shape_fits(c, shape)) return fail(RB_ERR_INVALID, "stream shape %d does not tile the grid", shape);
@@ -1493,16 +1495,20 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
     return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
   for (int l = 1; l < lf; l++)
     if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
-  if (c->uniform_method == 0) return uniform_run_dense(c, nsteps, use_graph, t_io, dt_last_out);
+  // the multi-dimensional limiter (slope_type 3) reads the 26 neighbours of
+  // every cell, which the z-streaming kernel does not hold: oct tiles only
+  if (c->uniform_method == 0 && c->hp.slope_type != 3)
+    return uniform_run_dense(c, nsteps, use_graph, t_io, dt_last_out);
   return uniform_run_tiles(c, nsteps, use_graph, t_io, dt_last_out);
 }
 
 int rb_get_uniform_info(rb_context* c, int* method, int* shape, int* hz, int* items) {
   if (!c) return fail(RB_ERR_INVALID, "null context");
-  if (method) *method = c->uniform_method;
-  if (shape) *shape = c->uniform_method == 0 ? c->stream_shape : (c->finest ? c->lv[c->finest].shape : -1);
-  if (hz) *hz = c->stream_hz;
-  if (items) *items = c->uniform_method == 0 ? c->stream_items : (c->finest ? c->lv[c->finest].ntile : 0);
+  const int m = (c->uniform_method == 0 && c->hp.slope_type != 3) ? 0 : 1;
+  if (method) *method = m;
+  if (shape) *shape = m == 0 ? c->stream_shape : (c->finest ? c->lv[c->finest].shape : -1);
+  if (hz) *hz = m == 0 ? c->stream_hz : 0;
+  if (items) *items = m == 0 ? c->stream_items : (c->finest ? c->lv[c->finest].ntile : 0);
   return RB_OK;
 }
 

@@ -287,8 +287,8 @@ int launch_round(rb_server* s) {
     RB_CUDA(cudaMemcpyAsync(s->d_off, ho, (nprob + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, s->stream));
     for (int st = 0; st < s->steps_per_round; st++) {
       cudaError_t e = s->precision == RB_PREC_MIXED
-                          ? rb::launch_batch_mixed(s->shape, s->d_desc, s->d_off, nprob, nitems, s->stream)
-                          : rb::launch_batch_f64(s->shape, s->d_desc, s->d_off, nprob, nitems, s->stream);
+                          ? rb::launch_batch_mixed(s->shape, s->hp, s->d_desc, s->d_off, nprob, nitems, s->stream)
+                          : rb::launch_batch_f64(s->shape, s->hp, s->d_desc, s->d_off, nprob, nitems, s->stream);
       if (e != cudaSuccess) return fail(RB_ERR_CUDA, "batched step launch failed: %s", cudaGetErrorString(e));
       rb::batch_clock_kernel<<<nprob, RB_RED_NT, 0, s->stream>>>(s->d_desc, s->d_off);
       RB_CUDA(cudaGetLastError());
@@ -411,6 +411,9 @@ int rb_server_create(const rb_hydro_params* hp, int precision, int64_t hbm_budge
   mp.nvector = 1;
   mp.boxlen = 1.0;
   RB_TRY(check_params(hp, &mp));  // the parameter rules of rb_create
+  if (hp->slope_type == 3)
+    return fail(RB_ERR_INVALID, "slope_type 3 (multi-dimensional limiter) is not served: dense problems run the "
+                                "z-streaming kernel, which holds axis neighbours only");
   if (precision != RB_PREC_FP64 && precision != RB_PREC_MIXED)
     return fail(RB_ERR_INVALID, "precision must be RB_PREC_FP64 or RB_PREC_MIXED");
   if (rb_device_count() == 0) return fail(RB_ERR_NO_DEVICE, "no CUDA device visible");
@@ -446,8 +449,9 @@ int rb_server_create(const rb_hydro_params* hp, int precision, int64_t hbm_budge
   s->free_slots.reserve(kMaxSlots);
   for (int i = kMaxSlots - 1; i >= 0; i--) s->free_slots.push_back(i);
   // attribute setup of the batched kernel (shared memory size) before any capture
-  cudaError_t e = precision == RB_PREC_MIXED ? rb::launch_batch_mixed(s->shape, nullptr, nullptr, 0, 0, s->stream)
-                                             : rb::launch_batch_f64(s->shape, nullptr, nullptr, 0, 0, s->stream);
+  cudaError_t e = precision == RB_PREC_MIXED
+                      ? rb::launch_batch_mixed(s->shape, s->hp, nullptr, nullptr, 0, 0, s->stream)
+                      : rb::launch_batch_f64(s->shape, s->hp, nullptr, nullptr, 0, 0, s->stream);
   if (e != cudaSuccess) return bail(fail(RB_ERR_CUDA, "batched kernel setup failed: %s", cudaGetErrorString(e)));
   *out = s;
   return RB_OK;

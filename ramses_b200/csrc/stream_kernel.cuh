@@ -68,8 +68,10 @@ struct StreamGeom {
 
 __device__ __forceinline__ int pmod(int a, int m) { return ((a % m) + m) % m; }
 
-// One work item (TX x TY column, z range) of one problem.
-template <typename R, int TX, int TY>
+// One work item (TX x TY column, z range) of one problem. RS (Riemann solver)
+// and ST (slope type) fix the scheme at compile time; RS = 0 / ST = -1 read it
+// from a.hp at run time.
+template <typename R, int TX, int TY, int RS, int ST>
 __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int item) {
   using G = StreamGeom<R, TX, TY>;
   constexpr int SX = G::SX, SY = G::SY, CX = G::CX, NS = G::NS, NC = G::NC;
@@ -93,6 +95,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   const int64_t vstr = plane * a.nz;
   const Consts<R> c = make_consts<R>(a.hp);
   const double dt = *a.dt_dev;
+  const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
   const R dtdx = (R)(dt / a.dx);
   const R dtd[3] = {dtdx, dtdx, dtdx};
 
@@ -178,9 +181,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 #pragma unroll
       for (int v = 0; v < 5; v++) {
         const R* qv = qk + v * NS;
-        dq[v][0] = slope1<R>(qv[sxm], own[v], qv[sxp], a.hp.slope_type, c.slope_theta);
-        dq[v][1] = slope1<R>(qv[sym], own[v], qv[syp], a.hp.slope_type, c.slope_theta);
-        dq[v][2] = slope1<R>(zm[v], own[v], zp[v], a.hp.slope_type, c.slope_theta);
+        dq[v][0] = slope1<R>(qv[sxm], own[v], qv[sxp], slope_type, c.slope_theta);
+        dq[v][1] = slope1<R>(qv[sym], own[v], qv[syp], slope_type, c.slope_theta);
+        dq[v][2] = slope1<R>(zm[v], own[v], zp[v], slope_type, c.slope_theta);
       }
     }
     Prim<R> sp[3], sm[3];
@@ -202,7 +205,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
       R ql[5], qr[5], fg[6];
       to_face(L, 0, ql);
       to_face(sp[0], 0, qr);
-      riemann<R>(ql, qr, c, fg);
+      riemann_sel<R, RS>(ql, qr, c, fg);
       from_face(fg, 0, fx);
     }
     if (upd_plane && valid && cy >= 0 && cx >= 0 && cx < TX) {
@@ -212,14 +215,14 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
       R ql[5], qr[5], fg[6];
       to_face(L, 1, ql);
       to_face(sp[1], 1, qr);
-      riemann<R>(ql, qr, c, fg);
+      riemann_sel<R, RS>(ql, qr, c, fg);
       from_face(fg, 1, fy);
     }
     if (inner && k >= z0) {
       R ql[5], qr[5], fg[6];
       to_face(qmz_prev, 2, ql);
       to_face(sp[2], 2, qr);
-      riemann<R>(ql, qr, c, fg);
+      riemann_sel<R, RS>(ql, qr, c, fg);
       from_face(fg, 2, fz);
     }
     qmz_prev = sm[2];
@@ -297,9 +300,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 // One step of one problem: one CTA per work item.
 // MINB: CTAs per SM the register allocation must allow (the register budget
 // knob of the autotuner).
-template <typename R, int TX, int TY, int MINB>
+template <typename R, int TX, int TY, int MINB, int RS, int ST>
 __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB) stream_step_kernel(StreamArgs a) {
-  stream_step_body<R, TX, TY>(a, blockIdx.x);
+  stream_step_body<R, TX, TY, RS, ST>(a, blockIdx.x);
 }
 
 // Problem descriptor of the batched (serving) step. The problem's device
@@ -318,7 +321,7 @@ struct BatchDesc {
 
 // One round of the serving engine: the work items of every active problem in
 // one launch. item_off[p] .. item_off[p+1]-1 are problem p's items.
-template <typename R, int TX, int TY, int MINB>
+template <typename R, int TX, int TY, int MINB, int RS, int ST>
 __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB)
     stream_batch_kernel(const BatchDesc* __restrict__ desc, const int32_t* __restrict__ item_off, int nprob) {
   const int b = blockIdx.x;
@@ -334,7 +337,7 @@ __global__ void __launch_bounds__(StreamGeom<R, TX, TY>::NT, MINB)
   a.uin = d.dense[cur];
   a.uout = d.dense[cur ^ 1];
   a.dt_dev = d.clock;
-  stream_step_body<R, TX, TY>(a, b - item_off[lo]);
+  stream_step_body<R, TX, TY, RS, ST>(a, b - item_off[lo]);
 }
 
 }  // namespace rb

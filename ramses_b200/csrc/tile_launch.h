@@ -5,6 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstddef>
+#include <cstdint>
+
+#include "rb_types.h"
 
 namespace rb {
 
@@ -41,9 +44,9 @@ size_t stream_smem_f64(int shape);
 size_t stream_smem_mixed(int shape);
 // batched z-streaming step over many problems (serving)
 struct BatchDesc;
-cudaError_t launch_batch_f64(int shape, const BatchDesc* desc, const int32_t* item_off, int nprob, int grid,
-                             cudaStream_t s);
-cudaError_t launch_batch_mixed(int shape, const BatchDesc* desc, const int32_t* item_off, int nprob, int grid,
-                               cudaStream_t s);
+cudaError_t launch_batch_f64(int shape, const rb_hydro_params& hp, const BatchDesc* desc, const int32_t* item_off,
+                             int nprob, int grid, cudaStream_t s);
+cudaError_t launch_batch_mixed(int shape, const rb_hydro_params& hp, const BatchDesc* desc,
+                               const int32_t* item_off, int nprob, int grid, cudaStream_t s);
 
 }  // namespace rb

@@ -172,6 +172,21 @@ def test_stream_kernel_equals_tiles_fp64(cuda_lib, level, slope_type):
         assert a.t == b.t
 
 
+@pytest.mark.parametrize("riemann", RIEMANNS)
+@pytest.mark.parametrize("slope_type", SLOPES)
+def test_stream_kernel_every_solver_and_slope(cuda_lib, riemann, slope_type):
+    """Every Riemann solver and slope type through the uniform-grid path
+    (slope_type 3 is routed to the oct tiles) equals the oct tiles, FP64."""
+    tree, hp, u = turbulent_uniform(4, slope_type=slope_type, riemann=riemann)
+    with runtime.Solver(tree, hp, uold=u) as a, runtime.Solver(tree, hp, uold=u) as b:
+        a.set_uniform_method("tiles")
+        b.set_uniform_method("stream")
+        a.uniform_run(3, graph=False)
+        b.uniform_run(3, graph=True)
+        np.testing.assert_array_equal(a.download_state(), b.download_state())
+        assert (b.uniform_info()["method"] == "tiles") == (slope_type == 3)
+
+
 def test_stream_kernel_matches_oracle(cuda_lib, oracle_lib):
     tree, hp, u = sedov_uniform(5, riemann="hllc", slope_type=1)
     orc = oracle.OracleRun(tree, hp, u)
