@@ -56,11 +56,13 @@ struct StreamGeom {
   static constexpr int NS = SX * SY;
   static constexpr int NEXTRA = NS - NC;                // q-only outer ring columns
   static constexpr int NRAW = 5;                        // raw planes in flight
-  static constexpr int NQ = 3;                          // primitive planes in shared memory
+  static constexpr int NQ = 2;                          // primitive planes in shared memory
   static constexpr int CHUNKS = 5 * SY * (SX / 2);      // 16-byte chunks per raw plane
   static constexpr size_t RAW_BYTES = sizeof(double) * NRAW * 5 * NS;
   static constexpr size_t Q_BYTES = sizeof(R) * NQ * 5 * NS;
-  static constexpr size_t X_BYTES = sizeof(double) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;  // Fx, Fy; qm_x, qm_y
+  // Fx, Fy (face fluxes times dt/dx, stored in R: in the mixed path they are
+  // FP32 products, widened to FP64 exactly on read) and qm_x, qm_y
+  static constexpr size_t X_BYTES = sizeof(R) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;
   static constexpr size_t SMEM = RAW_BYTES + Q_BYTES + X_BYTES;
   static_assert(NEXTRA <= NC, "one extra column per thread at most");
   static_assert(TX % 2 == 0 && TY % 2 == 0, "even tile");
@@ -78,9 +80,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* raw = reinterpret_cast<double*>(smem_raw);                      // [NRAW][5][NS]
   R* qb = reinterpret_cast<R*>(smem_raw + G::RAW_BYTES);                  // [NQ][5][NS]
-  double* fxs = reinterpret_cast<double*>(qb + G::NQ * 5 * NS);           // [5][NC] Fx (left face)
-  double* fys = fxs + 5 * NC;                                             // [5][NC] Fy (lower face)
-  R* xm = reinterpret_cast<R*>(fys + 5 * NC);                             // [5][NC] qm_x
+  R* fxs = qb + G::NQ * 5 * NS;                                           // [5][NC] Fx (left face)
+  R* fys = fxs + 5 * NC;                                                  // [5][NC] Fy (lower face)
+  R* xm = fys + 5 * NC;                                                   // [5][NC] qm_x
   R* ym = xm + 5 * NC;                                                    // [5][NC] qm_y
   __shared__ double red[G::NT / 32];
 
@@ -163,12 +165,6 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 
   for (int k = z0 - 1; k <= zend; k++) {
     const bool upd_plane = (k >= z0) && (k < zend);  // x/y fluxes and partial update at k
-    // A. ctoprim of plane k+2
-    if (k + 2 <= zend + 1) {
-      q_p2 = to_q(k + 2, s_own);
-      if (valid) put_q(k + 2, s_own, q_p2);
-      if (has_extra) put_q(k + 2, s_ext, to_q(k + 2, s_ext));
-    }
     // B. slopes and trace of plane k
     const R* qk = qb + ((k - zbase) % G::NQ) * 5 * NS;
     R dq[5][3];
@@ -196,6 +192,14 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     __syncthreads();
     if (k + 4 <= zend + 1) issue_plane(k + 4);
     cp_async_commit();
+    // A. ctoprim of plane k+2, into the primitive slot of plane k, which
+    // every thread has finished reading at the barrier above; plane k+2 landed
+    // at the previous iteration's wait
+    if (k + 2 <= zend + 1) {
+      q_p2 = to_q(k + 2, s_own);
+      if (valid) put_q(k + 2, s_own, q_p2);
+      if (has_extra) put_q(k + 2, s_ext, to_q(k + 2, s_ext));
+    }
     // C. Riemann problems
     R fx[5] = {0, 0, 0, 0, 0}, fy[5] = {0, 0, 0, 0, 0}, fz[5] = {0, 0, 0, 0, 0};
     if (upd_plane && valid && cx >= 0 && cy >= 0 && cy < TY) {
@@ -231,12 +235,12 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     // Each face flux is rounded to FP64 once, by the face's owner, so that the
     // FP64 accumulation below telescopes exactly (conservation to FP64
     // roundoff in both precisions).
-    auto scale = [&](R f) -> double {
+    auto scale = [&](R f) -> R {
       if (sizeof(R) == 8) {
         const double t = (double)f * dt;
-        return a.dx_pow2 ? t * a.inv_dx : t / a.dx;
+        return (R)(a.dx_pow2 ? t * a.inv_dx : t / a.dx);
       }
-      return (double)(f * dtdx);
+      return f * dtdx;
     };
     double fzd[5];
     if (upd_plane && valid) {
@@ -248,7 +252,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     }
     if (inner && k >= z0) {
 #pragma unroll
-      for (int v = 0; v < 5; v++) fzd[v] = scale(fz[v]);
+      for (int v = 0; v < 5; v++) fzd[v] = (double)scale(fz[v]);
     }
     cp_async_wait<1>();  // plane k+3 (converted at the next A) has landed
     __syncthreads();
@@ -270,8 +274,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
-          u = u + (fxs[v * NC + tid] - fxs[v * NC + tid + 1]);
-          u = u + (fys[v * NC + tid] - fys[v * NC + tid + CX]);
+          u = u + ((double)fxs[v * NC + tid] - (double)fxs[v * NC + tid + 1]);
+          u = u + ((double)fys[v * NC + tid] - (double)fys[v * NC + tid + CX]);
           upd[v] = u;
           fzb[v] = fzd[v];
         }
