@@ -61,6 +61,9 @@ def parse():
     ap.add_argument("--stream-config", default=None, metavar="SHAPE,HZ",
                     help="z-streaming method: use this column shape and z extent instead of autotuning "
                          "(profiling runs replay the autotuned choice without its probe launches)")
+    ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
+                    help="instead of the headline, time device-scheduled coarse steps (rb_run) on a static AMR "
+                         "tree: sedov = Sedov levels 6-9 refined on a shell, clumps = blast-clump levels 7-10")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
                     help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
@@ -232,10 +235,80 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def amr_workload(name):
+    """Static AMR trees of the Sedov and blast-clump configurations.
+    sedov: levels 6-9; levels 7-9 on a shell of radius 0.25 around the box
+    centre (where the shock of E=1 in rho=1 sits near t=0.02) plus the
+    initial blast region; the blast starts at t=0. clumps: levels 7-10 refined
+    on the relative density/pressure gradient 0.05 of the initial state."""
+    from ramses_b200 import ics, mesh
+    from ramses_b200.params import HydroParams
+    if name == "sedov":
+        lmin, lmax = 6, 9
+        hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+        prim = ics.sedov_prim(lmax)
+        ref = mesh.union_refine(mesh.shell_refine((0.5, 0.5, 0.5), 0.25, 2.5),
+                                mesh.sphere_refine((0.5, 0.5, 0.5), 2.5 * 0.5 ** lmax))
+        desc = ("Sedov E=1, rho=1, P=1e-5, levels 6-9 (static: shell of radius 0.25 and the blast region), "
+                "hllc, slope_type=1, courant 0.8, nsubcycle 2")
+    else:
+        lmin, lmax = 7, 10
+        hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=2, courant_factor=0.8)
+        prim = ics.blast_clumps_prim()
+
+        def fields(x):
+            q = prim(x)
+            return [q[0], q[4]]
+        ref = mesh.gradient_refine(fields, [0.05, 0.05])
+        desc = ("blast-clump: 32 seeded clumps (contrast 100) + Sedov E=10, levels 7-10 (static: gradient 0.05 "
+                "of the initial state), hllc, slope_type=2, courant 0.8, nsubcycle 2")
+    tree = mesh.build_tree(lmin, lmax, ref)
+    return tree, hp, ics.fill_all_levels(tree, prim, hp.gamma), desc
+
+
+def run_amr(args):
+    """Leaf-cell updates/s of rb_run (device-scheduled coarse steps from CUDA
+    graphs) on a static AMR tree, FP32-mixed and FP64."""
+    from ramses_b200 import runtime
+    runtime.load()
+    t0 = time.perf_counter()
+    tree, hp, u, desc = amr_workload(args.amr)
+    build_s = time.perf_counter() - t0
+    levels = [l for l in range(1, tree.nlevelmax + 1) if tree.noct(l)]
+    out = {}
+    for prec in ("mixed", "fp64"):
+        s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
+        for l in levels:
+            s.set_tile_shape(l, -1)
+        s.run(max_steps=args.warmup)
+        s.synchronize()
+        before = s.cell_updates
+        with ClockSampler(0) as clk:
+            time.sleep(0.3)
+            n = s.run(max_steps=args.steps)
+            s.synchronize()
+        ms = s.last_run_ms()
+        upd = s.cell_updates - before
+        out[prec] = {"value": upd / (ms / 1e3), "ms_per_coarse_step": ms / max(n, 1), "coarse_steps": n,
+                     "t": s.t, "tile_shapes": {l: s.tile_shape(l) for l in levels}, "clocks": clk.summary()}
+        s.close()
+    line = {"metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["mixed"]["ms_per_coarse_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": desc, "octs_per_level": {l: tree.noct(l) for l in levels},
+                       "leaf_cells": int(sum(tree.leaf_cells(l) for l in levels)), "path": "rb_run, graphs of 8 "
+                       "coarse steps, tile shapes autotuned per level", "tree_build_s": build_s},
+            "fp64": out["fp64"], "mixed": out["mixed"], "clocks": out["mixed"]["clocks"],
+            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.amr:
+        return run_amr(args)
     from ramses_b200 import runtime
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -119,7 +119,8 @@ int rb_uniform_run(rb_context *ctx, int nsteps, int use_graph, double *t_io, dou
 
 /* Kernel used by rb_uniform_run: 0 = z-streaming stencil over a dense
  * Cartesian mirror of the level (default), 1 = the godunov_fine oct tiles.
- * Both give identical results. */
+ * Both give bit-identical results in FP64 (in FP32-mixed they differ by
+ * FP32 rounding only). slope_type 3 always runs on the oct tiles. */
 int rb_set_uniform_method(rb_context *ctx, int method);
 /* Kernel configuration of the last rb_uniform_run: method, shape (z-streaming
  * column shape 0: 8x8, 1: 16x8, 2: 16x16 cells, or oct-tile shape), z extent
@@ -128,8 +129,8 @@ int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *
 /* Autotune the z-streaming step on the live state: every column shape and
  * register budget (0: 8x8, 1: 16x8, 2: 16x16, 3: 16x8 at 2 CTAs/SM, 4: 8x8 at
  * 4 CTAs/SM, 5: 16x8 at 3 CTAs/SM) and z extent 4..64 is timed; the fastest
- * is kept. The state,
- * the time and the next dt are unchanged. Outputs may be NULL. */
+ * is kept. The state, the time and the next dt are unchanged. Outputs may be
+ * NULL. */
 int rb_autotune_uniform(rb_context *ctx, int *shape, int *hz, float *ms);
 /* Set the z-streaming configuration by hand (shape as above; hz even and
  * dividing the grid's nz), e.g. to replay an autotuned choice. */
@@ -162,7 +163,7 @@ int rb_get_stream(rb_context *ctx, void **stream);
  * rb_godunov_fine call or un-graphed rb_uniform_run (CUDA events around the
  * kernel alone). */
 int rb_last_kernel_ms(rb_context *ctx, float *ms);
-/* Device milliseconds of the whole last rb_uniform_run (all steps). */
+/* Device milliseconds of the whole last rb_uniform_run or rb_run (all steps). */
 int rb_last_run_ms(rb_context *ctx, float *ms);
 
 /* ---- serving engine: many independent problems on one GPU ----------------

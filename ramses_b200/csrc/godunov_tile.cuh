@@ -74,7 +74,9 @@ constexpr size_t tile_smem_bytes() {
          sizeof(int32_t) * (size_t)G::NBLK + (size_t)((G::NS + 15) & ~15);
 }
 
-template <typename R, int TX, int TY, int TZ, int NT>
+// RS (Riemann solver) and ST (slope type) fix the scheme at compile time;
+// RS = 0 / ST = -1 read it from a.hp at run time.
+template <typename R, int TX, int TY, int TZ, int NT, int RS, int ST>
 __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   if (a.gate != nullptr && *a.gate != 0.0) return;
   using G = TileGeom<TX, TY, TZ>;
@@ -98,7 +100,8 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   __syncthreads();
 
   // ---- A. gather + ctoprim ------------------------------------------------
-  const bool slope27 = (a.hp.slope_type == 3);
+  const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
+  const bool slope27 = (slope_type == 3);
   for (int it = tid; it < NBLK * 8; it += NT) {
     const int b = it >> 3, ch = it & 7;
     const int bx = b % BX, by = (b / BX) % BY, bz = b / (BX * BY);
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     R dq[5][3];
     Prim<R> q0;
     q0.r = q[s]; q0.u = q[NS + s]; q0.v = q[2 * NS + s]; q0.w = q[3 * NS + s]; q0.p = q[4 * NS + s];
-    if (a.hp.slope_type == 0) {
+    if (slope_type == 0) {
 #pragma unroll
       for (int v = 0; v < 5; v++) { dq[v][0] = (R)0; dq[v][1] = (R)0; dq[v][2] = (R)0; }
     } else if (!slope27) {
@@ -176,7 +179,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
         const R qc = qv[s];
 #pragma unroll
         for (int d = 0; d < 3; d++)
-          dq[v][d] = slope1<R>(qv[s - st[d]], qc, qv[s + st[d]], a.hp.slope_type, c.slope_theta);
+          dq[v][d] = slope1<R>(qv[s - st[d]], qc, qv[s + st[d]], slope_type, c.slope_theta);
       }
     } else {
       // positivity-preserving multidimensional slope (umuscl.f90:1328-1392)
@@ -241,7 +244,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     R ql[5], qr[5], fg[6], fo[5];
     to_face(L, d, ql);
     to_face(Rr, d, qr);
-    riemann<R>(ql, qr, c, fg);
+    riemann_sel<R, RS>(ql, qr, c, fg);
     from_face(fg, d, fo);
     // refined interface: either neighbour cell refined -> zero flux
     const int sr = (x + 2) + SX * ((y + 2) + SY * (z + 2));

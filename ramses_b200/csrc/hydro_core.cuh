@@ -86,12 +86,13 @@ __device__ __forceinline__ Prim<R> ctoprim_cell(const double u[5], const rb_hydr
 template <typename R>
 __device__ __forceinline__ R slope1(R qm1, R q0, R qp1, int st, R theta) {
   const R zero = (R)0, half = (R)0.5, one = (R)1;
+  // minmod and van Leer are written as selects, not early returns: the same
+  // values, without divergent branches inside a warp
   if (st == 1) {
     R dlft = q0 - qm1;
     R drgt = qp1 - q0;
-    if ((dlft * drgt) <= zero) return zero;
-    if (dlft > 0) return fmn(dlft, drgt);
-    return fmx(dlft, drgt);
+    const R lim = dlft > 0 ? fmn(dlft, drgt) : fmx(dlft, drgt);
+    return (dlft * drgt) <= zero ? zero : lim;
   } else if (st == 2) {
     const R two = (R)2;
     R dlft = two * (q0 - qm1);
@@ -105,8 +106,8 @@ __device__ __forceinline__ R slope1(R qm1, R q0, R qp1, int st, R theta) {
   } else if (st == 7) {
     R dlft = (q0 - qm1);
     R drgt = (qp1 - q0);
-    if ((dlft * drgt) <= zero) return zero;
-    return ((R)2 * dlft * drgt / (dlft + drgt));
+    const R vl = ((R)2 * dlft * drgt / (dlft + drgt));  // unused (0/0 at worst) where the product is <= 0
+    return (dlft * drgt) <= zero ? zero : vl;
   } else if (st == 8) {
     R dlft = (q0 - qm1);
     R drgt = (qp1 - q0);
@@ -265,29 +266,48 @@ __device__ __forceinline__ void riemann_hllc(const R ql[5], const R qr[5], const
   R SR = fmx(ul, ur) + fmx(cfastl, cfastr);
   R rcl = rl * (ul - SL);
   R rcr = rr * (SR - ur);
-  R ustar = (rcr * ur + rcl * ul + (Ptotl - Ptotr)) / (rcr + rcl);
-  R Ptotstar = (rcr * Ptotl + rcl * Ptotr + rcl * rcr * (ul - ur)) / (rcr + rcl);
-  R ro, uo, Ptoto, etoto, eo;
-  if (SL > (R)0) {
-    ro = rl; uo = ul; Ptoto = Ptotl; etoto = etotl; eo = el;
-  } else if (ustar > (R)0) {
-    ro = rl * (SL - ul) / (SL - ustar);
-    uo = ustar; Ptoto = Ptotstar;
-    etoto = ((SL - ul) * etotl - Ptotl * ul + Ptotstar * ustar) / (SL - ustar);
-    eo = el * (SL - ul) / (SL - ustar);
-  } else if (SR > (R)0) {
-    ro = rr * (SR - ur) / (SR - ustar);
-    uo = ustar; Ptoto = Ptotstar;
-    etoto = ((SR - ur) * etotr - Ptotr * ur + Ptotstar * ustar) / (SR - ustar);
-    eo = er * (SR - ur) / (SR - ustar);
+  R ustar, Ptotstar;
+  if (sizeof(R) == 4) {  // FP32-mixed: one reciprocal for the two star quotients
+    const R inv = (R)1 / (rcr + rcl);
+    ustar = (rcr * ur + rcl * ul + (Ptotl - Ptotr)) * inv;
+    Ptotstar = (rcr * Ptotl + rcl * Ptotr + rcl * rcr * (ul - ur)) * inv;
   } else {
-    ro = rr; uo = ur; Ptoto = Ptotr; etoto = etotr; eo = er;
+    ustar = (rcr * ur + rcl * ul + (Ptotl - Ptotr)) / (rcr + rcl);
+    Ptotstar = (rcr * Ptotl + rcl * Ptotr + rcl * rcr * (ul - ur)) / (rcr + rcl);
   }
+  // Sampling at x/t = 0: the outer left state if SL > 0, else the left star
+  // state if ustar > 0, else the right star state if SR > 0, else the outer
+  // right state. Written with selects (no divergent branches): the star side
+  // is picked first and one star state is formed with the same operations as
+  // the reference's branch for that side.
+  const bool lft = ustar > (R)0;
+  const R rs = lft ? rl : rr, us = lft ? ul : ur, Ss = lft ? SL : SR;
+  const R Pts = lft ? Ptotl : Ptotr, ets = lft ? etotl : etotr, es = lft ? el : er;
+  const R num = Ss - us, den = Ss - ustar;
+  R ro_s, etoto_s, eo_s;
+  if (sizeof(R) == 4) {
+    const R inv = (R)1 / den;
+    ro_s = rs * num * inv;
+    etoto_s = (num * ets - Pts * us + Ptotstar * ustar) * inv;
+    eo_s = es * num * inv;
+  } else {
+    ro_s = rs * num / den;
+    etoto_s = (num * ets - Pts * us + Ptotstar * ustar) / den;
+    eo_s = es * num / den;
+  }
+  const bool outl = SL > (R)0;
+  const bool star = !outl && (lft || SR > (R)0);
+  const R ro = outl ? rl : (star ? ro_s : rr);
+  const R uo = outl ? ul : (star ? ustar : ur);
+  const R Ptoto = outl ? Ptotl : (star ? Ptotstar : Ptotr);
+  const R etoto = outl ? etotl : (star ? etoto_s : etotr);
+  const R eo = outl ? el : (star ? eo_s : er);
   f[0] = ro * uo;
   f[1] = ro * uo * uo + Ptoto;
   f[2] = (etoto + Ptoto) * uo;
-  if (ustar > (R)0) { f[3] = ro * uo * ql[3]; f[4] = ro * uo * ql[4]; }
-  else { f[3] = ro * uo * qr[3]; f[4] = ro * uo * qr[4]; }
+  const R t3 = lft ? ql[3] : qr[3], t4 = lft ? ql[4] : qr[4];
+  f[3] = ro * uo * t3;
+  f[4] = ro * uo * t4;
   f[5] = uo * eo;
 }
 

@@ -986,8 +986,11 @@ int rb_run(rb_context* c, int max_steps, double t_end, int use_graph, double* t_
   } scope{c};
   RB_TRY(run_async_begin(c, t_end, max_steps));
   const int chunk = std::max(1, std::min(max_steps, 8));
+  RB_CUDA(cudaEventRecord(c->ev0, c->stream));
+  RB_CUDA(cudaEventRecord(c->ev1, c->stream));
   for (int64_t launched = 0; launched < max_steps;) {
     RB_TRY(run_async_chunk(c, chunk, use_graph != 0));
+    RB_CUDA(cudaEventRecord(c->ev1, c->stream));
     launched += chunk;
     RB_CUDA(cudaMemcpyAsync(c->h_sched, c->d_sched, RB_S_SIZE * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     RB_CUDA(cudaStreamSynchronize(c->stream));
@@ -996,6 +999,7 @@ int rb_run(rb_context* c, int max_steps, double t_end, int use_graph, double* t_
   }
   int64_t coarse = 0;
   RB_TRY(run_async_end(c, &coarse));
+  RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));  // device time of all chunks
   if (t_io) *t_io = c->t;
   if (steps_done) *steps_done = (int)coarse;
   return RB_OK;

@@ -295,6 +295,23 @@ def sphere_refine(centre, radius: float, boxlen: float = 1.0, pad_cells: float =
     return refine
 
 
+def shell_refine(centre, radius: float, width_cells: float = 4.0, boxlen: float = 1.0
+                 ) -> Callable[[int, np.ndarray], np.ndarray]:
+    """Geometric refinement: flag level-``l`` cells whose centre lies within
+    ``width_cells*dx_l`` of the sphere of ``radius`` around ``centre``
+    (periodic distance): a static stand-in for refinement that follows a
+    spherical shock."""
+    c = np.asarray(centre, dtype=np.float64) * boxlen
+
+    def refine(level: int, cells: np.ndarray) -> np.ndarray:
+        dx = boxlen * 0.5 ** level
+        x = (cells + 0.5) * dx
+        d = np.abs(x - c)
+        d = np.minimum(d, boxlen - d)
+        return np.abs(np.sqrt(np.sum(d * d, axis=1)) - radius) < width_cells * dx
+    return refine
+
+
 def union_refine(*fns) -> Callable[[int, np.ndarray], np.ndarray]:
     def refine(level: int, cells: np.ndarray) -> np.ndarray:
         out = np.zeros(len(cells), dtype=bool)
