@@ -303,6 +303,37 @@ def run_amr(args):
     print(json.dumps(line), flush=True)
 
 
+class Replicas:
+    """The N>1 path: one process per GPU, each an independent replica of the
+    workload (the hydro path has no data-path collective). The only
+    collectives are a barrier around the timed region and the max over ranks
+    of the device time; the job's value is the units of all ranks divided by
+    the slowest rank's time. ``dist`` is torch.distributed (or None for one
+    process); ``device`` holds the reduction tensor ('cuda' under NCCL,
+    'cpu' under gloo)."""
+
+    def __init__(self, dist=None, device="cuda"):
+        self.dist = dist
+        self.device = device
+        self.world = dist.get_world_size() if dist is not None else 1
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_rate(self, units_per_rank: float, seconds: float) -> float:
+        """Whole-job units per second: all ranks' units over the slowest rank."""
+        return units_per_rank * self.world / self.max(seconds)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -328,17 +359,8 @@ def main():
     level = args.level
     cells = tree.leaf_cells(level)
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas(dist, "cuda")
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     if args.only:
         # one precision's timed steps only (profiling runs: one solver resident)
@@ -364,7 +386,7 @@ def main():
     run_ms = max_over_ranks(mixed.last_run_ms())
     kern_ms = mixed.last_kernel_ms()
     mixed_kernel = mixed.uniform_info()["kernel"]
-    value = cells * args.steps * world / (run_ms / 1e3)
+    value = rep.job_rate(cells * args.steps, run_ms / 1e3)
     u_mixed = mixed.download_state()
 
     # ---- FP64 drop-in path on the same steps ----------------------------
@@ -376,7 +398,7 @@ def main():
     barrier()
     f64_ms = max_over_ranks(f64.last_run_ms())
     f64_kern = f64.last_kernel_ms()
-    f64_value = cells * args.steps * world / (f64_ms / 1e3)
+    f64_value = rep.job_rate(cells * args.steps, f64_ms / 1e3)
     u_f64 = f64.download_state()
     idx = tree.cell_index(level).reshape(-1) - 1
     rm, rf = u_mixed[0, idx], u_f64[0, idx]
@@ -408,7 +430,7 @@ def main():
         mixed.download_state(out=host)
     mixed.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = cells * args.e2e_steps * world / e2e_s
+    e2e_value = rep.job_rate(cells * args.e2e_steps, e2e_s)
     mixed.close()
 
     peak, peak_kind = hbm_peak()

@@ -64,7 +64,9 @@ struct StreamGeom {
   // FP32 products, widened to FP64 exactly on read) and qm_x, qm_y
   static constexpr size_t X_BYTES = sizeof(R) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;
   static constexpr size_t SMEM = RAW_BYTES + Q_BYTES + X_BYTES;
-  static_assert(NEXTRA <= NC, "one extra column per thread at most");
+  static constexpr int NIN = TX * TY;                   // interior columns (threads 0..NIN-1)
+  static_assert(NIN % 32 == 0, "interior columns fill whole warps");
+  static_assert(NEXTRA <= NT - NIN, "the outer ring is converted by the threads after the interior");
   static_assert(TX % 2 == 0 && TY % 2 == 0, "even tile");
 };
 
@@ -86,10 +88,29 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   R* ym = xm + 5 * NC;                                                    // [5][NC] qm_y
   __shared__ double red[G::NT / 32];
 
+  // Thread -> column map. Threads 0..NIN-1 own the interior columns (they
+  // solve x, y and z faces and update). The trace ring follows in the order
+  // right column, top row (the ring columns with an x or a y face to solve),
+  // left column, bottom row, top corners (nothing to solve), so the solve and
+  // update predicates are uniform over most warps. Shared arrays are indexed
+  // by the column's slot (cx+1) + CX*(cy+1), independent of this map.
   const int tid = threadIdx.x;
   const bool valid = tid < NC;                       // padding threads own no column
-  const int cx = valid ? tid % CX - 1 : -1, cy = valid ? tid / CX - 1 : -1;
-  const bool inner = valid && cx >= 0 && cx < TX && cy >= 0 && cy < TY;
+  int cx = -1, cy = -1;
+  if (valid) {
+    if (tid < G::NIN) {
+      cx = tid % TX; cy = tid / TX;
+    } else {
+      int r = tid - G::NIN;
+      if (r < TY) { cx = TX; cy = r; }
+      else if ((r -= TY) < TX) { cx = r; cy = TY; }
+      else if ((r -= TX) < TY) { cx = -1; cy = r; }
+      else if ((r -= TY) < TX + 2) { cx = r - 1; cy = -1; }
+      else { r -= TX + 2; cx = r ? TX : -1; cy = TY; }
+    }
+  }
+  const int slot = valid ? (cx + 1) + CX * (cy + 1) : 0;
+  const bool inner = valid && tid < G::NIN;
   const int nxt = a.nx / TX, nyt = a.ny / TY;
   const int tx0 = (item % nxt) * TX, ty0 = ((item / nxt) % nyt) * TY, z0 = (item / (nxt * nyt)) * a.hz;
   const int zend = z0 + a.hz;                        // planes [z0, zend) are updated
@@ -103,9 +124,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 
   // extra (q-only) column of this thread, if any: the outer stencil ring
   int ex = 0, ey = 0;
-  const bool has_extra = tid < G::NEXTRA;
+  const bool has_extra = tid >= G::NIN && tid - G::NIN < G::NEXTRA;
   if (has_extra) {
-    int r = tid;
+    int r = tid - G::NIN;
     if (r < SX) { ex = r; ey = 0; }
     else if ((r -= SX) < SX) { ex = r; ey = SY - 1; }
     else if ((r -= SX) < SY - 2) { ex = 0; ey = 1 + r; }
@@ -185,7 +206,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     Prim<R> sp[3], sm[3];
     trace_cell<R>(q_0, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
     if (valid) {
-      const int o = tid;
+      const int o = slot;
       xm[o] = sm[0].r; xm[NC + o] = sm[0].u; xm[2 * NC + o] = sm[0].v; xm[3 * NC + o] = sm[0].w; xm[4 * NC + o] = sm[0].p;
       ym[o] = sm[1].r; ym[NC + o] = sm[1].u; ym[2 * NC + o] = sm[1].v; ym[3 * NC + o] = sm[1].w; ym[4 * NC + o] = sm[1].p;
     }
@@ -203,7 +224,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     // C. Riemann problems
     R fx[5] = {0, 0, 0, 0, 0}, fy[5] = {0, 0, 0, 0, 0}, fz[5] = {0, 0, 0, 0, 0};
     if (upd_plane && valid && cx >= 0 && cy >= 0 && cy < TY) {
-      const int o = tid - 1;  // column (cx-1, cy)
+      const int o = slot - 1;  // column (cx-1, cy)
       Prim<R> L;
       L.r = xm[o]; L.u = xm[NC + o]; L.v = xm[2 * NC + o]; L.w = xm[3 * NC + o]; L.p = xm[4 * NC + o];
       R ql[5], qr[5], fg[6];
@@ -213,7 +234,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
       from_face(fg, 0, fx);
     }
     if (upd_plane && valid && cy >= 0 && cx >= 0 && cx < TX) {
-      const int o = tid - CX;  // column (cx, cy-1)
+      const int o = slot - CX;  // column (cx, cy-1)
       Prim<R> L;
       L.r = ym[o]; L.u = ym[NC + o]; L.v = ym[2 * NC + o]; L.w = ym[3 * NC + o]; L.p = ym[4 * NC + o];
       R ql[5], qr[5], fg[6];
@@ -246,8 +267,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     if (upd_plane && valid) {
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        fxs[v * NC + tid] = scale(fx[v]);
-        fys[v * NC + tid] = scale(fy[v]);
+        fxs[v * NC + slot] = scale(fx[v]);
+        fys[v * NC + slot] = scale(fy[v]);
       }
     }
     if (inner && k >= z0) {
@@ -274,8 +295,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
-          u = u + ((double)fxs[v * NC + tid] - (double)fxs[v * NC + tid + 1]);
-          u = u + ((double)fys[v * NC + tid] - (double)fys[v * NC + tid + CX]);
+          u = u + ((double)fxs[v * NC + slot] - (double)fxs[v * NC + slot + 1]);
+          u = u + ((double)fys[v * NC + slot] - (double)fys[v * NC + slot + CX]);
           upd[v] = u;
           fzb[v] = fzd[v];
         }
