@@ -128,8 +128,7 @@ int rb_set_uniform_method(rb_context *ctx, int method);
 int rb_get_uniform_info(rb_context *ctx, int *method, int *shape, int *hz, int *items);
 /* Autotune the z-streaming step on the live state: every column shape and
  * register budget (0: 8x8, 1: 16x8, 2: 16x16, 3: 16x8 at 2 CTAs/SM, 4: 8x8 at
- * 4 CTAs/SM, 5: 16x8 at 3 CTAs/SM) and z extent 4..64 is timed; the fastest
- * is kept. The state, the time and the next dt are unchanged. Outputs may be
+ * 4 CTAs/SM) and z extent 4..64 is timed; the fastest is kept. The state, the time and the next dt are unchanged. Outputs may be
  * NULL. */
 int rb_autotune_uniform(rb_context *ctx, int *shape, int *hz, float *ms);
 /* Set the z-streaming configuration by hand (shape as above; hz even and

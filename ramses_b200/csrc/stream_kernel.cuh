@@ -60,12 +60,13 @@ struct StreamGeom {
   static constexpr int CHUNKS = 5 * SY * (SX / 2);      // 16-byte chunks per raw plane
   static constexpr size_t RAW_BYTES = sizeof(double) * NRAW * 5 * NS;
   static constexpr size_t Q_BYTES = sizeof(R) * NQ * 5 * NS;
-  // Fx, Fy (face fluxes times dt/dx, stored in R: in the mixed path they are
-  // FP32 products, widened to FP64 exactly on read) and qm_x, qm_y
-  static constexpr size_t X_BYTES = sizeof(R) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;
+  // Fx, Fy (face fluxes times dt/dx, FP64: in the mixed path the FP32
+  // product is widened once, by the face's owner) and qm_x, qm_y
+  static constexpr size_t X_BYTES = sizeof(double) * 2 * 5 * NC + sizeof(R) * 2 * 5 * NC;
   static constexpr size_t SMEM = RAW_BYTES + Q_BYTES + X_BYTES;
   static constexpr int NIN = TX * TY;                   // interior columns (threads 0..NIN-1)
   static_assert(NIN % 32 == 0, "interior columns fill whole warps");
+  static_assert((RAW_BYTES + Q_BYTES) % 16 == 0, "flux buffers start 16-byte aligned");
   static_assert(NEXTRA <= NT - NIN, "the outer ring is converted by the threads after the interior");
   static_assert(TX % 2 == 0 && TY % 2 == 0, "even tile");
 };
@@ -82,9 +83,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* raw = reinterpret_cast<double*>(smem_raw);                      // [NRAW][5][NS]
   R* qb = reinterpret_cast<R*>(smem_raw + G::RAW_BYTES);                  // [NQ][5][NS]
-  R* fxs = qb + G::NQ * 5 * NS;                                           // [5][NC] Fx (left face)
-  R* fys = fxs + 5 * NC;                                                  // [5][NC] Fy (lower face)
-  R* xm = fys + 5 * NC;                                                   // [5][NC] qm_x
+  double* fxs = reinterpret_cast<double*>(qb + G::NQ * 5 * NS);           // [5][NC] Fx (left face)
+  double* fys = fxs + 5 * NC;                                             // [5][NC] Fy (lower face)
+  R* xm = reinterpret_cast<R*>(fys + 5 * NC);                             // [5][NC] qm_x
   R* ym = xm + 5 * NC;                                                    // [5][NC] qm_y
   __shared__ double red[G::NT / 32];
 
@@ -267,8 +268,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     if (upd_plane && valid) {
 #pragma unroll
       for (int v = 0; v < 5; v++) {
-        fxs[v * NC + slot] = scale(fx[v]);
-        fys[v * NC + slot] = scale(fy[v]);
+        fxs[v * NC + slot] = (double)scale(fx[v]);
+        fys[v * NC + slot] = (double)scale(fy[v]);
       }
     }
     if (inner && k >= z0) {
@@ -295,8 +296,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
 #pragma unroll
         for (int v = 0; v < 5; v++) {
           double u = uo[v];
-          u = u + ((double)fxs[v * NC + slot] - (double)fxs[v * NC + slot + 1]);
-          u = u + ((double)fys[v * NC + slot] - (double)fys[v * NC + slot + CX]);
+          u = u + (fxs[v * NC + slot] - fxs[v * NC + slot + 1]);
+          u = u + (fys[v * NC + slot] - fys[v * NC + slot + CX]);
           upd[v] = u;
           fzb[v] = fzd[v];
         }

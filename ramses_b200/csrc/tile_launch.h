@@ -36,9 +36,8 @@ cudaError_t launch_tile_mixed(int shape, const TileArgs& a, int grid, cudaStream
 // z-streaming kernel of complete levels: column shape (TX x TY cells) and the
 // number of CTAs per SM the register allocation is bounded for
 struct StreamArgs;
-constexpr int kNumStreamShapes = 6;
-constexpr int kStreamShapes[kNumStreamShapes][3] = {{8, 8, 1},  {16, 8, 1}, {16, 16, 1},
-                                                     {16, 8, 2}, {8, 8, 4},  {16, 8, 3}};
+constexpr int kNumStreamShapes = 5;
+constexpr int kStreamShapes[kNumStreamShapes][3] = {{8, 8, 1}, {16, 8, 1}, {16, 16, 1}, {16, 8, 2}, {8, 8, 4}};
 cudaError_t launch_stream_f64(int shape, const StreamArgs& a, int grid, cudaStream_t s);
 cudaError_t launch_stream_mixed(int shape, const StreamArgs& a, int grid, cudaStream_t s);
 size_t stream_smem_f64(int shape);

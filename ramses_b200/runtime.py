@@ -312,8 +312,8 @@ class Solver:
         _check(load().rb_get_uniform_info(self._h, *[ctypes.byref(x) for x in v]), "rb_get_uniform_info")
         method, shape, hz, items = (x.value for x in v)
         if method == 0:
-            dims = ([(8, 8, 1), (16, 8, 1), (16, 16, 1), (16, 8, 2), (8, 8, 4), (16, 8, 3)][shape]
-                    if 0 <= shape < 6 else (0, 0, 0))
+            dims = ([(8, 8, 1), (16, 8, 1), (16, 16, 1), (16, 8, 2), (8, 8, 4)][shape]
+                    if 0 <= shape < 5 else (0, 0, 0))
             kern = "stream_step_kernel<%s,%d,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
                 "float" if self.precision == "mixed" else "double", dims[0], dims[1], dims[2], hz, items)
         else:
