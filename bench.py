@@ -276,10 +276,10 @@ def run_amr(args):
     build_s = time.perf_counter() - t0
     levels = [l for l in range(1, tree.nlevelmax + 1) if tree.noct(l)]
     out = {}
-    for prec in ("mixed", "fp64"):
+    for prec in ([args.only] if args.only else ["mixed", "fp64"]):
         s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
         for l in levels:
-            s.set_tile_shape(l, -1)
+            s.set_tile_shape(l, args.tile_shape)  # -1: autotuned per level
         s.run(max_steps=args.warmup)
         s.synchronize()
         before = s.cell_updates
@@ -292,6 +292,9 @@ def run_amr(args):
         out[prec] = {"value": upd / (ms / 1e3), "ms_per_coarse_step": ms / max(n, 1), "coarse_steps": n,
                      "t": s.t, "tile_shapes": {l: s.tile_shape(l) for l in levels}, "clocks": clk.summary()}
         s.close()
+    if args.only:
+        print(json.dumps({"only": args.only, "amr": args.amr, **out[args.only]}), flush=True)
+        return
     line = {"metric": METRIC, "value": out["mixed"]["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": out["mixed"]["ms_per_coarse_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",

@@ -77,6 +77,16 @@ int rb_upload_fine(rb_context *ctx, int ilevel);
 /* dt_io: in = current dtnew(ilevel); out = min(in, CFL dt of the level's leaf
  * cells). mass/ekin/eint: the level's totals (any may be NULL). */
 int rb_courant_fine(rb_context *ctx, int ilevel, double *dt_io, double *mass, double *ekin, double *eint);
+/* hydro_flag(ilevel) (hydro/hydro_flag.f90:1-180 with hydro_refine,
+ * hydro/godunov_utils.f90:125-263) on the device state: every cell of level
+ * ilevel's octs whose relative density, pressure or velocity jump to a face
+ * neighbour exceeds the rb_refine_params thresholds gets flag1[icell] = 1.
+ * flag1 is the host's flag1(0:ncell) (int32, indexed by the Fortran cell
+ * index); other entries are left as they are, as in the reference. Only one
+ * byte per cell of the level crosses PCIe, not uold. nflag_added (may be
+ * NULL) receives the number of cells that went from 0 to 1. Does nothing on
+ * the finest level, on an empty level or with every criterion off. */
+int rb_hydro_flag(rb_context *ctx, int ilevel, const rb_refine_params *rp, int32_t *flag1, int64_t *nflag_added);
 
 /* One coarse time step: the amr_step(levelmin) hydro call sequence with
  * subcycling, followed by the restriction of levels levelmin-1..1. t_io is

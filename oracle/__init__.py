@@ -62,6 +62,11 @@ _P64 = ctypes.POINTER(ctypes.c_int64)
 _PD = ctypes.POINTER(ctypes.c_double)
 
 
+class OrcRefine(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("err_grad_d", "err_grad_p", "err_grad_u",
+                                                "floor_d", "floor_u", "floor_p")]
+
+
 class OrcMesh(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
                 ("ncoarse", ctypes.c_int32), ("ngridmax", ctypes.c_int32),
@@ -93,6 +98,8 @@ def _declare(L):
     L.orc_get3cubefather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
     L.orc_getnborfather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
     L.orc_interpol_hydro.argtypes = [P, _PD, _PD, ctypes.c_int]
+    L.orc_hydro_flag.argtypes = [P, ctypes.POINTER(OrcRefine), M, ctypes.c_int, _P32]
+    L.orc_hydro_flag.restype = ctypes.c_int64
 
 
 def params_struct(hp) -> OrcParams:
@@ -189,6 +196,15 @@ class OracleRun:
 
     def dtnew(self, level):
         return self.m.dtnew[level]
+
+    def hydro_flag(self, ilevel, rp, flag1=None):
+        """hydro_flag(ilevel): returns (flag1 with the level's flagged cells
+        set to 1, number newly flagged); flag1 has ncell+1 entries (0..ncell)."""
+        f = np.zeros(self.tree.ncell + 1, np.int32) if flag1 is None else flag1
+        r = OrcRefine(rp.err_grad_d, rp.err_grad_p, rp.err_grad_u, rp.floor_d, rp.floor_u, rp.floor_p)
+        n = lib().orc_hydro_flag(ctypes.byref(self.p), ctypes.byref(r), ctypes.byref(self.m), ilevel,
+                                 _ptr(f, _P32))
+        return f, int(n)
 
     def get3cubefather(self, cell, ilevel):
         out = np.zeros(27, np.int32)

@@ -1149,3 +1149,104 @@ int orc_coarse_step(const orc_params *p, orc_mesh *m) {
   for (int il = m->levelmin - 1; il >= 1; il--) orc_upload_fine(p, m, il);
   return 0;
 }
+
+/* ------------------------------------------------------------------------ */
+/* hydro_flag: hydro/hydro_flag.f90:1-180, hydro_refine:                     */
+/* hydro/godunov_utils.f90:125-263                                           */
+/* ------------------------------------------------------------------------ */
+/* hydro_refine for one cell and one direction (the reference's vector loop
+ * body, k fixed): g, mm, d are conservative states of the left neighbour,
+ * the cell and the right neighbour, converted to primitives in place. */
+static int hydro_refine1(const orc_params *p, const orc_refine *r, double *g, double *mm, double *d) {
+  const double half = 0.5, one = 1.0, zero = 0.0;
+  g[0] = fmaxd(g[0], p->smallr);
+  mm[0] = fmaxd(mm[0], p->smallr);
+  d[0] = fmaxd(d[0], p->smallr);
+  for (int idim = 1; idim <= 3; idim++) {
+    g[idim] = g[idim] / g[0];
+    mm[idim] = mm[idim] / mm[0];
+    d[idim] = d[idim] / d[0];
+  }
+  double eking = zero, ekinm = zero, ekind = zero;
+  for (int idim = 1; idim <= 3; idim++) {
+    eking = eking + half * g[0] * (g[idim] * g[idim]);
+    ekinm = ekinm + half * mm[0] * (mm[idim] * mm[idim]);
+    ekind = ekind + half * d[0] * (d[idim] * d[idim]);
+  }
+  g[4] = (p->gamma - one) * (g[4] - eking);
+  mm[4] = (p->gamma - one) * (mm[4] - ekinm);
+  d[4] = (p->gamma - one) * (d[4] - ekind);
+  int ok = 0;
+  if (r->err_grad_d >= 0.) {
+    double dg = g[0], dm = mm[0], dd = d[0];
+    double error = 2.0 * fmaxd(fabs((dd - dm) / (dd + dm + r->floor_d)), fabs((dm - dg) / (dm + dg + r->floor_d)));
+    ok = ok || error > r->err_grad_d;
+  }
+  if (r->err_grad_p >= 0.) {
+    double pg = g[4], pm = mm[4], pd = d[4];
+    double error = 2.0 * fmaxd(fabs((pd - pm) / (pd + pm + r->floor_p)), fabs((pm - pg) / (pm + pg + r->floor_p)));
+    ok = ok || error > r->err_grad_p;
+  }
+  if (r->err_grad_u >= 0.) {
+    for (int idim = 1; idim <= 3; idim++) {
+      double vg = g[idim], vm = mm[idim], vd = d[idim];
+      double f2 = r->floor_u * r->floor_u;
+      double cg = sqrt(fmaxd(p->gamma * g[4] / g[0], f2));
+      double cm = sqrt(fmaxd(p->gamma * mm[4] / mm[0], f2));
+      double cd = sqrt(fmaxd(p->gamma * d[4] / d[0], f2));
+      double error = 2.0 * fmaxd(fabs((vd - vm) / (cd + cm + fabs(vd) + fabs(vm) + r->floor_u)),
+                                 fabs((vm - vg) / (cm + cg + fabs(vm) + fabs(vg) + r->floor_u)));
+      ok = ok || error > r->err_grad_u;
+    }
+  }
+  return ok;
+}
+
+int64_t orc_hydro_flag(const orc_params *p, const orc_refine *r, const orc_mesh *m, int ilevel, int32_t *flag1) {
+  if (ilevel == m->nlevelmax) return 0;                          /* :43 */
+  int ncache = (int)nactive(m, ilevel);
+  if (ncache == 0) return 0;                                     /* :44 */
+  if (r->err_grad_d == -1.0 && r->err_grad_p == -1.0 && r->err_grad_u == -1.0) return 0; /* :60-70 */
+  const int32_t *act = active_list(m, ilevel);
+  int64_t nok = 0;
+  for (int i = 0; i < ncache; i++) {
+    int grid = act[i];
+    /* getnborgrids (nbors_utils.f90:530-555): the 6 neighbour grids */
+    int igridn[7];
+    igridn[0] = grid;
+    for (int j = 1; j <= 6; j++) igridn[j] = SON(m, NBOR(m, grid, j));
+    for (int ind = 1; ind <= 8; ind++) {
+      int cell = m->ncoarse + (ind - 1) * m->ngridmax + grid;
+      /* getnborcells (nbors_utils.f90:363-399), evaluated geometrically:
+       * direction j moves along axis (j-1)/2; the neighbour is the child
+       * with that axis' bit flipped, in this grid when the move stays
+       * inside it, else in neighbour grid j; an absent grid gives 0, which
+       * hydro_flag replaces by nbor(grid,j) (:110-116) */
+      int c[3] = {(ind - 1) & 1, ((ind - 1) >> 1) & 1, ((ind - 1) >> 2) & 1};
+      int indn[7];
+      for (int j = 1; j <= 6; j++) {
+        int dd = (j - 1) / 2, plus = (j - 1) & 1;
+        int inside = plus ? (c[dd] == 0) : (c[dd] == 1);
+        int ig = inside ? igridn[0] : igridn[j];
+        int cc[3] = {c[0], c[1], c[2]};
+        cc[dd] = 1 - c[dd];
+        int ih = 1 + cc[0] + 2 * cc[1] + 4 * cc[2];
+        indn[j] = ig > 0 ? m->ncoarse + (ih - 1) * m->ngridmax + ig : 0;
+        if (indn[j] == 0) indn[j] = NBOR(m, grid, j);
+      }
+      int ok = 0;
+      for (int idim = 1; idim <= 3; idim++) {                    /* :118-134 */
+        double ug[5], um[5], ud[5];
+        for (int ivar = 1; ivar <= 5; ivar++) {
+          ug[ivar - 1] = *UOLD(m, indn[2 * idim - 1], ivar);
+          um[ivar - 1] = *UOLD(m, cell, ivar);
+          ud[ivar - 1] = *UOLD(m, indn[2 * idim], ivar);
+        }
+        if (hydro_refine1(p, r, ug, um, ud)) ok = 1;
+      }
+      if (flag1[cell] == 0 && ok) nok++;                         /* :156-161 */
+      if (ok) flag1[cell] = 1;                                   /* :163-165 */
+    }
+  }
+  return nok;
+}

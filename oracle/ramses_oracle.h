@@ -36,6 +36,12 @@ typedef struct orc_params {
   int32_t interpol_type; /* 0..4 */
 } orc_params;
 
+/* &REFINE_PARAMS gradient criterion (hydro/hydro_parameters.f90:47-52) */
+typedef struct orc_refine {
+  double err_grad_d, err_grad_p, err_grad_u;
+  double floor_d, floor_u, floor_p;
+} orc_refine;
+
 typedef struct orc_mesh {
   int32_t nx, ny, nz, ncoarse, ngridmax, nlevelmax, levelmin, nvector;
   double boxlen;
@@ -88,6 +94,12 @@ int orc_get3cubefather(const orc_mesh *m, int ind_cell_father, int ilevel,
 /* nbors_utils.f90:404-525: cell + 6 neighbour (or neighbour-father) cells. */
 int orc_getnborfather(const orc_mesh *m, int ind_cell, int ilevel,
                       int32_t *ind_father7);
+
+/* hydro_flag (hydro/hydro_flag.f90:1-180) with hydro_refine
+ * (hydro/godunov_utils.f90:125-263) on level ilevel: flag1[icell] = 1 for the
+ * cells meeting the gradient criterion (flag1 indexed 0..ncell, as flag1(0:ncell));
+ * returns the number of cells newly flagged. */
+int64_t orc_hydro_flag(const orc_params *p, const orc_refine *r, const orc_mesh *m, int ilevel, int32_t *flag1);
 
 /* interpol_hydro.f90:268-444 for nn father stencils:
  * u1(nn,0:6,5) -> u2(nn,1:8,5), column-major with leading dim nn. */

@@ -291,6 +291,100 @@ static __global__ void sched_finish_kernel(double* __restrict__ s) {
   s[RB_S_COARSE] = s[RB_S_COARSE] + 1.0;
 }
 
+// hydro_refine (godunov_utils.f90:125-263) for one cell along one direction:
+// ug, um, ud are the conservative states of the left neighbour, the cell and
+// the right neighbour; they are converted to primitives in place as the
+// reference does, then the relative density, pressure and velocity gradients
+// are compared with their thresholds. Operation order as in the reference.
+__device__ __forceinline__ bool hydro_refine_cell(double ug[5], double um[5], double ud[5],
+                                                  const rb_hydro_params& hp, const rb_refine_params& rp) {
+  const double half = 0.5, one = 1.0, zero = 0.0;
+  ug[0] = fmx(ug[0], hp.smallr);
+  um[0] = fmx(um[0], hp.smallr);
+  ud[0] = fmx(ud[0], hp.smallr);
+  for (int d = 1; d <= 3; d++) {
+    ug[d] = ug[d] / ug[0];
+    um[d] = um[d] / um[0];
+    ud[d] = ud[d] / ud[0];
+  }
+  double eking = zero, ekinm = zero, ekind = zero;
+  for (int d = 1; d <= 3; d++) {
+    eking = eking + half * ug[0] * (ug[d] * ug[d]);
+    ekinm = ekinm + half * um[0] * (um[d] * um[d]);
+    ekind = ekind + half * ud[0] * (ud[d] * ud[d]);
+  }
+  ug[4] = (hp.gamma - one) * (ug[4] - eking);
+  um[4] = (hp.gamma - one) * (um[4] - ekinm);
+  ud[4] = (hp.gamma - one) * (ud[4] - ekind);
+  bool ok = false;
+  if (rp.err_grad_d >= 0.0) {
+    const double dg = ug[0], dm = um[0], dd = ud[0];
+    const double error = 2.0 * fmx(fabs((dd - dm) / (dd + dm + rp.floor_d)), fabs((dm - dg) / (dm + dg + rp.floor_d)));
+    ok = ok || error > rp.err_grad_d;
+  }
+  if (rp.err_grad_p >= 0.0) {
+    const double pg = ug[4], pm = um[4], pd = ud[4];
+    const double error = 2.0 * fmx(fabs((pd - pm) / (pd + pm + rp.floor_p)), fabs((pm - pg) / (pm + pg + rp.floor_p)));
+    ok = ok || error > rp.err_grad_p;
+  }
+  if (rp.err_grad_u >= 0.0) {
+    for (int d = 1; d <= 3; d++) {
+      const double vg = ug[d], vm = um[d], vd = ud[d];
+      const double f2 = rp.floor_u * rp.floor_u;
+      const double cg = sqrt(fmx(hp.gamma * ug[4] / ug[0], f2));
+      const double cm = sqrt(fmx(hp.gamma * um[4] / um[0], f2));
+      const double cd = sqrt(fmx(hp.gamma * ud[4] / ud[0], f2));
+      const double error = 2.0 * fmx(fabs((vd - vm) / (cd + cm + fabs(vd) + fabs(vm) + rp.floor_u)),
+                                     fabs((vm - vg) / (cm + cg + fabs(vm) + fabs(vg) + rp.floor_u)));
+      ok = ok || error > rp.err_grad_u;
+    }
+  }
+  return ok;
+}
+
+// hydro_flag (hydro_flag.f90:1-180): out[i] = 1 when cell i of the level's
+// octs (oct i>>3, child slot i&7) meets a criterion towards its face
+// neighbours along any direction. A face neighbour is the adjacent child of
+// the same oct, or of the neighbouring oct (getnborgrids/getnborcells,
+// nbors_utils.f90:363-399: the child slot with that direction's bit flipped),
+// or, where that oct does not exist, the coarser neighbour cell
+// nbor(igrid,j) itself (hydro_flag.f90:110-116). nbor6[oct*6 + j] is the
+// device cell of nbor(igrid, j+1), j = 0..5 = -x,+x,-y,+y,-z,+z.
+static __global__ void hydro_flag_kernel(const double* __restrict__ uold, const int32_t* __restrict__ son,
+                                         const int32_t* __restrict__ active, const int32_t* __restrict__ nbor6,
+                                         int32_t noct, int64_t ncell, int32_t ncoarse, rb_hydro_params hp,
+                                         rb_refine_params rp, uint8_t* __restrict__ out) {
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t oct = i >> 3;
+    const int ch = (int)(i & 7);
+    const int64_t base = ncoarse + (int64_t)active[oct] * 8;
+    bool ok = false;
+    for (int d = 0; d < 3; d++) {
+      const int bit = 1 << d;
+      int64_t cell[2];
+      for (int side = 0; side < 2; side++) {  // 0: minus neighbour, 1: plus neighbour
+        const bool same_oct = side == 0 ? (ch & bit) != 0 : (ch & bit) == 0;
+        if (same_oct) {
+          cell[side] = base + (ch ^ bit);
+        } else {
+          const int64_t fc = nbor6[oct * 6 + 2 * d + side];
+          const int g = son[fc];
+          cell[side] = g > 0 ? ncoarse + (int64_t)(g - 1) * 8 + (ch ^ bit) : fc;
+        }
+      }
+      double ug[5], um[5], ud[5];
+      for (int v = 0; v < 5; v++) {
+        ug[v] = uold[v * ncell + cell[0]];
+        um[v] = uold[v * ncell + base + ch];
+        ud[v] = uold[v * ncell + cell[1]];
+      }
+      ok = hydro_refine_cell(ug, um, ud, hp, rp) || ok;
+    }
+    out[i] = ok ? 1 : 0;
+  }
+}
+
 // upload_fine / upl (interpol_hydro.f90:5-263): restriction of every split
 // cell of the level's active octs from its 8 children.
 static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,

@@ -92,6 +92,7 @@ struct Level {
   int32_t* d_tgt = nullptr;
   int32_t* d_tgt_off = nullptr;
   int32_t* d_contrib = nullptr;
+  int32_t* d_nbor6 = nullptr;     // [noct][6] device cell of nbor(igrid,j) (hydro_flag)
   int64_t leaf_cells = 0;
   double dx = 0.0;
   bool complete = false;
@@ -139,6 +140,8 @@ struct rb_context {
   double* h_red = nullptr;          // pinned [8]
   double* d_sched = nullptr;        // [RB_S_SIZE] device-resident amr_step clock
   double* h_sched = nullptr;        // pinned [RB_S_SIZE]
+  uint8_t* d_flag = nullptr;        // hydro_flag output, one byte per cell of a level
+  int64_t flag_cap = 0;
   const double* gate = nullptr;     // level kernels return early when *gate != 0
   cudaGraphExec_t amr_graph = nullptr;  // cached graph of amr_chunk coarse steps
   int amr_chunk = 0;

@@ -80,6 +80,7 @@ void free_level_tables(Level& L) {
   dfree(L.d_tgt);
   dfree(L.d_tgt_off);
   dfree(L.d_contrib);
+  dfree(L.d_nbor6);
   L.ntile = L.ninterp = L.nslot = L.ntgt = 0;
   L.tables_built = false;
 }
@@ -867,6 +868,7 @@ int rb_destroy(rb_context* c) {
   free_tree(c);
   dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son); dfree(c->d_corr_slot);
   dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
+  dfree(c->d_flag);
   if (c->h_red) cudaFreeHost(c->h_red);
   if (c->h_sched) cudaFreeHost(c->h_sched);
   for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
@@ -1002,6 +1004,52 @@ int rb_run(rb_context* c, int max_steps, double t_end, int use_graph, double* t_
   RB_CUDA(cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1));  // device time of all chunks
   if (t_io) *t_io = c->t;
   if (steps_done) *steps_done = (int)coarse;
+  return RB_OK;
+}
+
+int rb_hydro_flag(rb_context* c, int l, const rb_refine_params* rp, int32_t* flag1, int64_t* nflag_added) {
+  if (nflag_added) *nflag_added = 0;
+  RB_TRY(check_level(c, l));
+  if (!rp || !flag1) return fail(RB_ERR_INVALID, "null argument");
+  if (!c->have_state) return fail(RB_ERR_STATE, "the state must be uploaded first");
+  // hydro_flag.f90:43-44 and 60-70: nothing to do on the finest level, on an
+  // empty level, or with every criterion switched off
+  if (l == c->mp.nlevelmax) return RB_OK;
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  if (rp->err_grad_d == -1.0 && rp->err_grad_p == -1.0 && rp->err_grad_u == -1.0) return RB_OK;
+  RB_TRY(sync_oct(c));
+  if (!L.d_nbor6) {
+    std::vector<int32_t> nb((size_t)L.noct * 6);
+    for (int i = 0; i < L.noct; i++) {
+      const int g = L.h_active[i];
+      for (int j = 0; j < 6; j++)
+        nb[(size_t)i * 6 + j] = (int32_t)dev_of_fortran(c, c->nbor[(size_t)j * c->mp.ngridmax + (g - 1)]);
+    }
+    RB_TRY(dalloc(&L.d_nbor6, nb.size()));
+    RB_TRY(h2d(c, L.d_nbor6, nb.data(), nb.size() * sizeof(int32_t)));
+  }
+  const int64_t n = (int64_t)L.noct * 8;
+  if (n > c->flag_cap) {
+    dfree(c->d_flag);
+    RB_TRY(dalloc(&c->d_flag, (size_t)n));
+    c->flag_cap = n;
+  }
+  rb::hydro_flag_kernel<<<grid_for(n, 256), 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.d_nbor6, L.noct,
+                                                                 c->ncell, c->mp.ncoarse, c->hp, *rp, c->d_flag);
+  RB_CUDA(cudaGetLastError());
+  std::vector<uint8_t> f((size_t)n);
+  RB_CUDA(cudaMemcpyAsync(f.data(), c->d_flag, (size_t)n, cudaMemcpyDeviceToHost, c->stream));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  int64_t added = 0;
+  for (int i = 0; i < L.noct; i++)
+    for (int ind = 0; ind < 8; ind++) {
+      if (!f[(size_t)i * 8 + ind]) continue;
+      const int64_t icell = fcell(c, ind + 1, L.h_active[i]);
+      if (flag1[icell] == 0) added++;
+      flag1[icell] = 1;
+    }
+  if (nflag_added) *nflag_added = added;
   return RB_OK;
 }
 

@@ -41,6 +41,17 @@ typedef struct rb_hydro_params {
   double difmag;         /* must be 0                                      */
 } rb_hydro_params;
 
+/* Gradient refinement criterion of &REFINE_PARAMS
+ * (hydro/read_hydro_params.f90:59-60; defaults hydro/hydro_parameters.f90:47-52:
+ * err_grad_* = -1 (off), floor_* = 1e-10). A criterion is on when its
+ * err_grad_* >= 0. */
+typedef struct rb_refine_params {
+  double err_grad_d;     /* relative density gradient threshold            */
+  double err_grad_p;     /* relative pressure gradient threshold           */
+  double err_grad_u;     /* relative velocity gradient threshold           */
+  double floor_d, floor_u, floor_p;
+} rb_refine_params;
+
 /* &AMR_PARAMS / &RUN_PARAMS values and the tree dimensions
  * (amr/amr_parameters.f90, amr/amr_commons.f90). */
 typedef struct rb_mesh_params {

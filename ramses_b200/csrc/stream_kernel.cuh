@@ -57,7 +57,8 @@ struct StreamGeom {
   static constexpr int NEXTRA = NS - NC;                // q-only outer ring columns
   static constexpr int NRAW = 5;                        // raw planes in flight
   static constexpr int NQ = 2;                          // primitive planes in shared memory
-  static constexpr int CHUNKS = 5 * SY * (SX / 2);      // 16-byte chunks per raw plane
+  static constexpr int PAIRS = SY * (SX / 2);           // 16-byte (2-cell) pieces of one variable's plane
+  static_assert(PAIRS <= NT, "one plane piece per thread");
   static constexpr size_t RAW_BYTES = sizeof(double) * NRAW * 5 * NS;
   static constexpr size_t Q_BYTES = sizeof(R) * NQ * 5 * NS;
   // Fx, Fy (face fluxes times dt/dx, FP64: in the mixed path the FP32
@@ -140,18 +141,26 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   // non-negative offset and constant moduli; periodic wraps need one step
   const int zbase = z0 - 2;
   auto wrap = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
+  // Plane loads: thread tid < PAIRS owns the 2-cell (16-byte) piece (row, j)
+  // of the stencil plane for all 5 variables; its offsets inside a plane do
+  // not change along z, so they are computed once here.
+  const bool loader = tid < G::PAIRS;
+  int piece_s = 0;
+  int64_t piece_g = 0;
+  if (loader) {
+    const int j = tid % (SX / 2), row = tid / (SX / 2);
+    piece_s = row * SX + 2 * j;
+    piece_g = (int64_t)wrap(ty0 - 2 + row, a.ny) * a.nx + wrap(tx0 - 2 + 2 * j, a.nx);
+  }
   auto issue_plane = [&](int zp) {
-    double* dst = raw + ((zp - zbase) % G::NRAW) * 5 * NS;
-    const double* src = a.uin + (int64_t)wrap(zp, a.nz) * plane;
-    for (int ch = tid; ch < G::CHUNKS; ch += G::NT) {
-      const int j = ch % (SX / 2), r = ch / (SX / 2), row = r % SY, v = r / SY;
-      const int xg = wrap(tx0 - 2 + 2 * j, a.nx);
-      const int yg = wrap(ty0 - 2 + row, a.ny);
-      cp_async16(dst + v * NS + row * SX + 2 * j, src + v * vstr + (int64_t)yg * a.nx + xg);
-    }
+    if (!loader) return;
+    double* dst = raw + ((unsigned)(zp - zbase) % G::NRAW) * 5 * NS + piece_s;
+    const double* src = a.uin + (int64_t)wrap(zp, a.nz) * plane + piece_g;
+#pragma unroll
+    for (int v = 0; v < 5; v++) cp_async16(dst + v * NS, src + v * vstr);
   };
   auto load_u = [&](int zp, int s, double u[5]) {
-    const double* p = raw + ((zp - zbase) % G::NRAW) * 5 * NS + s;
+    const double* p = raw + ((unsigned)(zp - zbase) % G::NRAW) * 5 * NS + s;
 #pragma unroll
     for (int v = 0; v < 5; v++) u[v] = p[v * NS];
   };
@@ -161,7 +170,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     return ctoprim_cell<R>(u, a.hp);
   };
   auto put_q = [&](int zp, int s, const Prim<R>& q) {
-    R* p = qb + ((zp - zbase) % G::NQ) * 5 * NS + s;
+    R* p = qb + ((unsigned)(zp - zbase) % G::NQ) * 5 * NS + s;
     p[0] = q.r; p[NS] = q.u; p[2 * NS] = q.v; p[3 * NS] = q.w; p[4 * NS] = q.p;
   };
 
@@ -188,7 +197,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   for (int k = z0 - 1; k <= zend; k++) {
     const bool upd_plane = (k >= z0) && (k < zend);  // x/y fluxes and partial update at k
     // B. slopes and trace of plane k
-    const R* qk = qb + ((k - zbase) % G::NQ) * 5 * NS;
+    const R* qk = qb + ((unsigned)(k - zbase) % G::NQ) * 5 * NS;
     R dq[5][3];
     {
       const R own[5] = {q_0.r, q_0.u, q_0.v, q_0.w, q_0.p};

@@ -97,6 +97,28 @@ def hydro_params_from_namelist(text: str) -> HydroParams:
     return hp
 
 
+@dataclasses.dataclass
+class RefineParams:
+    """Gradient refinement criterion of &REFINE_PARAMS with the reference's
+    defaults (hydro/hydro_parameters.f90:47-52): a negative err_grad_* switches
+    that criterion off."""
+    err_grad_d: float = -1.0
+    err_grad_p: float = -1.0
+    err_grad_u: float = -1.0
+    floor_d: float = 1e-10
+    floor_u: float = 1e-10
+    floor_p: float = 1e-10
+
+
+def refine_params_from_namelist(text: str) -> RefineParams:
+    rp = RefineParams()
+    fields = {f.name for f in dataclasses.fields(RefineParams)}
+    for k, v in parse_namelist(text).get("REFINE_PARAMS", {}).items():
+        if k in fields:
+            setattr(rp, k, float(_fortran_value(v)))
+    return rp
+
+
 def nsubcycle_from_namelist(text: str, nlevelmax: int) -> List[int]:
     """``nsubcycle`` of ``&RUN_PARAMS`` (default 2 for every level), with
     Fortran repeat counts (``3*1,2``)."""

@@ -26,6 +26,11 @@ module rb_b200
      integer(c_int32_t) :: nsubcycle(0:32)
   end type rb_mesh_params_t
 
+  type, bind(c) :: rb_refine_params_t
+     real(c_double) :: err_grad_d, err_grad_p, err_grad_u
+     real(c_double) :: floor_d, floor_u, floor_p
+  end type rb_refine_params_t
+
   type(c_ptr), save :: rb_ctx = c_null_ptr
   integer(c_int64_t), save :: rb_tree_stamp = -1
 
@@ -80,6 +85,14 @@ module rb_b200
        real(c_double), intent(inout) :: dt
        real(c_double), intent(out) :: mass, ekin, eint
      end function rb_courant_fine
+     integer(c_int) function rb_hydro_flag(ctx, ilevel, rp, flag1, nflag_added) bind(c, name='rb_hydro_flag')
+       import :: c_int, c_int32_t, c_int64_t, c_ptr, rb_refine_params_t
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+       type(rb_refine_params_t), intent(in) :: rp
+       integer(c_int32_t), dimension(*) :: flag1
+       integer(c_int64_t) :: nflag_added
+     end function rb_hydro_flag
      type(c_ptr) function rb_last_error() bind(c, name='rb_last_error')
        import :: c_ptr
      end function rb_last_error

@@ -37,6 +37,11 @@ class HydroParamsC(ctypes.Structure):
                 ("pressure_fix", ctypes.c_int32), ("difmag", ctypes.c_double)]
 
 
+class RefineParamsC(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("err_grad_d", "err_grad_p", "err_grad_u",
+                                                "floor_d", "floor_u", "floor_p")]
+
+
 class MeshParamsC(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
                 ("ncoarse", ctypes.c_int32), ("ngridmax", ctypes.c_int32), ("nlevelmax", ctypes.c_int32),
@@ -74,6 +79,7 @@ _PROTOS = {
     "rb_courant_fine": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _PD, _PD, _PD, _PD]),
     "rb_coarse_step": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
     "rb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, _PD, _P32]),
+    "rb_hydro_flag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(RefineParamsC), _P32, _P64]),
     "rb_cell_updates": (ctypes.c_int, [ctypes.c_void_p, _P64]),
     "rb_set_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     "rb_get_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P32]),
@@ -302,6 +308,18 @@ class Solver:
         _check(load().rb_autotune_uniform(self._h, ctypes.byref(s), ctypes.byref(hz), ctypes.byref(ms)),
                "rb_autotune_uniform")
         return {"shape": s.value, "hz": hz.value, "ms": ms.value}
+
+    def hydro_flag(self, ilevel: int, rp, flag1: Optional[np.ndarray] = None):
+        """hydro_flag(ilevel) on the device: returns (flag1, newly flagged)
+        where flag1 (int32, ncell+1 entries, index = Fortran cell index) has
+        the level's flagged cells set to 1."""
+        f = np.zeros(self.tree.ncell + 1, np.int32) if flag1 is None else flag1
+        assert f.dtype == np.int32 and f.shape == (self.tree.ncell + 1,) and f.flags.c_contiguous
+        r = RefineParamsC(rp.err_grad_d, rp.err_grad_p, rp.err_grad_u, rp.floor_d, rp.floor_u, rp.floor_p)
+        n = ctypes.c_int64()
+        _check(load().rb_hydro_flag(self._h, int(ilevel), ctypes.byref(r), _ptr(f, _P32), ctypes.byref(n)),
+               "rb_hydro_flag")
+        return f, n.value
 
     def set_stream_shape(self, shape: int, hz: int):
         """Fix the z-streaming column shape and z extent (no autotuning)."""

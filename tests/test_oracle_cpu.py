@@ -169,3 +169,82 @@ def test_unsplit_batch_independence():
     f8, _ = oracle.unsplit(hp, u, None, dx=0.05, dt=1e-3)
     f1, _ = oracle.unsplit(hp, np.ascontiguousarray(u[..., 3:4]), None, dx=0.05, dt=1e-3)
     np.testing.assert_array_equal(f8[..., 3], f1[..., 0])
+
+
+def _numpy_hydro_refine_flags(u, gamma, smallr, rp):
+    """Independent numpy statement of hydro_refine (godunov_utils.f90:125-263)
+    on a complete periodic level given as conservative [5, z, y, x]: flag =
+    any direction meets a criterion."""
+    def prim(w):
+        r = np.maximum(w[0], smallr)
+        v = [w[1 + d] / r for d in range(3)]
+        ek = np.zeros_like(r)
+        for d in range(3):
+            ek = ek + 0.5 * r * (v[d] * v[d])
+        return r, v, (gamma - 1.0) * (w[4] - ek)
+
+    def rel(a, b, c, floor):
+        return 2.0 * np.maximum(np.abs((c - b) / (c + b + floor)), np.abs((b - a) / (b + a + floor)))
+    flag = np.zeros(u.shape[1:], dtype=bool)
+    for axis in range(3):
+        ax = 3 - axis  # x is the last array axis
+        g = prim(np.roll(u, 1, axis=ax))
+        m = prim(u)
+        d = prim(np.roll(u, -1, axis=ax))
+        if rp.err_grad_d >= 0:
+            flag |= rel(g[0], m[0], d[0], rp.floor_d) > rp.err_grad_d
+        if rp.err_grad_p >= 0:
+            flag |= rel(g[2], m[2], d[2], rp.floor_p) > rp.err_grad_p
+        if rp.err_grad_u >= 0:
+            c = [np.sqrt(np.maximum(gamma * s[2] / s[0], rp.floor_u ** 2)) for s in (g, m, d)]
+            for k in range(3):
+                vg, vm, vd = g[1][k], m[1][k], d[1][k]
+                e = 2.0 * np.maximum(np.abs((vd - vm) / (c[2] + c[1] + np.abs(vd) + np.abs(vm) + rp.floor_u)),
+                                     np.abs((vm - vg) / (c[1] + c[0] + np.abs(vm) + np.abs(vg) + rp.floor_u)))
+                flag |= e > rp.err_grad_u
+    return flag
+
+
+@pytest.mark.parametrize("crit", ["d", "p", "u", "all"])
+def test_hydro_flag_oracle_on_complete_level(crit):
+    """hydro_flag on a complete level (every face neighbour at the same
+    level) equals the numpy statement of hydro_refine, cell by cell, and
+    ORs into existing flags with the reference's count of new flags."""
+    from ramses_b200.params import RefineParams
+    lvl = 4
+    tree = mesh.build_tree(lvl, lvl + 1, None)
+    assert tree.noct(lvl + 1) == 0 and tree.noct(lvl) == (2 ** lvl // 2) ** 3
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1)
+    q = ics.turbulent_box_prim_grid(2 ** lvl, seed=5, gamma=hp.gamma)
+    u = ics.fill_uniform_level_from_grid(tree, lvl, q, hp.gamma)
+    thr = {"d": dict(err_grad_d=0.3), "p": dict(err_grad_p=0.5), "u": dict(err_grad_u=1.2),
+           "all": dict(err_grad_d=0.6, err_grad_p=0.8, err_grad_u=1.5)}[crit]
+    rp = RefineParams(**thr)
+    orc = oracle.OracleRun(tree, hp, u)
+    idx = tree.cell_index(lvl)
+    want = _numpy_hydro_refine_flags(u[:, idx - 1], hp.gamma, hp.smallr, rp)
+    assert 0 < want.sum() < want.size
+    f, n = orc.hydro_flag(lvl, rp)
+    np.testing.assert_array_equal(f[idx] == 1, want)
+    assert n == int(want.sum())
+    # only sets, never clears; counts only cells that were 0
+    pre = np.zeros(tree.ncell + 1, np.int32)
+    pre[idx.reshape(-1)[::3]] = 1
+    f2, n2 = orc.hydro_flag(lvl, rp, pre.copy())
+    assert np.all(f2[idx.reshape(-1)[::3]] == 1)
+    np.testing.assert_array_equal(f2[idx] == 1, want | (pre[idx] == 1))
+    assert n2 == int((want & (pre[idx] == 0)).sum())
+
+
+def test_hydro_flag_oracle_skips():
+    from ramses_b200.params import RefineParams
+    tree, hp, u = sedov_amr(3, 5)
+    orc = oracle.OracleRun(tree, hp, u)
+    f, n = orc.hydro_flag(5, RefineParams(err_grad_d=0.01))      # finest level: nothing
+    assert n == 0 and not f.any()
+    f, n = orc.hydro_flag(4, RefineParams())                       # every criterion off
+    assert n == 0 and not f.any()
+    f, n = orc.hydro_flag(4, RefineParams(err_grad_d=0.05))   # uniform density at t=0
+    assert n == 0
+    f, n = orc.hydro_flag(4, RefineParams(err_grad_p=0.05))   # the blast's pressure jump
+    assert n > 0 and int(f.sum()) == n
