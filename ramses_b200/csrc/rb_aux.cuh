@@ -117,23 +117,31 @@ static __global__ void apply_corrections_kernel(double* __restrict__ unew, const
 
 // courant_fine (courant_fine.f90:1-159): per-block partial (min dt, mass,
 // total energy, internal energy) over the leaf cells of the level's octs.
-// A second single-block pass reduces the partials in a fixed order.
+// A second single-block pass reduces the partials in a fixed order. With
+// unew non-null the kernel also does the set_unew that follows courant_fine
+// in amr_step (godunov_fine.f90:40-130): unew = uold for every cell.
 template <int NT>
 static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __restrict__ uold,
                                                              const int32_t* __restrict__ son,
                                                              const int32_t* __restrict__ active, int32_t noct,
                                                              int64_t ncell, int32_t ncoarse, double dx,
                                                              rb_hydro_params hp, double* __restrict__ partial,
-                                                             const double* __restrict__ gate) {
+                                                             const double* __restrict__ gate,
+                                                             double* __restrict__ unew = nullptr) {
   RB_GATE(gate);
   const double vol = dx * dx * dx;
   double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
   const int64_t n = (int64_t)noct * 8;
   for (int64_t i = blockIdx.x * (int64_t)NT + threadIdx.x; i < n; i += (int64_t)gridDim.x * NT) {
     const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
-    if (son[dc] != 0) continue;
+    const bool leaf = son[dc] == 0;
+    if (!leaf && !unew) continue;
     double u[5];
     for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    // set_unew fused in (it follows courant_fine in amr_step): every cell
+    if (unew)
+      for (int v = 0; v < 5; v++) unew[v * ncell + dc] = u[v];
+    if (!leaf) continue;
     mass = mass + u[0] * vol;
     etot = etot + u[4] * vol;
     double ei = u[4] * vol;
@@ -387,15 +395,10 @@ static __global__ void hydro_flag_kernel(const double* __restrict__ uold, const 
 
 // upload_fine / upl (interpol_hydro.f90:5-263): restriction of every split
 // cell of the level's active octs from its 8 children.
-static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,
-                                   const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
-                                   int32_t ncoarse, rb_hydro_params hp, const double* __restrict__ gate) {
-  RB_GATE(gate);
-  const int64_t n = (int64_t)noct * 8;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
-    const int gs = son[dc];
-    if (gs <= 0) continue;
+// Restriction of one split cell dc from its 8 children (oct gs).
+__device__ __forceinline__ void restrict_cell(double* __restrict__ uold, int64_t dc, int gs, int64_t ncell,
+                                              int32_t ncoarse, const rb_hydro_params& hp) {
+  {
     const int64_t c0 = ncoarse + (int64_t)(gs - 1) * 8;
     double getx = 0.0;
     for (int is = 0; is < 8; is++) getx = getx + fmx(uold[c0 + is], hp.smallr);
@@ -420,6 +423,41 @@ static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32
         ekin = ekin + 0.5 * (uold[d * ncell + dc] * uold[d * ncell + dc]) / fmx(uold[dc], hp.smallr);
       const double erad = 0.0;
       uold[4 * ncell + dc] = getx / 8.0 + ekin + erad;
+    }
+  }
+}
+
+static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32_t* __restrict__ son,
+                                   const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
+                                   int32_t ncoarse, rb_hydro_params hp, const double* __restrict__ gate) {
+  RB_GATE(gate);
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    const int gs = son[dc];
+    if (gs > 0) restrict_cell(uold, dc, gs, ncell, ncoarse, hp);
+  }
+}
+
+// set_uold followed by upload_fine on the same level (amr_step.f90:424,442),
+// in one pass: set_uold copies unew to uold for every cell and upload_fine
+// then overwrites every variable of the split cells with the restriction of
+// their children, so each cell's final uold is written once. do_upload = 0
+// where upload_fine does nothing (finest level, or no split cell).
+static __global__ void set_uold_upload_kernel(double* __restrict__ uold, const double* __restrict__ unew,
+                                              const int32_t* __restrict__ son, const int32_t* __restrict__ active,
+                                              int32_t noct, int64_t ncell, int32_t ncoarse, rb_hydro_params hp,
+                                              int do_upload, const double* __restrict__ gate) {
+  RB_GATE(gate);
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    const int gs = do_upload ? son[dc] : 0;
+    if (gs > 0) {
+      restrict_cell(uold, dc, gs, ncell, ncoarse, hp);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v++) uold[v * ncell + dc] = unew[v * ncell + dc];
     }
   }
 }

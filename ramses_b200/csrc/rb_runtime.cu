@@ -429,6 +429,17 @@ int set_uold_impl(rb_context* c, int l) {
   return RB_OK;
 }
 
+// set_uold + upload_fine of level l in one pass (set_uold_upload_kernel)
+int set_uold_upload_impl(rb_context* c, int l) {
+  Level& L = c->lv[l];
+  if (!L.noct) return RB_OK;
+  const int do_upload = (l < c->mp.nlevelmax && L.has_refined) ? 1 : 0;
+  rb::set_uold_upload_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_uold, c->d_unew, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, do_upload, c->gate);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
 int upload_fine_impl(rb_context* c, int l) {
   if (l == c->mp.nlevelmax) return RB_OK;  // interpol_hydro.f90:16
   Level& L = c->lv[l];
@@ -569,14 +580,16 @@ int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_d
   return RB_OK;
 }
 
-int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin, double* eint) {
+int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin, double* eint,
+                 bool with_set_unew = false) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   const int nt = 256;
   const int nblk = grid_for((int64_t)L.noct * 8, nt, 148 * 8);
   RB_TRY(ensure_partial(c, nblk));
   rb::courant_partial_kernel<256><<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate);
+                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate,
+                                                              with_set_unew ? c->d_unew : nullptr);
   RB_CUDA(cudaGetLastError());
   const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
   rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, *dt_io, dt0,
@@ -598,12 +611,11 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   c->dtold[l] = c->dtnew[l];
   c->dtnew[l] = c->mp.boxlen / c->hp.smallc;
   double dt_all = c->dtnew[l], ma = 0, ek = 0, ei = 0;
-  RB_TRY(courant_impl(c, l, &dt_all, &ma, &ek, &ei));
+  RB_TRY(courant_impl(c, l, &dt_all, &ma, &ek, &ei, /*with_set_unew=*/true));
   c->mass_tot += ma; c->ekin_tot += ek; c->eint_tot += ei;
   c->dtnew[l] = rb_min_host(c->dtnew[l], dt_all);
   if (l > c->mp.levelmin)
     c->dtnew[l] = rb_min_host(c->dtnew[l - 1] / (double)(float)c->mp.nsubcycle[l - 1], c->dtnew[l]);
-  RB_TRY(set_unew_impl(c, l));
   if (l < c->mp.nlevelmax) {
     if (c->lv[l + 1].noct > 0) {
       if (c->mp.nsubcycle[l] == 2) {
@@ -624,8 +636,7 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   }
   RB_TRY(godunov_impl(c, l, c->dtnew[l], false));
   c->cell_updates += c->lv[l].leaf_cells;
-  RB_TRY(set_uold_impl(c, l));
-  RB_TRY(upload_fine_impl(c, l));
+  RB_TRY(set_uold_upload_impl(c, l));
   if (l > c->mp.levelmin) {
     if (c->mp.nsubcycle[l - 1] == 1) c->dtnew[l - 1] = c->dtnew[l];
     if (icount == 2) c->dtnew[l - 1] = c->dtold[l] + c->dtnew[l];
@@ -645,14 +656,14 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   double* s = c->d_sched;
   const int nblk = courant_blocks(c, l);
   rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate);
+                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate,
+                                                              c->d_unew);  // + set_unew
   RB_CUDA(cudaGetLastError());
   const double nsub_prev = l > c->mp.levelmin ? (double)(float)c->mp.nsubcycle[l - 1] : 1.0;
   rb::sched_courant_kernel<<<1, RB_RED_NT, 0, c->stream>>>(
       c->d_partial, nblk, l, c->mp.levelmin, c->hp.courant_factor * L.dx / c->hp.smallc, L.leaf_cells > 0 ? 1 : 0,
       c->mp.boxlen / c->hp.smallc, nsub_prev, s);
   RB_CUDA(cudaGetLastError());
-  RB_TRY(set_unew_impl(c, l));
   if (l < c->mp.nlevelmax) {
     if (c->lv[l + 1].noct > 0) {
       RB_TRY(amr_step_dev(c, l + 1, 1));
@@ -665,8 +676,7 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   }
   RB_CUDA(cudaGetLastError());
   RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l));
-  RB_TRY(set_uold_impl(c, l));
-  RB_TRY(upload_fine_impl(c, l));
+  RB_TRY(set_uold_upload_impl(c, l));
   if (l > c->mp.levelmin && (c->mp.nsubcycle[l - 1] == 1 || icount == 2)) {
     rb::sched_end_kernel<<<1, 1, 0, c->stream>>>(s, l, c->mp.nsubcycle[l - 1] == 1 ? 1 : 0, icount);
     RB_CUDA(cudaGetLastError());
