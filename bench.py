@@ -235,6 +235,34 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def prim_errors(u_test, u_ref, cells, gamma):
+    """L1 (sum |d| / sum |ref|) and L-inf (max |d| / max |ref|) errors of
+    density, pressure and velocity magnitude of u_test against u_ref
+    (conservative (5, ncell) arrays) over the given 0-based cells."""
+    def prim(u):
+        r = u[0, cells]
+        v = u[1:4, cells] / r
+        p = (gamma - 1.0) * (u[4, cells] - 0.5 * r * (v * v).sum(axis=0))
+        return {"rho": r, "P": p, "v": np.sqrt((v * v).sum(axis=0))}
+    a, b = prim(u_test), prim(u_ref)
+    out = {}
+    for k in ("rho", "P", "v"):
+        d = np.abs(a[k] - b[k])
+        out[k] = {"l1": float(d.sum() / np.abs(b[k]).sum()), "linf": float(d.max() / np.abs(b[k]).max())}
+    return out
+
+
+def leaf_cell_index(tree):
+    """0-based Fortran-layout indices of every leaf cell of the tree."""
+    out = []
+    for l in range(1, tree.nlevelmax + 1):
+        if tree.noct(l) == 0:
+            continue
+        cells, _ = tree.cell_centres(l)
+        out.append(cells[tree.son[cells - 1] == 0] - 1)
+    return np.concatenate(out)
+
+
 def amr_workload(name):
     """Static AMR trees of the Sedov and blast-clump configurations.
     sedov: levels 6-9; levels 7-9 on a shell of radius 0.25 around the box
@@ -275,7 +303,7 @@ def run_amr(args):
     tree, hp, u, desc = amr_workload(args.amr)
     build_s = time.perf_counter() - t0
     levels = [l for l in range(1, tree.nlevelmax + 1) if tree.noct(l)]
-    out = {}
+    out, states = {}, {}
     for prec in ([args.only] if args.only else ["mixed", "fp64"]):
         s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
         for l in levels:
@@ -291,6 +319,20 @@ def run_amr(args):
         upd = s.cell_updates - before
         out[prec] = {"value": upd / (ms / 1e3), "ms_per_coarse_step": ms / max(n, 1), "coarse_steps": n,
                      "t": s.t, "tile_shapes": {l: s.tile_shape(l) for l in levels}, "clocks": clk.summary()}
+        if prec == "mixed" or args.only:
+            # hydro_flag on every level but the finest, on the final state
+            # (density and pressure gradients of 0.1): the refinement flags
+            # a remeshing step would use
+            from ramses_b200.params import RefineParams
+            rp = RefineParams(err_grad_d=0.1, err_grad_p=0.1)
+            flag1 = np.zeros(tree.ncell + 1, np.int32)
+            s.synchronize()
+            t0f = time.perf_counter()
+            nflag = sum(s.hydro_flag(l, rp, flag1)[1] for l in levels if l < tree.nlevelmax)
+            out[prec]["hydro_flag"] = {"ms_all_levels": (time.perf_counter() - t0f) * 1e3, "flagged": nflag,
+                                       "cells": int(sum(8 * tree.noct(l) for l in levels if l < tree.nlevelmax)),
+                                       "note": "host wall time incl. the flag download and OR into flag1"}
+        states[prec] = s.download_state()
         s.close()
     if args.only:
         print(json.dumps({"only": args.only, "amr": args.amr, **out[args.only]}), flush=True)
@@ -302,7 +344,10 @@ def run_amr(args):
                        "leaf_cells": int(sum(tree.leaf_cells(l) for l in levels)), "path": "rb_run, graphs of 8 "
                        "coarse steps, tile shapes autotuned per level", "tree_build_s": build_s},
             "fp64": out["fp64"], "mixed": out["mixed"], "clocks": out["mixed"]["clocks"],
-            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"]}
+            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "accuracy": {"mixed_vs_fp64_leaf_cells": prim_errors(states["mixed"], states["fp64"],
+                                                                 leaf_cell_index(tree), hp.gamma),
+                         "coarse_steps_compared": args.warmup + args.steps}}
     print(json.dumps(line), flush=True)
 
 
@@ -407,6 +452,7 @@ def main():
     rm, rf = u_mixed[0, idx], u_f64[0, idx]
     l1_rho = float(np.abs(rm - rf).sum() / np.abs(rf).sum())
     linf_rho = float(np.max(np.abs(rm - rf) / np.abs(rf)))
+    errs = prim_errors(u_mixed, u_f64, idx, hp.gamma)
     f64.close()
 
     # ---- end to end through the C ABI with host buffers ------------------
@@ -467,6 +513,7 @@ def main():
                      "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak},
             "mixed_over_fp64": value / f64_value,
             "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,
+                         "mixed_vs_fp64": errs,
                          "steps_compared": args.warmup + args.steps},
         }
         print(json.dumps(line), flush=True)

@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     q[2 * NS + s] = pq.v;
     q[3 * NS + s] = pq.w;
     q[4 * NS + s] = pq.p;
-    okf[s] = ok;
+    // bit 0: the cell is refined (its faces carry no flux); bit 1: the cell
+    // is a tile-interior cell of a present oct (its faces are used)
+    const bool interior = sx >= 2 && sx < 2 + TX && sy >= 2 && sy < 2 + TY && sz >= 2 && sz < 2 + TZ;
+    okf[s] = ok | ((interior && code >= 0) ? 2 : 0);
   }
   __syncthreads();
 
@@ -145,23 +148,32 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     const double dtdx = dt / a.dx;  // trace3d.f90 dtdx = dt/dx (dx=dy=dz)
     dtd[0] = dtd[1] = dtd[2] = (R)dtdx;
   }
+  // present(x,y,z): the tile-interior cell belongs to an oct of this level
+  // (its update and its faces are used; bit 1 of okf). A block coded -1 is
+  // absent and not a stencil source of any present oct, so no face touching
+  // it is used.
+  auto present = [&](int x, int y, int z) { return (okf[(x + 2) + SX * ((y + 2) + SY * (z + 2))] & 2) != 0; };
   for (int it = tid; it < G::NTRACE; it += NT) {
     int x, y, z;
     unsigned mask;
     if (it < G::NCELL) {
       x = it % TX; y = (it / TX) % TY; z = it / (TX * TY); mask = 7u;
+      if (blk[(x / 2 + 1) + BX * ((y / 2 + 1) + BY * (z / 2 + 1))] == -1) continue;
     } else {
       int r = it - G::NCELL;
       if (r < 2 * TY * TZ) {           // x slabs: x = -1 (qm only) and x = TX (qp only)
         const int side = r / (TY * TZ); r %= TY * TZ;
         x = side ? TX : -1; y = r % TY; z = r / TY; mask = 1u;
+        if (!present(side ? TX - 1 : 0, y, z)) continue;
       } else if ((r -= 2 * TY * TZ) < 2 * TX * TZ) {
         const int side = r / (TX * TZ); r %= TX * TZ;
         y = side ? TY : -1; x = r % TX; z = r / TX; mask = 2u;
+        if (!present(x, side ? TY - 1 : 0, z)) continue;
       } else {
         r -= 2 * TX * TZ;
         const int side = r / (TX * TY); r %= TX * TY;
         z = side ? TZ : -1; x = r % TX; y = r / TX; mask = 4u;
+        if (!present(x, y, side ? TZ - 1 : 0)) continue;
       }
     }
     const int s = (x + 2) + SX * ((y + 2) + SY * (z + 2));
@@ -238,6 +250,12 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     if (f < NFX) { d = 0; x = f % (TX + 1); y = (f / (TX + 1)) % TY; z = f / ((TX + 1) * TY); }
     else if (f < NFX + NFY) { const int r = f - NFX; d = 1; x = r % TX; y = (r / TX) % (TY + 1); z = r / (TX * (TY + 1)); }
     else { const int r = f - NFX - NFY; d = 2; x = r % TX; y = (r / TX) % TY; z = r / (TX * TY); }
+    // the face between cell (x,y,z) and its lower neighbour along d is used
+    // only when one of the two is a present cell
+    const int sr = (x + 2) + SX * ((y + 2) + SY * (z + 2));
+    const int sl = sr - (d == 0 ? 1 : d == 1 ? SX : SX * SY);
+    const int fl = okf[sl] | okf[sr];
+    if (!(fl & 2)) continue;
     Prim<R> L, Rr;
     L.r = qm[f]; L.u = qm[NF + f]; L.v = qm[2 * NF + f]; L.w = qm[3 * NF + f]; L.p = qm[4 * NF + f];
     Rr.r = qp[f]; Rr.u = qp[NF + f]; Rr.v = qp[2 * NF + f]; Rr.w = qp[3 * NF + f]; Rr.p = qp[4 * NF + f];
@@ -247,9 +265,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     riemann_sel<R, RS>(ql, qr, c, fg);
     from_face(fg, d, fo);
     // refined interface: either neighbour cell refined -> zero flux
-    const int sr = (x + 2) + SX * ((y + 2) + SY * (z + 2));
-    const int sl = sr - (d == 0 ? 1 : d == 1 ? SX : SX * SY);
-    const bool zero_face = okf[sl] | okf[sr];
+    const bool zero_face = (fl & 1) != 0;
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       R val;

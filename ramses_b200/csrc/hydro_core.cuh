@@ -462,8 +462,10 @@ __device__ __forceinline__ double cfl_speed(const double uu_in[5], const rb_hydr
   return e;
 }
 
-// Same speed with one reciprocal instead of four divisions (FP32-mixed path;
-// differs from cfl_speed in the last bits only).
+// Same speed for the FP32-mixed path: one reciprocal instead of four
+// divisions, the internal energy E - rho v^2/2 and its floor in FP64, the
+// sound speed's square root in FP32 (relative difference ~1e-7 from
+// cfl_speed; the dt minimum over cells stays an FP64 reduction).
 __device__ __forceinline__ double cfl_speed_fast(const double u[5], const rb_hydro_params& hp) {
   const double gamma = hp.gamma;
   const double rho = fmx(u[0], hp.smallr);
@@ -471,7 +473,7 @@ __device__ __forceinline__ double cfl_speed_fast(const double u[5], const rb_hyd
   const double v1 = u[1] * ir, v2 = u[2] * ir, v3 = u[3] * ir;
   double e = u[4] - 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
   e = fmx((gamma - 1.0) * e, rho * (hp.smallc * hp.smallc / gamma));
-  return 3.0 * sqrt(gamma * e * ir) + fabs(v1) + fabs(v2) + fabs(v3);
+  return 3.0 * (double)sqrtf((float)(gamma * e * ir)) + fabs(v1) + fabs(v2) + fabs(v3);
 }
 
 // With zero gravity the gravity-strength ratio of cmpdt is its floor 1e-4 in
