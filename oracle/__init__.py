@@ -99,6 +99,8 @@ def _declare(L):
     L.orc_getnborfather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
     L.orc_interpol_hydro.argtypes = [P, _PD, _PD, ctypes.c_int]
     L.orc_hydro_flag.argtypes = [P, ctypes.POINTER(OrcRefine), M, ctypes.c_int, _P32]
+    L.orc_dense_step.argtypes = [P, _PD, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int, ctypes.c_int, _PD]
     L.orc_hydro_flag.restype = ctypes.c_int64
 
 
@@ -128,6 +130,22 @@ def unsplit(hp, uin, gravin, dx, dt, ngrid=None):
     if rc:
         raise RuntimeError("orc_unsplit failed: %d" % rc)
     return flux, tmp
+
+
+def dense_step(hp, u, boxlen=1.0, bc_outflow=0, nvector=32):
+    """One coarse step of a complete level given as conservative
+    [5, nz, ny, nx] (advanced in place); returns dt. bc_outflow: bit d set
+    makes axis d an outflow (zero-gradient) boundary, else periodic."""
+    assert u.dtype == np.float64 and u.flags.c_contiguous and u.shape[0] == 5
+    nz, ny, nx = u.shape[1:]
+    dx = boxlen / nx
+    dt = ctypes.c_double()
+    p = params_struct(hp)
+    rc = lib().orc_dense_step(ctypes.byref(p), _ptr(u, _PD), nx, ny, nz, dx, boxlen / hp.smallc,
+                              int(bc_outflow), nvector, ctypes.byref(dt))
+    if rc:
+        raise RuntimeError("orc_dense_step failed: %d" % rc)
+    return dt.value
 
 
 class OracleRun:

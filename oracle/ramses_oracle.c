@@ -1250,3 +1250,82 @@ int64_t orc_hydro_flag(const orc_params *p, const orc_refine *r, const orc_mesh 
   }
   return nok;
 }
+
+/* ------------------------------------------------------------------------ */
+/* One coarse step of a complete level held as a dense grid                  */
+/* ------------------------------------------------------------------------ */
+/* u[v][z][y][x] (x fastest): courant_fine's dt (courant_fine.f90, cmpdt),
+ * then godfine1 on every oct: the 6^3 gather with the boundary rule of each
+ * axis, unsplit, and the conservative update in godfine1's order
+ * (godunov_fine.f90:751-792). Boundary rule per axis d (bit d of
+ * bc_outflow): periodic, or outflow (bound_type 2): the ghost cells take the
+ * value of the nearest interior cell, as make_boundary_hydro fills the
+ * boundary octs with ind_ref (hydro/hydro_boundary.f90:80-85,141-150). */
+int orc_dense_step(const orc_params *p, double *u, int nx, int ny, int nz, double dx, double dt_max,
+                   int bc_outflow, int nvector, double *dt_out) {
+  const int64_t n = (int64_t)nx * ny * nz;
+  const int nv = nvector;
+  const int dims[3] = {nx, ny, nz};
+  double *uu = (double *)malloc(sizeof(double) * nv * NV);
+  double *gg = (double *)calloc((size_t)nv * 3, sizeof(double));
+  double *unew = (double *)malloc(sizeof(double) * NV * n);
+  double *uin = (double *)malloc(sizeof(double) * (size_t)nv * 216 * NV);
+  double *gin = (double *)calloc((size_t)nv * 216 * 3, sizeof(double));
+  double *flux = (double *)malloc(sizeof(double) * (size_t)nv * 27 * NV * 3);
+  double *tmp = (double *)malloc(sizeof(double) * (size_t)nv * 27 * 2 * 3);
+  int64_t *cell0 = (int64_t *)malloc(sizeof(int64_t) * nv);
+  if (!uu || !gg || !unew || !uin || !gin || !flux || !tmp || !cell0) return -4;
+  /* courant_fine: dt = min(boxlen/smallc, courant_factor*dx/smallc, cell dts) */
+  double dt = dt_max;
+  for (int64_t c0 = 0; c0 < n; c0 += nv) {
+    int nb = (int)((n - c0) < nv ? (n - c0) : nv);
+    for (int ivar = 1; ivar <= NV; ivar++)
+      for (int i = 0; i < nb; i++) uu[i + (size_t)nv * (ivar - 1)] = u[(size_t)(ivar - 1) * n + c0 + i];
+    dt = fmind(dt, orc_cmpdt(p, uu, gg, dx, nb, nv));
+  }
+  memcpy(unew, u, sizeof(double) * NV * n);
+  const int ox_n = nx / 2, oy_n = ny / 2, oz_n = nz / 2;
+  const int64_t noct = (int64_t)ox_n * oy_n * oz_n;
+  for (int64_t o0 = 0; o0 < noct; o0 += nv) {
+    int ngrid = (int)((noct - o0) < nv ? (noct - o0) : nv);
+    for (int i = 0; i < ngrid; i++) {
+      int64_t o = o0 + i;
+      int ox = (int)(o % ox_n), oy = (int)((o / ox_n) % oy_n), oz = (int)(o / ((int64_t)ox_n * oy_n));
+      cell0[i] = (2 * ox) + (int64_t)nx * ((2 * oy) + (int64_t)ny * (2 * oz));
+      for (int kk = -1; kk <= 4; kk++)
+        for (int jj = -1; jj <= 4; jj++)
+          for (int ii = -1; ii <= 4; ii++) {
+            int c[3] = {2 * ox + ii - 1, 2 * oy + jj - 1, 2 * oz + kk - 1};
+            for (int d = 0; d < 3; d++) {
+              if (bc_outflow & (1 << d)) c[d] = c[d] < 0 ? 0 : (c[d] >= dims[d] ? dims[d] - 1 : c[d]);
+              else c[d] = (c[d] % dims[d] + dims[d]) % dims[d];
+            }
+            int64_t src = c[0] + (int64_t)nx * (c[1] + (int64_t)ny * c[2]);
+            for (int ivar = 1; ivar <= NV; ivar++)
+              uin[i + (size_t)nv * ((ii + 1) + 6 * ((jj + 1) + 6 * ((kk + 1) + 6 * (size_t)(ivar - 1))))] =
+                  u[(size_t)(ivar - 1) * n + src];
+          }
+    }
+    int rc = orc_unsplit(p, uin, gin, flux, tmp, dx, dx, dx, dt, ngrid, nv);
+    if (rc) return rc;
+    for (int idim = 1; idim <= 3; idim++) {
+      int i0 = idim == 1, j0 = idim == 2, k0 = idim == 3;
+      for (int k2 = 0; k2 <= 1; k2++)
+        for (int j2 = 0; j2 <= 1; j2++)
+          for (int i2 = 0; i2 <= 1; i2++) {
+            int i3 = 1 + i2, j3 = 1 + j2, k3 = 1 + k2;
+            int64_t off = i2 + (int64_t)nx * (j2 + (int64_t)ny * k2);
+            for (int ivar = 1; ivar <= NV; ivar++)
+              for (int i = 0; i < ngrid; i++) {
+                double *w = &unew[(size_t)(ivar - 1) * n + cell0[i] + off];
+                *w = *w + (flux[FI(nv, i, i3, j3, k3, ivar, idim)] -
+                           flux[FI(nv, i, i3 + i0, j3 + j0, k3 + k0, ivar, idim)]);
+              }
+          }
+    }
+  }
+  memcpy(u, unew, sizeof(double) * NV * n);
+  free(uu); free(gg); free(unew); free(uin); free(gin); free(flux); free(tmp); free(cell0);
+  if (dt_out) *dt_out = dt;
+  return 0;
+}

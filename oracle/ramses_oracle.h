@@ -101,6 +101,13 @@ int orc_getnborfather(const orc_mesh *m, int ind_cell, int ilevel,
  * returns the number of cells newly flagged. */
 int64_t orc_hydro_flag(const orc_params *p, const orc_refine *r, const orc_mesh *m, int ilevel, int32_t *flag1);
 
+/* One coarse step of a complete level held as a dense grid u[v][z][y][x]:
+ * courant_fine's dt, then godfine1 on every oct with a periodic or outflow
+ * (zero-gradient) boundary per axis (bit d of bc_outflow set: axis d
+ * outflow). u is advanced in place; dt_out receives the step's dt. */
+int orc_dense_step(const orc_params *p, double *u, int nx, int ny, int nz, double dx, double dt_max,
+                   int bc_outflow, int nvector, double *dt_out);
+
 /* interpol_hydro.f90:268-444 for nn father stencils:
  * u1(nn,0:6,5) -> u2(nn,1:8,5), column-major with leading dim nn. */
 int orc_interpol_hydro(const orc_params *p, double *u1, double *u2, int nn);

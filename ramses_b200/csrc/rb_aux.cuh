@@ -120,7 +120,8 @@ static __global__ void apply_corrections_kernel(double* __restrict__ unew, const
 // A second single-block pass reduces the partials in a fixed order. With
 // unew non-null the kernel also does the set_unew that follows courant_fine
 // in amr_step (godunov_fine.f90:40-130): unew = uold for every cell.
-template <int NT>
+// FAST (FP32-mixed contexts): the wave speed of cfl_speed_fast.
+template <int NT, bool FAST = false>
 static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double* __restrict__ uold,
                                                              const int32_t* __restrict__ son,
                                                              const int32_t* __restrict__ active, int32_t noct,
@@ -145,9 +146,14 @@ static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double
     mass = mass + u[0] * vol;
     etot = etot + u[4] * vol;
     double ei = u[4] * vol;
-    for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (u[d] * u[d]) / fmx(u[0], hp.smallr) * vol;
+    if (FAST) {
+      const double ir = __drcp_rn(fmx(u[0], hp.smallr));
+      for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (u[d] * u[d]) * ir * vol;
+    } else {
+      for (int d = 1; d <= 3; d++) ei = ei - 0.5 * (u[d] * u[d]) / fmx(u[0], hp.smallr) * vol;
+    }
     eint = eint + ei;
-    smax = fmx(smax, cfl_speed(u, hp));
+    smax = fmx(smax, FAST ? cfl_speed_fast(u, hp) : cfl_speed(u, hp));
   }
   __shared__ double red[4][NT / 32];
   for (int o = 16; o > 0; o >>= 1) {

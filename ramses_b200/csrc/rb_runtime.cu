@@ -587,9 +587,9 @@ int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin
   const int nt = 256;
   const int nblk = grid_for((int64_t)L.noct * 8, nt, 148 * 8);
   RB_TRY(ensure_partial(c, nblk));
-  rb::courant_partial_kernel<256><<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate,
-                                                              with_set_unew ? c->d_unew : nullptr);
+  auto k = c->precision == RB_PREC_MIXED ? rb::courant_partial_kernel<256, true> : rb::courant_partial_kernel<256, false>;
+  k<<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, c->hp,
+                                c->d_partial, c->gate, with_set_unew ? c->d_unew : nullptr);
   RB_CUDA(cudaGetLastError());
   const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
   rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, *dt_io, dt0,
@@ -655,9 +655,9 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   if (L.noct == 0) return RB_OK;
   double* s = c->d_sched;
   const int nblk = courant_blocks(c, l);
-  rb::courant_partial_kernel<256><<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell,
-                                                              c->mp.ncoarse, L.dx, c->hp, c->d_partial, c->gate,
-                                                              c->d_unew);  // + set_unew
+  auto k = c->precision == RB_PREC_MIXED ? rb::courant_partial_kernel<256, true> : rb::courant_partial_kernel<256, false>;
+  k<<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, c->hp,
+                                 c->d_partial, c->gate, c->d_unew);  // + set_unew
   RB_CUDA(cudaGetLastError());
   const double nsub_prev = l > c->mp.levelmin ? (double)(float)c->mp.nsubcycle[l - 1] : 1.0;
   rb::sched_courant_kernel<<<1, RB_RED_NT, 0, c->stream>>>(

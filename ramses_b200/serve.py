@@ -214,10 +214,13 @@ def draw_requests(count: int, seed: int = 0, sizes: Sequence[int] = (32, 64, 128
     return out
 
 
-def _prim_fn(spec: RequestSpec, gamma: float):
+def _prim_fn(spec: RequestSpec, gamma: float, outflow: bool = False):
     if spec.kind == "tube":
         p = spec.params
-        return ics.shock_tube_prim(p["rho_l"], p["p_l"], p["u_l"], p["rho_r"], p["p_r"], p["u_r"])
+        # with outflow in x the tube is [0, 1) with one interface at 0.5;
+        # in a periodic box its wrapped second interface sits half a box away
+        return ics.shock_tube_prim(p["rho_l"], p["p_l"], p["u_l"], p["rho_r"], p["p_r"], p["u_r"],
+                                   periodic_mirror=not outflow)
     # blast energy deposited in the cells of the finest level (the region of
     # r < 2.5 finest cells), as a RAMSES run of that levelmax would set it
     return ics.sedov_prim(spec.levelmin + spec.extra, energy=spec.params["energy"], gamma=gamma)
@@ -227,6 +230,7 @@ def _prim_fn(spec: RequestSpec, gamma: float):
 class BuiltRequest:
     spec: RequestSpec
     dense: Optional[np.ndarray] = None   # uniform problems
+    outflow_mask: int = 0                # dense problems: bit d = outflow boundaries along axis d
     tree: Optional[mesh.Octree] = None   # AMR problems (and the uniform tree of the baseline)
     uold: Optional[np.ndarray] = None
 
@@ -235,11 +239,13 @@ class BuiltRequest:
         return self.dense is not None
 
 
-def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 0.1) -> BuiltRequest:
+def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 0.1,
+                  outflow: bool = False) -> BuiltRequest:
     """Initial state of a request. Uniform requests become dense grids; AMR
     requests a static octree refined on the relative density/pressure
-    gradients of the initial state."""
-    prim = _prim_fn(spec, hp.gamma)
+    gradients of the initial state. outflow: the tube of a uniform request
+    has outflow (zero-gradient) boundaries in x instead of a periodic box."""
+    prim = _prim_fn(spec, hp.gamma, outflow and spec.extra == 0)
     lmin = spec.levelmin
     if spec.extra == 0:
         tree = mesh.uniform_tree(lmin)
@@ -247,7 +253,8 @@ def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 
         q = prim(x)
         u = np.zeros((5, tree.ncell))
         u[:, cells - 1] = ics.prim_to_cons(q, hp.gamma)
-        return BuiltRequest(spec, dense=dense_from_octree(tree, lmin, u))
+        mask = 1 if (outflow and spec.kind == "tube") else 0
+        return BuiltRequest(spec, dense=dense_from_octree(tree, lmin, u), outflow_mask=mask)
 
     def fields(x):
         q = prim(x)

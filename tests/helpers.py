@@ -62,3 +62,20 @@ def leaf_values(tree, u):
 
 def max_rel(a, b, floor=1e-300):
     return float(np.max(np.abs(a - b) / np.maximum(np.maximum(np.abs(a), np.abs(b)), floor)))
+
+
+def fingerprint(tree, u, gamma):
+    """Whole-state fingerprint in the style of the reference's regression
+    check (tests/visu/visu_ramses.py check_solution): over the leaf cells,
+    sum(log10|x|) for density and pressure and sum(|x|) for each velocity
+    component, components below 2e-14 |v| set to zero, summed with fsum."""
+    import math
+    _, q = leaf_values(tree, u)
+    rho = q[0]
+    v = q[1:4] / rho
+    p = (gamma - 1.0) * (q[4] - 0.5 * rho * (v * v).sum(axis=0))
+    vmag = np.sqrt((v * v).sum(axis=0))
+    v = np.where(np.abs(v) < 2e-14 * vmag, 0.0, v)
+    return {"density": math.fsum(np.log10(np.abs(rho))), "velocity_x": math.fsum(np.abs(v[0])),
+            "velocity_y": math.fsum(np.abs(v[1])), "velocity_z": math.fsum(np.abs(v[2])),
+            "pressure": math.fsum(np.log10(np.abs(p)))}

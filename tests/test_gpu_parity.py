@@ -253,3 +253,32 @@ def test_errors_are_reported(cuda_lib):
     bad.slope_type = 5
     with pytest.raises(ValueError):
         runtime.Solver(tree, bad)
+
+
+@pytest.mark.parametrize("case", ["sedov64_uniform_10", "sedov_amr_4_6_5"])
+def test_fingerprint_fixture(cuda_lib, case):
+    """Whole-state fingerprint of the device run against the committed
+    fixture (tests/golden/fingerprints.json) at the reference's regression
+    tolerance 3e-13; the uniform case runs through the z-streaming path and
+    through rb_run."""
+    import json
+    from pathlib import Path
+    from helpers import fingerprint
+    fx = json.loads((Path(__file__).parent / "golden" / "fingerprints.json").read_text())[case]
+    tree, hp, u = sedov_uniform(6) if case.startswith("sedov64") else sedov_amr(4, 6)
+    runs = []
+    with runtime.Solver(tree, hp, nsubcycle=[2] * 33, uold=u) as s:
+        for _ in range(fx["steps"]):
+            s.coarse_step()
+        runs.append((s.t, s.download_state()))
+    with runtime.Solver(tree, hp, nsubcycle=[2] * 33, uold=u) as s:
+        if case.startswith("sedov64"):
+            s.uniform_run(fx["steps"])
+        else:
+            s.run(max_steps=fx["steps"])
+        runs.append((s.t, s.download_state()))
+    for t, state in runs:
+        assert t == pytest.approx(fx["t"], rel=1e-15)
+        got = fingerprint(tree, state, hp.gamma)
+        for k, v in fx["fingerprint"].items():
+            assert got[k] == pytest.approx(v, rel=3e-13, abs=0), k

@@ -248,3 +248,69 @@ def test_hydro_flag_oracle_skips():
     assert n == 0
     f, n = orc.hydro_flag(4, RefineParams(err_grad_p=0.05))   # the blast's pressure jump
     assert n > 0 and int(f.sum()) == n
+
+
+@pytest.mark.parametrize("case", ["sedov64_uniform_10", "sedov_amr_4_6_5"])
+def test_oracle_matches_fingerprint_fixture(case):
+    """The oracle reproduces its committed whole-state fingerprints
+    (tests/golden/make_fingerprints.py) at the reference's regression
+    tolerance of 3e-13 (tests/visu/visu_ramses.py)."""
+    import json
+    from helpers import fingerprint, sedov_amr, sedov_uniform
+    fx = json.loads((Path(__file__).parent / "golden" / "fingerprints.json").read_text())[case]
+    tree, hp, u = sedov_uniform(6) if case.startswith("sedov64") else sedov_amr(4, 6)
+    orc = oracle.OracleRun(tree, hp, u, nsubcycle=[2] * 33)
+    for _ in range(fx["steps"]):
+        orc.coarse_step()
+    got = fingerprint(tree, orc.uold, hp.gamma)
+    for k, v in fx["fingerprint"].items():
+        assert got[k] == pytest.approx(v, rel=3e-13, abs=0), k
+
+
+@pytest.mark.parametrize("slope_type", [1, 2])
+def test_dense_step_periodic_equals_octree_step(slope_type):
+    """The dense-grid oracle step (used to pin outflow boundaries) equals the
+    octree oracle's coarse step bit for bit on a periodic complete level."""
+    from ramses_b200 import serve
+    lvl = 4
+    tree = mesh.uniform_tree(lvl)
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=slope_type, courant_factor=0.8)
+    q = ics.turbulent_box_prim_grid(2 ** lvl, seed=9, gamma=hp.gamma)
+    u = ics.fill_uniform_level_from_grid(tree, lvl, q, hp.gamma)
+    orc = oracle.OracleRun(tree, hp, u)
+    d = serve.dense_from_octree(tree, lvl, u)
+    t = 0.0
+    for _ in range(4):
+        orc.coarse_step()
+        t += oracle.dense_step(hp, d)
+        np.testing.assert_array_equal(d, serve.dense_from_octree(tree, lvl, orc.uold))
+    assert t == orc.t
+
+
+def test_dense_step_outflow_is_zero_gradient():
+    """Outflow along x: a uniform state stays uniform, and a planar tube's
+    wave leaves the box without the periodic image that a periodic x
+    boundary brings back."""
+    from ramses_b200 import serve
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+    n = 16
+    u = np.zeros((5, n, n, n))
+    u[0] = 1.0
+    u[1] = 0.3
+    u[4] = 2.5 + 0.5 * 0.09
+    w = u.copy()
+    oracle.dense_step(hp, w, bc_outflow=1)
+    np.testing.assert_allclose(w, u, rtol=1e-14, atol=1e-14)
+    spec = serve.RequestSpec("tube", n, 0, {"rho_l": 1.0, "p_l": 1.0, "u_l": 0.0, "rho_r": 0.125, "p_r": 0.1,
+                                            "u_r": 0.0})
+    a = serve.build_request(spec, hp, outflow=True).dense
+    b = a.copy()
+    for _ in range(3):
+        oracle.dense_step(hp, a, bc_outflow=1)
+        oracle.dense_step(hp, b, bc_outflow=0)
+    # the tube's state is uniform along y and z in both runs
+    assert np.all(a[0] == a[0][:1, :1, :])
+    # at the x edges the outflow run still holds the initial left/right states,
+    # the periodic run has the second interface's waves there
+    assert a[0, 0, 0, 0] == pytest.approx(1.0, abs=1e-12) and a[0, 0, 0, -1] == pytest.approx(0.125, abs=1e-12)
+    assert abs(b[0, 0, 0, 0] - 1.0) > 1e-3
