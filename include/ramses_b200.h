@@ -195,12 +195,14 @@ typedef struct rb_server rb_server;
 int rb_server_create(const rb_hydro_params *hp, int precision, int64_t hbm_budget_bytes, int steps_per_round,
                      rb_server **out);
 int rb_server_destroy(rb_server *srv);
-/* A periodic uniform problem as a dense grid: u[v][z][y][x] conservative
+/* A uniform problem as a dense grid: u[v][z][y][x] conservative
  * (rho, rho*u, rho*v, rho*w, E), nx = ny = nz, nx a multiple of 16. Every
  * step is a time step of the complete level (the z-streaming kernel, batched
- * with every other active dense problem); result has the layout of u. */
-int rb_server_submit_dense(rb_server *srv, int32_t nx, int32_t ny, int32_t nz, double boxlen, const double *u,
-                           double t_end, int64_t max_steps, double *result, int64_t *id);
+ * with every other active dense problem); result has the layout of u.
+ * outflow_mask bit d (x=0, y=1, z=2): outflow (zero-gradient, bound_type 2)
+ * boundaries along axis d; clear bits are periodic. */
+int rb_server_submit_dense(rb_server *srv, int32_t nx, int32_t ny, int32_t nz, double boxlen, int32_t outflow_mask,
+                           const double *u, double t_end, int64_t max_steps, double *result, int64_t *id);
 /* An AMR problem in the rb_sync_tree / rb_upload_state form; stepped by
  * coarse steps as rb_run does; result is uold(ncell,5). */
 int rb_server_submit_octree(rb_server *srv, const rb_mesh_params *mp, const int32_t *son, const int32_t *father,

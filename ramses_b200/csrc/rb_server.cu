@@ -46,6 +46,7 @@ struct Request {
   // dense
   int32_t nx = 0, ny = 0, nz = 0;
   int hz = 0, items = 0;
+  int outflow = 0;  // bit d: outflow boundaries along axis d
   double dx = 0.0;
   double* d_buf = nullptr;  // [2][5][n]
   int slot = -1;            // clock slot
@@ -263,6 +264,7 @@ int launch_round(rb_server* s) {
       d.a.partial = s->d_partial + (int64_t)off * 4;
       d.a.nx = r->nx; d.a.ny = r->ny; d.a.nz = r->nz;
       d.a.hz = r->hz;
+      d.a.outflow = r->outflow;
       int e2;
       d.a.dx_pow2 = std::frexp(r->dx, &e2) == 0.5;
       d.a.dx = r->dx;
@@ -490,10 +492,11 @@ static int check_stop(double t_end, int64_t max_steps) {
   return RB_OK;
 }
 
-int rb_server_submit_dense(rb_server* s, int32_t nx, int32_t ny, int32_t nz, double boxlen, const double* u,
-                           double t_end, int64_t max_steps, double* result, int64_t* id_out) {
+int rb_server_submit_dense(rb_server* s, int32_t nx, int32_t ny, int32_t nz, double boxlen, int32_t outflow_mask,
+                           const double* u, double t_end, int64_t max_steps, double* result, int64_t* id_out) {
   if (!s || !u || !result || !id_out) return fail(RB_ERR_INVALID, "null argument");
   RB_TRY(check_stop(t_end, max_steps));
+  if (outflow_mask < 0 || outflow_mask > 7) return fail(RB_ERR_INVALID, "outflow_mask %d: bits 0-2 only", outflow_mask);
   const int tx = rb::kStreamShapes[s->shape][0], ty = rb::kStreamShapes[s->shape][1];
   if (nx < tx || ny < ty || nz < 2 || nx % tx || ny % ty || nz % 2)
     return fail(RB_ERR_INVALID, "dense grid %dx%dx%d: nx must be a multiple of %d, ny of %d, nz even", nx, ny, nz,
@@ -507,6 +510,7 @@ int rb_server_submit_dense(rb_server* s, int32_t nx, int32_t ny, int32_t nz, dou
   r->h_in = u;
   r->h_out = result;
   r->nx = nx; r->ny = ny; r->nz = nz;
+  r->outflow = outflow_mask;
   r->dx = boxlen / nx;
   if (std::fabs(r->dx * ny - boxlen) > 1e-12 * boxlen || std::fabs(r->dx * nz - boxlen) > 1e-12 * boxlen) {
     delete r;

@@ -35,10 +35,15 @@ struct StreamArgs {
   int32_t nx, ny, nz;               // cells per dimension (multiples of TX, TY, hz; even)
   int32_t hz;                       // z extent of one work item
   int32_t dx_pow2;
+  int32_t outflow;                  // bit d: outflow (zero-gradient) boundaries along axis d, else periodic
   double dx, inv_dx;
   rb_hydro_params hp;
 };
 
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -140,24 +145,44 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   // every plane index used below is >= z0-2, so ring slots come from a
   // non-negative offset and constant moduli; periodic wraps need one step
   const int zbase = z0 - 2;
-  auto wrap = [](int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); };
+  // cell index along axis d outside [0, n): periodic wrap (one step is
+  // enough, every index is within 2 cells of the box), or with outflow
+  // boundaries the nearest interior cell, the zero-gradient ghost value that
+  // make_boundary_hydro gives (hydro/hydro_boundary.f90:80-85)
+  auto bnd = [&](int v, int n, int d) {
+    if (a.outflow & (1 << d)) return v < 0 ? 0 : (v >= n ? n - 1 : v);
+    return v < 0 ? v + n : (v >= n ? v - n : v);
+  };
   // Plane loads: thread tid < PAIRS owns the 2-cell (16-byte) piece (row, j)
   // of the stencil plane for all 5 variables; its offsets inside a plane do
   // not change along z, so they are computed once here.
+  // A piece starts at an even x and so lies wholly inside or wholly outside
+  // the box; with outflow in x an outside piece is two copies of the edge cell.
   const bool loader = tid < G::PAIRS;
   int piece_s = 0;
   int64_t piece_g = 0;
+  bool piece_dup = false;
   if (loader) {
     const int j = tid % (SX / 2), row = tid / (SX / 2);
+    const int x0 = tx0 - 2 + 2 * j;
     piece_s = row * SX + 2 * j;
-    piece_g = (int64_t)wrap(ty0 - 2 + row, a.ny) * a.nx + wrap(tx0 - 2 + 2 * j, a.nx);
+    piece_dup = (a.outflow & 1) && (x0 < 0 || x0 >= a.nx);
+    piece_g = (int64_t)bnd(ty0 - 2 + row, a.ny, 1) * a.nx + bnd(x0, a.nx, 0);
   }
   auto issue_plane = [&](int zp) {
     if (!loader) return;
     double* dst = raw + ((unsigned)(zp - zbase) % G::NRAW) * 5 * NS + piece_s;
-    const double* src = a.uin + (int64_t)wrap(zp, a.nz) * plane + piece_g;
+    const double* src = a.uin + (int64_t)bnd(zp, a.nz, 2) * plane + piece_g;
+    if (piece_dup) {
 #pragma unroll
-    for (int v = 0; v < 5; v++) cp_async16(dst + v * NS, src + v * vstr);
+      for (int v = 0; v < 5; v++) {
+        cp_async8(dst + v * NS, src + v * vstr);
+        cp_async8(dst + v * NS + 1, src + v * vstr);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v++) cp_async16(dst + v * NS, src + v * vstr);
+    }
   };
   auto load_u = [&](int zp, int s, double u[5]) {
     const double* p = raw + ((unsigned)(zp - zbase) % G::NRAW) * 5 * NS + s;

@@ -96,7 +96,8 @@ _PROTOS = {
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "rb_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rb_server_submit_dense": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
-                                              ctypes.c_double, _PD, ctypes.c_double, ctypes.c_int64, _PD, _P64]),
+                                              ctypes.c_double, ctypes.c_int32, _PD, ctypes.c_double, ctypes.c_int64,
+                                              _PD, _P64]),
     "rb_server_submit_octree": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MeshParamsC), _P32, _P32, _P32,
                                                _P32, _P32, _PD, ctypes.c_double, ctypes.c_int64, _PD, _P64]),
     "rb_server_progress": (ctypes.c_int, [ctypes.c_void_p, _P64, ctypes.c_int, _P32]),

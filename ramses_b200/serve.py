@@ -13,9 +13,10 @@ process. It reports p50/p99 time-to-solution (arrival -> result in host
 memory) and aggregate leaf-cell updates per second, beside the same stream
 served one request at a time by the plain FP64 path (``Solver.run``).
 
-Boundaries are periodic (the library's boundary condition); a tube sits in a
-periodic box as [x0-1/2, x0+1/2) so that its wrapped second interface is half
-a box away.
+Boundaries: uniform tubes have outflow (zero-gradient) boundaries in x and
+are periodic in y and z; Sedov blasts are periodic. AMR requests run on the
+octree, which is periodic, so an AMR tube sits in a periodic box with its
+wrapped second interface half a box away.
 """
 from __future__ import annotations
 
@@ -100,14 +101,15 @@ class Server:
         self.close()
 
     def submit_dense(self, u: np.ndarray, boxlen: float = 1.0, t_end: float = math.inf,
-                     max_steps: int = 1 << 40) -> int:
-        """Queue a periodic uniform problem given as conservative [5, n, n, n]."""
+                     max_steps: int = 1 << 40, outflow_mask: int = 0) -> int:
+        """Queue a uniform problem given as conservative [5, n, n, n];
+        outflow_mask bit d: outflow boundaries along axis d, else periodic."""
         u = np.ascontiguousarray(u, np.float64)
         assert u.ndim == 4 and u.shape[0] == 5
         nz, ny, nx = u.shape[1:]
         out = np.empty_like(u)
         rid = ctypes.c_int64()
-        _check(load().rb_server_submit_dense(self._h, nx, ny, nz, boxlen, _ptr(u, _PD), float(t_end),
+        _check(load().rb_server_submit_dense(self._h, nx, ny, nz, boxlen, int(outflow_mask), _ptr(u, _PD), float(t_end),
                                              int(max_steps), _ptr(out, _PD), ctypes.byref(rid)),
                "rb_server_submit_dense")
         self._keep[rid.value] = (u, out)
@@ -310,7 +312,7 @@ def run_stream(server: Server, reqs: Sequence[BuiltRequest], arrivals: Sequence[
         while k < n and arrivals[order[k]] <= now:
             i = int(order[k])
             b = reqs[i]
-            rid = (server.submit_dense(b.dense, t_end=t_end) if b.is_dense
+            rid = (server.submit_dense(b.dense, t_end=t_end, outflow_mask=b.outflow_mask) if b.is_dense
                    else server.submit_octree(b.tree, b.uold, t_end=t_end))
             ids[rid] = i
             arrive[i] = arrivals[i]
@@ -336,22 +338,19 @@ def run_stream(server: Server, reqs: Sequence[BuiltRequest], arrivals: Sequence[
 
 def one_at_a_time(reqs: Sequence[BuiltRequest], hp: HydroParams, t_end: float, precision: str = "fp64"
                   ) -> dict:
-    """Plain path, one request at a time: per request, a Solver (octree,
-    device-resident), rb_run to t_end, download. Returns service times."""
+    """The same requests served one at a time by the plain FP64 path: one
+    request on the GPU at a time (the FP64 z-streaming step for dense
+    problems, device-scheduled coarse steps as Solver.run for AMR ones),
+    submission to result in host memory. Returns the service times."""
     service, updates = [], 0
-    for b in reqs:
-        t0 = time.perf_counter()
-        if b.is_dense:
-            lvl = b.spec.levelmin
-            tree = mesh.uniform_tree(lvl)
-            u = octree_from_dense(tree, lvl, b.dense)
-        else:
-            tree, u = b.tree, b.uold
-        with Solver(tree, hp, precision=precision, uold=u) as s:
-            s.run(t_end=t_end)
-            s.download_state()
-            updates += s.cell_updates
-        service.append(time.perf_counter() - t0)
+    with Server(hp, precision=precision) as srv:
+        for b in reqs:
+            t0 = time.perf_counter()
+            rid = (srv.submit_dense(b.dense, t_end=t_end, outflow_mask=b.outflow_mask) if b.is_dense
+                   else srv.submit_octree(b.tree, b.uold, t_end=t_end))
+            srv.drain()
+            service.append(time.perf_counter() - t0)
+            updates += srv.info(rid)["cell_updates"]
     return {"service_s": service, "cell_updates": updates}
 
 
@@ -366,11 +365,13 @@ def main(argv=None):
     ap.add_argument("--steps-per-round", type=int, default=8)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--baseline", action="store_true", help="also serve the stream one at a time with plain FP64")
+    ap.add_argument("--periodic-tubes", action="store_true",
+                    help="tubes in a periodic box instead of outflow boundaries in x")
     args = ap.parse_args(argv)
     hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
     specs = draw_requests(args.requests, args.seed, [int(x) for x in args.sizes.split(",")], args.max_extra)
     t0 = time.perf_counter()
-    reqs = [build_request(s, hp) for s in specs]
+    reqs = [build_request(s, hp, outflow=not args.periodic_tubes) for s in specs]
     build_s = time.perf_counter() - t0
     arrivals = poisson_arrivals(len(reqs), args.rate, args.seed + 1)
     with Server(hp, precision=args.precision, steps_per_round=args.steps_per_round) as srv:

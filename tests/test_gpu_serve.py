@@ -151,3 +151,41 @@ def test_stream_harness(cuda_lib):
         res = serve.run_stream(srv, reqs, arr, t_end=2e-3)
     assert len(res["tts"]) == 6 and min(res["tts"]) > 0
     assert res["cell_updates"] > 0 and res["latency_s"]["p99"] >= res["latency_s"]["p50"]
+
+
+@pytest.mark.parametrize("mask", [0, 1, 7])
+def test_dense_request_matches_dense_oracle(cuda_lib, oracle_lib, mask):
+    """Dense problems with periodic (0), x-outflow (1) or all-outflow (7)
+    boundaries: the served FP64 state equals the oracle's dense step bit for
+    bit (outflow = the zero-gradient ghost cells of bound_type 2)."""
+    import oracle
+    spec = serve.RequestSpec("tube", 32, 0, {"rho_l": 2.0, "p_l": 3.0, "u_l": 0.4, "rho_r": 0.5, "p_r": 0.2,
+                                             "u_r": -0.3})
+    d = serve.build_request(spec, HP, outflow=True).dense
+    ref = d.copy()
+    t = 0.0
+    for _ in range(6):
+        t += oracle.dense_step(HP, ref, bc_outflow=mask)
+    with serve.Server(HP, precision="fp64", steps_per_round=4) as srv:
+        rid = srv.submit_dense(d, max_steps=6, outflow_mask=mask)
+        srv.drain()
+        inf = srv.info(rid)
+        assert inf["steps"] == 6 and inf["t"] == t
+        np.testing.assert_array_equal(srv.results[rid], ref)
+
+
+def test_outflow_mixed_close_to_fp64(cuda_lib):
+    spec = serve.RequestSpec("tube", 64, 0, {"rho_l": 1.0, "p_l": 1.0, "u_l": 0.0, "rho_r": 0.125, "p_r": 0.1,
+                                             "u_r": 0.0})
+    d = serve.build_request(spec, HP, outflow=True).dense
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with serve.Server(HP, precision=prec) as srv:
+            rid = srv.submit_dense(d, t_end=0.05, outflow_mask=1)
+            srv.drain()
+            out[prec] = srv.results[rid].copy()
+    r64, r32 = out["fp64"][0], out["mixed"][0]
+    assert np.abs(r32 - r64).sum() / np.abs(r64).sum() < 1e-5
+    # nothing re-entered through the x boundaries: the far left and right
+    # states are still the initial ones
+    assert r64[0, 0, 0] == pytest.approx(1.0, abs=1e-10) and r64[0, 0, -1] == pytest.approx(0.125, abs=1e-10)
