@@ -318,77 +318,6 @@ __device__ __forceinline__ void riemann(const R ql[5], const R qr[5], const Cons
   else riemann_llf(ql, qr, c, f);
 }
 
-// ---------------------------------------------------------------------------
-// Two HLLC problems at once in FP32 (the x and y faces a thread solves in the
-// FP32-mixed path): additions, multiplications and fused multiply-adds run as
-// the packed two-lane FP32 instructions of sm_100 (__fadd2_rn, __fmul2_rn,
-// __ffma2_rn); compares, selects, square roots and reciprocals per lane. Same
-// formulas as riemann_hllc<float>; f[5] (thermal flux) is not formed.
-// ---------------------------------------------------------------------------
-namespace f2 {
-__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
-__device__ __forceinline__ float2 add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-// a - b as fma(b, -1, a): the product is exact, so one rounding, as a - b
-__device__ __forceinline__ float2 sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-__device__ __forceinline__ float2 max(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
-__device__ __forceinline__ float2 min(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
-__device__ __forceinline__ float2 rcp(float2 a) { return make_float2(1.f / a.x, 1.f / a.y); }
-__device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
-__device__ __forceinline__ float2 sel(bool cx, bool cy, float2 a, float2 b) {
-  return make_float2(cx ? a.x : b.x, cy ? a.y : b.y);
-}
-}  // namespace f2
-
-__device__ __forceinline__ void riemann_hllc_pair(const float qa[5], const float qb[5], const float ra[5],
-                                                  const float rb[5], const Consts<float>& c, float fa[5],
-                                                  float fb[5]) {
-  using namespace f2;
-  const float2 half = mk(0.5f, 0.5f), smallr = mk(c.smallr, c.smallr), smallp = mk(c.smallp, c.smallp);
-  const float2 entho = mk(c.entho, c.entho), gam = mk(c.gamma, c.gamma);
-  const float2 smallc2 = mk(c.smallc * c.smallc, c.smallc * c.smallc);
-  // left states (a: first problem, b: second) and right states
-  const float2 rl = max(mk(qa[0], qb[0]), smallr), rr = max(mk(ra[0], rb[0]), smallr);
-  const float2 Pl = max(mk(qa[2], qb[2]), mul(rl, smallp)), Pr = max(mk(ra[2], rb[2]), mul(rr, smallp));
-  const float2 ul = mk(qa[1], qb[1]), ur = mk(ra[1], rb[1]);
-  const float2 vl = mk(qa[3], qb[3]), wl = mk(qa[4], qb[4]), vr = mk(ra[3], rb[3]), wr = mk(ra[4], rb[4]);
-  const float2 el = mul(Pl, entho), er = mul(Pr, entho);
-  const float2 hrl = mul(half, rl), hrr = mul(half, rr);
-  float2 ecinl = mul(mul(hrl, ul), ul), ecinr = mul(mul(hrr, ur), ur);
-  ecinl = add(ecinl, mul(hrl, mul(vl, vl)));
-  ecinr = add(ecinr, mul(hrr, mul(vr, vr)));
-  ecinl = add(ecinl, mul(hrl, mul(wl, wl)));
-  ecinr = add(ecinr, mul(hrr, mul(wr, wr)));
-  const float2 etotl = add(el, ecinl), etotr = add(er, ecinr);
-  const float2 cfastl = sqrt2(max(mul(mul(gam, Pl), rcp(rl)), smallc2));
-  const float2 cfastr = sqrt2(max(mul(mul(gam, Pr), rcp(rr)), smallc2));
-  const float2 cmax = max(cfastl, cfastr);
-  const float2 SL = sub(min(ul, ur), cmax), SR = add(max(ul, ur), cmax);
-  const float2 rcl = mul(rl, sub(ul, SL)), rcr = mul(rr, sub(SR, ur));
-  const float2 inv = rcp(add(rcr, rcl));
-  const float2 ustar = mul(add(add(mul(rcr, ur), mul(rcl, ul)), sub(Pl, Pr)), inv);
-  const float2 Pstar = mul(add(add(mul(rcr, Pl), mul(rcl, Pr)), mul(mul(rcl, rcr), sub(ul, ur))), inv);
-  // sampling at x/t = 0 with the star side picked first (as riemann_hllc)
-  const bool lx = ustar.x > 0.f, ly = ustar.y > 0.f;
-  const float2 rs = sel(lx, ly, rl, rr), us = sel(lx, ly, ul, ur), Ss = sel(lx, ly, SL, SR);
-  const float2 Pts = sel(lx, ly, Pl, Pr), ets = sel(lx, ly, etotl, etotr);
-  const float2 num = sub(Ss, us), invd = rcp(sub(Ss, ustar));
-  const float2 ro_s = mul(mul(rs, num), invd);
-  const float2 etoto_s = mul(add(sub(mul(num, ets), mul(Pts, us)), mul(Pstar, ustar)), invd);
-  const bool ox = SL.x > 0.f, oy = SL.y > 0.f;
-  const bool sx = !ox && (lx || SR.x > 0.f), sy = !oy && (ly || SR.y > 0.f);
-  const float2 ro = sel(ox, oy, rl, sel(sx, sy, ro_s, rr));
-  const float2 uo = sel(ox, oy, ul, sel(sx, sy, ustar, ur));
-  const float2 Ptoto = sel(ox, oy, Pl, sel(sx, sy, Pstar, Pr));
-  const float2 etoto = sel(ox, oy, etotl, sel(sx, sy, etoto_s, etotr));
-  const float2 rou = mul(ro, uo);
-  const float2 f0 = rou, f1 = add(mul(rou, uo), Ptoto), f2v = mul(add(etoto, Ptoto), uo);
-  const float2 f3 = mul(rou, sel(lx, ly, vl, vr)), f4 = mul(rou, sel(lx, ly, wl, wr));
-  fa[0] = f0.x; fa[1] = f1.x; fa[2] = f2v.x; fa[3] = f3.x; fa[4] = f4.x;
-  fb[0] = f0.y; fb[1] = f1.y; fb[2] = f2v.y; fb[3] = f3.y; fb[4] = f4.y;
-}
-
 // Riemann solver fixed at compile time (RS = RB_RIEMANN_*), or chosen at run
 // time from c.riemann when RS == 0.
 template <typename R, int RS>

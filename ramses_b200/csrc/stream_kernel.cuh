@@ -260,53 +260,25 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     R fx[5] = {0, 0, 0, 0, 0}, fy[5] = {0, 0, 0, 0, 0}, fz[5] = {0, 0, 0, 0, 0};
     const bool xface = upd_plane && valid && cx >= 0 && cy >= 0 && cy < TY;
     const bool yface = upd_plane && valid && cy >= 0 && cx >= 0 && cx < TX;
-    constexpr bool kPair = (RS == RB_RIEMANN_HLLC) && (sizeof(R) == 4);
-    if constexpr (kPair) {
-      if (xface || yface) {
-        // the x and y faces as one packed two-lane HLLC solve; a lane that
-        // needs only one of them reads its own column for the other (in range)
-        const int ox = xface ? slot - 1 : slot, oy = yface ? slot - CX : slot;
-        Prim<R> Lx, Ly;
-        Lx.r = xm[ox]; Lx.u = xm[NC + ox]; Lx.v = xm[2 * NC + ox]; Lx.w = xm[3 * NC + ox]; Lx.p = xm[4 * NC + ox];
-        Ly.r = ym[oy]; Ly.u = ym[NC + oy]; Ly.v = ym[2 * NC + oy]; Ly.w = ym[3 * NC + oy]; Ly.p = ym[4 * NC + oy];
-        float qlx[5], qrx[5], qly[5], qry[5], gx[5], gy[5];
-        to_face(Lx, 0, qlx);
-        to_face(sp[0], 0, qrx);
-        to_face(Ly, 1, qly);
-        to_face(sp[1], 1, qry);
-        riemann_hllc_pair(qlx, qly, qrx, qry, c, gx, gy);
-        const R gx6[6] = {gx[0], gx[1], gx[2], gx[3], gx[4], (R)0};
-        const R gy6[6] = {gy[0], gy[1], gy[2], gy[3], gy[4], (R)0};
-        R tx[5], ty[5];
-        from_face(gx6, 0, tx);
-        from_face(gy6, 1, ty);
-#pragma unroll
-        for (int v = 0; v < 5; v++) {
-          fx[v] = xface ? tx[v] : (R)0;
-          fy[v] = yface ? ty[v] : (R)0;
-        }
-      }
-    } else {
-      if (xface) {
-        const int o = slot - 1;  // column (cx-1, cy)
-        Prim<R> L;
-        L.r = xm[o]; L.u = xm[NC + o]; L.v = xm[2 * NC + o]; L.w = xm[3 * NC + o]; L.p = xm[4 * NC + o];
-        R ql[5], qr[5], fg[6];
-        to_face(L, 0, ql);
-        to_face(sp[0], 0, qr);
-        riemann_sel<R, RS>(ql, qr, c, fg);
-        from_face(fg, 0, fx);
-      }
-      if (yface) {
-        const int o = slot - CX;  // column (cx, cy-1)
-        Prim<R> L;
-        L.r = ym[o]; L.u = ym[NC + o]; L.v = ym[2 * NC + o]; L.w = ym[3 * NC + o]; L.p = ym[4 * NC + o];
-        R ql[5], qr[5], fg[6];
-        to_face(L, 1, ql);
-        to_face(sp[1], 1, qr);
-        riemann_sel<R, RS>(ql, qr, c, fg);
-        from_face(fg, 1, fy);
-      }
+    if (xface) {
+      const int o = slot - 1;  // column (cx-1, cy)
+      Prim<R> L;
+      L.r = xm[o]; L.u = xm[NC + o]; L.v = xm[2 * NC + o]; L.w = xm[3 * NC + o]; L.p = xm[4 * NC + o];
+      R ql[5], qr[5], fg[6];
+      to_face(L, 0, ql);
+      to_face(sp[0], 0, qr);
+      riemann_sel<R, RS>(ql, qr, c, fg);
+      from_face(fg, 0, fx);
+    }
+    if (yface) {
+      const int o = slot - CX;  // column (cx, cy-1)
+      Prim<R> L;
+      L.r = ym[o]; L.u = ym[NC + o]; L.v = ym[2 * NC + o]; L.w = ym[3 * NC + o]; L.p = ym[4 * NC + o];
+      R ql[5], qr[5], fg[6];
+      to_face(L, 1, ql);
+      to_face(sp[1], 1, qr);
+      riemann_sel<R, RS>(ql, qr, c, fg);
+      from_face(fg, 1, fy);
     }
     if (inner && k >= z0) {
       R ql[5], qr[5], fg[6];
