@@ -53,13 +53,33 @@ __device__ __forceinline__ Consts<R> make_consts(const rb_hydro_params& hp) {
 // ctoprim for one cell (umuscl.f90:861-965), conservative FP64 input.
 // The sound speed of ctoprim is only used by the PLMDE trace and is not formed.
 // ---------------------------------------------------------------------------
+// FP64 reciprocal for the FP32-mixed path: the FP32 reciprocal of x refined
+// by one Newton-Raphson step r <- r + r(1 - xr) in FP64, which squares the
+// relative error (~1e-7 -> ~1e-14). Valid for x inside the normal FP32 range
+// (1.2e-38 .. 3.4e38), which holds for densities floored at smallr.
+__device__ __forceinline__ double rcp_newton(double x) {
+  const double r = (double)(1.0f / (float)x);
+  return fma(r, fma(-x, r, 1.0), r);
+}
+
 template <typename R>
 __device__ __forceinline__ Prim<R> ctoprim_cell(const double u[5], const rb_hydro_params& hp) {
   const double gamma = hp.gamma;
   const double smalle = hp.smallc * hp.smallc / gamma / (gamma - 1.0);
   double q1 = fmx(u[0], hp.smallr);
-  // FP64 path: IEEE division as the reference; FP32-mixed: IEEE reciprocal
-  double oneoverrho = sizeof(R) == 8 ? 1.0 / q1 : __drcp_rn(q1);
+  if constexpr (sizeof(R) == 4) {
+    // FP32-mixed: velocities, E/rho - v^2/2 and its floor in FP64 from a
+    // Newton-refined reciprocal; the zero gravity predictor is dropped (it
+    // only changes the sign of a zero velocity)
+    const double ir = rcp_newton(q1);
+    const double q2 = u[1] * ir, q3 = u[2] * ir, q4 = u[3] * ir;
+    const double eint = fmx(u[4] * ir - 0.5 * (q2 * q2 + q3 * q3 + q4 * q4), smalle);
+    Prim<R> q;
+    q.r = (R)q1; q.u = (R)q2; q.v = (R)q3; q.w = (R)q4; q.p = (R)((gamma - 1.0) * q1 * eint);
+    return q;
+  }
+  // FP64 path: IEEE division as the reference
+  double oneoverrho = 1.0 / q1;
   double q2 = u[1] * oneoverrho;
   double q3 = u[2] * oneoverrho;
   double q4 = u[3] * oneoverrho;
@@ -83,8 +103,24 @@ __device__ __forceinline__ Prim<R> ctoprim_cell(const double u[5], const rb_hydr
 // One-direction limited slope (uslope, umuscl.f90:1241-1473) for slope types
 // 1 (minmod), 2 (moncen), 7 (van Leer), 8 (generalised moncen).
 // ---------------------------------------------------------------------------
+// FP32 form of the same limiters for the mixed path: the values of the
+// expressions below, with the factors of two moved out of the min/max
+// (exact scalings) and the sign applied last; a zero slope is +0.
+__device__ __forceinline__ float slope1_f32(float qm1, float q0, float qp1, int st, float theta) {
+  const float a = q0 - qm1, b = qp1 - q0;
+  const float m = fminf(fabsf(a), fabsf(b));
+  float s;
+  if (st == 1) s = copysignf(m, a);
+  else if (st == 2) { const float cen = 0.5f * (a + b); s = copysignf(fminf(2.0f * m, fabsf(cen)), cen); }
+  else if (st == 7) s = __fdividef(2.0f * a * b, a + b);
+  else if (st == 8) { const float cen = 0.5f * (a + b); s = copysignf(fminf(theta * m, fabsf(cen)), cen); }
+  else return 0.0f;
+  return a * b <= 0.0f ? 0.0f : s;
+}
+
 template <typename R>
 __device__ __forceinline__ R slope1(R qm1, R q0, R qp1, int st, R theta) {
+  if constexpr (sizeof(R) == 4) return slope1_f32(qm1, q0, qp1, st, theta);
   const R zero = (R)0, half = (R)0.5, one = (R)1;
   // minmod and van Leer are written as selects, not early returns: the same
   // values, without divergent branches inside a warp
@@ -136,6 +172,33 @@ __device__ __forceinline__ void trace_cell(const Prim<R>& q, const R dq[5][3], R
   const R dvx = dq[2][0], dvy = dq[2][1], dvz = dq[2][2];
   const R dwx = dq[3][0], dwy = dq[3][1], dwz = dq[3][2];
   const R dpx = dq[4][0], dpy = dq[4][1], dpz = dq[4][2];
+  if constexpr (sizeof(R) == 4) {
+    // FP32-mixed: the same predictor with the half-step source term
+    // s*dt/(2dx), equal in every direction on a cubic cell, added once:
+    // q -/+ dq/2 + s*dt/(2dx) = (q + s*dt/(2dx)) -/+ dq/2
+    const float th = dtd[0] * 0.5f;
+    const float divv = dux + dvy + dwz;
+    const float ir = 1.0f / r;
+    const float hr = r - th * (u * drx + v * dry + w * drz + divv * r);
+    const float hp = p - th * (u * dpx + v * dpy + w * dpz + divv * gamma * p);
+    const float hu = u - th * (u * dux + v * duy + w * duz + dpx * ir);
+    const float hv = v - th * (u * dvx + v * dvy + w * dvz + dpy * ir);
+    const float hw = w - th * (u * dwx + v * dwy + w * dwz + dpz * ir);
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      if (!(dirmask & (1u << d))) continue;
+      const float dr = half * dq[0][d], du = half * dq[1][d], dv = half * dq[2][d], dw = half * dq[3][d],
+                  dp = half * dq[4][d];
+      Prim<R> P, M;
+      P.r = hr - dr; P.u = hu - du; P.v = hv - dv; P.w = hw - dw; P.p = hp - dp;
+      M.r = hr + dr; M.u = hu + du; M.v = hv + dv; M.w = hw + dw; M.p = hp + dp;
+      if (P.r < smallr) P.r = r;
+      if (M.r < smallr) M.r = r;
+      qp[d] = P;
+      qm[d] = M;
+    }
+    return;
+  }
   // source terms (:576-580)
   const R sr0 = -(u * drx) - v * dry - w * drz - (dux + dvy + dwz) * r;
   const R sp0 = -(u * dpx) - v * dpy - w * dpz - (dux + dvy + dwz) * gamma * p;
@@ -238,6 +301,44 @@ __device__ __forceinline__ void riemann_hll(const R ql[5], const R qr[5], const 
 template <typename R>
 __device__ __forceinline__ void riemann_hllc(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
   // :988-1209 (only the sampled star state is formed; the others are dead)
+  if constexpr (sizeof(R) == 4) {
+    // FP32-mixed: the same solver with the kinetic energy summed before the
+    // product with rho/2, and the sampled state picked by one side select
+    // (left if SL > 0 or ustar > 0) and one star-or-outer select
+    const float rl = fmaxf(ql[0], c.smallr), ul = ql[1], Pl = fmaxf(ql[2], rl * c.smallp);
+    const float rr = fmaxf(qr[0], c.smallr), ur = qr[1], Pr = fmaxf(qr[2], rr * c.smallp);
+    const float el = Pl * c.entho, er = Pr * c.entho;
+    const float etotl = el + 0.5f * rl * (ul * ul + ql[3] * ql[3] + ql[4] * ql[4]);
+    const float etotr = er + 0.5f * rr * (ur * ur + qr[3] * qr[3] + qr[4] * qr[4]);
+    const float smallc2 = c.smallc * c.smallc;
+    const float cfastl = sqrtf(fmaxf(c.gamma * Pl * __fdividef(1.0f, rl), smallc2));
+    const float cfastr = sqrtf(fmaxf(c.gamma * Pr * __fdividef(1.0f, rr), smallc2));
+    const float cmax = fmaxf(cfastl, cfastr);
+    const float SL = fminf(ul, ur) - cmax, SR = fmaxf(ul, ur) + cmax;
+    const float rcl = rl * (ul - SL), rcr = rr * (SR - ur);
+    const float inv = __fdividef(1.0f, rcr + rcl);
+    const float ustar = (rcr * ur + rcl * ul + (Pl - Pr)) * inv;
+    const float Pstar = (rcr * Pl + rcl * Pr + rcl * rcr * (ul - ur)) * inv;
+    const bool outl = SL > 0.0f, lft = ustar > 0.0f;
+    const bool side = outl || lft;
+    const bool star = !outl && (lft || SR > 0.0f);
+    const float rs = side ? rl : rr, us = side ? ul : ur, Ss = side ? SL : SR;
+    const float Ps = side ? Pl : Pr, ets = side ? etotl : etotr, es = side ? el : er;
+    const float num = Ss - us, iden = __fdividef(1.0f, Ss - ustar);
+    const float ro = star ? rs * num * iden : rs;
+    const float uo = star ? ustar : us;
+    const float Po = star ? Pstar : Ps;
+    const float eto = star ? (num * ets - Ps * us + Pstar * ustar) * iden : ets;
+    const float eo = star ? es * num * iden : es;
+    const float mo = ro * uo;
+    f[0] = mo;
+    f[1] = mo * uo + Po;
+    f[2] = (eto + Po) * uo;
+    f[3] = mo * (lft ? ql[3] : qr[3]);
+    f[4] = mo * (lft ? ql[4] : qr[4]);
+    f[5] = uo * eo;
+    return;
+  }
   const R half = c.half;
   R rl = fmx(ql[0], c.smallr);
   R Pl = fmx(ql[2], rl * c.smallp);
@@ -462,18 +563,20 @@ __device__ __forceinline__ double cfl_speed(const double uu_in[5], const rb_hydr
   return e;
 }
 
-// Same speed for the FP32-mixed path: one reciprocal instead of four
-// divisions, the internal energy E - rho v^2/2 and its floor in FP64, the
-// sound speed's square root in FP32 (relative difference ~1e-7 from
-// cfl_speed; the dt minimum over cells stays an FP64 reduction).
+// Same speed for the FP32-mixed path: the internal energy
+// E - |m|^2/(2 rho) and its floor in FP64 (a Newton-refined reciprocal instead
+// of four divisions), the sound speed and the velocity sum in FP32 (relative
+// difference ~1e-7 from cfl_speed; the dt minimum over cells is formed from
+// the maximum speed as in the FP64 path).
 __device__ __forceinline__ double cfl_speed_fast(const double u[5], const rb_hydro_params& hp) {
   const double gamma = hp.gamma;
-  const double rho = fmx(u[0], hp.smallr);
-  const double ir = __drcp_rn(rho);
-  const double v1 = u[1] * ir, v2 = u[2] * ir, v3 = u[3] * ir;
-  double e = u[4] - 0.5 * rho * (v1 * v1 + v2 * v2 + v3 * v3);
-  e = fmx((gamma - 1.0) * e, rho * (hp.smallc * hp.smallc / gamma));
-  return 3.0 * (double)sqrtf((float)(gamma * e * ir)) + fabs(v1) + fabs(v2) + fabs(v3);
+  const double rho = fmax(u[0], hp.smallr);
+  const double ir = rcp_newton(rho);
+  double e = u[4] - 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) * ir;
+  e = fmax((gamma - 1.0) * e, rho * (hp.smallc * hp.smallc / gamma));
+  const float irf = (float)ir;
+  const float vs = (fabsf((float)u[1]) + fabsf((float)u[2]) + fabsf((float)u[3])) * irf;
+  return (double)(3.0f * sqrtf((float)(gamma * e) * irf) + vs);
 }
 
 // With zero gravity the gravity-strength ratio of cmpdt is its floor 1e-4 in

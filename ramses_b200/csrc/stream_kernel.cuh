@@ -238,8 +238,9 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
         dq[v][2] = slope1<R>(zm[v], own[v], zp[v], slope_type, c.slope_theta);
       }
     }
+    // the ring columns (whole warps after the interior ones) solve no z face
     Prim<R> sp[3], sm[3];
-    trace_cell<R>(q_0, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
+    trace_cell<R>(q_0, dq, c.gamma, c.smallr, dtd, sp, sm, inner ? 7u : 3u);
     if (valid) {
       const int o = slot;
       xm[o] = sm[0].r; xm[NC + o] = sm[0].u; xm[2 * NC + o] = sm[0].v; xm[3 * NC + o] = sm[0].w; xm[4 * NC + o] = sm[0].p;
@@ -287,7 +288,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
       riemann_sel<R, RS>(ql, qr, c, fg);
       from_face(fg, 2, fz);
     }
-    qmz_prev = sm[2];
+    if (inner) qmz_prev = sm[2];
     // flux*dt/dx evaluated as (fx*dt)/dx (umuscl.f90:101-163); dividing by an
     // exact power-of-two dx equals multiplying by its reciprocal
     // Each face flux is rounded to FP64 once, by the face's owner, so that the
@@ -324,7 +325,8 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
           un[v] = upd[v] + (fzb[v] - fzd[v]);
           a.uout[v * vstr + zo + col] = un[v];
         }
-        smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(un, a.hp) : cfl_speed_fast(un, a.hp));
+        if constexpr (sizeof(R) == 8) smax = fmx(smax, cfl_speed(un, a.hp));
+        else smax = fmax(smax, cfl_speed_fast(un, a.hp));
       }
       if (upd_plane) {
         double uo[5];
