@@ -66,6 +66,47 @@ struct TileGeom {
   static_assert(5 * NF <= 5 * NS, "flux must fit in the stencil buffer");
 };
 
+// Stencil cells read by the slopes of types 0, 1, 2, 7 and 8: the tile, its
+// one-cell face slabs and their six neighbours. Listed block-major as
+// (block << 3 | child): all children of a block with at most one halo
+// coordinate, the two inner-layer children of an edge block (two halo
+// coordinates), nothing of a corner block.
+template <int TX, int TY, int TZ>
+constexpr int gather_children(int b, int ch) {
+  using G = TileGeom<TX, TY, TZ>;
+  const int bx = b % G::BX, by = (b / G::BX) % G::BY, bz = b / (G::BX * G::BY);
+  const bool hx = bx == 0 || bx == G::BX - 1, hy = by == 0 || by == G::BY - 1, hz = bz == 0 || bz == G::BZ - 1;
+  const int nh = (int)hx + (int)hy + (int)hz;
+  if (nh <= 1) return 1;
+  if (nh == 3) return 0;
+  // inner layer: child 1 of the first block, child 0 of the last
+  const int px = ch & 1, py = (ch >> 1) & 1, pz = ch >> 2;
+  if (hx && px != (bx == 0 ? 1 : 0)) return 0;
+  if (hy && py != (by == 0 ? 1 : 0)) return 0;
+  if (hz && pz != (bz == 0 ? 1 : 0)) return 0;
+  return 1;
+}
+template <int TX, int TY, int TZ>
+constexpr int gather_count() {
+  int n = 0;
+  for (int b = 0; b < TileGeom<TX, TY, TZ>::NBLK; b++)
+    for (int ch = 0; ch < 8; ch++) n += gather_children<TX, TY, TZ>(b, ch);
+  return n;
+}
+template <int TX, int TY, int TZ>
+struct GatherList {
+  static constexpr int N = gather_count<TX, TY, TZ>();
+  uint16_t e[N];
+  constexpr GatherList() : e{} {
+    int n = 0;
+    for (int b = 0; b < TileGeom<TX, TY, TZ>::NBLK; b++)
+      for (int ch = 0; ch < 8; ch++)
+        if (gather_children<TX, TY, TZ>(b, ch)) e[n++] = (uint16_t)(b << 3 | ch);
+  }
+};
+template <int TX, int TY, int TZ>
+__device__ const GatherList<TX, TY, TZ> kGatherList{};
+
 template <typename R, int TX, int TY, int TZ>
 constexpr size_t tile_smem_bytes() {
   using G = TileGeom<TX, TY, TZ>;
@@ -102,42 +143,69 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   // ---- A. gather + ctoprim ------------------------------------------------
   const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
   const bool slope27 = (slope_type == 3);
-  for (int it = tid; it < NBLK * 8; it += NT) {
-    const int b = it >> 3, ch = it & 7;
+  // one stencil cell: its raw state is loaded by gather_cell and converted by
+  // put_cell, so that the loads of several cells are in flight together.
+  // Blocks coded -1 are read by no present cell: only their flags are set.
+  auto gather_cell = [&](int b, int ch, double u[5], int& code, int& sonv, int& inner) -> int {
     const int bx = b % BX, by = (b / BX) % BY, bz = b / (BX * BY);
     const int sx = 2 * bx + (ch & 1), sy = 2 * by + ((ch >> 1) & 1), sz = 2 * bz + (ch >> 2);
-    const int s = sx + SX * (sy + SY * sz);
-    const int code = blk[b];
-    double u[5];
-    unsigned char ok = 0;
-    bool have = true;
-    if (!slope27) {
-      // corner cells of the stencil are read by no slope of types 0,1,2,7,8
-      const int hx = (sx < 2) | (sx >= SX - 2), hy = (sy < 2) | (sy >= SY - 2), hz = (sz < 2) | (sz >= SZ - 2);
-      if (hx + hy + hz == 3) have = false;
-    }
-    if (have && code >= 0) {
+    code = blk[b];
+    sonv = 0;
+    if (code >= 0) {
       const int64_t dc = (int64_t)a.ncoarse + (int64_t)code * 8 + ch;
 #pragma unroll
       for (int v = 0; v < 5; v++) u[v] = __ldg(a.uold + v * ncell + dc);
-      if (a.has_refined) ok = __ldg(a.son + dc) > 0;
-    } else if (have && code <= -2) {
+      if (a.has_refined) sonv = __ldg(a.son + dc);
+    } else if (code <= -2) {
       const int64_t e = (int64_t)(-code - 2) * 8 + ch;
 #pragma unroll
       for (int v = 0; v < 5; v++) u[v] = __ldg(a.interp + v * a.ninterp8 + e);
-    } else {
-      u[0] = 1.0; u[1] = 0.0; u[2] = 0.0; u[3] = 0.0; u[4] = 1.0;
     }
-    Prim<R> pq = ctoprim_cell<R>(u, a.hp);
+    // a tile-interior cell of a present oct (its faces and update are used)
+    inner = sx >= 2 && sx < 2 + TX && sy >= 2 && sy < 2 + TY && sz >= 2 && sz < 2 + TZ && code >= 0;
+    return sx + SX * (sy + SY * sz);
+  };
+  auto put_cell = [&](int s, const double u[5], int code, int sonv, int inner) {
+    // okf bit 0: the cell is refined (its faces carry no flux); bit 1: a
+    // tile-interior cell of a present oct
+    okf[s] = (unsigned char)((sonv > 0 ? 1 : 0) | (inner ? 2 : 0));
+    if (code == -1) return;
+    const Prim<R> pq = ctoprim_cell<R>(u, a.hp);
     q[0 * NS + s] = pq.r;
     q[1 * NS + s] = pq.u;
     q[2 * NS + s] = pq.v;
     q[3 * NS + s] = pq.w;
     q[4 * NS + s] = pq.p;
-    // bit 0: the cell is refined (its faces carry no flux); bit 1: the cell
-    // is a tile-interior cell of a present oct (its faces are used)
-    const bool interior = sx >= 2 && sx < 2 + TX && sy >= 2 && sy < 2 + TY && sz >= 2 && sz < 2 + TZ;
-    okf[s] = ok | ((interior && code >= 0) ? 2 : 0);
+  };
+  if (!slope27) {
+    using GL = GatherList<TX, TY, TZ>;
+    constexpr int NG = GL::N;
+    constexpr int PER = (NG + NT - 1) / NT;
+    constexpr int NB = PER < 2 ? PER : 2;
+    for (int j0 = 0; j0 < PER; j0 += NB) {
+      double u[NB][5];
+      int sidx[NB], code[NB], sonv[NB], inner[NB];
+#pragma unroll
+      for (int j = 0; j < NB; j++) {
+        const int it = tid + (j0 + j) * NT;
+        sidx[j] = -1;
+        if (j0 + j < PER && it < NG) {
+          const int e = __ldg(&kGatherList<TX, TY, TZ>.e[it]);
+          sidx[j] = gather_cell(e >> 3, e & 7, u[j], code[j], sonv[j], inner[j]);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < NB; j++)
+        if (sidx[j] >= 0) put_cell(sidx[j], u[j], code[j], sonv[j], inner[j]);
+    }
+  } else {
+    // the 27-point slopes read every cell of the stencil
+    for (int it = tid; it < NBLK * 8; it += NT) {
+      double u[5];
+      int code, sonv, inner;
+      const int s = gather_cell(it >> 3, it & 7, u, code, sonv, inner);
+      put_cell(s, u, code, sonv, inner);
+    }
   }
   __syncthreads();
 
@@ -339,14 +407,30 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
 
   // ---- E. boundary fluxes for the fine-to-coarse correction --------------------
   if (a.corr_slot != nullptr) {
+    // list the tile's octs that own a correction slot (one slot lookup per
+    // oct), then store their 6 x 4 x 5 boundary fluxes; the list order does
+    // not matter, each oct writes only its own slot
     constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
-    for (int it = tid; it < NOCT * 120; it += NT) {
-      const int o = it / 120, r = it % 120;
-      const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
+    static_assert(NOCT <= NT, "one thread per oct of the tile");
+    __shared__ int32_t corr_oct[NOCT], corr_at[NOCT];
+    __shared__ int32_t ncorr;
+    if (tid == 0) ncorr = 0;
+    __syncthreads();
+    if (tid < NOCT) {
+      const int ox = tid % (TX / 2), oy = (tid / (TX / 2)) % (TY / 2), oz = tid / ((TX / 2) * (TY / 2));
       const int code = blk[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
-      if (code < 0) continue;
-      const int slot = __ldg(a.corr_slot + code);
-      if (slot < 0) continue;
+      const int slot = code >= 0 ? __ldg(a.corr_slot + code) : -1;
+      if (slot >= 0) {
+        const int i = atomicAdd(&ncorr, 1);
+        corr_oct[i] = tid;
+        corr_at[i] = slot;
+      }
+    }
+    __syncthreads();
+    for (int it = tid; it < ncorr * 120; it += NT) {
+      const int i = it / 120, r = it % 120;
+      const int o = corr_oct[i], slot = corr_at[i];
+      const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
       const int face = r / 20, cc = (r / 5) % 4, v = r % 5;   // face 0..5 = -x,+x,-y,+y,-z,+z
       const int d = face >> 1, side = face & 1;
       const int t1 = cc & 1, t2 = cc >> 1;
