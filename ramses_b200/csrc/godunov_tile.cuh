@@ -32,7 +32,8 @@ struct TileArgs {
   const int32_t* __restrict__ son;      // [ncell], device cell layout
   const double* __restrict__ interp;    // [5][ninterp*8] prolongated blocks
   const int32_t* __restrict__ tile_blk; // [ntile][NBLK] block codes
-  const int32_t* __restrict__ corr_slot;// [ngridmax] slot or -1 (may be null)
+  const int32_t* __restrict__ tile_corr;// [ntile][1 + 2*NOCT]: count, then (oct in tile, slot)
+                                        // of the octs owning a correction slot (null: none)
   double* __restrict__ corr_flux;       // [nslot][6][4][5]
   int64_t ncell;
   int64_t ninterp8;                     // ninterp*8 (stride of interp)
@@ -137,7 +138,12 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   const Consts<R> c = make_consts<R>(a.hp);
   const int64_t ncell = a.ncell;
 
+  constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
+  constexpr int NREC = 1 + 2 * NOCT;
+  __shared__ int32_t corr_rec[NREC];
   for (int i = tid; i < NBLK; i += NT) blk[i] = a.tile_blk[(int64_t)tile * NBLK + i];
+  if (a.tile_corr != nullptr)
+    for (int i = tid; i < NREC; i += NT) corr_rec[i] = a.tile_corr[(int64_t)tile * NREC + i];
   __syncthreads();
 
   // ---- A. gather + ctoprim ------------------------------------------------
@@ -406,30 +412,11 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   }
 
   // ---- E. boundary fluxes for the fine-to-coarse correction --------------------
-  if (a.corr_slot != nullptr) {
-    // list the tile's octs that own a correction slot (one slot lookup per
-    // oct), then store their 6 x 4 x 5 boundary fluxes; the list order does
-    // not matter, each oct writes only its own slot
-    constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
-    static_assert(NOCT <= NT, "one thread per oct of the tile");
-    __shared__ int32_t corr_oct[NOCT], corr_at[NOCT];
-    __shared__ int32_t ncorr;
-    if (tid == 0) ncorr = 0;
-    __syncthreads();
-    if (tid < NOCT) {
-      const int ox = tid % (TX / 2), oy = (tid / (TX / 2)) % (TY / 2), oz = tid / ((TX / 2) * (TY / 2));
-      const int code = blk[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
-      const int slot = code >= 0 ? __ldg(a.corr_slot + code) : -1;
-      if (slot >= 0) {
-        const int i = atomicAdd(&ncorr, 1);
-        corr_oct[i] = tid;
-        corr_at[i] = slot;
-      }
-    }
-    __syncthreads();
+  if (a.tile_corr != nullptr) {
+    const int ncorr = corr_rec[0];
     for (int it = tid; it < ncorr * 120; it += NT) {
       const int i = it / 120, r = it % 120;
-      const int o = corr_oct[i], slot = corr_at[i];
+      const int o = corr_rec[1 + 2 * i], slot = corr_rec[2 + 2 * i];
       const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
       const int face = r / 20, cc = (r / 5) % 4, v = r % 5;   // face 0..5 = -x,+x,-y,+y,-z,+z
       const int d = face >> 1, side = face & 1;

@@ -82,6 +82,7 @@ struct Level {
   int shape = -1;
   int ntile = 0;
   int32_t* d_tile_blk = nullptr;
+  int32_t* d_tile_corr = nullptr; // [ntile][1 + 2*octs per tile] correction-slot octs (null: none)
   int ninterp = 0;
   int32_t* d_interp7 = nullptr;
   double* d_interp_buf = nullptr;
@@ -131,7 +132,6 @@ struct rb_context {
   double* d_uold = nullptr;
   double* d_unew = nullptr;
   int32_t* d_son = nullptr;
-  int32_t* d_corr_slot = nullptr;   // [ngridmax]
   double* d_stage = nullptr;        // Fortran-layout staging [5*ncell]
   double* d_partial = nullptr;      // CFL partials
   int64_t partial_cap = 0;
@@ -155,7 +155,7 @@ struct rb_context {
   rbi::Level lv[RB_MAXLEVEL + 2];
   std::vector<rbi::OctIndex> idx;        // per-level position -> igrid lookup
   int finest = 0;                   // finest level holding octs
-  std::vector<int32_t> h_corr_slot; // host copy of d_corr_slot
+  std::vector<int32_t> h_corr_slot; // [ngridmax] correction slot of each oct or -1 (table building)
   std::vector<cudaEvent_t> evpool;  // per-step kernel timing events
   float kernel_ms_avg = 0.f;        // mean tile-kernel time of the last timed run
   cudaGraphExec_t graph = nullptr;  // cached uniform-run graph

@@ -74,6 +74,7 @@ inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
 
 void free_level_tables(Level& L) {
   dfree(L.d_tile_blk);
+  dfree(L.d_tile_corr);
   dfree(L.d_interp7);
   dfree(L.d_interp_buf);
   dfree(L.d_corr_flux);
@@ -304,7 +305,27 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   // this level's entries of the per-oct correction slot table
   for (int32_t g : L.h_active) c->h_corr_slot[g - 1] = -1;
   for (size_t i = 0; i + 1 < h_slot_upd.size(); i += 2) c->h_corr_slot[h_slot_upd[i]] = h_slot_upd[i + 1];
-  RB_TRY(h2d(c, c->d_corr_slot, c->h_corr_slot.data(), c->h_corr_slot.size() * 4));
+  // per tile, the octs that own a correction slot: [count, (oct position in
+  // the tile, slot) x count], so that the godunov kernel stores their
+  // boundary fluxes without looking slots up
+  if (nslot) {
+    const int NOCT = TOX * TOY * TOZ, REC = 1 + 2 * NOCT;
+    std::vector<int32_t> rec((size_t)L.ntile * REC, 0);
+    for (int t = 0; t < L.ntile; t++) {
+      const int32_t* B = &blk[(size_t)t * NBLK];
+      int32_t* Rt = &rec[(size_t)t * REC];
+      for (int o = 0; o < NOCT; o++) {
+        const int ox = o % TOX, oy = (o / TOX) % TOY, oz = o / (TOX * TOY);
+        const int32_t code = B[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
+        if (code < 0 || c->h_corr_slot[code] < 0) continue;
+        Rt[1 + 2 * Rt[0]] = o;
+        Rt[2 + 2 * Rt[0]] = c->h_corr_slot[code];
+        Rt[0]++;
+      }
+    }
+    RB_TRY(dalloc(&L.d_tile_corr, rec.size()));
+    RB_TRY(h2d(c, L.d_tile_corr, rec.data(), rec.size() * 4));
+  }
   L.tables_built = true;
   return RB_OK;
 }
@@ -528,7 +549,7 @@ rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
   a.son = c->d_son;
   a.interp = L.d_interp_buf;
   a.tile_blk = L.d_tile_blk;
-  a.corr_slot = L.nslot ? c->d_corr_slot : nullptr;
+  a.tile_corr = L.nslot ? L.d_tile_corr : nullptr;
   a.corr_flux = L.d_corr_flux;
   a.ncell = c->ncell;
   a.ninterp8 = (int64_t)L.ninterp * 8;
@@ -853,7 +874,7 @@ int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision
     return bail(fail(RB_ERR_CUDA, "stream/event creation failed"));
   int rc;
   if ((rc = dalloc(&c->d_uold, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_unew, (size_t)c->ncell * 5)) ||
-      (rc = dalloc(&c->d_son, (size_t)c->ncell)) || (rc = dalloc(&c->d_corr_slot, (size_t)mp->ngridmax)) ||
+      (rc = dalloc(&c->d_son, (size_t)c->ncell)) ||
       (rc = dalloc(&c->d_stage, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_red, 8)) ||
       (rc = dalloc(&c->d_clock, 8)) || (rc = dalloc(&c->d_sched, RB_S_SIZE)))
     return bail(rc);
@@ -876,7 +897,7 @@ int rb_destroy(rb_context* c) {
   if (!c) return RB_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_tree(c);
-  dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son); dfree(c->d_corr_slot);
+  dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son);
   dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
   dfree(c->d_flag);
   if (c->h_red) cudaFreeHost(c->h_red);
