@@ -120,7 +120,6 @@ constexpr size_t tile_smem_bytes() {
 // RS = 0 / ST = -1 read it from a.hp at run time.
 template <typename R, int TX, int TY, int TZ, int NT, int RS, int ST>
 __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
-  if (a.gate != nullptr && *a.gate != 0.0) return;
   using G = TileGeom<TX, TY, TZ>;
   constexpr int SX = G::SX, SY = G::SY, SZ = G::SZ, NS = G::NS;
   constexpr int BX = G::BX, BY = G::BY, NBLK = G::NBLK;
@@ -141,9 +140,14 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
   constexpr int NREC = 1 + 2 * NOCT;
   __shared__ int32_t corr_rec[NREC];
+  // the gate (the device scheduler's end-of-run flag) is read together with
+  // the tile's codes, so that the two loads overlap; every thread reads the
+  // same value, so the return is uniform and precedes the barrier
+  const double gate = a.gate != nullptr ? *a.gate : 0.0;
   for (int i = tid; i < NBLK; i += NT) blk[i] = a.tile_blk[(int64_t)tile * NBLK + i];
   if (a.tile_corr != nullptr)
     for (int i = tid; i < NREC; i += NT) corr_rec[i] = a.tile_corr[(int64_t)tile * NREC + i];
+  if (gate != 0.0) return;
   __syncthreads();
 
   // ---- A. gather + ctoprim ------------------------------------------------
