@@ -22,6 +22,7 @@
 #pragma once
 #include <cstdint>
 
+#include "cp_async.cuh"
 #include "hydro_core.cuh"
 
 namespace rb {
@@ -32,8 +33,9 @@ struct TileArgs {
   const int32_t* __restrict__ son;      // [ncell], device cell layout
   const double* __restrict__ interp;    // [5][ninterp*8] prolongated blocks
   const int32_t* __restrict__ tile_blk; // [ntile][NBLK] block codes
-  const int32_t* __restrict__ tile_corr;// [ntile][1 + 2*NOCT]: count, then (oct in tile, slot)
-                                        // of the octs owning a correction slot (null: none)
+  const int32_t* __restrict__ tile_corr_off; // [ntile+1] (null: no correction slots)
+  const int32_t* __restrict__ tile_corr;     // [entries][2] (oct in tile | face << 8, slot): the
+                                             // faces whose fluxes the fine-to-coarse correction reads
   double* __restrict__ corr_flux;       // [nslot][6][4][5]
   int64_t ncell;
   int64_t ninterp8;                     // ninterp*8 (stride of interp)
@@ -138,17 +140,23 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   const int64_t ncell = a.ncell;
 
   constexpr int NOCT = (TX / 2) * (TY / 2) * (TZ / 2);
-  constexpr int NREC = 1 + 2 * NOCT;
-  __shared__ int32_t corr_rec[NREC];
+  __shared__ int32_t corr_range[2];
+  __shared__ int32_t corr_ent[2 * 6 * NOCT];
   // the gate (the device scheduler's end-of-run flag) is read together with
   // the tile's codes, so that the two loads overlap; every thread reads the
   // same value, so the return is uniform and precedes the barrier
   const double gate = a.gate != nullptr ? *a.gate : 0.0;
   for (int i = tid; i < NBLK; i += NT) blk[i] = a.tile_blk[(int64_t)tile * NBLK + i];
-  if (a.tile_corr != nullptr)
-    for (int i = tid; i < NREC; i += NT) corr_rec[i] = a.tile_corr[(int64_t)tile * NREC + i];
+  if (a.tile_corr_off != nullptr && tid < 2) corr_range[tid] = a.tile_corr_off[tile + tid];
   if (gate != 0.0) return;
   __syncthreads();
+
+  // the tile's correction-face entries are copied to shared memory while the
+  // tile is computed (they are read at the end)
+  if (a.tile_corr_off != nullptr)
+    for (int i = tid; i < 2 * (corr_range[1] - corr_range[0]); i += NT)
+      cp_async4(corr_ent + i, a.tile_corr + 2 * corr_range[0] + i);
+  cp_async_commit();
 
   // ---- A. gather + ctoprim ------------------------------------------------
   const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
@@ -358,6 +366,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       F[v * NF + f] = zero_face ? (R)0 : val;
     }
   }
+  cp_async_wait<0>();  // this thread's correction entries (E)
   __syncthreads();
 
   // ---- D. conservative update of active octs ----------------------------------
@@ -416,20 +425,21 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   }
 
   // ---- E. boundary fluxes for the fine-to-coarse correction --------------------
-  if (a.tile_corr != nullptr) {
-    const int ncorr = corr_rec[0];
-    for (int it = tid; it < ncorr * 120; it += NT) {
-      const int i = it / 120, r = it % 120;
-      const int o = corr_rec[1 + 2 * i], slot = corr_rec[2 + 2 * i];
+  if (a.tile_corr_off != nullptr) {
+    const int n = corr_range[1] - corr_range[0];
+    for (int it = tid; it < n * 20; it += NT) {
+      const int i = it / 20, r = it % 20;
+      const int ent = corr_ent[2 * i], slot = corr_ent[2 * i + 1];
+      const int o = ent & 0xff, face = ent >> 8;   // face 0..5 = -x,+x,-y,+y,-z,+z
       const int ox = o % (TX / 2), oy = (o / (TX / 2)) % (TY / 2), oz = o / ((TX / 2) * (TY / 2));
-      const int face = r / 20, cc = (r / 5) % 4, v = r % 5;   // face 0..5 = -x,+x,-y,+y,-z,+z
+      const int cc = r / 5, v = r % 5;
       const int d = face >> 1, side = face & 1;
       const int t1 = cc & 1, t2 = cc >> 1;
       int fidx;
       if (d == 0) { const int fx = 2 * ox + 2 * side; fidx = fx + (TX + 1) * ((2 * oy + t1) + TY * (2 * oz + t2)); }
       else if (d == 1) { const int fy = 2 * oy + 2 * side; fidx = NFX + (2 * ox + t1) + TX * (fy + (TY + 1) * (2 * oz + t2)); }
       else { const int fz = 2 * oz + 2 * side; fidx = NFX + NFY + (2 * ox + t1) + TX * ((2 * oy + t2) + TY * fz); }
-      a.corr_flux[(int64_t)slot * 120 + r] = (double)F[v * NF + fidx];
+      a.corr_flux[(int64_t)slot * 120 + face * 20 + r] = (double)F[v * NF + fidx];
     }
   }
 }

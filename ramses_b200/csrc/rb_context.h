@@ -82,7 +82,8 @@ struct Level {
   int shape = -1;
   int ntile = 0;
   int32_t* d_tile_blk = nullptr;
-  int32_t* d_tile_corr = nullptr; // [ntile][1 + 2*octs per tile] correction-slot octs (null: none)
+  int32_t* d_tile_corr_off = nullptr; // [ntile+1] first correction face entry of each tile (null: none)
+  int32_t* d_tile_corr = nullptr;     // [entries][2] (oct in tile | face << 8, slot)
   int ninterp = 0;
   int32_t* d_interp7 = nullptr;
   double* d_interp_buf = nullptr;

@@ -75,6 +75,7 @@ inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
 void free_level_tables(Level& L) {
   dfree(L.d_tile_blk);
   dfree(L.d_tile_corr);
+  dfree(L.d_tile_corr_off);
   dfree(L.d_interp7);
   dfree(L.d_interp_buf);
   dfree(L.d_corr_flux);
@@ -264,6 +265,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   std::vector<int32_t> slot_of((size_t)L.noct, -1);
   int nslot = 0;
   std::vector<int32_t> h_slot_upd;  // (igrid-1, slot) pairs
+  std::vector<uint8_t> slot_faces;  // faces of each slot that border an unrefined coarser cell
   for (int p = 0; p < L.noct; p++) {
     const int32_t g = L.h_active[p];
     int slot = -1;
@@ -271,7 +273,8 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
       const int64_t nc = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (g - 1)];
       if (nc < 1 || nc > c->ncell) return fail(RB_ERR_TREE, "nbor(%d,%d)=%lld out of range", g, j, (long long)nc);
       if (c->son[nc - 1] == 0) {
-        if (slot < 0) slot = nslot++;
+        if (slot < 0) { slot = nslot++; slot_faces.push_back(0); }
+        slot_faces[slot] |= (uint8_t)(1u << (j - 1));
         cons.push_back({dev_of_fortran(c, nc), p / c->mp.nvector, j - 1, slot});
       }
     }
@@ -305,26 +308,29 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   // this level's entries of the per-oct correction slot table
   for (int32_t g : L.h_active) c->h_corr_slot[g - 1] = -1;
   for (size_t i = 0; i + 1 < h_slot_upd.size(); i += 2) c->h_corr_slot[h_slot_upd[i]] = h_slot_upd[i + 1];
-  // per tile, the octs that own a correction slot: [count, (oct position in
-  // the tile, slot) x count], so that the godunov kernel stores their
-  // boundary fluxes without looking slots up
+  // per tile, the faces whose fluxes the fine-to-coarse correction reads:
+  // entries (oct position in the tile | face << 8, slot), tile t's in
+  // [off[t], off[t+1]), so that the godunov kernel stores only those
   if (nslot) {
-    const int NOCT = TOX * TOY * TOZ, REC = 1 + 2 * NOCT;
-    std::vector<int32_t> rec((size_t)L.ntile * REC, 0);
+    const int NOCT = TOX * TOY * TOZ;
+    std::vector<int32_t> off((size_t)L.ntile + 1, 0), ent;
     for (int t = 0; t < L.ntile; t++) {
       const int32_t* B = &blk[(size_t)t * NBLK];
-      int32_t* Rt = &rec[(size_t)t * REC];
+      off[t] = (int32_t)(ent.size() / 2);
       for (int o = 0; o < NOCT; o++) {
         const int ox = o % TOX, oy = (o / TOX) % TOY, oz = o / (TOX * TOY);
         const int32_t code = B[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
         if (code < 0 || c->h_corr_slot[code] < 0) continue;
-        Rt[1 + 2 * Rt[0]] = o;
-        Rt[2 + 2 * Rt[0]] = c->h_corr_slot[code];
-        Rt[0]++;
+        const int32_t slot = c->h_corr_slot[code];
+        for (int f = 0; f < 6; f++)
+          if (slot_faces[slot] >> f & 1) { ent.push_back(o | f << 8); ent.push_back(slot); }
       }
     }
-    RB_TRY(dalloc(&L.d_tile_corr, rec.size()));
-    RB_TRY(h2d(c, L.d_tile_corr, rec.data(), rec.size() * 4));
+    off[L.ntile] = (int32_t)(ent.size() / 2);
+    RB_TRY(dalloc(&L.d_tile_corr_off, off.size()));
+    RB_TRY(h2d(c, L.d_tile_corr_off, off.data(), off.size() * 4));
+    RB_TRY(dalloc(&L.d_tile_corr, ent.size()));
+    RB_TRY(h2d(c, L.d_tile_corr, ent.data(), ent.size() * 4));
   }
   L.tables_built = true;
   return RB_OK;
@@ -550,6 +556,7 @@ rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
   a.interp = L.d_interp_buf;
   a.tile_blk = L.d_tile_blk;
   a.tile_corr = L.nslot ? L.d_tile_corr : nullptr;
+  a.tile_corr_off = L.nslot ? L.d_tile_corr_off : nullptr;
   a.corr_flux = L.d_corr_flux;
   a.ncell = c->ncell;
   a.ninterp8 = (int64_t)L.ninterp * 8;
