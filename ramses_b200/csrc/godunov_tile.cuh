@@ -169,15 +169,17 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     const int sx = 2 * bx + (ch & 1), sy = 2 * by + ((ch >> 1) & 1), sz = 2 * bz + (ch >> 2);
     code = blk[b];
     sonv = 0;
+    // L2-only loads: the tile reads each stencil cell once, and leaving L1
+    // to the loads in flight lets more of them be outstanding
     if (code >= 0) {
       const int64_t dc = (int64_t)a.ncoarse + (int64_t)code * 8 + ch;
 #pragma unroll
-      for (int v = 0; v < 5; v++) u[v] = __ldg(a.uold + v * ncell + dc);
-      if (a.has_refined) sonv = __ldg(a.son + dc);
+      for (int v = 0; v < 5; v++) u[v] = __ldcg(a.uold + v * ncell + dc);
+      if (a.has_refined) sonv = __ldcg(a.son + dc);
     } else if (code <= -2) {
       const int64_t e = (int64_t)(-code - 2) * 8 + ch;
 #pragma unroll
-      for (int v = 0; v < 5; v++) u[v] = __ldg(a.interp + v * a.ninterp8 + e);
+      for (int v = 0; v < 5; v++) u[v] = __ldcg(a.interp + v * a.ninterp8 + e);
     }
     // a tile-interior cell of a present oct (its faces and update are used)
     inner = sx >= 2 && sx < 2 + TX && sy >= 2 && sy < 2 + TY && sz >= 2 && sz < 2 + TZ && code >= 0;
@@ -387,7 +389,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const R* Fv = F + v * NF;
-      double un = a.fused ? __ldg(a.uold + v * ncell + dc) : a.unew[v * ncell + dc];
+      double un = a.fused ? __ldcg(a.uold + v * ncell + dc) : a.unew[v * ncell + dc];
       un = un + ((double)Fv[fxl] - (double)Fv[fxl + 1]);
       un = un + ((double)Fv[fyl] - (double)Fv[fyl + TX]);
       un = un + ((double)Fv[fzl] - (double)Fv[fzl + TX * TY]);
