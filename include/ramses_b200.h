@@ -68,6 +68,10 @@ int rb_download_state(rb_context *ctx, double *uold);
 /* Same for unew (for callers that interleave host work with a level step). */
 int rb_upload_unew(rb_context *ctx, const double *unew);
 int rb_download_unew(rb_context *ctx, double *unew);
+/* pressure_fix: Fortran-layout divu(ncell) and enew(ncell)
+ * (hydro/hydro_commons.f90 divu, enew) as the last set_unew / godunov_fine /
+ * set_uold left them. RB_ERR_STATE for a context without pressure_fix. */
+int rb_download_pressure_fix(rb_context *ctx, double *divu, double *enew);
 
 /* Level operations on the device mirrors (same semantics as the Fortran). */
 int rb_set_unew(rb_context *ctx, int ilevel);

@@ -53,7 +53,8 @@ class OrcParams(ctypes.Structure):
                 ("smallc", ctypes.c_double), ("courant_factor", ctypes.c_double),
                 ("slope_theta", ctypes.c_double), ("riemann", ctypes.c_int32),
                 ("slope_type", ctypes.c_int32), ("interpol_var", ctypes.c_int32),
-                ("interpol_type", ctypes.c_int32)]
+                ("interpol_type", ctypes.c_int32), ("pressure_fix", ctypes.c_int32),
+                ("beta_fix", ctypes.c_double)]
 
 
 MAXLEVEL = 32
@@ -80,7 +81,7 @@ class OrcMesh(ctypes.Structure):
                 ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
                 ("mass_tot", ctypes.c_double), ("ekin_tot", ctypes.c_double),
                 ("eint_tot", ctypes.c_double), ("cell_updates", ctypes.c_int64),
-                ("nthreads", ctypes.c_int32)]
+                ("nthreads", ctypes.c_int32), ("divu", _PD), ("enew", _PD)]
 
 
 def _declare(L):
@@ -107,7 +108,8 @@ def _declare(L):
 def params_struct(hp) -> OrcParams:
     hp.validate()
     return OrcParams(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta,
-                     hp.riemann_code, hp.slope_type, hp.interpol_var, hp.interpol_type)
+                     hp.riemann_code, hp.slope_type, hp.interpol_var, hp.interpol_type,
+                     1 if hp.pressure_fix else 0, hp.beta_fix)
 
 
 def _ptr(a, t):
@@ -175,6 +177,10 @@ class OracleRun:
         for i in range(MAXLEVEL + 1):
             m.nsubcycle[i] = ns[i] if i < len(ns) else 2
         m.nthreads = nthreads
+        # pressure_fix: velocity divergence and internal energy per cell
+        self.divu = np.zeros(tree.ncell)
+        self.enew = np.zeros(tree.ncell)
+        m.divu, m.enew = _ptr(self.divu, _PD), _ptr(self.enew, _PD)
         self.m = m
 
     def _check(self, rc, what):

@@ -768,29 +768,100 @@ int orc_interpol_hydro(const orc_params *p, double *u1, double *u2, int nn) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* set_unew / set_uold: hydro/godunov_fine.f90:40-130, 135-232               */
-/* (no pressure_fix, no momentum feedback, nvar = ndim+2, one CPU)           */
+/* set_unew / set_uold: hydro/godunov_fine.f90:40-130, 135-232, with         */
+/* add_pdv_source_terms :287-471 (no gravity, no momentum feedback,          */
+/* nvar = ndim+2, nener = 0, one CPU, hexp = 0: no cosmology)                */
 /* ------------------------------------------------------------------------ */
+/* internal energy E - d/2 (u^2+v^2+w^2) of set_unew / add_pdv_source_terms */
+static double eint_of(const orc_params *p, const orc_mesh *m, int cell, const double *u) {
+  size_t nc = (size_t)ncell_of(m);
+  double d = fmaxd(u[(size_t)(cell - 1)], p->smallr);
+  double uu = u[nc + (size_t)(cell - 1)] / d, vv = u[2 * nc + (size_t)(cell - 1)] / d,
+         ww = u[3 * nc + (size_t)(cell - 1)] / d;
+  return u[4 * nc + (size_t)(cell - 1)] - 0.5 * d * (uu * uu + vv * vv + ww * ww);
+}
+
 int orc_set_unew(const orc_params *p, orc_mesh *m, int ilevel) {
-  (void)p;
   const int32_t *act = active_list(m, ilevel);
   int64_t n = nactive(m, ilevel);
   for (int ind = 1; ind <= 8; ind++) {
     int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
     for (int ivar = 1; ivar <= NV; ivar++)
       for (int64_t i = 0; i < n; i++) *UNEW(m, act[i] + iskip, ivar) = *UOLD(m, act[i] + iskip, ivar);
+    if (p->pressure_fix) { /* :71-86 */
+      for (int64_t i = 0; i < n; i++) m->divu[act[i] + iskip - 1] = 0;
+      for (int64_t i = 0; i < n; i++) m->enew[act[i] + iskip - 1] = eint_of(p, m, act[i] + iskip, m->uold);
+    }
   }
   return 0;
 }
 
-int orc_set_uold(const orc_params *p, orc_mesh *m, int ilevel) {
-  (void)p;
+/* add_pdv_source_terms (:287-432, the active vector-sweep variant): enew -=
+ * (gamma-1) eold div(u) dt with div(u) from the neighbouring cells' uold
+ * velocities; a missing finer neighbour is replaced by its coarse father
+ * cell at 1.5 dx. */
+static void add_pdv_source_terms(const orc_params *p, orc_mesh *m, int ilevel) {
   const int32_t *act = active_list(m, ilevel);
   int64_t n = nactive(m, ilevel);
+  size_t nc = (size_t)ncell_of(m);
+  double scale = m->boxlen / (double)m->nx;
+  double dx_loc = pow(0.5, ilevel) * scale;
+  for (int64_t i = 0; i < n; i++) {
+    int g = act[i];
+    for (int ind = 1; ind <= 8; ind++) {
+      int cell = m->ncoarse + (ind - 1) * m->ngridmax + g;
+      int cc[3] = {(ind - 1) & 1, ((ind - 1) >> 1) & 1, ((ind - 1) >> 2) & 1};
+      double divu_loc = 0.0;
+      for (int idim = 1; idim <= 3; idim++) {
+        double vel[2], dxs[2];
+        for (int side = 0; side < 2; side++) {
+          /* the neighbouring cell along idim (side 0: left, 1: right) */
+          int jnd = 1 + ((ind - 1) ^ (1 << (idim - 1)));
+          int inside = side == 0 ? cc[idim - 1] == 1 : cc[idim - 1] == 0;
+          int nb_cell, coarse = 0;
+          if (inside) nb_cell = m->ncoarse + (jnd - 1) * m->ngridmax + g;
+          else {
+            int fcell = NBOR(m, g, 2 * idim - 1 + side);
+            int gn = SON(m, fcell);
+            if (gn > 0) nb_cell = m->ncoarse + (jnd - 1) * m->ngridmax + gn;
+            else { nb_cell = fcell; coarse = 1; }
+          }
+          vel[side] = m->uold[(size_t)idim * nc + (size_t)(nb_cell - 1)] / fmaxd(m->uold[(size_t)(nb_cell - 1)], p->smallr);
+          dxs[side] = coarse ? dx_loc * 1.5 : dx_loc;
+        }
+        divu_loc = divu_loc + (vel[1] - vel[0]) / (dxs[0] + dxs[1]);
+      }
+      double eold = eint_of(p, m, cell, m->uold);
+      m->enew[cell - 1] = m->enew[cell - 1] - (p->gamma - 1.0) * eold * divu_loc * m->dtnew[ilevel];
+    }
+  }
+}
+
+int orc_set_uold(const orc_params *p, orc_mesh *m, int ilevel) {
+  const int32_t *act = active_list(m, ilevel);
+  int64_t n = nactive(m, ilevel);
+  if (p->pressure_fix) add_pdv_source_terms(p, m, ilevel);
+  double scale = m->boxlen / (double)m->nx;
+  double dx = pow(0.5, ilevel) * scale;
+  const double hexp = 0.0;
   for (int ind = 1; ind <= 8; ind++) {
     int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
     for (int ivar = 1; ivar <= NV; ivar++)
       for (int64_t i = 0; i < n; i++) *UOLD(m, act[i] + iskip, ivar) = *UNEW(m, act[i] + iskip, ivar);
+    if (p->pressure_fix) { /* :203-227 */
+      for (int64_t i = 0; i < n; i++) {
+        int c = act[i] + iskip;
+        double d = fmaxd(*UOLD(m, c, 1), p->smallr);
+        double u = *UOLD(m, c, 2) / d, v = *UOLD(m, c, 3) / d, w = *UOLD(m, c, 4) / d;
+        double e_kin = 0.5 * d * (u * u + v * v + w * w);
+        double e_cons = *UOLD(m, c, 5) - e_kin;
+        double e_prim = m->enew[c - 1];
+        double div = fabs(m->divu[c - 1]) * dx / m->dtnew[ilevel];
+        double mx = fmaxd(div, 3.0 * hexp * dx);
+        double e_trunc = p->beta_fix * d * (mx * mx);
+        if (e_cons < e_trunc) *UOLD(m, c, 5) = e_prim + e_kin;
+      }
+    }
   }
   return 0;
 }
@@ -969,14 +1040,22 @@ static int godfine1_flux(const orc_params *p, const orc_mesh *m, work *w, const 
             for (int i = 0; i < ncache; i++)
               if (ok[S6(nv, i, i3 - i0, j3 - j0, k3 - k0)] || ok[S6(nv, i, i3, j3, k3)])
                 flux[FI(nv, i, i3, j3, k3, ivar, idim)] = 0.0;
+    if (p->pressure_fix) /* :735-744 */
+      for (int k3 = 1; k3 <= 2 + k0; k3++)
+        for (int j3 = 1; j3 <= 2 + j0; j3++)
+          for (int i3 = 1; i3 <= 2 + i0; i3++)
+            for (int ivar = 1; ivar <= 2; ivar++)
+              for (int i = 0; i < ncache; i++)
+                if (ok[S6(nv, i, i3 - i0, j3 - j0, k3 - k0)] || ok[S6(nv, i, i3, j3, k3)])
+                  tmp[TI(nv, i, i3, j3, k3, ivar, idim)] = 0.0;
   }
 done:
   free(nfc); free(ind_exist); free(ind_nexist); free(igrid_nbor); free(ind_buffer);
   return rc;
 }
 
-static void godfine1_update(const orc_mesh *m, const int32_t *ind_grid, int ncache,
-                            const double *flux) {
+static void godfine1_update(const orc_params *p, const orc_mesh *m, const int32_t *ind_grid, int ncache,
+                            const double *flux, const double *tmp) {
   const int nv = m->nvector;
   const double oneontwotondim = 1.0 / 8.0;
   /* Conservative update at level ilevel :751-792 */
@@ -994,6 +1073,16 @@ static void godfine1_update(const orc_mesh *m, const int32_t *ind_grid, int ncac
               *u = *u + (flux[FI(nv, i, i3, j3, k3, ivar, idim)] -
                          flux[FI(nv, i, i3 + i0, j3 + j0, k3 + k0, ivar, idim)]);
             }
+          if (p->pressure_fix) { /* velocity divergence and internal energy :775-789 */
+            for (int i = 0; i < ncache; i++) {
+              double *u = &m->divu[iskip + ind_grid[i] - 1];
+              *u = *u + (tmp[TI(nv, i, i3, j3, k3, 1, idim)] - tmp[TI(nv, i, i3 + i0, j3 + j0, k3 + k0, 1, idim)]);
+            }
+            for (int i = 0; i < ncache; i++) {
+              double *u = &m->enew[iskip + ind_grid[i] - 1];
+              *u = *u + (tmp[TI(nv, i, i3, j3, k3, 2, idim)] - tmp[TI(nv, i, i3 + i0, j3 + j0, k3 + k0, 2, idim)]);
+            }
+          }
         }
   }
   /* Conservative update at level ilevel-1 :798-908 */
@@ -1015,6 +1104,15 @@ static void godfine1_update(const orc_mesh *m, const int32_t *ind_grid, int ncac
               double *u = UNEW(m, buf[i], ivar);
               *u = *u - flux[FI(nv, cel[i], i3, j3, k3, ivar, idim)] * oneontwotondim;
             }
+    if (p->pressure_fix) /* :831-856: divu, then enew */
+      for (int t = 1; t <= 2; t++)
+        for (int k3 = 1; k3 <= 2 - k0; k3++)
+          for (int j3 = 1; j3 <= 2 - j0; j3++)
+            for (int i3 = 1; i3 <= 2 - i0; i3++)
+              for (int i = 0; i < nb; i++) {
+                double *u = t == 1 ? &m->divu[buf[i] - 1] : &m->enew[buf[i] - 1];
+                *u = *u - tmp[TI(nv, cel[i], i3, j3, k3, t, idim)] * oneontwotondim;
+              }
     /* right */
     nb = 0;
     for (int i = 0; i < ncache; i++)
@@ -1030,6 +1128,15 @@ static void godfine1_update(const orc_mesh *m, const int32_t *ind_grid, int ncac
               double *u = UNEW(m, buf[i], ivar);
               *u = *u + flux[FI(nv, cel[i], i3 + i0, j3 + j0, k3 + k0, ivar, idim)] * oneontwotondim;
             }
+    if (p->pressure_fix) /* :883-906: divu, then enew */
+      for (int t = 1; t <= 2; t++)
+        for (int k3 = 1 + k0; k3 <= 2; k3++)
+          for (int j3 = 1 + j0; j3 <= 2; j3++)
+            for (int i3 = 1 + i0; i3 <= 2; i3++)
+              for (int i = 0; i < nb; i++) {
+                double *u = t == 1 ? &m->divu[buf[i] - 1] : &m->enew[buf[i] - 1];
+                *u = *u + tmp[TI(nv, cel[i], i3 + i0, j3 + j0, k3 + k0, t, idim)] * oneontwotondim;
+              }
   }
   free(buf); free(cel);
 }
@@ -1045,9 +1152,14 @@ int orc_godunov_fine(const orc_params *p, orc_mesh *m, int ilevel, double dt) {
   nth = m->nthreads > 0 ? m->nthreads : omp_get_max_threads();
 #endif
   const int64_t chunk = 64 * (int64_t)nth;
-  const size_t fsz = (size_t)nv * 27 * NV * 3;
-  double *fbuf = (double *)malloc(sizeof(double) * fsz * (size_t)(chunk < nbatch ? chunk : nbatch));
-  if (!fbuf) return -4;
+  const size_t fsz = (size_t)nv * 27 * NV * 3, tsz = (size_t)nv * 27 * 2 * 3;
+  const size_t nbuf = (size_t)(chunk < nbatch ? chunk : nbatch);
+  double *fbuf = (double *)malloc(sizeof(double) * fsz * nbuf);
+  /* tmp (velocity divergence, internal-energy flux) is kept per batch for the
+   * serial update when pressure_fix is on */
+  double *tbuf = p->pressure_fix ? (double *)malloc(sizeof(double) * tsz * nbuf) : NULL;
+  if (!fbuf || (p->pressure_fix && !tbuf)) { free(fbuf); free(tbuf); return -4; }
+  m->dtnew[ilevel] = dt; /* dtnew(ilevel), read again by set_uold */
   int err = 0;
   for (int64_t b0 = 0; b0 < nbatch && !err; b0 += chunk) {
     int64_t nb = (nbatch - b0) < chunk ? (nbatch - b0) : chunk;
@@ -1068,7 +1180,7 @@ int orc_godunov_fine(const orc_params *p, orc_mesh *m, int ilevel, double dt) {
         int64_t g0 = (b0 + b) * nv;
         int n = (int)((ncache - g0) < nv ? (ncache - g0) : nv);
         int rc = godfine1_flux(p, m, &w, act + g0, n, ilevel, dt, uloc, gloc, ok,
-                               fbuf + fsz * (size_t)b, tmp, u1, u2);
+                               fbuf + fsz * (size_t)b, tbuf ? tbuf + tsz * (size_t)b : tmp, u1, u2);
         if (rc) lerr = rc;
       }
       if (lerr) {
@@ -1082,10 +1194,11 @@ int orc_godunov_fine(const orc_params *p, orc_mesh *m, int ilevel, double dt) {
     for (int64_t b = 0; b < nb; b++) {
       int64_t g0 = (b0 + b) * nv;
       int n = (int)((ncache - g0) < nv ? (ncache - g0) : nv);
-      godfine1_update(m, act + g0, n, fbuf + fsz * (size_t)b);
+      godfine1_update(p, m, act + g0, n, fbuf + fsz * (size_t)b, tbuf ? tbuf + tsz * (size_t)b : NULL);
     }
   }
   free(fbuf);
+  free(tbuf);
   return err;
 }
 

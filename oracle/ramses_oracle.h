@@ -34,6 +34,8 @@ typedef struct orc_params {
   int32_t slope_type;    /* 0,1,2,3,7,8 */
   int32_t interpol_var;  /* 0,1,2 */
   int32_t interpol_type; /* 0..4 */
+  int32_t pressure_fix;  /* dual-energy fix: enew/divu tracked, set_uold repairs E */
+  double beta_fix;       /* pressure-fix threshold (amr/amr_parameters.f90:167) */
 } orc_params;
 
 /* &REFINE_PARAMS gradient criterion (hydro/hydro_parameters.f90:47-52) */
@@ -56,6 +58,7 @@ typedef struct orc_mesh {
   double mass_tot, ekin_tot, eint_tot;
   int64_t cell_updates; /* leaf-cell updates accumulated by orc_coarse_step */
   int32_t nthreads;     /* OpenMP threads for the flux phase (0 = default) */
+  double *divu, *enew;  /* divu(1:ncell), enew(1:ncell); used when pressure_fix */
 } orc_mesh;
 
 #ifdef __cplusplus

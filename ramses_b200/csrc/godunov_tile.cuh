@@ -49,6 +49,9 @@ struct TileArgs {
   const double* __restrict__ dt_dev;    // if non-null, dt is read here
   double* __restrict__ partial;         // fused: [ntile][4] (min dt, mass, E, eint)
   const double* __restrict__ gate;      // if non-null and *gate != 0 the launch is a no-op
+  double* __restrict__ divu;            // pressure_fix (PF kernels): [ncell] velocity divergence
+  double* __restrict__ enew;            //   and internal energy, updated like unew
+  double* __restrict__ corr_tmp;        //   [nslot][6][4][2] their correction-face fluxes
   rb_hydro_params hp;
 };
 
@@ -119,8 +122,11 @@ constexpr size_t tile_smem_bytes() {
 }
 
 // RS (Riemann solver) and ST (slope type) fix the scheme at compile time;
-// RS = 0 / ST = -1 read it from a.hp at run time.
-template <typename R, int TX, int TY, int TZ, int NT, int RS, int ST>
+// RS = 0 / ST = -1 read it from a.hp at run time. PF: pressure_fix, the
+// velocity-divergence and internal-energy fluxes of every face (umuscl.f90
+// cmpflxm's tmp, :845-849) update a.divu and a.enew beside unew
+// (godunov_fine.f90:735-744, 775-789).
+template <typename R, int TX, int TY, int TZ, int NT, int RS, int ST, bool PF = false>
 __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   using G = TileGeom<TX, TY, TZ>;
   constexpr int SX = G::SX, SY = G::SY, SZ = G::SZ, NS = G::NS;
@@ -354,18 +360,23 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     from_face(fg, d, fo);
     // refined interface: either neighbour cell refined -> zero flux
     const bool zero_face = (fl & 1) != 0;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      R val;
+    auto scaled = [&](R x) -> R {
       if (sizeof(R) == 8) {
         // flux = fx*dt/dx, evaluated as (fx*dt)/dx (umuscl.f90:101-163);
         // division by an exact power of two equals the multiplication
-        const double t = (double)fo[v] * dt;
-        val = (R)(a.dx_pow2 ? t * a.inv_dx : t / a.dx);
-      } else {
-        val = fo[v] * dtd[0];
+        const double t = (double)x * dt;
+        return (R)(a.dx_pow2 ? t * a.inv_dx : t / a.dx);
       }
-      F[v * NF + f] = zero_face ? (R)0 : val;
+      return x * dtd[0];
+    };
+#pragma unroll
+    for (int v = 0; v < 5; v++) F[v * NF + f] = zero_face ? (R)0 : scaled(fo[v]);
+    if (PF) {
+      // tmp: the face-normal velocity average and the internal-energy flux,
+      // kept in this face's qm slots (read above, by this thread only)
+      const R half = (R)0.5;
+      qm[f] = zero_face ? (R)0 : scaled(half * (ql[1] + qr[1]));
+      qm[NF + f] = zero_face ? (R)0 : scaled(fg[5]);
     }
   }
   cp_async_wait<0>();  // this thread's correction entries (E)
@@ -395,6 +406,33 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       un = un + ((double)Fv[fzl] - (double)Fv[fzl + TX * TY]);
       a.unew[v * ncell + dc] = un;
       unv[v] = un;
+    }
+    if (PF) {
+      // divu, then enew, each x then y then z, as unew (the fused form
+      // starts them from set_unew's values: 0 and the internal energy of uold)
+      const R* T1 = qm;
+      const R* T2 = qm + NF;
+      double dv, en;
+      if (a.fused) {
+        double uo[5];
+#pragma unroll
+        for (int v = 0; v < 5; v++) uo[v] = __ldcg(a.uold + v * ncell + dc);
+        const double d = fmx(uo[0], a.hp.smallr);
+        const double uu = uo[1] / d, vv = uo[2] / d, ww = uo[3] / d;
+        dv = 0.0;
+        en = uo[4] - 0.5 * d * (uu * uu + vv * vv + ww * ww);
+      } else {
+        dv = a.divu[dc];
+        en = a.enew[dc];
+      }
+      dv = dv + ((double)T1[fxl] - (double)T1[fxl + 1]);
+      dv = dv + ((double)T1[fyl] - (double)T1[fyl + TX]);
+      dv = dv + ((double)T1[fzl] - (double)T1[fzl + TX * TY]);
+      en = en + ((double)T2[fxl] - (double)T2[fxl + 1]);
+      en = en + ((double)T2[fyl] - (double)T2[fyl + TX]);
+      en = en + ((double)T2[fzl] - (double)T2[fzl + TX * TY]);
+      a.divu[dc] = dv;
+      a.enew[dc] = en;
     }
     if (a.fused) {
       // courant_fine on the updated state (the next step's CFL condition);
@@ -442,6 +480,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       else if (d == 1) { const int fy = 2 * oy + 2 * side; fidx = NFX + (2 * ox + t1) + TX * (fy + (TY + 1) * (2 * oz + t2)); }
       else { const int fz = 2 * oz + 2 * side; fidx = NFX + NFY + (2 * ox + t1) + TX * ((2 * oy + t2) + TY * fz); }
       a.corr_flux[(int64_t)slot * 120 + face * 20 + r] = (double)F[v * NF + fidx];
+      if (PF && v < 2) a.corr_tmp[(int64_t)slot * 48 + face * 8 + cc * 2 + v] = (double)qm[v * NF + fidx];
     }
   }
 }

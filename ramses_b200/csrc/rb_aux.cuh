@@ -51,6 +51,111 @@ static __global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t
     d[dev_cell_of_fortran(i + 1, ncoarse, ngridmax)] = f[i];
 }
 
+// Internal energy E - d/2 (u^2+v^2+w^2), d = max(rho, smallr), u = m/d, of
+// set_unew, add_pdv_source_terms and set_uold's pressure fix
+// (godunov_fine.f90:75-81, 396-401, 208-213).
+__device__ __forceinline__ double pf_eint(const double u[5], double smallr) {
+  const double d = fmx(u[0], smallr);
+  const double uu = u[1] / d, vv = u[2] / d, ww = u[3] / d;
+  return u[4] - 0.5 * d * (uu * uu + vv * vv + ww * ww);
+}
+
+// pressure_fix part of set_unew (godunov_fine.f90:71-86): divu = 0 and enew
+// = the internal energy of uold, for every cell of the active octs.
+static __global__ void pf_set_unew_kernel(const double* __restrict__ uold, double* __restrict__ divu,
+                                          double* __restrict__ enew, const int32_t* __restrict__ active,
+                                          int32_t noct, int64_t ncell, int32_t ncoarse, double smallr,
+                                          const double* __restrict__ gate) {
+  RB_GATE(gate);
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    double u[5];
+    for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    divu[dc] = 0.0;
+    enew[dc] = pf_eint(u, smallr);
+  }
+}
+
+// add_pdv_source_terms (godunov_fine.f90:287-432): enew -= (gamma-1) eold
+// div(u) dt, with div(u) = sum over directions of (v_right - v_left) /
+// (dx_left + dx_right) from the uold velocities of the neighbouring cells;
+// a neighbour whose oct does not exist is its coarse father cell at 1.5 dx.
+// nbor6[p*6 + j]: device cell of nbor(igrid, j+1) of the level's oct p.
+// dt: *dt_dev if non-null, else dt_val.
+static __global__ void pdv_kernel(const double* __restrict__ uold, const int32_t* __restrict__ son,
+                                  const int32_t* __restrict__ active, const int32_t* __restrict__ nbor6,
+                                  int32_t noct, int64_t ncell, int32_t ncoarse, double dx_loc,
+                                  const double* __restrict__ dt_dev, double dt_val, rb_hydro_params hp,
+                                  double* __restrict__ enew, const double* __restrict__ gate) {
+  RB_GATE(gate);
+  const double dt = dt_dev ? *dt_dev : dt_val;
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i >> 3;
+    const int ind = (int)(i & 7);
+    const int64_t g = active[p];
+    const int64_t dc = ncoarse + g * 8 + ind;
+    double divu_loc = 0.0;
+    for (int d = 0; d < 3; d++) {
+      const int bit = (ind >> d) & 1, jnd = ind ^ (1 << d);
+      double vel[2], dxs[2];
+      for (int side = 0; side < 2; side++) {
+        const bool inside = side == 0 ? bit == 1 : bit == 0;
+        int64_t nb = ncoarse + g * 8 + jnd;
+        dxs[side] = dx_loc;
+        if (!inside) {
+          const int64_t fcell = nbor6[p * 6 + 2 * d + side];
+          const int gn = son[fcell];
+          if (gn > 0) {
+            nb = ncoarse + (int64_t)(gn - 1) * 8 + jnd;
+          } else {
+            nb = fcell;
+            dxs[side] = dx_loc * 1.5;
+          }
+        }
+        vel[side] = uold[(int64_t)(1 + d) * ncell + nb] / fmx(uold[nb], hp.smallr);
+      }
+      divu_loc = divu_loc + (vel[1] - vel[0]) / (dxs[0] + dxs[1]);
+    }
+    double u[5];
+    for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    const double eold = pf_eint(u, hp.smallr);
+    enew[dc] = enew[dc] - (hp.gamma - 1.0) * eold * divu_loc * dt;
+  }
+}
+
+// pressure fix of set_uold (godunov_fine.f90:203-227, hexp = 0: no
+// cosmology): where the conservative internal energy E - ekin falls below
+// beta_fix * d * (|divu| dx/dt)^2, E = enew + ekin. Runs on uold after the
+// copy from unew; skip_split leaves the split cells alone (upload_fine has
+// overwritten them with the restriction, which in the reference follows
+// the fix).
+static __global__ void pf_fix_kernel(double* __restrict__ uold, const double* __restrict__ divu,
+                                     const double* __restrict__ enew, const int32_t* __restrict__ son,
+                                     const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
+                                     int32_t ncoarse, double dx, const double* __restrict__ dt_dev, double dt_val,
+                                     double smallr, double beta_fix, int skip_split,
+                                     const double* __restrict__ gate) {
+  RB_GATE(gate);
+  const double dt = dt_dev ? *dt_dev : dt_val;
+  const double hexp = 0.0;
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
+    if (skip_split && son[dc] > 0) continue;
+    const double d = fmx(uold[dc], smallr);
+    const double u = uold[ncell + dc] / d, v = uold[2 * ncell + dc] / d, w = uold[3 * ncell + dc] / d;
+    const double e_kin = 0.5 * d * (u * u + v * v + w * w);
+    const double e_cons = uold[4 * ncell + dc] - e_kin;
+    const double e_prim = enew[dc];
+    const double div = fabs(divu[dc]) * dx / dt;
+    const double mx = fmx(div, 3.0 * hexp * dx);
+    const double e_trunc = beta_fix * d * (mx * mx);
+    if (e_cons < e_trunc) uold[4 * ncell + dc] = e_prim + e_kin;
+  }
+}
+
 // set_unew / set_uold (godunov_fine.f90:40-130, 135-232): copy the 8x5
 // values of every active oct. active[] holds igrid-1.
 static __global__ void copy_octs_kernel(const double* __restrict__ src, double* __restrict__ dst,
@@ -91,10 +196,14 @@ static __global__ void interp_blocks_kernel(const double* __restrict__ uold, con
 // batch of the contributing oct, then direction, then left before right, and
 // within one face its 4 fine cells in (k3,j3,i3) order.
 // contrib[k] = slot*6 + face (face 0..5 = -x,+x,-y,+y,-z,+z).
+// With pressure_fix (divu non-null) divu and enew get the same corrections
+// from corr_tmp[slot][face][4][2] (godunov_fine.f90:831-856, 883-906).
 static __global__ void apply_corrections_kernel(double* __restrict__ unew, const int32_t* __restrict__ tgt,
                                          const int32_t* __restrict__ off, const int32_t* __restrict__ contrib,
                                          int32_t ntgt, const double* __restrict__ corr_flux, int64_t ncell,
-                                         const double* __restrict__ gate) {
+                                         const double* __restrict__ gate, double* __restrict__ divu = nullptr,
+                                         double* __restrict__ enew = nullptr,
+                                         const double* __restrict__ corr_tmp = nullptr) {
   RB_GATE(gate);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntgt) return;
@@ -113,6 +222,22 @@ static __global__ void apply_corrections_kernel(double* __restrict__ unew, const
     }
     unew[v * ncell + dc] = u;
   }
+  if (divu) {
+    for (int t2 = 0; t2 < 2; t2++) {
+      double* arr = t2 == 0 ? divu : enew;
+      double u = arr[dc];
+      for (int k = off[t]; k < off[t + 1]; k++) {
+        const int slot = contrib[k] / 6, face = contrib[k] % 6;
+        const double* tl = corr_tmp + (int64_t)slot * 48 + face * 8;
+        if ((face & 1) == 0) {
+          for (int c = 0; c < 4; c++) u = u - tl[c * 2 + t2] * oneontwotondim;
+        } else {
+          for (int c = 0; c < 4; c++) u = u + tl[c * 2 + t2] * oneontwotondim;
+        }
+      }
+      arr[dc] = u;
+    }
+  }
 }
 
 // courant_fine (courant_fine.f90:1-159): per-block partial (min dt, mass,
@@ -128,7 +253,9 @@ static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double
                                                              int64_t ncell, int32_t ncoarse, double dx,
                                                              rb_hydro_params hp, double* __restrict__ partial,
                                                              const double* __restrict__ gate,
-                                                             double* __restrict__ unew = nullptr) {
+                                                             double* __restrict__ unew = nullptr,
+                                                             double* __restrict__ divu = nullptr,
+                                                             double* __restrict__ enew = nullptr) {
   RB_GATE(gate);
   const double vol = dx * dx * dx;
   double smax = 0.0, mass = 0.0, etot = 0.0, eint = 0.0;
@@ -142,6 +269,10 @@ static __global__ void __launch_bounds__(NT) courant_partial_kernel(const double
     // set_unew fused in (it follows courant_fine in amr_step): every cell
     if (unew)
       for (int v = 0; v < 5; v++) unew[v * ncell + dc] = u[v];
+    if (divu) {  // pressure_fix (godunov_fine.f90:71-86)
+      divu[dc] = 0.0;
+      enew[dc] = pf_eint(u, hp.smallr);
+    }
     if (!leaf) continue;
     mass = mass + u[0] * vol;
     etot = etot + u[4] * vol;

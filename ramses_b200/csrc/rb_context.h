@@ -90,6 +90,7 @@ struct Level {
   int has_refined = 0;
   int nslot = 0;
   double* d_corr_flux = nullptr;
+  double* d_corr_tmp = nullptr;   // pressure_fix: [nslot][6][4][2] (divu, enew) fluxes of the correction faces
   int ntgt = 0;
   int32_t* d_tgt = nullptr;
   int32_t* d_tgt_off = nullptr;
@@ -132,6 +133,9 @@ struct rb_context {
   float last_ms = 0.f;
   double* d_uold = nullptr;
   double* d_unew = nullptr;
+  double* d_divu = nullptr;         // pressure_fix: velocity divergence x (-dt) per cell
+  double* d_enew = nullptr;         // pressure_fix: internal energy per cell
+  double dt_godunov[RB_MAXLEVEL + 2] = {0};  // dt of the last rb_godunov_fine per level (set_uold's dtnew)
   int32_t* d_son = nullptr;
   double* d_stage = nullptr;        // Fortran-layout staging [5*ncell]
   double* d_partial = nullptr;      // CFL partials

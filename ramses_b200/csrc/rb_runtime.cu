@@ -32,7 +32,10 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
   if (!(st == 0 || st == 1 || st == 2 || st == 3 || st == 7 || st == 8))
     return fail(RB_ERR_INVALID, "Unknown slope type %d", st);
   if (hp->scheme != 0) return fail(RB_ERR_INVALID, "scheme %d not supported (muscl only)", hp->scheme);
-  if (hp->pressure_fix) return fail(RB_ERR_INVALID, "pressure_fix is not supported");
+  if (hp->pressure_fix != 0 && hp->pressure_fix != 1)
+    return fail(RB_ERR_INVALID, "pressure_fix must be 0 or 1 (got %d)", hp->pressure_fix);
+  if (!(hp->beta_fix >= 0.0) || !std::isfinite(hp->beta_fix))
+    return fail(RB_ERR_INVALID, "beta_fix=%g must be finite and >= 0", hp->beta_fix);
   if (hp->difmag != 0.0) return fail(RB_ERR_INVALID, "difmag>0 is not supported");
   if (hp->interpol_var < 0 || hp->interpol_var > 2 || hp->interpol_type < 0 || hp->interpol_type > 4)
     return fail(RB_ERR_INVALID, "bad interpol_var/interpol_type");
@@ -79,6 +82,7 @@ void free_level_tables(Level& L) {
   dfree(L.d_interp7);
   dfree(L.d_interp_buf);
   dfree(L.d_corr_flux);
+  dfree(L.d_corr_tmp);
   dfree(L.d_tgt);
   dfree(L.d_tgt_off);
   dfree(L.d_contrib);
@@ -123,6 +127,21 @@ int default_shape(const rb_context* c, const Level& L) {
   if (L.complete && L.noct >= 64 * 148) return 4;   // 8x8x8 cells
   if (L.noct >= 8 * 64) return 1;                   // 4x4x4 cells
   return 0;                                         // single oct
+}
+
+// Device cell of nbor(igrid,j), j = 1..6, for the level's octs in active
+// order (hydro_flag and the pdV term of pressure_fix).
+int ensure_nbor6(rb_context* c, Level& L) {
+  if (L.d_nbor6 || !L.noct) return RB_OK;
+  std::vector<int32_t> nb((size_t)L.noct * 6);
+  for (int i = 0; i < L.noct; i++) {
+    const int g = L.h_active[i];
+    for (int j = 0; j < 6; j++)
+      nb[(size_t)i * 6 + j] = (int32_t)dev_of_fortran(c, c->nbor[(size_t)j * c->mp.ngridmax + (g - 1)]);
+  }
+  RB_TRY(dalloc(&L.d_nbor6, nb.size()));
+  RB_TRY(h2d(c, L.d_nbor6, nb.data(), nb.size() * sizeof(int32_t)));
+  return RB_OK;
 }
 
 // Build the godunov tile / prolongation / correction tables of level l.
@@ -301,6 +320,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(dalloc(&L.d_tgt_off, off.size()));
     RB_TRY(dalloc(&L.d_contrib, contrib.size()));
     RB_TRY(dalloc(&L.d_corr_flux, (size_t)nslot * 120));
+    if (c->hp.pressure_fix) RB_TRY(dalloc(&L.d_corr_tmp, (size_t)nslot * 48));
     RB_TRY(h2d(c, L.d_tgt, tgt.data(), tgt.size() * 4));
     RB_TRY(h2d(c, L.d_tgt_off, off.data(), off.size() * 4));
     RB_TRY(h2d(c, L.d_contrib, contrib.data(), contrib.size() * 4));
@@ -332,6 +352,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(dalloc(&L.d_tile_corr, ent.size()));
     RB_TRY(h2d(c, L.d_tile_corr, ent.data(), ent.size() * 4));
   }
+  if (c->hp.pressure_fix) RB_TRY(ensure_nbor6(c, L));
   L.tables_built = true;
   return RB_OK;
 }
@@ -444,26 +465,60 @@ int set_unew_impl(rb_context* c, int l) {
   rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
       c->d_uold, c->d_unew, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
+  if (c->hp.pressure_fix) {
+    rb::pf_set_unew_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+        c->d_uold, c->d_divu, c->d_enew, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp.smallr, c->gate);
+    RB_CUDA(cudaGetLastError());
+  }
   return RB_OK;
 }
 
+// pressure_fix: the pdV term of set_uold on the old state (before the copy)
+int pdv_impl(rb_context* c, int l, const double* dt_dev, double dt) {
+  Level& L = c->lv[l];
+  RB_TRY(ensure_nbor6(c, L));
+  rb::pdv_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_uold, c->d_son, L.d_active, L.d_nbor6, L.noct, c->ncell, c->mp.ncoarse, L.dx, dt_dev, dt, c->hp,
+      c->d_enew, c->gate);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+// pressure_fix: the energy fix of set_uold on the new state (after the copy)
+int pf_fix_impl(rb_context* c, int l, const double* dt_dev, double dt, int skip_split) {
+  Level& L = c->lv[l];
+  rb::pf_fix_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_uold, c->d_divu, c->d_enew, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, dt_dev, dt,
+      c->hp.smallr, c->hp.beta_fix, skip_split, c->gate);
+  RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+// set_uold (per call): with pressure_fix, dtnew(ilevel) is the dt of the
+// level's last rb_godunov_fine
 int set_uold_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
+  if (c->hp.pressure_fix) RB_TRY(pdv_impl(c, l, nullptr, c->dt_godunov[l]));
   rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
       c->d_unew, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
+  if (c->hp.pressure_fix) RB_TRY(pf_fix_impl(c, l, nullptr, c->dt_godunov[l], 0));
   return RB_OK;
 }
 
-// set_uold + upload_fine of level l in one pass (set_uold_upload_kernel)
-int set_uold_upload_impl(rb_context* c, int l) {
+// set_uold + upload_fine of level l in one pass (set_uold_upload_kernel);
+// with pressure_fix, the pdV term before and the energy fix of the cells
+// upload_fine does not overwrite after. dt: *dt_dev if non-null.
+int set_uold_upload_impl(rb_context* c, int l, const double* dt_dev, double dt) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   const int do_upload = (l < c->mp.nlevelmax && L.has_refined) ? 1 : 0;
+  if (c->hp.pressure_fix) RB_TRY(pdv_impl(c, l, dt_dev, dt));
   rb::set_uold_upload_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
       c->d_uold, c->d_unew, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, do_upload, c->gate);
   RB_CUDA(cudaGetLastError());
+  if (c->hp.pressure_fix) RB_TRY(pf_fix_impl(c, l, dt_dev, dt, do_upload));
   return RB_OK;
 }
 
@@ -558,6 +613,9 @@ rb::TileArgs tile_args(rb_context* c, Level& L, double dt) {
   a.tile_corr = L.nslot ? L.d_tile_corr : nullptr;
   a.tile_corr_off = L.nslot ? L.d_tile_corr_off : nullptr;
   a.corr_flux = L.d_corr_flux;
+  a.divu = c->d_divu;    // null unless pressure_fix
+  a.enew = c->d_enew;
+  a.corr_tmp = L.d_corr_tmp;
   a.ncell = c->ncell;
   a.ninterp8 = (int64_t)L.ninterp * 8;
   a.ncoarse = c->mp.ncoarse;
@@ -597,12 +655,14 @@ int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_d
   }
   rb::TileArgs a = tile_args(c, L, dt);
   a.dt_dev = dt_dev;
+  if (!dt_dev) c->dt_godunov[l] = dt;
   if (timed) RB_CUDA(cudaEventRecord(c->ev0, c->stream));
   RB_TRY(launch_tile(c, L.shape, a, L.ntile));
   if (timed) RB_CUDA(cudaEventRecord(c->ev1, c->stream));
   if (L.ntgt) {
     rb::apply_corrections_kernel<<<(L.ntgt + 127) / 128, 128, 0, c->stream>>>(
-        c->d_unew, L.d_tgt, L.d_tgt_off, L.d_contrib, L.ntgt, L.d_corr_flux, c->ncell, c->gate);
+        c->d_unew, L.d_tgt, L.d_tgt_off, L.d_contrib, L.ntgt, L.d_corr_flux, c->ncell, c->gate, c->d_divu, c->d_enew,
+        L.d_corr_tmp);
     RB_CUDA(cudaGetLastError());
   }
   return RB_OK;
@@ -617,7 +677,8 @@ int courant_impl(rb_context* c, int l, double* dt_io, double* mass, double* ekin
   RB_TRY(ensure_partial(c, nblk));
   auto k = c->precision == RB_PREC_MIXED ? rb::courant_partial_kernel<256, true> : rb::courant_partial_kernel<256, false>;
   k<<<nblk, nt, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, c->hp,
-                                c->d_partial, c->gate, with_set_unew ? c->d_unew : nullptr);
+                                c->d_partial, c->gate, with_set_unew ? c->d_unew : nullptr,
+                                with_set_unew ? c->d_divu : nullptr, with_set_unew ? c->d_enew : nullptr);
   RB_CUDA(cudaGetLastError());
   const double dt0 = c->hp.courant_factor * L.dx / c->hp.smallc;
   rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, *dt_io, dt0,
@@ -664,7 +725,7 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   }
   RB_TRY(godunov_impl(c, l, c->dtnew[l], false));
   c->cell_updates += c->lv[l].leaf_cells;
-  RB_TRY(set_uold_upload_impl(c, l));
+  RB_TRY(set_uold_upload_impl(c, l, nullptr, c->dtnew[l]));
   if (l > c->mp.levelmin) {
     if (c->mp.nsubcycle[l - 1] == 1) c->dtnew[l - 1] = c->dtnew[l];
     if (icount == 2) c->dtnew[l - 1] = c->dtold[l] + c->dtnew[l];
@@ -685,7 +746,7 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   const int nblk = courant_blocks(c, l);
   auto k = c->precision == RB_PREC_MIXED ? rb::courant_partial_kernel<256, true> : rb::courant_partial_kernel<256, false>;
   k<<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, c->hp,
-                                 c->d_partial, c->gate, c->d_unew);  // + set_unew
+                                 c->d_partial, c->gate, c->d_unew, c->d_divu, c->d_enew);  // + set_unew
   RB_CUDA(cudaGetLastError());
   const double nsub_prev = l > c->mp.levelmin ? (double)(float)c->mp.nsubcycle[l - 1] : 1.0;
   rb::sched_courant_kernel<<<1, RB_RED_NT, 0, c->stream>>>(
@@ -704,7 +765,7 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   }
   RB_CUDA(cudaGetLastError());
   RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l));
-  RB_TRY(set_uold_upload_impl(c, l));
+  RB_TRY(set_uold_upload_impl(c, l, s + RB_S_DTNEW + l, 0.0));
   if (l > c->mp.levelmin && (c->mp.nsubcycle[l - 1] == 1 || icount == 2)) {
     rb::sched_end_kernel<<<1, 1, 0, c->stream>>>(s, l, c->mp.nsubcycle[l - 1] == 1 ? 1 : 0, icount);
     RB_CUDA(cudaGetLastError());
@@ -885,6 +946,12 @@ int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision
       (rc = dalloc(&c->d_stage, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_red, 8)) ||
       (rc = dalloc(&c->d_clock, 8)) || (rc = dalloc(&c->d_sched, RB_S_SIZE)))
     return bail(rc);
+  if (c->hp.pressure_fix) {
+    if ((rc = dalloc(&c->d_divu, (size_t)c->ncell)) || (rc = dalloc(&c->d_enew, (size_t)c->ncell))) return bail(rc);
+    if (cudaMemsetAsync(c->d_divu, 0, (size_t)c->ncell * sizeof(double), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->d_enew, 0, (size_t)c->ncell * sizeof(double), c->stream) != cudaSuccess)
+      return bail(fail(RB_ERR_CUDA, "initialising device buffers failed"));
+  }
   if (cudaMallocHost((void**)&c->h_red, 8 * sizeof(double)) != cudaSuccess ||
       cudaMallocHost((void**)&c->h_sched, RB_S_SIZE * sizeof(double)) != cudaSuccess)
     return bail(fail(RB_ERR_NOMEM, "pinned allocation failed"));
@@ -905,6 +972,7 @@ int rb_destroy(rb_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_tree(c);
   dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son);
+  dfree(c->d_divu); dfree(c->d_enew);
   dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
   dfree(c->d_flag);
   if (c->h_red) cudaFreeHost(c->h_red);
@@ -959,6 +1027,19 @@ int rb_download_state(rb_context* c, double* uold) {
   return download_impl(c, c->d_uold, uold);
 }
 int rb_upload_unew(rb_context* c, const double* unew) { return upload_impl(c, unew, c ? c->d_unew : nullptr); }
+int rb_download_pressure_fix(rb_context* c, double* divu, double* enew) {
+  if (!c || !divu || !enew) return fail(RB_ERR_INVALID, "null argument");
+  if (!c->hp.pressure_fix) return fail(RB_ERR_STATE, "the context was created without pressure_fix");
+  for (int k = 0; k < 2; k++) {
+    rb::permute_d2f_kernel<<<grid_for(c->ncell, 256), 256, 0, c->stream>>>(
+        k == 0 ? c->d_divu : c->d_enew, c->d_stage, c->ncell, c->mp.ncoarse, c->mp.ngridmax, 1);
+    RB_CUDA(cudaGetLastError());
+    RB_CUDA(cudaMemcpyAsync(k == 0 ? divu : enew, c->d_stage, (size_t)c->ncell * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  return RB_OK;
+}
 int rb_download_unew(rb_context* c, double* unew) { return download_impl(c, c ? c->d_unew : nullptr, unew); }
 
 int rb_set_unew(rb_context* c, int l) {
@@ -1057,16 +1138,7 @@ int rb_hydro_flag(rb_context* c, int l, const rb_refine_params* rp, int32_t* fla
   if (!L.noct) return RB_OK;
   if (rp->err_grad_d == -1.0 && rp->err_grad_p == -1.0 && rp->err_grad_u == -1.0) return RB_OK;
   RB_TRY(sync_oct(c));
-  if (!L.d_nbor6) {
-    std::vector<int32_t> nb((size_t)L.noct * 6);
-    for (int i = 0; i < L.noct; i++) {
-      const int g = L.h_active[i];
-      for (int j = 0; j < 6; j++)
-        nb[(size_t)i * 6 + j] = (int32_t)dev_of_fortran(c, c->nbor[(size_t)j * c->mp.ngridmax + (g - 1)]);
-    }
-    RB_TRY(dalloc(&L.d_nbor6, nb.size()));
-    RB_TRY(h2d(c, L.d_nbor6, nb.data(), nb.size() * sizeof(int32_t)));
-  }
+  RB_TRY(ensure_nbor6(c, L));
   const int64_t n = (int64_t)L.noct * 8;
   if (n > c->flag_cap) {
     dfree(c->d_flag);
@@ -1205,6 +1277,9 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
     c->d_unew = c->d_stage;
     rb::TileArgs a = tile_args(c, L, 1e-30);
     c->d_unew = keep_unew;
+    // the trial launches leave divu/enew alone (shapes are timed on the
+    // variant without the pressure fix)
+    a.divu = a.enew = a.corr_tmp = nullptr;
     float ms = 1e30f;
     for (int rep = 0; rep < 4; rep++) {
       RB_CUDA(cudaEventRecord(c->ev0, c->stream));
@@ -1585,6 +1660,15 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
     return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
   for (int l = 1; l < lf; l++)
     if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
+  // with pressure_fix the pdV term and the energy fix come between the update
+  // and the next CFL condition: the amr_step sequence, step by step
+  if (c->hp.pressure_fix) {
+    if (t_io) c->t = *t_io;
+    for (int s = 0; s < nsteps; s++) RB_TRY(rb_coarse_step(c, nullptr, nullptr));
+    if (t_io) *t_io = c->t;
+    if (dt_last_out) *dt_last_out = c->dtnew[lf];
+    return RB_OK;
+  }
   // the multi-dimensional limiter (slope_type 3) reads the 26 neighbours of
   // every cell, which the z-streaming kernel does not hold: oct tiles only
   if (c->uniform_method == 0 && c->hp.slope_type != 3)

@@ -37,8 +37,10 @@ typedef struct rb_hydro_params {
   int32_t scheme;        /* 0 = 'muscl' ('plmde' is rejected)              */
   int32_t interpol_var;  /* 0,1,2                                          */
   int32_t interpol_type; /* 0..4                                           */
-  int32_t pressure_fix;  /* must be 0                                      */
+  int32_t pressure_fix;  /* 1: dual-energy fix (enew/divu tracked, set_uold  */
+                         /*    repairs E where E - ekin is too small)       */
   double difmag;         /* must be 0                                      */
+  double beta_fix;       /* pressure-fix threshold, >= 0 (default 0)       */
 } rb_hydro_params;
 
 /* Gradient refinement criterion of &REFINE_PARAMS

@@ -31,6 +31,7 @@ class HydroParams:
     interpol_type: int = 1
     pressure_fix: bool = False
     difmag: float = 0.0
+    beta_fix: float = 0.0
 
     @property
     def riemann_code(self) -> int:
@@ -45,10 +46,10 @@ class HydroParams:
             raise ValueError("Unknown slope type %r" % self.slope_type)
         if self.scheme.strip().lower() != "muscl":
             raise ValueError("scheme %r not supported (muscl only)" % self.scheme)
-        if self.pressure_fix:
-            raise ValueError("pressure_fix is not supported")
         if self.difmag != 0.0:
             raise ValueError("difmag>0 is not supported")
+        if not (self.beta_fix >= 0.0) or self.beta_fix == float("inf"):
+            raise ValueError("beta_fix must be finite and >= 0")
         if self.interpol_var not in (0, 1, 2) or self.interpol_type not in (0, 1, 2, 3, 4):
             raise ValueError("bad interpol_var/interpol_type")
         if self.interpol_type == 4 and self.interpol_var != 2:

@@ -34,7 +34,8 @@ class HydroParamsC(ctypes.Structure):
                 ("courant_factor", ctypes.c_double), ("slope_theta", ctypes.c_double),
                 ("riemann", ctypes.c_int32), ("slope_type", ctypes.c_int32), ("scheme", ctypes.c_int32),
                 ("interpol_var", ctypes.c_int32), ("interpol_type", ctypes.c_int32),
-                ("pressure_fix", ctypes.c_int32), ("difmag", ctypes.c_double)]
+                ("pressure_fix", ctypes.c_int32), ("difmag", ctypes.c_double),
+                ("beta_fix", ctypes.c_double)]
 
 
 class RefineParamsC(ctypes.Structure):
@@ -70,6 +71,7 @@ _PROTOS = {
     "rb_sync_tree": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32, _P32]),
     "rb_upload_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_download_pressure_fix": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
     "rb_upload_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_set_unew": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -146,7 +148,8 @@ def _check(rc: int, where: str):
 def hydro_params_c(hp: HydroParams) -> HydroParamsC:
     hp.validate()
     return HydroParamsC(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta, hp.riemann_code,
-                        hp.slope_type, 0, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix), hp.difmag)
+                        hp.slope_type, 0, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix), hp.difmag,
+                        hp.beta_fix)
 
 
 def mesh_params_c(tree: Octree, nsubcycle: Optional[Sequence[int]] = None, nvector: int = 32) -> MeshParamsC:
@@ -245,6 +248,12 @@ class Solver:
         u = np.empty((5, self.tree.ncell))
         _check(load().rb_download_unew(self._h, _ptr(u, _PD)), "rb_download_unew")
         return u
+
+    def download_pressure_fix(self):
+        """pressure_fix arrays (divu, enew), Fortran layout (ncell,) each."""
+        dv, en = np.empty(self.tree.ncell), np.empty(self.tree.ncell)
+        _check(load().rb_download_pressure_fix(self._h, _ptr(dv, _PD), _ptr(en, _PD)), "rb_download_pressure_fix")
+        return dv, en
 
     # -- level operations (reference names) ------------------------------
     def set_unew(self, ilevel: int):

@@ -314,3 +314,74 @@ def test_dense_step_outflow_is_zero_gradient():
     # the periodic run has the second interface's waves there
     assert a[0, 0, 0, 0] == pytest.approx(1.0, abs=1e-12) and a[0, 0, 0, -1] == pytest.approx(0.125, abs=1e-12)
     assert abs(b[0, 0, 0, 0] - 1.0) > 1e-3
+
+
+# ---- pressure_fix (dual energy): godunov_fine.f90:71-86, 203-227, 287-432,
+# 735-744, 775-789, 831-856, 883-906 ----------------------------------------
+
+def _pf(hp, beta):
+    hp.pressure_fix = True
+    hp.beta_fix = beta
+    return hp
+
+
+def test_pressure_fix_set_unew_internal_energy():
+    """set_unew: divu = 0 and enew = E - d/2 |m/d|^2 on every active cell."""
+    tree, hp, u = sedov_amr(3, 5)
+    run = oracle.OracleRun(tree, _pf(hp, 0.5), u)
+    run.divu[:] = 7.0
+    run.set_unew(4)
+    a = tree.active[4]
+    c = (tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + a[None, :]).reshape(-1) - 1
+    d = np.maximum(u[0, c], hp.smallr)
+    v = u[1:4, c] / d
+    e = u[4, c] - 0.5 * d * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    np.testing.assert_array_equal(run.divu[c], 0.0)
+    np.testing.assert_array_equal(run.enew[c], e)
+
+
+def test_pressure_fix_off_threshold_changes_nothing():
+    """beta_fix = 0 repairs only negative E - ekin: on the Sedov AMR run, where
+    that never happens, the state equals the run without the pressure fix."""
+    tree, hp, u = sedov_amr(3, 5)
+    a = oracle.OracleRun(tree, hp, u)
+    b = oracle.OracleRun(tree, _pf(HydroParams(**{**hp.__dict__}), 0.0), u)
+    for _ in range(4):
+        a.coarse_step()
+        b.coarse_step()
+    np.testing.assert_array_equal(a.uold, b.uold)
+    assert np.any(b.enew != 0.0) and np.any(b.divu != 0.0)
+
+
+def test_pressure_fix_repairs_energy_only():
+    """beta_fix > 0 replaces E by enew + ekin in the cells with a large
+    velocity divergence: only E changes, and the repaired internal energy is
+    the tracked one."""
+    tree, hp, u = sedov_amr(3, 5)
+    a = oracle.OracleRun(tree, hp, u)
+    b = oracle.OracleRun(tree, _pf(HydroParams(**{**hp.__dict__}), 10.0), u)
+    for _ in range(3):
+        a.coarse_step()
+        b.coarse_step()
+    assert np.all(np.isfinite(b.uold))
+    diff = np.any(a.uold != b.uold, axis=0)
+    assert diff.sum() > 0
+    # on a single level the fix is the last thing a coarse step does: at the
+    # first step where the runs part, only E of the repaired cells differs
+    t, hp2, u2 = sedov_uniform(4)
+    c = oracle.OracleRun(t, hp2, u2)
+    d = oracle.OracleRun(t, _pf(HydroParams(**{**hp2.__dict__}), 10.0), u2)
+    for _ in range(30):
+        c.coarse_step()
+        d.coarse_step()
+        changed = c.uold[4] != d.uold[4]
+        if changed.any():
+            break
+    assert changed.sum() > 0
+    np.testing.assert_array_equal(c.uold[:4], d.uold[:4])
+    cells = np.nonzero(changed)[0]
+    dd = np.maximum(d.uold[0, cells], hp2.smallr)
+    v = d.uold[1:4, cells] / dd
+    ekin = 0.5 * dd * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2])
+    fine = t.son[cells] == 0  # split cells hold the restriction of their children
+    np.testing.assert_array_equal(d.uold[4, cells[fine]], d.enew[cells[fine]] + ekin[fine])
