@@ -17,7 +17,7 @@ module rb_b200
   type, bind(c) :: rb_hydro_params_t
      real(c_double) :: gamma, smallr, smallc, courant_factor, slope_theta
      integer(c_int32_t) :: riemann, slope_type, scheme, interpol_var, interpol_type, pressure_fix
-     real(c_double) :: difmag
+     real(c_double) :: difmag, beta_fix
   end type rb_hydro_params_t
 
   type, bind(c) :: rb_mesh_params_t
@@ -127,6 +127,7 @@ contains
     hp%courant_factor = courant_factor; hp%slope_theta = slope_theta
     hp%slope_type = slope_type; hp%scheme = 0; hp%pressure_fix = 0
     hp%interpol_var = interpol_var; hp%interpol_type = interpol_type; hp%difmag = difmag
+    hp%beta_fix = beta_fix
     if (scheme /= 'muscl') hp%scheme = 1
     if (pressure_fix) hp%pressure_fix = 1
     hp%riemann = 0
