@@ -358,6 +358,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description="ensemble serving of independent hydro problems")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=100.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--rates", default=None,
+                    help="comma-separated arrival rates: the same requests served once per rate (a rate sweep)")
     ap.add_argument("--sizes", default="32,64,128")
     ap.add_argument("--max-extra", type=int, default=2)
     ap.add_argument("--t-end", type=float, default=0.1)
@@ -373,23 +375,34 @@ def main(argv=None):
     t0 = time.perf_counter()
     reqs = [build_request(s, hp, outflow=not args.periodic_tubes) for s in specs]
     build_s = time.perf_counter() - t0
-    arrivals = poisson_arrivals(len(reqs), args.rate, args.seed + 1)
-    with Server(hp, precision=args.precision, steps_per_round=args.steps_per_round) as srv:
-        res = run_stream(srv, reqs, arrivals, args.t_end)
-        launches = srv.stats()["batch_launches"]
-    out = {"workload": "ensemble serving: %d requests (%s), Poisson %.0f req/s, t_end=%g, seed %d"
-           % (len(reqs), args.sizes, args.rate, args.t_end, args.seed),
-           "precision": args.precision, "latency_s": res["latency_s"], "makespan_s": res["makespan_s"],
-           "cell_updates_per_s": res["cell_updates_per_s"], "cell_updates": res["cell_updates"],
-           "batched_launches": launches, "ic_build_s": build_s,
+    rates = [float(r) for r in args.rates.split(",")] if args.rates else [args.rate]
+    base = one_at_a_time(reqs, hp, args.t_end, "fp64") if args.baseline else None
+    sweep = []
+    for rate in rates:
+        arrivals = poisson_arrivals(len(reqs), rate, args.seed + 1)
+        with Server(hp, precision=args.precision, steps_per_round=args.steps_per_round) as srv:
+            res = run_stream(srv, reqs, arrivals, args.t_end)
+            launches = srv.stats()["batch_launches"]
+        row = {"rate_per_s": rate, "latency_s": res["latency_s"], "makespan_s": res["makespan_s"],
+               "cell_updates_per_s": res["cell_updates_per_s"], "cell_updates": res["cell_updates"],
+               "batched_launches": launches}
+        if base is not None:
+            # the same arrivals through one FIFO server with the measured
+            # one-at-a-time FP64 service times
+            comp = fifo_completion(arrivals, base["service_s"])
+            tts = comp - arrivals
+            row["one_at_a_time_fp64"] = {"latency_s": percentiles(tts), "makespan_s": float(comp[-1] - arrivals[0]),
+                                         "cell_updates_per_s": base["cell_updates"] / float(sum(base["service_s"])),
+                                         "cell_updates": base["cell_updates"]}
+        sweep.append(row)
+    out = {"workload": "ensemble serving: %d requests (%s), Poisson %s req/s, t_end=%g, seed %d"
+           % (len(reqs), args.sizes, ",".join("%g" % r for r in rates), args.t_end, args.seed),
+           "precision": args.precision, "ic_build_s": build_s,
            "dense_requests": sum(r.is_dense for r in reqs), "amr_requests": sum(not r.is_dense for r in reqs)}
-    if args.baseline:
-        base = one_at_a_time(reqs, hp, args.t_end, "fp64")
-        comp = fifo_completion(arrivals, base["service_s"])
-        tts = comp - arrivals
-        out["one_at_a_time_fp64"] = {"latency_s": percentiles(tts), "makespan_s": float(comp[-1] - arrivals[0]),
-                                     "cell_updates_per_s": base["cell_updates"] / float(sum(base["service_s"])),
-                                     "cell_updates": base["cell_updates"]}
+    if len(sweep) == 1:
+        out.update(sweep[0])
+    else:
+        out["sweep"] = sweep
     print(json.dumps(out))
     return out
 
