@@ -129,7 +129,7 @@ constexpr size_t tile_smem_bytes() {
 template <typename R, int TX, int TY, int TZ, int NT, int RS, int ST, bool PF = false>
 __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   using G = TileGeom<TX, TY, TZ>;
-  constexpr int SX = G::SX, SY = G::SY, SZ = G::SZ, NS = G::NS;
+  constexpr int SX = G::SX, SY = G::SY, NS = G::NS;
   constexpr int BX = G::BX, BY = G::BY, NBLK = G::NBLK;
   constexpr int NFX = G::NFX, NFY = G::NFY, NF = G::NF;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -1566,8 +1566,8 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
     RB_CUDA(cudaGetLastError());
     c->dense_valid = true;
   }
-  // a representative dt in a scratch slot of the reduction buffer
-  double dt_probe = 0.0;
+  // a representative dt in a scratch slot of the reduction buffer (the
+  // trial launches read it there)
   {
     double d = c->mp.boxlen / c->hp.smallc;
     const int nblk = grid_for((int64_t)L.noct * 8, 256, 148 * 8);
@@ -1577,11 +1577,7 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
     RB_CUDA(cudaGetLastError());
     rb::reduce_partials_kernel<<<1, RB_RED_NT, 0, c->stream>>>(c->d_partial, nblk, d, c->hp.courant_factor * L.dx / c->hp.smallc, 1, c->d_red + 4, 0);
     RB_CUDA(cudaGetLastError());
-    RB_CUDA(cudaMemcpyAsync(c->h_red, c->d_red + 4, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    RB_CUDA(cudaStreamSynchronize(c->stream));
-    dt_probe = c->h_red[0];
   }
-  (void)dt_probe;
   int best_s = -1, best_hz = 0;
   float best_ms = 1e30f;
   for (int s = 0; s < rb::kNumStreamShapes; s++) {
