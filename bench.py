@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--stream-config", default=None, metavar="SHAPE,HZ",
                     help="z-streaming method: use this column shape and z extent instead of autotuning "
                          "(profiling runs replay the autotuned choice without its probe launches)")
+    ap.add_argument("--pressure-fix", type=float, default=None, metavar="BETA",
+                    help="AMR runs with pressure_fix on and beta_fix=BETA (the dual-energy fix)")
     ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
                     help="instead of the headline, time device-scheduled coarse steps (rb_run) on a static AMR "
                          "tree: sedov = Sedov levels 6-9 refined on a shell, clumps = blast-clump levels 7-10")
@@ -301,6 +303,10 @@ def run_amr(args):
     runtime.load()
     t0 = time.perf_counter()
     tree, hp, u, desc = amr_workload(args.amr)
+    if args.pressure_fix is not None:
+        hp.pressure_fix = True
+        hp.beta_fix = args.pressure_fix
+        desc += ", pressure_fix with beta_fix=%g" % args.pressure_fix
     build_s = time.perf_counter() - t0
     levels = [l for l in range(1, tree.nlevelmax + 1) if tree.noct(l)]
     out, states = {}, {}

@@ -60,6 +60,21 @@ __device__ __forceinline__ double pf_eint(const double u[5], double smallr) {
   return u[4] - 0.5 * d * (uu * uu + vv * vv + ww * ww);
 }
 
+// pressure fix of one cell (godunov_fine.f90:203-227, hexp = 0) on its new
+// state u: E = enew + ekin where E - ekin < beta_fix d (|divu| dx/dt)^2.
+__device__ __forceinline__ void pf_fix_cell(double u[5], double divu, double enew, double dx, double dt,
+                                            double smallr, double beta_fix) {
+  const double hexp = 0.0;
+  const double d = fmx(u[0], smallr);
+  const double uu = u[1] / d, vv = u[2] / d, ww = u[3] / d;
+  const double e_kin = 0.5 * d * (uu * uu + vv * vv + ww * ww);
+  const double e_cons = u[4] - e_kin;
+  const double div = fabs(divu) * dx / dt;
+  const double mx = fmx(div, 3.0 * hexp * dx);
+  const double e_trunc = beta_fix * d * (mx * mx);
+  if (e_cons < e_trunc) u[4] = enew + e_kin;
+}
+
 // pressure_fix part of set_unew (godunov_fine.f90:71-86): divu = 0 and enew
 // = the internal energy of uold, for every cell of the active octs.
 static __global__ void pf_set_unew_kernel(const double* __restrict__ uold, double* __restrict__ divu,
@@ -81,47 +96,55 @@ static __global__ void pf_set_unew_kernel(const double* __restrict__ uold, doubl
 // div(u) dt, with div(u) = sum over directions of (v_right - v_left) /
 // (dx_left + dx_right) from the uold velocities of the neighbouring cells;
 // a neighbour whose oct does not exist is its coarse father cell at 1.5 dx.
-// nbor6[p*6 + j]: device cell of nbor(igrid, j+1) of the level's oct p.
-// dt: *dt_dev if non-null, else dt_val.
-static __global__ void pdv_kernel(const double* __restrict__ uold, const int32_t* __restrict__ son,
-                                  const int32_t* __restrict__ active, const int32_t* __restrict__ nbor6,
-                                  int32_t noct, int64_t ncell, int32_t ncoarse, double dx_loc,
-                                  const double* __restrict__ dt_dev, double dt_val, rb_hydro_params hp,
-                                  double* __restrict__ enew, const double* __restrict__ gate) {
+// nres6[p*6 + j] resolves nbor(igrid, j+1) of the level's oct p: >= 0 the
+// device cell of child 0 of the neighbouring oct at this level, else
+// -(device cell of the coarse neighbour) - 1. dt: *dt_dev if non-null, else
+// dt_val. dx_pow2: dx_loc is a power of two, so the quotient by 2 dx_loc is
+// the product with its exact reciprocal.
+static __global__ void pdv_kernel(const double* __restrict__ uold, const int32_t* __restrict__ active,
+                                  const int64_t* __restrict__ nres6, int32_t noct, int64_t ncell,
+                                  int32_t ncoarse, double dx_loc, int dx_pow2, const double* __restrict__ dt_dev,
+                                  double dt_val, rb_hydro_params hp, double* __restrict__ enew,
+                                  const double* __restrict__ gate) {
   RB_GATE(gate);
   const double dt = dt_dev ? *dt_dev : dt_val;
+  const double inv_2dx = 1.0 / (dx_loc + dx_loc);
   const int64_t n = (int64_t)noct * 8;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t p = i >> 3;
+  // 8 consecutive lanes hold one oct's cells: a neighbour inside the oct
+  // hands over its velocity by a shuffle (the same IEEE quotient the
+  // reference forms again); the loop bound keeps whole warps in it
+  const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += nthreads) {
+    const int64_t i = i0 + threadIdx.x;
+    const bool live = i < n;
+    const int64_t p = live ? i >> 3 : 0;
     const int ind = (int)(i & 7);
-    const int64_t g = active[p];
+    const int64_t g = live ? active[p] : 0;
     const int64_t dc = ncoarse + g * 8 + ind;
+    double u[5] = {1.0, 0.0, 0.0, 0.0, 1.0};
+    if (live)
+      for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    const double d0 = fmx(u[0], hp.smallr);
+    const double own[3] = {u[1] / d0, u[2] / d0, u[3] / d0};
     double divu_loc = 0.0;
     for (int d = 0; d < 3; d++) {
       const int bit = (ind >> d) & 1, jnd = ind ^ (1 << d);
-      double vel[2], dxs[2];
-      for (int side = 0; side < 2; side++) {
-        const bool inside = side == 0 ? bit == 1 : bit == 0;
-        int64_t nb = ncoarse + g * 8 + jnd;
-        dxs[side] = dx_loc;
-        if (!inside) {
-          const int64_t fcell = nbor6[p * 6 + 2 * d + side];
-          const int gn = son[fcell];
-          if (gn > 0) {
-            nb = ncoarse + (int64_t)(gn - 1) * 8 + jnd;
-          } else {
-            nb = fcell;
-            dxs[side] = dx_loc * 1.5;
-          }
-        }
-        vel[side] = uold[(int64_t)(1 + d) * ncell + nb] / fmx(uold[nb], hp.smallr);
-      }
-      divu_loc = divu_loc + (vel[1] - vel[0]) / (dxs[0] + dxs[1]);
+      // the velocity of the neighbour inside the oct (lane ^ (1 << d))
+      const double inner = __shfl_xor_sync(0xffffffffu, own[d], 1 << d);
+      // the other neighbour along d: left if bit == 0, right if bit == 1
+      const int64_t r = live ? nres6[p * 6 + 2 * d + bit] : 0;
+      const bool coarse = r < 0;
+      const int64_t nb = coarse ? -r - 1 : r + jnd;
+      const double outer = uold[(int64_t)(1 + d) * ncell + nb] / fmx(uold[nb], hp.smallr);
+      const double dx_out = coarse ? dx_loc * 1.5 : dx_loc;
+      const double vl = bit ? inner : outer, vr = bit ? outer : inner;
+      const double den = bit ? dx_loc + dx_out : dx_out + dx_loc;
+      const double diff = vr - vl;
+      divu_loc = divu_loc + ((dx_pow2 && !coarse) ? diff * inv_2dx : diff / den);
     }
-    double u[5];
-    for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
-    const double eold = pf_eint(u, hp.smallr);
-    enew[dc] = enew[dc] - (hp.gamma - 1.0) * eold * divu_loc * dt;
+    // eold = E - d/2 (u^2+v^2+w^2) with the velocities above
+    const double eold = u[4] - 0.5 * d0 * (own[0] * own[0] + own[1] * own[1] + own[2] * own[2]);
+    if (live) enew[dc] = enew[dc] - (hp.gamma - 1.0) * eold * divu_loc * dt;
   }
 }
 
@@ -139,20 +162,14 @@ static __global__ void pf_fix_kernel(double* __restrict__ uold, const double* __
                                      const double* __restrict__ gate) {
   RB_GATE(gate);
   const double dt = dt_dev ? *dt_dev : dt_val;
-  const double hexp = 0.0;
   const int64_t n = (int64_t)noct * 8;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
     if (skip_split && son[dc] > 0) continue;
-    const double d = fmx(uold[dc], smallr);
-    const double u = uold[ncell + dc] / d, v = uold[2 * ncell + dc] / d, w = uold[3 * ncell + dc] / d;
-    const double e_kin = 0.5 * d * (u * u + v * v + w * w);
-    const double e_cons = uold[4 * ncell + dc] - e_kin;
-    const double e_prim = enew[dc];
-    const double div = fabs(divu[dc]) * dx / dt;
-    const double mx = fmx(div, 3.0 * hexp * dx);
-    const double e_trunc = beta_fix * d * (mx * mx);
-    if (e_cons < e_trunc) uold[4 * ncell + dc] = e_prim + e_kin;
+    double u[5];
+    for (int v = 0; v < 5; v++) u[v] = uold[v * ncell + dc];
+    pf_fix_cell(u, divu[dc], enew[dc], dx, dt, smallr, beta_fix);
+    uold[4 * ncell + dc] = u[4];
   }
 }
 
@@ -580,12 +597,19 @@ static __global__ void upload_fine_kernel(double* __restrict__ uold, const int32
 // in one pass: set_uold copies unew to uold for every cell and upload_fine
 // then overwrites every variable of the split cells with the restriction of
 // their children, so each cell's final uold is written once. do_upload = 0
-// where upload_fine does nothing (finest level, or no split cell).
+// where upload_fine does nothing (finest level, or no split cell). With
+// pressure_fix (divu non-null) the copied cells get set_uold's energy fix
+// (dt: *dt_dev if non-null, else dt_val); the split cells' fix would be
+// overwritten by the restriction.
 static __global__ void set_uold_upload_kernel(double* __restrict__ uold, const double* __restrict__ unew,
                                               const int32_t* __restrict__ son, const int32_t* __restrict__ active,
                                               int32_t noct, int64_t ncell, int32_t ncoarse, rb_hydro_params hp,
-                                              int do_upload, const double* __restrict__ gate) {
+                                              int do_upload, const double* __restrict__ gate,
+                                              const double* __restrict__ divu = nullptr,
+                                              const double* __restrict__ enew = nullptr, double dx = 0.0,
+                                              const double* __restrict__ dt_dev = nullptr, double dt_val = 0.0) {
   RB_GATE(gate);
+  const double dt = dt_dev ? *dt_dev : dt_val;
   const int64_t n = (int64_t)noct * 8;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t dc = ncoarse + (int64_t)active[i >> 3] * 8 + (i & 7);
@@ -593,8 +617,12 @@ static __global__ void set_uold_upload_kernel(double* __restrict__ uold, const d
     if (gs > 0) {
       restrict_cell(uold, dc, gs, ncell, ncoarse, hp);
     } else {
+      double u[5];
 #pragma unroll
-      for (int v = 0; v < 5; v++) uold[v * ncell + dc] = unew[v * ncell + dc];
+      for (int v = 0; v < 5; v++) u[v] = unew[v * ncell + dc];
+      if (divu) pf_fix_cell(u, divu[dc], enew[dc], dx, dt, hp.smallr, hp.beta_fix);
+#pragma unroll
+      for (int v = 0; v < 5; v++) uold[v * ncell + dc] = u[v];
     }
   }
 }

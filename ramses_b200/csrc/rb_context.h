@@ -96,6 +96,7 @@ struct Level {
   int32_t* d_tgt_off = nullptr;
   int32_t* d_contrib = nullptr;
   int32_t* d_nbor6 = nullptr;     // [noct][6] device cell of nbor(igrid,j) (hydro_flag)
+  int64_t* d_nres6 = nullptr;     // [noct][6] nbor(igrid,j) resolved to the neighbouring oct (pressure_fix pdV)
   int64_t leaf_cells = 0;
   double dx = 0.0;
   bool complete = false;

@@ -87,6 +87,7 @@ void free_level_tables(Level& L) {
   dfree(L.d_tgt_off);
   dfree(L.d_contrib);
   dfree(L.d_nbor6);
+  dfree(L.d_nres6);
   L.ntile = L.ninterp = L.nslot = L.ntgt = 0;
   L.tables_built = false;
 }
@@ -141,6 +142,25 @@ int ensure_nbor6(rb_context* c, Level& L) {
   }
   RB_TRY(dalloc(&L.d_nbor6, nb.size()));
   RB_TRY(h2d(c, L.d_nbor6, nb.data(), nb.size() * sizeof(int32_t)));
+  return RB_OK;
+}
+
+// nbor(igrid,j) of the level's octs resolved for the pdV term: the device
+// cell of child 0 of the neighbouring oct at this level where it exists,
+// else -(device cell of the coarse neighbour) - 1.
+int ensure_nres6(rb_context* c, Level& L) {
+  if (L.d_nres6 || !L.noct) return RB_OK;
+  std::vector<int64_t> nr((size_t)L.noct * 6);
+  for (int i = 0; i < L.noct; i++) {
+    const int g = L.h_active[i];
+    for (int j = 0; j < 6; j++) {
+      const int64_t fcell = c->nbor[(size_t)j * c->mp.ngridmax + (g - 1)];
+      const int32_t gn = c->son[fcell - 1];
+      nr[(size_t)i * 6 + j] = gn > 0 ? (int64_t)c->mp.ncoarse + 8 * (int64_t)(gn - 1) : -dev_of_fortran(c, fcell) - 1;
+    }
+  }
+  RB_TRY(dalloc(&L.d_nres6, nr.size()));
+  RB_TRY(h2d(c, L.d_nres6, nr.data(), nr.size() * sizeof(int64_t)));
   return RB_OK;
 }
 
@@ -352,7 +372,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(dalloc(&L.d_tile_corr, ent.size()));
     RB_TRY(h2d(c, L.d_tile_corr, ent.data(), ent.size() * 4));
   }
-  if (c->hp.pressure_fix) RB_TRY(ensure_nbor6(c, L));
+  if (c->hp.pressure_fix) RB_TRY(ensure_nres6(c, L));
   L.tables_built = true;
   return RB_OK;
 }
@@ -476,9 +496,11 @@ int set_unew_impl(rb_context* c, int l) {
 // pressure_fix: the pdV term of set_uold on the old state (before the copy)
 int pdv_impl(rb_context* c, int l, const double* dt_dev, double dt) {
   Level& L = c->lv[l];
-  RB_TRY(ensure_nbor6(c, L));
+  RB_TRY(ensure_nres6(c, L));
+  int e2;
+  const int dx_pow2 = std::frexp(L.dx, &e2) == 0.5;
   rb::pdv_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
-      c->d_uold, c->d_son, L.d_active, L.d_nbor6, L.noct, c->ncell, c->mp.ncoarse, L.dx, dt_dev, dt, c->hp,
+      c->d_uold, L.d_active, L.d_nres6, L.noct, c->ncell, c->mp.ncoarse, L.dx, dx_pow2, dt_dev, dt, c->hp,
       c->d_enew, c->gate);
   RB_CUDA(cudaGetLastError());
   return RB_OK;
@@ -508,17 +530,17 @@ int set_uold_impl(rb_context* c, int l) {
 }
 
 // set_uold + upload_fine of level l in one pass (set_uold_upload_kernel);
-// with pressure_fix, the pdV term before and the energy fix of the cells
-// upload_fine does not overwrite after. dt: *dt_dev if non-null.
+// with pressure_fix, the pdV term before, and the energy fix in the same
+// pass. dt: *dt_dev if non-null.
 int set_uold_upload_impl(rb_context* c, int l, const double* dt_dev, double dt) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   const int do_upload = (l < c->mp.nlevelmax && L.has_refined) ? 1 : 0;
   if (c->hp.pressure_fix) RB_TRY(pdv_impl(c, l, dt_dev, dt));
   rb::set_uold_upload_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
-      c->d_uold, c->d_unew, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, do_upload, c->gate);
+      c->d_uold, c->d_unew, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, do_upload, c->gate,
+      c->d_divu, c->d_enew, L.dx, dt_dev, dt);
   RB_CUDA(cudaGetLastError());
-  if (c->hp.pressure_fix) RB_TRY(pf_fix_impl(c, l, dt_dev, dt, do_upload));
   return RB_OK;
 }
 
