@@ -385,6 +385,117 @@ static void riemann_hllc(const orc_params *p, const double *ql, const double *qr
 /* cmpflxm: hydro/umuscl.f90:714-856; the left state of face i is qm of cell  */
 /* i-1 (bounds shifted by one in the caller), the right state qp of cell i.  */
 /* ------------------------------------------------------------------------ */
+/* fluxes of a sampled state q(1:6) of riemann_approx / riemann_acoustic
+ * (godunov_utils.f90:461-491, 628-655); q[5] is the specific internal energy */
+static void flux_of_state(const orc_params *p, const double *q, double *fg) {
+  const double entho = one / (p->gamma - one);
+  fg[0] = q[0] * q[1];
+  fg[1] = q[2] + q[0] * (q[1] * q[1]);
+  double etot = q[2] * entho + half * q[0] * (q[1] * q[1]);
+  etot = etot + half * q[0] * (q[3] * q[3]);
+  etot = etot + half * q[0] * (q[4] * q[4]);
+  fg[2] = q[1] * (etot + q[2]);
+  fg[3] = fg[0] * q[3];
+  fg[4] = fg[0] * q[4];
+  fg[5] = fg[0] * q[5];
+}
+
+/* riemann_acoustic: godunov_utils.f90:500-655 */
+static void riemann_acoustic(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  const double gamma = p->gamma, smallp = p->smallc * p->smallc / gamma, entho = one / (gamma - one);
+  double rl = fmaxd(ql[0], p->smallr), ul = ql[1], pl = fmaxd(ql[2], rl * smallp);
+  double rr = fmaxd(qr[0], p->smallr), ur = qr[1], pr = fmaxd(qr[2], rr * smallp);
+  double cl = sqrt(gamma * pl / rl), cr = sqrt(gamma * pr / rr);
+  double wl = cl * rl, wr = cr * rr;
+  double pstar = ((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr);
+  double ustar = ((wr * ur + wl * ul) + (pl - pr)) / (wl + wr);
+  double sgnm = copysign(one, ustar);
+  double ro, uo, po, co;
+  if (sgnm == one) { ro = rl; uo = ul; po = pl; co = cl; }
+  else { ro = rr; uo = ur; po = pr; co = cr; }
+  double rstar = ro + (pstar - po) / (co * co);
+  rstar = fmaxd(rstar, p->smallr);
+  double cstar = sqrt(fabs(gamma * pstar / rstar));
+  cstar = fmaxd(cstar, p->smallc);
+  double spout = co - sgnm * uo;
+  double spin = cstar - sgnm * ustar;
+  double ushock = half * (spin + spout);
+  ushock = fmaxd(ushock, -sgnm * ustar);
+  if (pstar >= po) { spout = ushock; spin = spout; }
+  double q[6];
+  if (spout < zero) { q[0] = ro; q[1] = uo; q[2] = po; }
+  else if (spin >= zero) { q[0] = rstar; q[1] = ustar; q[2] = pstar; }
+  else {
+    double frac = spout / (spout - spin);
+    q[0] = frac * rstar + (one - frac) * ro;
+    q[1] = frac * ustar + (one - frac) * uo;
+    q[2] = frac * pstar + (one - frac) * po;
+  }
+  q[3] = sgnm == one ? ql[3] : qr[3];
+  q[4] = sgnm == one ? ql[4] : qr[4];
+  q[5] = po / ro * entho;
+  flux_of_state(p, q, fg);
+}
+
+/* riemann_approx ('exact'): godunov_utils.f90:268-495; the vector loop's
+ * active-set bookkeeping stops each face's Newton iterations once
+ * |dp/(p+smallr*smallp)| <= 1e-6 */
+static void riemann_exact(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  const double gamma = p->gamma, smallp = p->smallc * p->smallc / gamma;
+  const double smallpp = p->smallr * smallp, gamma6 = (gamma + one) / (two * gamma), entho = one / (gamma - one);
+  double rl = fmaxd(ql[0], p->smallr), ul = ql[1], pl = fmaxd(ql[2], rl * smallp);
+  double rr = fmaxd(qr[0], p->smallr), ur = qr[1], pr = fmaxd(qr[2], rr * smallp);
+  double cl = gamma * pl * rl, cr = gamma * pr * rr;
+  double wl = sqrt(cl), wr = sqrt(cr);
+  double pstar = ((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr);
+  pstar = fmaxd(pstar, 0.0);
+  double pold = pstar;
+  for (int iter = 1; iter <= p->niter_riemann; iter++) {
+    double wwl = sqrt(cl * (one + gamma6 * (pold - pl) / pl));
+    double wwr = sqrt(cr * (one + gamma6 * (pold - pr) / pr));
+    double qlw = two * (wwl * wwl * wwl) / (wwl * wwl + cl);
+    double qrw = two * (wwr * wwr * wwr) / (wwr * wwr + cr);
+    double usl = ul - (pold - pl) / wwl;
+    double usr = ur + (pold - pr) / wwr;
+    double delp = fmaxd(qrw * qlw / (qrw + qlw) * (usl - usr), -pold);
+    pold = pold + delp;
+    double uo = fabs(delp / (pold + smallpp));
+    if (!(uo > 1e-06)) break;
+  }
+  pstar = pold;
+  wl = sqrt(cl * (one + gamma6 * (pstar - pl) / pl));
+  wr = sqrt(cr * (one + gamma6 * (pstar - pr) / pr));
+  double ustar = half * (ul + (pl - pstar) / wl + ur - (pr - pstar) / wr);
+  double sgnm = copysign(one, ustar);
+  double ro, uo, po, wo;
+  if (sgnm == one) { ro = rl; uo = ul; po = pl; wo = wl; }
+  else { ro = rr; uo = ur; po = pr; wo = wr; }
+  double co = fmaxd(p->smallc, sqrt(fabs(gamma * po / ro)));
+  double rstar;
+  if (pstar >= po) rstar = ro / (one + ro * (po - pstar) / (wo * wo));
+  else rstar = ro * pow(pstar / po, one / gamma);
+  rstar = fmaxd(rstar, p->smallr);
+  double cstar = sqrt(fabs(gamma * pstar / rstar));
+  cstar = fmaxd(cstar, p->smallc);
+  double spout = co - sgnm * uo;
+  double spin = cstar - sgnm * ustar;
+  double ushock = wo / ro - sgnm * uo;
+  if (pstar >= po) { spout = ushock; spin = spout; }
+  double q[6];
+  if (spout <= zero) { q[0] = ro; q[1] = uo; q[2] = po; }
+  else if (spin >= zero) { q[0] = rstar; q[1] = ustar; q[2] = pstar; }
+  else {
+    double frac = spout / (spout - spin);
+    q[1] = frac * ustar + (one - frac) * uo;
+    q[2] = frac * pstar + (one - frac) * po;
+    q[0] = ro * pow(q[2] / po, one / gamma);
+  }
+  q[3] = sgnm == one ? ql[3] : qr[3];
+  q[4] = sgnm == one ? ql[4] : qr[4];
+  q[5] = po / ro * entho;
+  flux_of_state(p, q, fg);
+}
+
 static int cmpflxm(const orc_params *p, const double *qm, const double *qp, int idim,
                    int ilo, int ihi, int jlo, int jhi, int klo, int khi, double *fx,
                    double *tx, int ngrid, int nv) {
@@ -410,6 +521,8 @@ static int cmpflxm(const orc_params *p, const double *qm, const double *qp, int 
           if (p->riemann == ORC_RIEMANN_LLF) riemann_llf(p, ql, qr, fg);
           else if (p->riemann == ORC_RIEMANN_HLLC) riemann_hllc(p, ql, qr, fg);
           else if (p->riemann == ORC_RIEMANN_HLL) riemann_hll(p, ql, qr, fg);
+          else if (p->riemann == ORC_RIEMANN_ACOUSTIC) riemann_acoustic(p, ql, qr, fg);
+          else if (p->riemann == ORC_RIEMANN_EXACT) riemann_exact(p, ql, qr, fg);
           else return -1; /* :801-803 unknown Riemann solver */
           fx[QI(nv, l, i, j, k, 1)] = fg[0];
           fx[QI(nv, l, i, j, k, ln)] = fg[1];

@@ -26,7 +26,7 @@
 #define ORC_NVAR 5
 #define ORC_MAXLEVEL 32
 
-enum { ORC_RIEMANN_LLF = 1, ORC_RIEMANN_HLL = 2, ORC_RIEMANN_HLLC = 3 };
+enum { ORC_RIEMANN_LLF = 1, ORC_RIEMANN_HLL = 2, ORC_RIEMANN_HLLC = 3, ORC_RIEMANN_ACOUSTIC = 4, ORC_RIEMANN_EXACT = 5 };
 
 typedef struct orc_params {
   double gamma, smallr, smallc, courant_factor, slope_theta;
@@ -36,6 +36,7 @@ typedef struct orc_params {
   int32_t interpol_type; /* 0..4 */
   int32_t pressure_fix;  /* dual-energy fix: enew/divu tracked, set_uold repairs E */
   double beta_fix;       /* pressure-fix threshold (amr/amr_parameters.f90:167) */
+  int32_t niter_riemann; /* Newton iterations of riemann_approx (hydro_parameters.f90:75) */
 } orc_params;
 
 /* &REFINE_PARAMS gradient criterion (hydro/hydro_parameters.f90:47-52) */

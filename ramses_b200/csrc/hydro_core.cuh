@@ -29,7 +29,7 @@ template <typename R> struct Prim { R r, u, v, w, p; };
 // Hydro constants in compute precision.
 template <typename R> struct Consts {
   R gamma, smallr, smallc, smallp, entho, half, slope_theta, courant;
-  int slope_type, riemann;
+  int slope_type, riemann, niter_riemann;
 };
 
 template <typename R>
@@ -46,6 +46,7 @@ __device__ __forceinline__ Consts<R> make_consts(const rb_hydro_params& hp) {
   c.courant = (R)hp.courant_factor;
   c.slope_type = hp.slope_type;
   c.riemann = hp.riemann;
+  c.niter_riemann = hp.niter_riemann;
   return c;
 }
 
@@ -412,10 +413,124 @@ __device__ __forceinline__ void riemann_hllc(const R ql[5], const R qr[5], const
   f[5] = uo * eo;
 }
 
+// Fluxes of the sampled face state q = (rho, u_n, P, u_t1, u_t2, e) of the
+// acoustic and exact solvers (godunov_utils.f90:461-491, 628-655).
+template <typename R>
+__device__ __forceinline__ void flux_of_state(const R q[6], const Consts<R>& c, R f[6]) {
+  const R half = c.half;
+  f[0] = q[0] * q[1];
+  f[1] = q[2] + q[0] * (q[1] * q[1]);
+  R etot = q[2] * c.entho + half * q[0] * (q[1] * q[1]);
+  etot = etot + half * q[0] * (q[3] * q[3]);
+  etot = etot + half * q[0] * (q[4] * q[4]);
+  f[2] = q[1] * (etot + q[2]);
+  f[3] = f[0] * q[3];
+  f[4] = f[0] * q[4];
+  f[5] = f[0] * q[5];
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann_acoustic(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  // :500-655, linearised (acoustic) star state
+  const R one = (R)1, half = c.half, zero = (R)0;
+  const R rl = fmx(ql[0], c.smallr), ul = ql[1], pl = fmx(ql[2], rl * c.smallp);
+  const R rr = fmx(qr[0], c.smallr), ur = qr[1], pr = fmx(qr[2], rr * c.smallp);
+  const R cl = sqrt(c.gamma * pl / rl), cr = sqrt(c.gamma * pr / rr);
+  const R wl = cl * rl, wr = cr * rr;
+  const R pstar = ((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr);
+  const R ustar = ((wr * ur + wl * ul) + (pl - pr)) / (wl + wr);
+  const R sgnm = copysign(one, ustar);
+  const bool left = sgnm == one;
+  const R ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr, co = left ? cl : cr;
+  R rstar = ro + (pstar - po) / (co * co);
+  rstar = fmx(rstar, c.smallr);
+  R cstar = sqrt(fabs(c.gamma * pstar / rstar));
+  cstar = fmx(cstar, c.smallc);
+  R spout = co - sgnm * uo;
+  R spin = cstar - sgnm * ustar;
+  R ushock = half * (spin + spout);
+  ushock = fmx(ushock, -sgnm * ustar);
+  if (pstar >= po) { spout = ushock; spin = spout; }
+  R q[6];
+  if (spout < zero) { q[0] = ro; q[1] = uo; q[2] = po; }
+  else if (spin >= zero) { q[0] = rstar; q[1] = ustar; q[2] = pstar; }
+  else {
+    const R frac = spout / (spout - spin);
+    q[0] = frac * rstar + (one - frac) * ro;
+    q[1] = frac * ustar + (one - frac) * uo;
+    q[2] = frac * pstar + (one - frac) * po;
+  }
+  q[3] = left ? ql[3] : qr[3];
+  q[4] = left ? ql[4] : qr[4];
+  q[5] = po / ro * c.entho;
+  flux_of_state(q, c, f);
+}
+
+template <typename R>
+__device__ __forceinline__ void riemann_exact(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
+  // riemann_approx :268-495: two-shock Newton iterations for the star
+  // pressure (at most niter_riemann, until |dp/p| <= 1e-6), then the exact
+  // sampling with rarefaction fans
+  const R one = (R)1, two = (R)2, half = c.half, zero = (R)0;
+  const R smallpp = c.smallr * c.smallp;
+  const R gamma6 = (c.gamma + one) / (two * c.gamma);
+  const R rl = fmx(ql[0], c.smallr), ul = ql[1], pl = fmx(ql[2], rl * c.smallp);
+  const R rr = fmx(qr[0], c.smallr), ur = qr[1], pr = fmx(qr[2], rr * c.smallp);
+  const R cl = c.gamma * pl * rl, cr = c.gamma * pr * rr;
+  R wl = sqrt(cl), wr = sqrt(cr);
+  R pstar = ((wr * pl + wl * pr) + wl * wr * (ul - ur)) / (wl + wr);
+  pstar = fmx(pstar, zero);
+  R pold = pstar;
+  for (int iter = 1; iter <= c.niter_riemann; iter++) {
+    const R wwl = sqrt(cl * (one + gamma6 * (pold - pl) / pl));
+    const R wwr = sqrt(cr * (one + gamma6 * (pold - pr) / pr));
+    const R qlw = two * (wwl * wwl * wwl) / (wwl * wwl + cl);
+    const R qrw = two * (wwr * wwr * wwr) / (wwr * wwr + cr);
+    const R usl = ul - (pold - pl) / wwl;
+    const R usr = ur + (pold - pr) / wwr;
+    const R delp = fmx(qrw * qlw / (qrw + qlw) * (usl - usr), -pold);
+    pold = pold + delp;
+    if (!(fabs(delp / (pold + smallpp)) > (R)1e-06)) break;  // converged
+  }
+  pstar = pold;
+  wl = sqrt(cl * (one + gamma6 * (pstar - pl) / pl));
+  wr = sqrt(cr * (one + gamma6 * (pstar - pr) / pr));
+  const R ustar = half * (ul + (pl - pstar) / wl + ur - (pr - pstar) / wr);
+  const R sgnm = copysign(one, ustar);
+  const bool left = sgnm == one;
+  const R ro = left ? rl : rr, uo = left ? ul : ur, po = left ? pl : pr, wo = left ? wl : wr;
+  const R co = fmx(c.smallc, (R)sqrt(fabs(c.gamma * po / ro)));
+  R rstar;
+  if (pstar >= po) rstar = ro / (one + ro * (po - pstar) / (wo * wo));
+  else rstar = ro * pow(pstar / po, one / c.gamma);
+  rstar = fmx(rstar, c.smallr);
+  R cstar = sqrt(fabs(c.gamma * pstar / rstar));
+  cstar = fmx(cstar, c.smallc);
+  R spout = co - sgnm * uo;
+  R spin = cstar - sgnm * ustar;
+  const R ushock = wo / ro - sgnm * uo;
+  if (pstar >= po) { spout = ushock; spin = spout; }
+  R q[6];
+  if (spout <= zero) { q[0] = ro; q[1] = uo; q[2] = po; }
+  else if (spin >= zero) { q[0] = rstar; q[1] = ustar; q[2] = pstar; }
+  else {
+    const R frac = spout / (spout - spin);
+    q[1] = frac * ustar + (one - frac) * uo;
+    q[2] = frac * pstar + (one - frac) * po;
+    q[0] = ro * pow(q[2] / po, one / c.gamma);
+  }
+  q[3] = left ? ql[3] : qr[3];
+  q[4] = left ? ql[4] : qr[4];
+  q[5] = po / ro * c.entho;
+  flux_of_state(q, c, f);
+}
+
 template <typename R>
 __device__ __forceinline__ void riemann(const R ql[5], const R qr[5], const Consts<R>& c, R f[6]) {
   if (c.riemann == RB_RIEMANN_HLLC) riemann_hllc(ql, qr, c, f);
   else if (c.riemann == RB_RIEMANN_HLL) riemann_hll(ql, qr, c, f);
+  else if (c.riemann == RB_RIEMANN_ACOUSTIC) riemann_acoustic(ql, qr, c, f);
+  else if (c.riemann == RB_RIEMANN_EXACT) riemann_exact(ql, qr, c, f);
   else riemann_llf(ql, qr, c, f);
 }
 

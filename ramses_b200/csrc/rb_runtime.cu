@@ -26,8 +26,11 @@ int h2d(rb_context* c, void* dst, const void* src, size_t bytes) {
 
 int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
   if (!hp || !mp) return fail(RB_ERR_INVALID, "null parameter struct");
-  if (hp->riemann != RB_RIEMANN_LLF && hp->riemann != RB_RIEMANN_HLL && hp->riemann != RB_RIEMANN_HLLC)
-    return fail(RB_ERR_INVALID, "unknown Riemann solver code %d (llf=1, hll=2, hllc=3)", hp->riemann);
+  if (hp->riemann < RB_RIEMANN_LLF || hp->riemann > RB_RIEMANN_EXACT)
+    return fail(RB_ERR_INVALID, "unknown Riemann solver code %d (llf=1, hll=2, hllc=3, acoustic=4, exact=5)",
+                hp->riemann);
+  if (hp->riemann == RB_RIEMANN_EXACT && hp->niter_riemann < 1)
+    return fail(RB_ERR_INVALID, "niter_riemann=%d must be >= 1 for the exact Riemann solver", hp->niter_riemann);
   const int st = hp->slope_type;
   if (!(st == 0 || st == 1 || st == 2 || st == 3 || st == 7 || st == 8))
     return fail(RB_ERR_INVALID, "Unknown slope type %d", st);

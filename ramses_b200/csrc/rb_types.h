@@ -8,7 +8,7 @@
 #define RB_NVAR 5
 #define RB_MAXLEVEL 32
 
-enum { RB_RIEMANN_LLF = 1, RB_RIEMANN_HLL = 2, RB_RIEMANN_HLLC = 3 };
+enum { RB_RIEMANN_LLF = 1, RB_RIEMANN_HLL = 2, RB_RIEMANN_HLLC = 3, RB_RIEMANN_ACOUSTIC = 4, RB_RIEMANN_EXACT = 5 };
 enum { RB_PREC_FP64 = 0, RB_PREC_MIXED = 1 };
 
 /* Status codes returned by every C-ABI entry point (0 = success). */
@@ -32,7 +32,7 @@ typedef struct rb_hydro_params {
   double smallc;
   double courant_factor;
   double slope_theta;
-  int32_t riemann;       /* RB_RIEMANN_*; 'exact'/'acoustic' are rejected  */
+  int32_t riemann;       /* RB_RIEMANN_*                                    */
   int32_t slope_type;    /* 0,1,2,3,7,8                                    */
   int32_t scheme;        /* 0 = 'muscl' ('plmde' is rejected)              */
   int32_t interpol_var;  /* 0,1,2                                          */
@@ -41,6 +41,8 @@ typedef struct rb_hydro_params {
                          /*    repairs E where E - ekin is too small)       */
   double difmag;         /* must be 0                                      */
   double beta_fix;       /* pressure-fix threshold, >= 0 (default 0)       */
+  int32_t niter_riemann; /* Newton iterations of the 'exact' solver (10)    */
+  int32_t pad_;          /* zero                                            */
 } rb_hydro_params;
 
 /* Gradient refinement criterion of &REFINE_PARAMS

@@ -13,7 +13,7 @@ import dataclasses
 import re
 from typing import Dict, List
 
-RIEMANN_CODES = {"llf": 1, "hll": 2, "hllc": 3}
+RIEMANN_CODES = {"llf": 1, "hll": 2, "hllc": 3, "acoustic": 4, "exact": 5}
 SLOPE_TYPES = (0, 1, 2, 3, 7, 8)
 
 
@@ -32,13 +32,14 @@ class HydroParams:
     pressure_fix: bool = False
     difmag: float = 0.0
     beta_fix: float = 0.0
+    niter_riemann: int = 10
 
     @property
     def riemann_code(self) -> int:
         try:
             return RIEMANN_CODES[self.riemann.strip().lower()]
         except KeyError:
-            raise ValueError("unknown Riemann solver %r (supported: llf, hll, hllc)" % self.riemann)
+            raise ValueError("unknown Riemann solver %r (supported: llf, hll, hllc, acoustic, exact)" % self.riemann)
 
     def validate(self) -> None:
         self.riemann_code  # noqa: B018 - raises on unknown solver
@@ -50,6 +51,8 @@ class HydroParams:
             raise ValueError("difmag>0 is not supported")
         if not (self.beta_fix >= 0.0) or self.beta_fix == float("inf"):
             raise ValueError("beta_fix must be finite and >= 0")
+        if self.riemann_code == 5 and self.niter_riemann < 1:
+            raise ValueError("niter_riemann must be >= 1 for the exact Riemann solver")
         if self.interpol_var not in (0, 1, 2) or self.interpol_type not in (0, 1, 2, 3, 4):
             raise ValueError("bad interpol_var/interpol_type")
         if self.interpol_type == 4 and self.interpol_var != 2:

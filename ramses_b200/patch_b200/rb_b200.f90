@@ -18,6 +18,7 @@ module rb_b200
      real(c_double) :: gamma, smallr, smallc, courant_factor, slope_theta
      integer(c_int32_t) :: riemann, slope_type, scheme, interpol_var, interpol_type, pressure_fix
      real(c_double) :: difmag, beta_fix
+     integer(c_int32_t) :: niter_riemann, pad_
   end type rb_hydro_params_t
 
   type, bind(c) :: rb_mesh_params_t
@@ -128,12 +129,15 @@ contains
     hp%slope_type = slope_type; hp%scheme = 0; hp%pressure_fix = 0
     hp%interpol_var = interpol_var; hp%interpol_type = interpol_type; hp%difmag = difmag
     hp%beta_fix = beta_fix
+    hp%niter_riemann = niter_riemann; hp%pad_ = 0
     if (scheme /= 'muscl') hp%scheme = 1
     if (pressure_fix) hp%pressure_fix = 1
     hp%riemann = 0
     if (riemann == 'llf') hp%riemann = 1
     if (riemann == 'hll') hp%riemann = 2
     if (riemann == 'hllc') hp%riemann = 3
+    if (riemann == 'acoustic') hp%riemann = 4
+    if (riemann == 'exact') hp%riemann = 5
     mp%nx = nx; mp%ny = ny; mp%nz = nz; mp%ncoarse = ncoarse; mp%ngridmax = ngridmax
     mp%nlevelmax = nlevelmax; mp%levelmin = levelmin; mp%nvector = nvector
     mp%boxlen = boxlen

@@ -35,7 +35,7 @@ class HydroParamsC(ctypes.Structure):
                 ("riemann", ctypes.c_int32), ("slope_type", ctypes.c_int32), ("scheme", ctypes.c_int32),
                 ("interpol_var", ctypes.c_int32), ("interpol_type", ctypes.c_int32),
                 ("pressure_fix", ctypes.c_int32), ("difmag", ctypes.c_double),
-                ("beta_fix", ctypes.c_double)]
+                ("beta_fix", ctypes.c_double), ("niter_riemann", ctypes.c_int32), ("pad_", ctypes.c_int32)]
 
 
 class RefineParamsC(ctypes.Structure):
@@ -149,7 +149,7 @@ def hydro_params_c(hp: HydroParams) -> HydroParamsC:
     hp.validate()
     return HydroParamsC(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta, hp.riemann_code,
                         hp.slope_type, 0, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix), hp.difmag,
-                        hp.beta_fix)
+                        hp.beta_fix, hp.niter_riemann, 0)
 
 
 def mesh_params_c(tree: Octree, nsubcycle: Optional[Sequence[int]] = None, nvector: int = 32) -> MeshParamsC:

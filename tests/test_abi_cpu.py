@@ -66,7 +66,11 @@ def test_no_device_reported(lib):
 
 def test_python_params_validation():
     with pytest.raises(ValueError):
-        HydroParams(riemann="exact").validate()
+        HydroParams(riemann="roe").validate()
+    HydroParams(riemann="exact").validate()
+    HydroParams(riemann="acoustic").validate()
+    with pytest.raises(ValueError):
+        HydroParams(riemann="exact", niter_riemann=0).validate()
     with pytest.raises(ValueError):
         HydroParams(slope_type=4).validate()
     with pytest.raises(ValueError):
