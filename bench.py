@@ -312,6 +312,15 @@ def run_amr(args):
     out, states = {}, {}
     for prec in ([args.only] if args.only else ["mixed", "fp64"]):
         s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
+        # the cost of a remeshing round trip through the drop-in boundary: a
+        # full tree re-sync (tables rebuilt on the host) and a state upload
+        t0s = time.perf_counter()
+        s.sync_tree()
+        s.synchronize()
+        t1s = time.perf_counter()
+        s.upload_state(u)
+        s.synchronize()
+        sync = {"sync_tree_s": t1s - t0s, "upload_state_s": time.perf_counter() - t1s}
         for l in levels:
             s.set_tile_shape(l, args.tile_shape)  # -1: autotuned per level
         s.run(max_steps=args.warmup)
@@ -324,7 +333,8 @@ def run_amr(args):
         ms = s.last_run_ms()
         upd = s.cell_updates - before
         out[prec] = {"value": upd / (ms / 1e3), "ms_per_coarse_step": ms / max(n, 1), "coarse_steps": n,
-                     "t": s.t, "tile_shapes": {l: s.tile_shape(l) for l in levels}, "clocks": clk.summary()}
+                     "t": s.t, "tile_shapes": {l: s.tile_shape(l) for l in levels}, "clocks": clk.summary(),
+                     "remesh_round_trip": sync}
         if prec == "mixed" or args.only:
             # hydro_flag on every level but the finest, on the final state
             # (density and pressure gradients of 0.1): the refinement flags

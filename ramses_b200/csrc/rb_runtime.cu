@@ -268,12 +268,26 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   for (int t = 0; t < L.ntile; t++) {
     const int64_t ox0 = tiles[t].second[0] * TOX, oy0 = tiles[t].second[1] * TOY, oz0 = tiles[t].second[2] * TOZ;
     int32_t* B = &blk[(size_t)t * NBLK];
+    const bool x_inside = ox0 - 1 >= 0 && ox0 - 1 + BX <= I.nx;
     for (int bz = 0; bz < BZ; bz++)
-      for (int by = 0; by < BY; by++)
-        for (int bx = 0; bx < BX; bx++) {
-          const int32_t g = I.find(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
-          B[bx + BX * (by + BY * bz)] = g > 0 ? g - 1 : -1;
+      for (int by = 0; by < BY; by++) {
+        int32_t* row = B + BX * (by + BY * bz);
+        if (x_inside) {
+          // one search per row of blocks: the row's positions are
+          // consecutive keys, so its octs follow each other in I.v
+          const int64_t k0 = I.key(ox0 - 1, oy0 - 1 + by, oz0 - 1 + bz);
+          auto it = std::lower_bound(I.v.begin(), I.v.end(), std::make_pair(k0, (int32_t)INT32_MIN));
+          for (int bx = 0; bx < BX; bx++) {
+            while (it != I.v.end() && it->first < k0 + bx) ++it;
+            row[bx] = (it != I.v.end() && it->first == k0 + bx) ? it->second - 1 : -1;
+          }
+        } else {
+          for (int bx = 0; bx < BX; bx++) {
+            const int32_t g = I.find(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
+            row[bx] = g > 0 ? g - 1 : -1;
+          }
         }
+      }
     for (int z = 0; z < TOZ; z++)
       for (int y = 0; y < TOY; y++)
         for (int x = 0; x < TOX; x++) inner[x + TOX * (y + TOY * z)] = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))] >= 0;
