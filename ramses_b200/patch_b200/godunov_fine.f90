@@ -34,10 +34,12 @@ subroutine set_uold(ilevel)
   implicit none
   integer::ilevel
   if(numbtot(1,ilevel)==0)return
-  if(poisson .or. pressure_fix .or. nener>0)then
-     write(*,*)'rb_b200: gravity and pdV source terms are not supported'
+  if(poisson .or. nener>0)then
+     write(*,*)'rb_b200: gravity and non-thermal energy source terms are not supported'
      call clean_stop
   end if
+  ! with pressure_fix, rb_set_uold adds the pdV term to enew and repairs the
+  ! total energy on the device (add_pdv_source_terms and the fix of set_uold)
   call rb_b200_check(rb_set_uold(rb_ctx, int(ilevel, c_int)), 'set_uold')
   ! restriction to the coarser level on the device; the host's own
   ! upload_fine, called next by amr_step, recomputes the same values
@@ -55,6 +57,6 @@ end subroutine add_gravity_source_terms
 subroutine add_pdv_source_terms(ilevel)
   implicit none
   integer::ilevel
-  write(*,*)'rb_b200: add_pdv_source_terms is not supported', ilevel
+  write(*,*)'rb_b200: add_pdv_source_terms runs inside rb_set_uold', ilevel
   call clean_stop
 end subroutine add_pdv_source_terms
