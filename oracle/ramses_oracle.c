@@ -558,6 +558,75 @@ static void work_free(work *w) {
 }
 
 /* unsplit: hydro/umuscl.f90:22-171 (scheme='muscl', difmag=0) */
+/* cmpdivu (hydro/uplmde.f90:702-764, NDIM=3): velocity divergence at the
+ * cell corners (i-1/2, j-1/2, k-1/2), i,j,k = 1..3, from the primitive
+ * velocities; div[l + nv*((i-1) + 3*((j-1) + 3*(k-1)))] */
+static void cmpdivu(const double *q, double *div, double dx, double dy, double dz, int ngrid, int nv) {
+  const double factorx = half * half / dx, factory = half * half / dy, factorz = half * half / dz;
+#define QV(i, j, k, v) q[QI(nv, l, i, j, k, v)]
+  for (int k = 1; k <= 3; k++)
+    for (int j = 1; j <= 3; j++)
+      for (int i = 1; i <= 3; i++)
+        for (int l = 0; l < ngrid; l++) {
+          double ux = zero, vy = zero, wz = zero;
+          ux = ux + factorx * (QV(i, j, k, 2) - QV(i - 1, j, k, 2));
+          ux = ux + factorx * (QV(i, j - 1, k, 2) - QV(i - 1, j - 1, k, 2));
+          vy = vy + factory * (QV(i, j, k, 3) - QV(i, j - 1, k, 3) + QV(i - 1, j, k, 3) - QV(i - 1, j - 1, k, 3));
+          ux = ux + factorx * (QV(i, j, k - 1, 2) - QV(i - 1, j, k - 1, 2) + QV(i, j - 1, k - 1, 2) -
+                               QV(i - 1, j - 1, k - 1, 2));
+          vy = vy + factory * (QV(i, j, k - 1, 3) - QV(i, j - 1, k - 1, 3) + QV(i - 1, j, k - 1, 3) -
+                               QV(i - 1, j - 1, k - 1, 3));
+          wz = wz + factorz * (QV(i, j, k, 4) - QV(i, j, k - 1, 4) + QV(i, j - 1, k, 4) - QV(i, j - 1, k - 1, 4) +
+                               QV(i - 1, j, k, 4) - QV(i - 1, j, k - 1, 4) + QV(i - 1, j - 1, k, 4) -
+                               QV(i - 1, j - 1, k - 1, 4));
+          div[(size_t)l + (size_t)nv * ((size_t)(i - 1) + 3u * ((size_t)(j - 1) + 3u * (size_t)(k - 1)))] = ux + vy + wz;
+        }
+#undef QV
+}
+
+/* consup (hydro/uplmde.f90:769-866, NDIM=3): diffusive flux
+ * dt*difmag*min(0, div1)*(u_i - u_{i-1}) where the flow converges, div1 the
+ * mean of the face's four corner divergences */
+static void consup(const orc_params *p, const double *uin, double *flux, const double *div, double dt,
+                   int ngrid, int nv) {
+  const double factor = half * half;
+#define DV(i, j, k) div[(size_t)l + (size_t)nv * ((size_t)((i) - 1) + 3u * ((size_t)((j) - 1) + 3u * (size_t)((k) - 1)))]
+  for (int n = 1; n <= NV; n++) {
+    for (int k = 1; k <= 2; k++)
+      for (int j = 1; j <= 2; j++)
+        for (int i = 1; i <= 3; i++)
+          for (int l = 0; l < ngrid; l++) {
+            double div1 = factor * DV(i, j, k);
+            div1 = div1 + factor * DV(i, j + 1, k);
+            div1 = div1 + factor * (DV(i, j, k + 1) + DV(i, j + 1, k + 1));
+            div1 = p->difmag * fmind(zero, div1);
+            flux[FI(nv, l, i, j, k, n, 1)] = flux[FI(nv, l, i, j, k, n, 1)] +
+                                             dt * div1 * (uin[QI(nv, l, i, j, k, n)] - uin[QI(nv, l, i - 1, j, k, n)]);
+          }
+    for (int k = 1; k <= 2; k++)
+      for (int j = 1; j <= 3; j++)
+        for (int i = 1; i <= 2; i++)
+          for (int l = 0; l < ngrid; l++) {
+            double div1 = zero;
+            div1 = div1 + factor * (DV(i, j, k) + DV(i + 1, j, k));
+            div1 = div1 + factor * (DV(i, j, k + 1) + DV(i + 1, j, k + 1));
+            div1 = p->difmag * fmind(zero, div1);
+            flux[FI(nv, l, i, j, k, n, 2)] = flux[FI(nv, l, i, j, k, n, 2)] +
+                                             dt * div1 * (uin[QI(nv, l, i, j, k, n)] - uin[QI(nv, l, i, j - 1, k, n)]);
+          }
+    for (int k = 1; k <= 3; k++)
+      for (int j = 1; j <= 2; j++)
+        for (int i = 1; i <= 2; i++)
+          for (int l = 0; l < ngrid; l++) {
+            double div1 = factor * (DV(i, j, k) + DV(i + 1, j, k) + DV(i, j + 1, k) + DV(i + 1, j + 1, k));
+            div1 = p->difmag * fmind(zero, div1);
+            flux[FI(nv, l, i, j, k, n, 3)] = flux[FI(nv, l, i, j, k, n, 3)] +
+                                             dt * div1 * (uin[QI(nv, l, i, j, k, n)] - uin[QI(nv, l, i, j, k - 1, n)]);
+          }
+  }
+#undef DV
+}
+
 static int unsplit_w(const orc_params *p, work *w, const double *uin, const double *gravin,
                      double *flux, double *tmp, double dx, double dy, double dz, double dt,
                      int ngrid) {
@@ -586,6 +655,13 @@ static int unsplit_w(const orc_params *p, work *w, const double *uin, const doub
               tmp[TI(nv, l, i, j, k, ivar, idim)] =
                   w->tx[S6(nv, l, i, j, k) + ST(nv) * (size_t)(ivar - 1)] * dt / dd_;
         }
+  }
+  if (p->difmag > 0.0) { /* umuscl.f90:166-169 */
+    double *div = (double *)malloc(sizeof(double) * (size_t)nv * 27);
+    if (!div) return -4;
+    cmpdivu(w->qin, div, dx, dy, dz, ngrid, nv);
+    consup(p, uin, flux, div, dt, ngrid, nv);
+    free(div);
   }
   return 0;
 }

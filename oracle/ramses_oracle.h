@@ -37,6 +37,7 @@ typedef struct orc_params {
   int32_t pressure_fix;  /* dual-energy fix: enew/divu tracked, set_uold repairs E */
   double beta_fix;       /* pressure-fix threshold (amr/amr_parameters.f90:167) */
   int32_t niter_riemann; /* Newton iterations of riemann_approx (hydro_parameters.f90:75) */
+  double difmag;         /* artificial diffusion where the flow converges (0: off) */
 } orc_params;
 
 /* &REFINE_PARAMS gradient criterion (hydro/hydro_parameters.f90:47-52) */

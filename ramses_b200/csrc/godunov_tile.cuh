@@ -167,9 +167,13 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   // ---- A. gather + ctoprim ------------------------------------------------
   const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
   const bool slope27 = (slope_type == 3);
+  // the 27-point slopes and the corner divergence of difmag read the edge and
+  // corner cells of the stencil too
+  const bool full_gather = slope27 || (RS == 0 && a.hp.difmag > 0.0);
   // one stencil cell: its raw state is loaded by gather_cell and converted by
-  // put_cell, so that the loads of several cells are in flight together.
-  // Blocks coded -1 are read by no present cell: only their flags are set.
+  // put_cell (the listed gather keeps the loads of two cells in flight
+  // before their conversion). Blocks coded -1 are read by no present cell:
+  // only their flags are set.
   auto gather_cell = [&](int b, int ch, double u[5], int& code, int& sonv, int& inner) -> int {
     const int bx = b % BX, by = (b / BX) % BY, bz = b / (BX * BY);
     const int sx = 2 * bx + (ch & 1), sy = 2 * by + ((ch >> 1) & 1), sz = 2 * bz + (ch >> 2);
@@ -203,7 +207,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
     q[3 * NS + s] = pq.w;
     q[4 * NS + s] = pq.p;
   };
-  if (!slope27) {
+  if (!full_gather) {
     using GL = GatherList<TX, TY, TZ>;
     constexpr int NG = GL::N;
     constexpr int PER = (NG + NT - 1) / NT;
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
         if (sidx[j] >= 0) put_cell(sidx[j], u[j], code[j], sonv[j], inner[j]);
     }
   } else {
-    // the 27-point slopes read every cell of the stencil
+    // every cell of the stencil
     for (int it = tid; it < NBLK * 8; it += NT) {
       double u[5];
       int code, sonv, inner;
@@ -335,9 +339,53 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       }
     }
   }
+  // difmag > 0 (run-time scheme variant): cmpdivu (uplmde.f90:702-764), the
+  // velocity divergence at the cell corners (x-1/2, y-1/2, z-1/2) of the tile,
+  // x in 0..TX etc., from the primitive velocities, before phase C reuses q
+  constexpr int CXN = TX + 1, CYN = TY + 1, NCORN = (TX + 1) * (TY + 1) * (TZ + 1);
+  R* cdiv = nullptr;
+  if constexpr (RS == 0) {
+    __shared__ R cdiv_s[NCORN];
+    cdiv = cdiv_s;
+    if (a.hp.difmag > 0.0) {
+      const R quarter = (R)0.5 * (R)0.5;
+      const R fxd = (R)(quarter / (R)a.dx), fyd = fxd, fzd = fxd;
+      for (int it = tid; it < NCORN; it += NT) {
+        const int x = it % CXN, y = (it / CXN) % CYN, z = it / (CXN * CYN);
+        auto Q = [&](int ox, int oy, int oz, int v) {
+          return q[v * NS + (x + ox + 2) + SX * ((y + oy + 2) + SY * (z + oz + 2))];
+        };
+        R ux = (R)0, vy = (R)0, wz = (R)0;
+        ux = ux + fxd * (Q(0, 0, 0, 1) - Q(-1, 0, 0, 1));
+        ux = ux + fxd * (Q(0, -1, 0, 1) - Q(-1, -1, 0, 1));
+        vy = vy + fyd * (Q(0, 0, 0, 2) - Q(0, -1, 0, 2) + Q(-1, 0, 0, 2) - Q(-1, -1, 0, 2));
+        ux = ux + fxd * (Q(0, 0, -1, 1) - Q(-1, 0, -1, 1) + Q(0, -1, -1, 1) - Q(-1, -1, -1, 1));
+        vy = vy + fyd * (Q(0, 0, -1, 2) - Q(0, -1, -1, 2) + Q(-1, 0, -1, 2) - Q(-1, -1, -1, 2));
+        wz = wz + fzd * (Q(0, 0, 0, 3) - Q(0, 0, -1, 3) + Q(0, -1, 0, 3) - Q(0, -1, -1, 3) + Q(-1, 0, 0, 3) -
+                         Q(-1, 0, -1, 3) + Q(-1, -1, 0, 3) - Q(-1, -1, -1, 3));
+        cdiv[it] = ux + vy + wz;
+      }
+    }
+  }
   __syncthreads();
 
   // ---- C. Riemann fluxes (flux buffer aliases q) ------------------------------
+  // raw (conservative) state of stencil cell s, as phase A gathered it
+  auto raw_cell = [&](int s, double u[5]) {
+    const int sx = s % SX, sy = (s / SX) % SY, sz = s / (SX * SY);
+    const int b = (sx >> 1) + BX * ((sy >> 1) + BY * (sz >> 1));
+    const int ch = (sx & 1) + 2 * (sy & 1) + 4 * (sz & 1);
+    const int code = blk[b];
+    if (code >= 0) {
+      const int64_t dc = (int64_t)a.ncoarse + (int64_t)code * 8 + ch;
+      for (int v = 0; v < 5; v++) u[v] = __ldcg(a.uold + v * ncell + dc);
+    } else if (code <= -2) {
+      const int64_t e = (int64_t)(-code - 2) * 8 + ch;
+      for (int v = 0; v < 5; v++) u[v] = __ldcg(a.interp + v * a.ninterp8 + e);
+    } else {
+      for (int v = 0; v < 5; v++) u[v] = 0.0;
+    }
+  };
   R* F = q;
   for (int f = tid; f < NF; f += NT) {
     int d, x, y, z;
@@ -369,8 +417,38 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       }
       return x * dtd[0];
     };
+    if (RS == 0 && a.hp.difmag > 0.0) {
+      // consup (uplmde.f90:769-866): + dt*difmag*min(0, div1)*(u_R - u_L)
+      // with div1 the mean of the face's four corner divergences, added
+      // before the refined-face zeroing
+      const R quarter = (R)0.5 * (R)0.5;
+      auto D = [&](int cx, int cy, int cz) { return cdiv[cx + CXN * (cy + CYN * cz)]; };
+      R div1;
+      if (d == 0) {
+        div1 = quarter * D(x, y, z);
+        div1 = div1 + quarter * D(x, y + 1, z);
+        div1 = div1 + quarter * (D(x, y, z + 1) + D(x, y + 1, z + 1));
+      } else if (d == 1) {
+        div1 = (R)0;
+        div1 = div1 + quarter * (D(x, y, z) + D(x + 1, y, z));
+        div1 = div1 + quarter * (D(x, y, z + 1) + D(x + 1, y, z + 1));
+      } else {
+        div1 = quarter * (D(x, y, z) + D(x + 1, y, z) + D(x, y + 1, z) + D(x + 1, y + 1, z));
+      }
+      div1 = (R)a.hp.difmag * fmn((R)0, div1);
+      double ul[5], ur[5];
+      raw_cell(sl, ul);
+      raw_cell(sr, ur);
 #pragma unroll
-    for (int v = 0; v < 5; v++) F[v * NF + f] = zero_face ? (R)0 : scaled(fo[v]);
+      for (int v = 0; v < 5; v++) {
+        const R t = sizeof(R) == 8 ? (R)((double)(dt * (double)div1) * (ur[v] - ul[v]))
+                                   : (R)(dt * (double)div1 * (ur[v] - ul[v]));
+        F[v * NF + f] = zero_face ? (R)0 : scaled(fo[v]) + t;
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 5; v++) F[v * NF + f] = zero_face ? (R)0 : scaled(fo[v]);
+    }
     if (PF) {
       // tmp: the face-normal velocity average and the internal-energy flux,
       // kept in this face's qm slots (read above, by this thread only)

@@ -737,6 +737,44 @@ static __global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double
     const int64_t base = (int64_t)l + nv * ((i - 1) + 3 * ((j - 1) + 3 * (k - 1)));
     const int64_t s3 = nv * 27;
     for (int v = 0; v < 5; v++) flux[base + s3 * (v + 5 * d)] = fo[v] * dt / ddd[d];
+    if (hp.difmag > 0.0) {
+      // consup (uplmde.f90:769-866): + dt*difmag*min(0, div1)*(u_i - u_{i-1}),
+      // div1 from the face's four corner divergences (cmpdivu, :702-764)
+      const double factorx = 0.5 * 0.5 / dx, factory = 0.5 * 0.5 / dy, factorz = 0.5 * 0.5 / dz;
+      auto Q = [&](int ii, int jj, int kk, int v) { return q[v][(ii + 1) + 6 * ((jj + 1) + 6 * (kk + 1))]; };
+      auto DV = [&](int ii, int jj, int kk) {  // corner (ii-1/2, jj-1/2, kk-1/2)
+        double ux = 0.0, vy = 0.0, wz = 0.0;
+        ux = ux + factorx * (Q(ii, jj, kk, 1) - Q(ii - 1, jj, kk, 1));
+        ux = ux + factorx * (Q(ii, jj - 1, kk, 1) - Q(ii - 1, jj - 1, kk, 1));
+        vy = vy + factory * (Q(ii, jj, kk, 2) - Q(ii, jj - 1, kk, 2) + Q(ii - 1, jj, kk, 2) - Q(ii - 1, jj - 1, kk, 2));
+        ux = ux + factorx * (Q(ii, jj, kk - 1, 1) - Q(ii - 1, jj, kk - 1, 1) + Q(ii, jj - 1, kk - 1, 1) -
+                             Q(ii - 1, jj - 1, kk - 1, 1));
+        vy = vy + factory * (Q(ii, jj, kk - 1, 2) - Q(ii, jj - 1, kk - 1, 2) + Q(ii - 1, jj, kk - 1, 2) -
+                             Q(ii - 1, jj - 1, kk - 1, 2));
+        wz = wz + factorz * (Q(ii, jj, kk, 3) - Q(ii, jj, kk - 1, 3) + Q(ii, jj - 1, kk, 3) - Q(ii, jj - 1, kk - 1, 3) +
+                             Q(ii - 1, jj, kk, 3) - Q(ii - 1, jj, kk - 1, 3) + Q(ii - 1, jj - 1, kk, 3) -
+                             Q(ii - 1, jj - 1, kk - 1, 3));
+        return ux + vy + wz;
+      };
+      const double factor = 0.5 * 0.5;
+      double div1;
+      if (d == 0) {
+        div1 = factor * DV(i, j, k);
+        div1 = div1 + factor * DV(i, j + 1, k);
+        div1 = div1 + factor * (DV(i, j, k + 1) + DV(i, j + 1, k + 1));
+      } else if (d == 1) {
+        div1 = 0.0;
+        div1 = div1 + factor * (DV(i, j, k) + DV(i + 1, j, k));
+        div1 = div1 + factor * (DV(i, j, k + 1) + DV(i + 1, j, k + 1));
+      } else {
+        div1 = factor * (DV(i, j, k) + DV(i + 1, j, k) + DV(i, j + 1, k) + DV(i + 1, j + 1, k));
+      }
+      div1 = hp.difmag * fmn(0.0, div1);
+      const int di = d == 0, dj = d == 1, dk = d == 2;
+      for (int v = 0; v < 5; v++)
+        flux[base + s3 * (v + 5 * d)] = flux[base + s3 * (v + 5 * d)] +
+                                        dt * div1 * (uin[S6(i, j, k) + st * v] - uin[S6(i - di, j - dj, k - dk) + st * v]);
+    }
     tmp[base + s3 * (0 + 2 * d)] = 0.5 * (ql[1] + qr[1]) * dt / ddd[d];
     tmp[base + s3 * (1 + 2 * d)] = fg[5] * dt / ddd[d];
   }

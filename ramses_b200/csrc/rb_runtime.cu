@@ -39,7 +39,8 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
     return fail(RB_ERR_INVALID, "pressure_fix must be 0 or 1 (got %d)", hp->pressure_fix);
   if (!(hp->beta_fix >= 0.0) || !std::isfinite(hp->beta_fix))
     return fail(RB_ERR_INVALID, "beta_fix=%g must be finite and >= 0", hp->beta_fix);
-  if (hp->difmag != 0.0) return fail(RB_ERR_INVALID, "difmag>0 is not supported");
+  if (!(hp->difmag >= 0.0) || !std::isfinite(hp->difmag))
+    return fail(RB_ERR_INVALID, "difmag=%g must be finite and >= 0", hp->difmag);
   if (hp->interpol_var < 0 || hp->interpol_var > 2 || hp->interpol_type < 0 || hp->interpol_type > 4)
     return fail(RB_ERR_INVALID, "bad interpol_var/interpol_type");
   if (hp->interpol_type == 4 && hp->interpol_var != 2)
@@ -1705,15 +1706,16 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
     return RB_OK;
   }
   // the multi-dimensional limiter (slope_type 3) reads the 26 neighbours of
-  // every cell, which the z-streaming kernel does not hold: oct tiles only
-  if (c->uniform_method == 0 && c->hp.slope_type != 3)
+  // every cell, and the artificial diffusion (difmag) the cell corners, which
+  // the z-streaming kernel does not hold: oct tiles only
+  if (c->uniform_method == 0 && c->hp.slope_type != 3 && c->hp.difmag == 0.0)
     return uniform_run_dense(c, nsteps, use_graph, t_io, dt_last_out);
   return uniform_run_tiles(c, nsteps, use_graph, t_io, dt_last_out);
 }
 
 int rb_get_uniform_info(rb_context* c, int* method, int* shape, int* hz, int* items) {
   if (!c) return fail(RB_ERR_INVALID, "null context");
-  const int m = (c->uniform_method == 0 && c->hp.slope_type != 3) ? 0 : 1;
+  const int m = (c->uniform_method == 0 && c->hp.slope_type != 3 && c->hp.difmag == 0.0) ? 0 : 1;
   if (method) *method = m;
   if (shape) *shape = m == 0 ? c->stream_shape : (c->finest ? c->lv[c->finest].shape : -1);
   if (hz) *hz = m == 0 ? c->stream_hz : 0;

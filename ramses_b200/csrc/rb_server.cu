@@ -418,6 +418,8 @@ int rb_server_create(const rb_hydro_params* hp, int precision, int64_t hbm_budge
                                 "z-streaming kernel, which holds axis neighbours only");
   if (hp->pressure_fix)
     return fail(RB_ERR_INVALID, "pressure_fix is not served: the batched z-streaming step keeps no enew/divu");
+  if (hp->difmag > 0.0)
+    return fail(RB_ERR_INVALID, "difmag > 0 is not served: the batched z-streaming step has no corner divergence");
   if (precision != RB_PREC_FP64 && precision != RB_PREC_MIXED)
     return fail(RB_ERR_INVALID, "precision must be RB_PREC_FP64 or RB_PREC_MIXED");
   if (rb_device_count() == 0) return fail(RB_ERR_NO_DEVICE, "no CUDA device visible");

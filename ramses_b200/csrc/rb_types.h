@@ -39,7 +39,7 @@ typedef struct rb_hydro_params {
   int32_t interpol_type; /* 0..4                                           */
   int32_t pressure_fix;  /* 1: dual-energy fix (enew/divu tracked, set_uold  */
                          /*    repairs E where E - ekin is too small)       */
-  double difmag;         /* must be 0                                      */
+  double difmag;         /* artificial diffusion coefficient, >= 0 (0: off)  */
   double beta_fix;       /* pressure-fix threshold, >= 0 (default 0)       */
   int32_t niter_riemann; /* Newton iterations of the 'exact' solver (10)    */
   int32_t pad_;          /* zero                                            */

@@ -47,8 +47,8 @@ class HydroParams:
             raise ValueError("Unknown slope type %r" % self.slope_type)
         if self.scheme.strip().lower() != "muscl":
             raise ValueError("scheme %r not supported (muscl only)" % self.scheme)
-        if self.difmag != 0.0:
-            raise ValueError("difmag>0 is not supported")
+        if not (self.difmag >= 0.0) or self.difmag == float("inf"):
+            raise ValueError("difmag must be finite and >= 0")
         if not (self.beta_fix >= 0.0) or self.beta_fix == float("inf"):
             raise ValueError("beta_fix must be finite and >= 0")
         if self.riemann_code == 5 and self.niter_riemann < 1:

@@ -71,6 +71,9 @@ def test_python_params_validation():
     HydroParams(riemann="acoustic").validate()
     with pytest.raises(ValueError):
         HydroParams(riemann="exact", niter_riemann=0).validate()
+    HydroParams(difmag=0.1).validate()
+    with pytest.raises(ValueError):
+        HydroParams(difmag=-0.1).validate()
     with pytest.raises(ValueError):
         HydroParams(slope_type=4).validate()
     with pytest.raises(ValueError):
