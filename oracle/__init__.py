@@ -55,7 +55,7 @@ class OrcParams(ctypes.Structure):
                 ("slope_type", ctypes.c_int32), ("interpol_var", ctypes.c_int32),
                 ("interpol_type", ctypes.c_int32), ("pressure_fix", ctypes.c_int32),
                 ("beta_fix", ctypes.c_double), ("niter_riemann", ctypes.c_int32),
-                ("difmag", ctypes.c_double)]
+                ("difmag", ctypes.c_double), ("scheme", ctypes.c_int32)]
 
 
 MAXLEVEL = 32
@@ -110,7 +110,8 @@ def params_struct(hp) -> OrcParams:
     hp.validate()
     return OrcParams(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta,
                      hp.riemann_code, hp.slope_type, hp.interpol_var, hp.interpol_type,
-                     1 if hp.pressure_fix else 0, hp.beta_fix, hp.niter_riemann, hp.difmag)
+                     1 if hp.pressure_fix else 0, hp.beta_fix, hp.niter_riemann, hp.difmag,
+                     hp.scheme_code)
 
 
 def _ptr(a, t):

@@ -232,6 +232,112 @@ static void trace3d(const orc_params *p, const double *q, const double *dq, doub
         }
 }
 
+/* tracexyz, one direction (hydro/uplmde.f90:470-520 for x): face frame
+ * (r, un, p, t1, t2); P = right state at the lower face (qp), M = left state
+ * at the upper face (qm), same order. project_out = one (:416). */
+static void plmde_dir(double r, double un, double pp, double t1, double t2, double cc, double csq,
+                      double dr, double dun, double dp, double dt1, double dt2, double dtd, double sr,
+                      double sun, double sp, double st1, double st2, double smallr, double P[5], double M[5]) {
+  const double project_out = one, three = 3.0;
+  double alpham = half * (dp / csq - dun * r / cc);
+  double alphap = half * (dp / csq + dun * r / cc);
+  double alpha0r = dr - dp / csq;
+  double alpha0t1 = dt1, alpha0t2 = dt2;
+  double ccc = cc; /* supersonic fix (:478-479) */
+  if (fabs(dun) > three * cc) ccc = zero;
+  /* right state (:481-498) */
+  double spminus = (un - ccc) * dtd, spplus = (un + ccc) * dtd, spzero = (un)*dtd;
+  if ((un + ccc) > zero) spplus = -project_out;
+  if ((un - ccc) > zero) spminus = -project_out;
+  if (un > zero) spzero = -project_out;
+  double apright = half * (-one - spplus) * alphap;
+  double amright = half * (-one - spminus) * alpham;
+  double azrright = half * (-one - spzero) * alpha0r;
+  double az1right = half * (-one - spzero) * alpha0t1;
+  double az2right = half * (-one - spzero) * alpha0t2;
+  P[0] = r + (apright + amright + azrright) + sr;
+  P[1] = un + (apright - amright) * cc / r + sun;
+  P[2] = pp + (apright + amright) * csq + sp;
+  P[3] = t1 + (az1right) + st1;
+  P[4] = t2 + (az2right) + st2;
+  P[0] = fmaxd(smallr, P[0]);
+  /* left state (:500-519) */
+  spminus = (un - ccc) * dtd;
+  spplus = (un + ccc) * dtd;
+  spzero = (un)*dtd;
+  if ((un + ccc) <= zero) spplus = +project_out;
+  if ((un - ccc) <= zero) spminus = +project_out;
+  if (un <= zero) spzero = +project_out;
+  double apleft = half * (+one - spplus) * alphap;
+  double amleft = half * (+one - spminus) * alpham;
+  double azrleft = half * (+one - spzero) * alpha0r;
+  double az1left = half * (+one - spzero) * alpha0t1;
+  double az2left = half * (+one - spzero) * alpha0t2;
+  M[0] = r + (apleft + amleft + azrleft) + sr;
+  M[1] = un + (apleft - amleft) * cc / r + sun;
+  M[2] = pp + (apleft + amleft) * csq + sp;
+  M[3] = t1 + (az1left) + st1;
+  M[4] = t2 + (az2left) + st2;
+  M[0] = fmaxd(smallr, M[0]);
+}
+
+/* tracexyz (hydro/uplmde.f90:375-696): scheme='plmde' predictor, from the
+ * primitive state, its slopes and ctoprim's sound speed c */
+static void tracexyz(const orc_params *p, const double *q, const double *dq, const double *c, double *qm,
+                     double *qp, double dx, double dy, double dz, double dt, int ngrid, int nv) {
+  const double gamma = p->gamma, smallr = p->smallr;
+  const double dtdx = dt / dx, dtdy = dt / dy, dtdz = dt / dz; /* :412 */
+  enum { ir = 1, iu = 2, iv = 3, iw = 4, ip = 5 };
+  for (int k = 0; k <= 3; k++)
+    for (int j = 0; j <= 3; j++)
+      for (int i = 0; i <= 3; i++)
+        for (int l = 0; l < ngrid; l++) {
+          double cc = c[S6(nv, l, i, j, k)]; /* :424-431 */
+          double r = q[QI(nv, l, i, j, k, ir)];
+          double u = q[QI(nv, l, i, j, k, iu)];
+          double v = q[QI(nv, l, i, j, k, iv)];
+          double w = q[QI(nv, l, i, j, k, iw)];
+          double pp = q[QI(nv, l, i, j, k, ip)];
+          double csq = gamma * pp / r;
+#define DQ(var, d) dq[QD(nv, l, i, j, k, var, d)]
+          double drx = DQ(ir, 1), dux = DQ(iu, 1), dvx = DQ(iv, 1), dwx = DQ(iw, 1), dpx = DQ(ip, 1);
+          double dry = DQ(ir, 2), duy = DQ(iu, 2), dvy = DQ(iv, 2), dwy = DQ(iw, 2), dpy = DQ(ip, 2);
+          double drz = DQ(ir, 3), duz = DQ(iu, 3), dvz = DQ(iv, 3), dwz = DQ(iw, 3), dpz = DQ(ip, 3);
+#undef DQ
+          /* transverse derivatives (:458-469), every one scaled by dt/dx */
+          double srx = half * dtdx * (-v * dry - w * drz - (dvy + dwz) * r);
+          double spx = half * dtdx * (-v * dpy - w * dpz - (dvy + dwz) * gamma * pp);
+          double sux = half * dtdx * (-v * duy - w * duz);
+          double svx = half * dtdx * (-v * dvy - w * dvz - (dpy) / r);
+          double swx = half * dtdx * (-v * dwy - w * dwz - (dpz) / r);
+          double sry = half * dtdx * (-u * drx - w * drz - (dux + dwz) * r);
+          double spy = half * dtdx * (-u * dpx - w * dpz - (dux + dwz) * gamma * pp);
+          double suy = half * dtdx * (-u * dux - w * duz - (dpx) / r);
+          double svy = half * dtdx * (-u * dvx - w * dvz);
+          double swy = half * dtdx * (-u * dwx - w * dwz - (dpz) / r);
+          double srz = half * dtdx * (-v * dry - u * drx - (dvy + dux) * r);
+          double spz = half * dtdx * (-v * dpy - u * dpx - (dvy + dux) * gamma * pp);
+          double suz = half * dtdx * (-v * duy - u * dux - (dpx) / r);
+          double svz = half * dtdx * (-v * dvy - u * dvx - (dpy) / r);
+          double swz = half * dtdx * (-v * dwy - u * dwx);
+          double P[5], M[5];
+#define PUT(A, var, d, x) A[QD(nv, l, i, j, k, var, d)] = (x)
+          /* x (:470-520) */
+          plmde_dir(r, u, pp, v, w, cc, csq, drx, dux, dpx, dvx, dwx, dtdx, srx, sux, spx, svx, swx, smallr, P, M);
+          PUT(qp, ir, 1, P[0]); PUT(qp, iu, 1, P[1]); PUT(qp, ip, 1, P[2]); PUT(qp, iv, 1, P[3]); PUT(qp, iw, 1, P[4]);
+          PUT(qm, ir, 1, M[0]); PUT(qm, iu, 1, M[1]); PUT(qm, ip, 1, M[2]); PUT(qm, iv, 1, M[3]); PUT(qm, iw, 1, M[4]);
+          /* y (:522-571) */
+          plmde_dir(r, v, pp, u, w, cc, csq, dry, dvy, dpy, duy, dwy, dtdy, sry, svy, spy, suy, swy, smallr, P, M);
+          PUT(qp, ir, 2, P[0]); PUT(qp, iv, 2, P[1]); PUT(qp, ip, 2, P[2]); PUT(qp, iu, 2, P[3]); PUT(qp, iw, 2, P[4]);
+          PUT(qm, ir, 2, M[0]); PUT(qm, iv, 2, M[1]); PUT(qm, ip, 2, M[2]); PUT(qm, iu, 2, M[3]); PUT(qm, iw, 2, M[4]);
+          /* z (:573-622) */
+          plmde_dir(r, w, pp, u, v, cc, csq, drz, dwz, dpz, duz, dvz, dtdz, srz, swz, spz, suz, svz, smallr, P, M);
+          PUT(qp, ir, 3, P[0]); PUT(qp, iw, 3, P[1]); PUT(qp, ip, 3, P[2]); PUT(qp, iu, 3, P[3]); PUT(qp, iv, 3, P[4]);
+          PUT(qm, ir, 3, M[0]); PUT(qm, iw, 3, M[1]); PUT(qm, ip, 3, M[2]); PUT(qm, iu, 3, M[3]); PUT(qm, iv, 3, M[4]);
+#undef PUT
+        }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Riemann solvers: hydro/godunov_utils.f90                                  */
 /* ql/qr = (rho, u_normal, P, u_t1, u_t2); fg = 6 fluxes (5 + thermal)       */
@@ -557,7 +663,7 @@ static void work_free(work *w) {
   free(w->qin); free(w->cin); free(w->dq); free(w->qm); free(w->qp); free(w->fx); free(w->tx);
 }
 
-/* unsplit: hydro/umuscl.f90:22-171 (scheme='muscl', difmag=0) */
+/* unsplit: hydro/umuscl.f90:22-171 */
 /* cmpdivu (hydro/uplmde.f90:702-764, NDIM=3): velocity divergence at the
  * cell corners (i-1/2, j-1/2, k-1/2), i,j,k = 1..3, from the primitive
  * velocities; div[l + nv*((i-1) + 3*((j-1) + 3*(k-1)))] */
@@ -633,7 +739,10 @@ static int unsplit_w(const orc_params *p, work *w, const double *uin, const doub
   const int nv = w->nv;
   ctoprim(p, uin, w->qin, w->cin, gravin, dt, ngrid, nv);
   if (uslope(p, w->qin, w->dq, ngrid, nv)) return -2;
-  trace3d(p, w->qin, w->dq, w->qm, w->qp, dx, dy, dz, dt, ngrid, nv);
+  if (p->scheme == 1) /* umuscl.f90:73-94 */
+    tracexyz(p, w->qin, w->dq, w->cin, w->qm, w->qp, dx, dy, dz, dt, ngrid, nv);
+  else
+    trace3d(p, w->qin, w->dq, w->qm, w->qp, dx, dy, dz, dt, ngrid, nv);
   const double dd[3] = {dx, dy, dz};
   for (int idim = 1; idim <= 3; idim++) {
     /* x: i=if1..if2, j=jlo..jhi, k=klo..khi (:97-99); y, z analogously */

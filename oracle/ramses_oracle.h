@@ -38,6 +38,7 @@ typedef struct orc_params {
   double beta_fix;       /* pressure-fix threshold (amr/amr_parameters.f90:167) */
   int32_t niter_riemann; /* Newton iterations of riemann_approx (hydro_parameters.f90:75) */
   double difmag;         /* artificial diffusion where the flow converges (0: off) */
+  int32_t scheme;        /* 0: 'muscl' (trace3d), 1: 'plmde' (tracexyz) */
 } orc_params;
 
 /* &REFINE_PARAMS gradient criterion (hydro/hydro_parameters.f90:47-52) */

@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       }
     }
     Prim<R> sp[3], sm[3];
-    trace_cell<R>(q0, dq, c.gamma, c.smallr, dtd, sp, sm, mask);
+    trace_sel<R, RS>(q0, dq, c, dtd, sp, sm, mask);
     // store: qm of direction d at face index (coord+1), qp at face index coord
 #pragma unroll
     for (int d = 0; d < 3; d++) {

@@ -29,7 +29,7 @@ template <typename R> struct Prim { R r, u, v, w, p; };
 // Hydro constants in compute precision.
 template <typename R> struct Consts {
   R gamma, smallr, smallc, smallp, entho, half, slope_theta, courant;
-  int slope_type, riemann, niter_riemann;
+  int slope_type, riemann, niter_riemann, scheme;
 };
 
 template <typename R>
@@ -47,12 +47,14 @@ __device__ __forceinline__ Consts<R> make_consts(const rb_hydro_params& hp) {
   c.slope_type = hp.slope_type;
   c.riemann = hp.riemann;
   c.niter_riemann = hp.niter_riemann;
+  c.scheme = hp.scheme;
   return c;
 }
 
 // ---------------------------------------------------------------------------
 // ctoprim for one cell (umuscl.f90:861-965), conservative FP64 input.
-// The sound speed of ctoprim is only used by the PLMDE trace and is not formed.
+// The sound speed of ctoprim is only used by the PLMDE trace, which forms it
+// from the primitive state.
 // ---------------------------------------------------------------------------
 // FP64 reciprocal for the FP32-mixed path: the FP32 reciprocal of x refined
 // by one Newton-Raphson step r <- r + r(1 - xr) in FP64, which squares the
@@ -227,6 +229,122 @@ __device__ __forceinline__ void trace_cell(const Prim<R>& q, const R dq[5][3], R
     qp[d] = P;
     qm[d] = M;
   }
+}
+
+// PLMDE predictor, one direction (tracexyz, uplmde.f90:470-520 for x):
+// characteristic amplitudes of the slopes, each wave traced to the face only
+// when it moves towards it (project_out = 1 otherwise), the sound wave speed
+// zeroed where |du_n| > 3c (supersonic fix). In the face frame: r, normal
+// velocity un, p, transverse velocities t1, t2 and their half-step sources s*.
+// P/M = (r, un, p, t1, t2) of the right state at the lower face and of the
+// left state at the upper face.
+template <typename R>
+__device__ __forceinline__ void plmde_dir(R r, R un, R p, R t1, R t2, R cc, R csq, R dr, R dun, R dp, R dt1,
+                                          R dt2, R dtd, R sr, R sun, R sp, R st1, R st2, R smallr, R P[5],
+                                          R M[5]) {
+  const R half = (R)0.5, one = (R)1, zero = (R)0, three = (R)3;
+  const R alpham = half * (dp / csq - dun * r / cc);
+  const R alphap = half * (dp / csq + dun * r / cc);
+  const R alpha0r = dr - dp / csq;
+  const R ccc = ((R)fabs(dun) > three * cc) ? zero : cc;
+  {
+    R spminus = (un - ccc) * dtd, spplus = (un + ccc) * dtd, spzero = un * dtd;
+    if ((un + ccc) > zero) spplus = -one;
+    if ((un - ccc) > zero) spminus = -one;
+    if (un > zero) spzero = -one;
+    const R ap = half * (-one - spplus) * alphap;
+    const R am = half * (-one - spminus) * alpham;
+    const R azr = half * (-one - spzero) * alpha0r;
+    const R az1 = half * (-one - spzero) * dt1;
+    const R az2 = half * (-one - spzero) * dt2;
+    P[0] = fmx<R>(smallr, r + (ap + am + azr) + sr);
+    P[1] = un + (ap - am) * cc / r + sun;
+    P[2] = p + (ap + am) * csq + sp;
+    P[3] = t1 + az1 + st1;
+    P[4] = t2 + az2 + st2;
+  }
+  {
+    R spminus = (un - ccc) * dtd, spplus = (un + ccc) * dtd, spzero = un * dtd;
+    if ((un + ccc) <= zero) spplus = one;
+    if ((un - ccc) <= zero) spminus = one;
+    if (un <= zero) spzero = one;
+    const R ap = half * (one - spplus) * alphap;
+    const R am = half * (one - spminus) * alpham;
+    const R azr = half * (one - spzero) * alpha0r;
+    const R az1 = half * (one - spzero) * dt1;
+    const R az2 = half * (one - spzero) * dt2;
+    M[0] = fmx<R>(smallr, r + (ap + am + azr) + sr);
+    M[1] = un + (ap - am) * cc / r + sun;
+    M[2] = p + (ap + am) * csq + sp;
+    M[3] = t1 + az1 + st1;
+    M[4] = t2 + az2 + st2;
+  }
+}
+
+// PLMDE predictor for one cell (scheme='plmde': tracexyz, uplmde.f90:375-696),
+// same interface as trace_cell. The transverse source terms are the
+// reference's (:459-469), all scaled by dt/dx; the sound speed is ctoprim's
+// sqrt((gamma*p)*(1/rho)) (umuscl.f90:936-937).
+template <typename R>
+__device__ __forceinline__ void trace_plmde_cell(const Prim<R>& q, const R dq[5][3], R gamma, R smallr,
+                                                 const R dtd[3], Prim<R> qp[3], Prim<R> qm[3],
+                                                 unsigned dirmask = 7u) {
+  const R half = (R)0.5;
+  const R r = q.r, u = q.u, v = q.v, w = q.w, p = q.p;
+  R cc = gamma * p;
+  cc = (R)sqrt(cc * ((R)1 / r));
+  const R csq = gamma * p / r;
+  const R drx = dq[0][0], dry = dq[0][1], drz = dq[0][2];
+  const R dux = dq[1][0], duy = dq[1][1], duz = dq[1][2];
+  const R dvx = dq[2][0], dvy = dq[2][1], dvz = dq[2][2];
+  const R dwx = dq[3][0], dwy = dq[3][1], dwz = dq[3][2];
+  const R dpx = dq[4][0], dpy = dq[4][1], dpz = dq[4][2];
+  const R hdt = half * dtd[0];
+  R P[5], M[5];
+  if (dirmask & 1u) {
+    const R srx = hdt * (-v * dry - w * drz - (dvy + dwz) * r);
+    const R spx = hdt * (-v * dpy - w * dpz - (dvy + dwz) * gamma * p);
+    const R sux = hdt * (-v * duy - w * duz);
+    const R svx = hdt * (-v * dvy - w * dvz - (dpy) / r);
+    const R swx = hdt * (-v * dwy - w * dwz - (dpz) / r);
+    plmde_dir<R>(r, u, p, v, w, cc, csq, drx, dux, dpx, dvx, dwx, dtd[0], srx, sux, spx, svx, swx, smallr, P, M);
+    qp[0].r = P[0]; qp[0].u = P[1]; qp[0].p = P[2]; qp[0].v = P[3]; qp[0].w = P[4];
+    qm[0].r = M[0]; qm[0].u = M[1]; qm[0].p = M[2]; qm[0].v = M[3]; qm[0].w = M[4];
+  }
+  if (dirmask & 2u) {
+    const R sry = hdt * (-u * drx - w * drz - (dux + dwz) * r);
+    const R spy = hdt * (-u * dpx - w * dpz - (dux + dwz) * gamma * p);
+    const R suy = hdt * (-u * dux - w * duz - (dpx) / r);
+    const R svy = hdt * (-u * dvx - w * dvz);
+    const R swy = hdt * (-u * dwx - w * dwz - (dpz) / r);
+    plmde_dir<R>(r, v, p, u, w, cc, csq, dry, dvy, dpy, duy, dwy, dtd[1], sry, svy, spy, suy, swy, smallr, P, M);
+    qp[1].r = P[0]; qp[1].v = P[1]; qp[1].p = P[2]; qp[1].u = P[3]; qp[1].w = P[4];
+    qm[1].r = M[0]; qm[1].v = M[1]; qm[1].p = M[2]; qm[1].u = M[3]; qm[1].w = M[4];
+  }
+  if (dirmask & 4u) {
+    const R srz = hdt * (-v * dry - u * drx - (dvy + dux) * r);
+    const R spz = hdt * (-v * dpy - u * dpx - (dvy + dux) * gamma * p);
+    const R suz = hdt * (-v * duy - u * dux - (dpx) / r);
+    const R svz = hdt * (-v * dvy - u * dvx - (dpy) / r);
+    const R swz = hdt * (-v * dwy - u * dwx);
+    plmde_dir<R>(r, w, p, u, v, cc, csq, drz, dwz, dpz, duz, dvz, dtd[2], srz, swz, spz, suz, svz, smallr, P, M);
+    qp[2].r = P[0]; qp[2].w = P[1]; qp[2].p = P[2]; qp[2].u = P[3]; qp[2].v = P[4];
+    qm[2].r = M[0]; qm[2].w = M[1]; qm[2].p = M[2]; qm[2].u = M[3]; qm[2].v = M[4];
+  }
+}
+
+// The predictor of the scheme: MUSCL-Hancock, or PLMDE in the run-time
+// variant (RS == 0) when c.scheme says so.
+template <typename R, int RS>
+__device__ __forceinline__ void trace_sel(const Prim<R>& q, const R dq[5][3], const Consts<R>& c, const R dtd[3],
+                                          Prim<R> qp[3], Prim<R> qm[3], unsigned dirmask) {
+  if constexpr (RS == 0) {
+    if (c.scheme == RB_SCHEME_PLMDE) {
+      trace_plmde_cell<R>(q, dq, c.gamma, c.smallr, dtd, qp, qm, dirmask);
+      return;
+    }
+  }
+  trace_cell<R>(q, dq, c.gamma, c.smallr, dtd, qp, qm, dirmask);
 }
 
 // ---------------------------------------------------------------------------

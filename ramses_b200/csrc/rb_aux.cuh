@@ -707,7 +707,7 @@ static __global__ void __launch_bounds__(64) unsplit_fortran_kernel(const double
       }
     }
     Prim<double> sp[3], sm[3];
-    trace_cell<double>(q0, dq, c.gamma, c.smallr, dtd, sp, sm, 7u);
+    trace_sel<double, 0>(q0, dq, c, dtd, sp, sm, 7u);
     for (int d = 0; d < 3; d++) {
       qm[0][d][cidx] = sm[d].r; qm[1][d][cidx] = sm[d].u; qm[2][d][cidx] = sm[d].v;
       qm[3][d][cidx] = sm[d].w; qm[4][d][cidx] = sm[d].p;

@@ -34,7 +34,8 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
   const int st = hp->slope_type;
   if (!(st == 0 || st == 1 || st == 2 || st == 3 || st == 7 || st == 8))
     return fail(RB_ERR_INVALID, "Unknown slope type %d", st);
-  if (hp->scheme != 0) return fail(RB_ERR_INVALID, "scheme %d not supported (muscl only)", hp->scheme);
+  if (hp->scheme != RB_SCHEME_MUSCL && hp->scheme != RB_SCHEME_PLMDE)
+    return fail(RB_ERR_INVALID, "scheme %d not supported (muscl=0, plmde=1)", hp->scheme);
   if (hp->pressure_fix != 0 && hp->pressure_fix != 1)
     return fail(RB_ERR_INVALID, "pressure_fix must be 0 or 1 (got %d)", hp->pressure_fix);
   if (!(hp->beta_fix >= 0.0) || !std::isfinite(hp->beta_fix))

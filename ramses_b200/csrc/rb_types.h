@@ -10,6 +10,7 @@
 
 enum { RB_RIEMANN_LLF = 1, RB_RIEMANN_HLL = 2, RB_RIEMANN_HLLC = 3, RB_RIEMANN_ACOUSTIC = 4, RB_RIEMANN_EXACT = 5 };
 enum { RB_PREC_FP64 = 0, RB_PREC_MIXED = 1 };
+enum { RB_SCHEME_MUSCL = 0, RB_SCHEME_PLMDE = 1 };
 
 /* Status codes returned by every C-ABI entry point (0 = success). */
 enum {
@@ -34,7 +35,7 @@ typedef struct rb_hydro_params {
   double slope_theta;
   int32_t riemann;       /* RB_RIEMANN_*                                    */
   int32_t slope_type;    /* 0,1,2,3,7,8                                    */
-  int32_t scheme;        /* 0 = 'muscl' ('plmde' is rejected)              */
+  int32_t scheme;        /* RB_SCHEME_MUSCL ('muscl') or RB_SCHEME_PLMDE     */
   int32_t interpol_var;  /* 0,1,2                                          */
   int32_t interpol_type; /* 0..4                                           */
   int32_t pressure_fix;  /* 1: dual-energy fix (enew/divu tracked, set_uold  */

@@ -14,6 +14,7 @@ import re
 from typing import Dict, List
 
 RIEMANN_CODES = {"llf": 1, "hll": 2, "hllc": 3, "acoustic": 4, "exact": 5}
+SCHEME_CODES = {"muscl": 0, "plmde": 1}
 SLOPE_TYPES = (0, 1, 2, 3, 7, 8)
 
 
@@ -41,12 +42,18 @@ class HydroParams:
         except KeyError:
             raise ValueError("unknown Riemann solver %r (supported: llf, hll, hllc, acoustic, exact)" % self.riemann)
 
+    @property
+    def scheme_code(self) -> int:
+        try:
+            return SCHEME_CODES[self.scheme.strip().lower()]
+        except KeyError:
+            raise ValueError("scheme %r not supported (muscl, plmde)" % self.scheme)
+
     def validate(self) -> None:
         self.riemann_code  # noqa: B018 - raises on unknown solver
         if self.slope_type not in SLOPE_TYPES:
             raise ValueError("Unknown slope type %r" % self.slope_type)
-        if self.scheme.strip().lower() != "muscl":
-            raise ValueError("scheme %r not supported (muscl only)" % self.scheme)
+        self.scheme_code  # noqa: B018 - raises on unknown scheme
         if not (self.difmag >= 0.0) or self.difmag == float("inf"):
             raise ValueError("difmag must be finite and >= 0")
         if not (self.beta_fix >= 0.0) or self.beta_fix == float("inf"):

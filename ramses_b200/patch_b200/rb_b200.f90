@@ -130,7 +130,8 @@ contains
     hp%interpol_var = interpol_var; hp%interpol_type = interpol_type; hp%difmag = difmag
     hp%beta_fix = beta_fix
     hp%niter_riemann = niter_riemann; hp%pad_ = 0
-    if (scheme /= 'muscl') hp%scheme = 1
+    if (scheme == 'plmde') hp%scheme = 1
+    if (scheme /= 'muscl' .and. scheme /= 'plmde') hp%scheme = -1
     if (pressure_fix) hp%pressure_fix = 1
     hp%riemann = 0
     if (riemann == 'llf') hp%riemann = 1

@@ -148,7 +148,8 @@ def _check(rc: int, where: str):
 def hydro_params_c(hp: HydroParams) -> HydroParamsC:
     hp.validate()
     return HydroParamsC(hp.gamma, hp.smallr, hp.smallc, hp.courant_factor, hp.slope_theta, hp.riemann_code,
-                        hp.slope_type, 0, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix), hp.difmag,
+                        hp.slope_type, hp.scheme_code, hp.interpol_var, hp.interpol_type, int(hp.pressure_fix),
+                        hp.difmag,
                         hp.beta_fix, hp.niter_riemann, 0)
 
 

@@ -76,8 +76,9 @@ def test_python_params_validation():
         HydroParams(difmag=-0.1).validate()
     with pytest.raises(ValueError):
         HydroParams(slope_type=4).validate()
+    HydroParams(scheme="plmde").validate()
     with pytest.raises(ValueError):
-        HydroParams(scheme="plmde").validate()
+        HydroParams(scheme="induction").validate()
     HydroParams(riemann="hll", slope_type=8).validate()
 
 

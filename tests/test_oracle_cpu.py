@@ -439,3 +439,50 @@ def test_difmag_sod_stays_close():
         ana = exact_riemann.sample(x[m], run.t, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
         return np.abs(rho[0, 0][m] - ana[0]).sum() / np.abs(ana[0]).sum()
     assert l1(0.1) < 1.5 * l1(0.0)
+
+
+# ---- scheme='plmde' (tracexyz, uplmde.f90:375-696, selected in unsplit,
+# umuscl.f90:73-94) -------------------------------------------------------------
+
+def test_plmde_conserves_and_keeps_mirror_symmetry():
+    tree, hp, u = sedov_uniform(4)
+    hp = HydroParams(**{**hp.__dict__})
+    hp.scheme = "plmde"
+    run = oracle.OracleRun(tree, hp, u)
+    ref = oracle.OracleRun(tree, HydroParams(**{**hp.__dict__, "scheme": "muscl"}), u)
+    _, a0 = leaf_values(tree, u)
+    for _ in range(5):
+        run.coarse_step()
+        ref.coarse_step()
+    _, a1 = leaf_values(tree, run.uold)
+    assert abs(a1[0].sum() - a0[0].sum()) <= 1e-14 * a0[0].sum()
+    assert abs(a1[4].sum() - a0[4].sum()) <= 1e-13 * a0[4].sum()
+    # mirror symmetric up to the one-sided upwind test of tracexyz, which
+    # treats u = 0 (the Sedov box at rest) as moving left (uplmde.f90:484-486,
+    # 506-508): a few 1e-8 here
+    rho = run.uold[0][tree.cell_index(4) - 1]
+    np.testing.assert_allclose(rho, rho[:, :, ::-1], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(rho, rho[::-1], rtol=0, atol=1e-6)
+    assert np.any(run.uold != ref.uold)  # the predictor is not the MUSCL-Hancock one
+
+
+@pytest.mark.parametrize("riemann", ["hllc", "llf"])
+def test_plmde_sod_known_answer(riemann):
+    """The planar Sod tube with the PLMDE predictor: planar symmetry kept and
+    the density within 1.5x the MUSCL-Hancock L1 error of the exact solution."""
+    def l1(scheme):
+        hp = HydroParams(gamma=1.4, riemann=riemann, slope_type=2, courant_factor=0.8, scheme=scheme)
+        tree = mesh.build_tree(5, 5, None, boxlen=2.0)
+        prim = ics.shock_tube_prim(1.0, 1.0, 0.0, 0.125, 0.1, 0.0, x0=1.0, boxlen=2.0)
+        run = oracle.OracleRun(tree, hp, ics.fill_all_levels(tree, prim, hp.gamma))
+        while run.t < 0.245:
+            run.coarse_step()
+        idx = tree.cell_index(5)
+        x = (np.arange(32) + 0.5) * (2.0 / 32) - 0.5
+        rho = run.uold[0][idx - 1]
+        assert np.array_equal(rho, np.broadcast_to(rho[0, 0], rho.shape))
+        m = (x > 0) & (x < 1)
+        ana = exact_riemann.sample(x[m], run.t, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1)
+        return np.abs(rho[0, 0][m] - ana[0]).sum() / np.abs(ana[0]).sum()
+    e_plmde, e_muscl = l1("plmde"), l1("muscl")
+    assert e_plmde < 1.5 * e_muscl, (e_plmde, e_muscl)
