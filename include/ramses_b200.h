@@ -23,6 +23,9 @@
  *   set_uold(ilevel)                   hydro/godunov_fine.f90:135-232 -> rb_set_uold
  *   upload_fine(ilevel)                hydro/interpol_hydro.f90:5-68  -> rb_upload_fine
  *   amr_step hydro sequence            amr/amr_step.f90:320-445       -> rb_coarse_step
+ *   make_boundary_hydro(ilevel)        hydro/hydro_boundary.f90:5-260 -> rb_make_boundary_hydro
+ *   boundary(ibound,ilevel) lists      amr/amr_commons.f90, hydro/read_hydro_params.f90:310-420
+ *                                                                     -> rb_set_boundary
  *   &HYDRO_PARAMS                      hydro/read_hydro_params.f90:43-54 -> rb_hydro_params
  */
 #ifndef RAMSES_B200_H
@@ -61,6 +64,23 @@ int rb_destroy(rb_context *ctx);
  * active_igrid. Builds the device tile and interpolation tables. */
 int rb_sync_tree(rb_context *ctx, const int32_t *son, const int32_t *father, const int32_t *nbor,
                  const int32_t *numbl, const int32_t *active_igrid);
+
+/* Physical boundaries (simple_boundary): the boundary regions' codes
+ * boundary_type(1:nboundary) (1-6 walls, 11-16 free = zero-gradient, side
+ * 1..6 = -x,+x,-y,+y,-z,+z; imposed 21-26 are rejected), the grid counts
+ * numbb(1:nboundary,1:nlevelmax) (Fortran order) and the grids of
+ * boundary(ibound,ilevel)%igrid concatenated level by level, boundary by
+ * boundary within a level. The boundary octs are found by the stencil
+ * gathers and never updated; mesh params nx_loc gives the coarse cells
+ * across the box. Before or after rb_sync_tree (a synchronised tree is
+ * re-indexed). nboundary = 0 restores a periodic box. */
+int rb_set_boundary(rb_context *ctx, int32_t nboundary, const int32_t *boundary_type, const int32_t *numbb,
+                    const int32_t *boundary_igrid);
+/* make_boundary_hydro(ilevel): fill the boundary octs of ilevel from their
+ * reference octs (hydro/hydro_boundary.f90:5-260). rb_coarse_step, rb_run and
+ * rb_uniform_run call it after each level step (amr/amr_step.f90:515); the
+ * host calls it where the reference's init_flow_fine does. */
+int rb_make_boundary_hydro(rb_context *ctx, int ilevel);
 
 /* Fortran-layout uold(ncell,5) host <-> device mirror of uold. */
 int rb_upload_state(rb_context *ctx, const double *uold);

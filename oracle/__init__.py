@@ -82,7 +82,9 @@ class OrcMesh(ctypes.Structure):
                 ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
                 ("mass_tot", ctypes.c_double), ("ekin_tot", ctypes.c_double),
                 ("eint_tot", ctypes.c_double), ("cell_updates", ctypes.c_int64),
-                ("nthreads", ctypes.c_int32), ("divu", _PD), ("enew", _PD)]
+                ("nthreads", ctypes.c_int32), ("divu", _PD), ("enew", _PD),
+                ("nx_loc", ctypes.c_int32), ("nboundary", ctypes.c_int32),
+                ("boundary_type", _P32), ("bound_off", _P64), ("bound_igrid", _P32)]
 
 
 def _declare(L):
@@ -97,6 +99,7 @@ def _declare(L):
     L.orc_godunov_fine.argtypes = [P, M, ctypes.c_int, ctypes.c_double]
     L.orc_courant_fine.argtypes = [P, M, ctypes.c_int, _PD, _PD, _PD, _PD]
     L.orc_coarse_step.argtypes = [P, M]
+    L.orc_make_boundary_hydro.argtypes = [P, M, ctypes.c_int]
     L.orc_get3cubefather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
     L.orc_getnborfather.argtypes = [M, ctypes.c_int, ctypes.c_int, _P32]
     L.orc_interpol_hydro.argtypes = [P, _PD, _PD, ctypes.c_int]
@@ -183,7 +186,17 @@ class OracleRun:
         self.divu = np.zeros(tree.ncell)
         self.enew = np.zeros(tree.ncell)
         m.divu, m.enew = _ptr(self.divu, _PD), _ptr(self.enew, _PD)
+        # physical boundaries: filled once per level as init_flow_fine does
+        # (hydro/init_flow_fine.f90:19), then after every level step
+        m.nx_loc = getattr(tree, "nx_loc", 0)
+        self.btype, self.boff, self.bgrid = tree.boundary_concat()
+        m.nboundary = len(self.btype)
+        m.boundary_type, m.bound_off = _ptr(self.btype, _P32), _ptr(self.boff, _P64)
+        m.bound_igrid = _ptr(self.bgrid, _P32)
         self.m = m
+        if m.nboundary:
+            for l in range(1, tree.nlevelmax + 1):
+                self.make_boundary_hydro(l)
 
     def _check(self, rc, what):
         if rc:
@@ -200,6 +213,10 @@ class OracleRun:
 
     def set_uold(self, ilevel):
         lib().orc_set_uold(ctypes.byref(self.p), ctypes.byref(self.m), ilevel)
+
+    def make_boundary_hydro(self, ilevel):
+        self._check(lib().orc_make_boundary_hydro(ctypes.byref(self.p), ctypes.byref(self.m), ilevel),
+                    "make_boundary_hydro")
 
     def upload_fine(self, ilevel):
         lib().orc_upload_fine(ctypes.byref(self.p), ctypes.byref(self.m), ilevel)

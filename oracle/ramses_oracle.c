@@ -840,6 +840,9 @@ static inline double *UOLD(const orc_mesh *m, int icell, int ivar) {
 static inline double *UNEW(const orc_mesh *m, int icell, int ivar) {
   return &m->unew[(size_t)(ivar - 1) * (size_t)ncell_of(m) + (size_t)(icell - 1)];
 }
+/* nx_loc = icoarse_max-icoarse_min+1: the coarse cells across the box
+ * without the boundary layers (amr/init_amr.f90:44) */
+static inline int nx_loc_of(const orc_mesh *m) { return m->nx_loc > 0 ? m->nx_loc : m->nx; }
 static inline int64_t nactive(const orc_mesh *m, int ilevel) {
   return m->active_off[ilevel + 1] - m->active_off[ilevel];
 }
@@ -1102,7 +1105,7 @@ static void add_pdv_source_terms(const orc_params *p, orc_mesh *m, int ilevel) {
   const int32_t *act = active_list(m, ilevel);
   int64_t n = nactive(m, ilevel);
   size_t nc = (size_t)ncell_of(m);
-  double scale = m->boxlen / (double)m->nx;
+  double scale = m->boxlen / (double)nx_loc_of(m);
   double dx_loc = pow(0.5, ilevel) * scale;
   for (int64_t i = 0; i < n; i++) {
     int g = act[i];
@@ -1139,7 +1142,7 @@ int orc_set_uold(const orc_params *p, orc_mesh *m, int ilevel) {
   const int32_t *act = active_list(m, ilevel);
   int64_t n = nactive(m, ilevel);
   if (p->pressure_fix) add_pdv_source_terms(p, m, ilevel);
-  double scale = m->boxlen / (double)m->nx;
+  double scale = m->boxlen / (double)nx_loc_of(m);
   double dx = pow(0.5, ilevel) * scale;
   const double hexp = 0.0;
   for (int ind = 1; ind <= 8; ind++) {
@@ -1212,8 +1215,7 @@ int orc_courant_fine(const orc_params *p, orc_mesh *m, int ilevel, double *dt_io
                      double *mass, double *ekin, double *eint) {
   const int nv = m->nvector;
   double mass_loc = 0, ekin_loc = 0, eint_loc = 0, dt_loc = *dt_io;
-  int nx_loc = m->nx; /* icoarse_max-icoarse_min+1 */
-  double scale = m->boxlen / (double)nx_loc;
+  double scale = m->boxlen / (double)nx_loc_of(m);
   double dx = pow(0.5, ilevel) * scale;
   double vol = dx * dx * dx;
   const int32_t *act = active_list(m, ilevel);
@@ -1269,7 +1271,7 @@ static int godfine1_flux(const orc_params *p, const orc_mesh *m, work *w, const 
                          int ncache, int ilevel, double dt, double *uloc, double *gloc,
                          unsigned char *ok, double *flux, double *tmp, double *u1, double *u2) {
   const int nv = m->nvector;
-  double scale = m->boxlen / (double)m->nx;
+  double scale = m->boxlen / (double)nx_loc_of(m);
   double dx = pow(0.5, ilevel) * scale;
   int32_t nbf[27];
   /* gathered as (27, nv): nbors_father_cells(i, ind_father) */
@@ -1546,11 +1548,90 @@ static int amr_step(const orc_params *p, orc_mesh *m, int ilevel, int icount) {
   if ((rc = orc_godunov_fine(p, m, ilevel, m->dtnew[ilevel]))) return rc;
   orc_set_uold(p, m, ilevel);
   orc_upload_fine(p, m, ilevel);
+  if ((rc = orc_make_boundary_hydro(p, m, ilevel))) return rc; /* amr_step.f90:515 */
   if (ilevel > m->levelmin) {
     if (m->nsubcycle[ilevel - 1] == 1) m->dtnew[ilevel - 1] = m->dtnew[ilevel];
     if (icount == 2) m->dtnew[ilevel - 1] = m->dtold[ilevel] + m->dtnew[ilevel];
   }
   return 0;
+}
+
+/* make_boundary_hydro: hydro/hydro_boundary.f90:5-260. Every boundary grid
+ * of ilevel takes the state of the reference grid son(nbor(igrid,inbor)), the
+ * grid across the boundary face towards the box, cell ind from cell
+ * ind_ref(ind) (:57-76): mirrored with the normal velocity negated for walls
+ * (:141-157), the adjacent layer for free boundaries with E - ekin + ekin
+ * recomputed (:160-208; no_inflow = .false.). The sweep runs in nvector
+ * batches, each cell position gathered for the whole batch before it is
+ * scattered, in boundary order. */
+int orc_make_boundary_hydro(const orc_params *p, orc_mesh *m, int ilevel) {
+  if (m->nboundary == 0) return 0;
+  const int nv = m->nvector;
+  static const int inbor_of[7] = {0, 2, 1, 4, 3, 6, 5};
+  static const int ref_wall[3][8] = {{2, 1, 4, 3, 6, 5, 8, 7}, {3, 4, 1, 2, 7, 8, 5, 6}, {5, 6, 7, 8, 1, 2, 3, 4}};
+  static const int ref_free[6][8] = {{1, 1, 3, 3, 5, 5, 7, 7}, {2, 2, 4, 4, 6, 6, 8, 8}, {1, 2, 1, 2, 5, 6, 5, 6},
+                                     {3, 4, 3, 4, 7, 8, 7, 8}, {1, 2, 3, 4, 1, 2, 3, 4}, {5, 6, 7, 8, 5, 6, 7, 8}};
+  int32_t *ind_grid = (int32_t *)malloc(sizeof(int32_t) * nv);
+  int32_t *ind_grid_ref = (int32_t *)malloc(sizeof(int32_t) * nv);
+  double *uu = (double *)malloc(sizeof(double) * nv * 5);
+  int rc = 0;
+  for (int ib = 1; ib <= m->nboundary && !rc; ib++) {
+    const int bt = m->boundary_type[ib - 1];
+    const int dir = bt - 10 * (bt / 10);
+    if (dir < 1 || dir > 6 || (bt / 10 != 0 && bt / 10 != 1)) { rc = -1; break; }
+    const int inbor = inbor_of[dir];
+    const int *ind_ref = bt / 10 == 0 ? ref_wall[(dir - 1) / 2] : ref_free[dir - 1];
+    double gs[3] = {1, 1, 1};
+    if (bt / 10 == 0) gs[(dir - 1) / 2] = -1;
+    const int64_t k = (int64_t)(ilevel - 1) * m->nboundary + (ib - 1);
+    const int32_t *list = m->bound_igrid + m->bound_off[k];
+    const int64_t ncache = m->bound_off[k + 1] - m->bound_off[k];
+    for (int64_t i0 = 0; i0 < ncache; i0 += nv) {
+      const int ngrid = (int)(ncache - i0 < nv ? ncache - i0 : nv);
+      for (int i = 0; i < ngrid; i++) {
+        ind_grid[i] = list[i0 + i];
+        ind_grid_ref[i] = SON(m, NBOR(m, ind_grid[i], inbor));
+        if (ind_grid_ref[i] <= 0) { rc = -2; break; }
+      }
+      if (rc) break;
+      for (int ind = 1; ind <= 8; ind++) {
+        const int iskip = m->ncoarse + (ind - 1) * m->ngridmax;
+        const int iskip_ref = m->ncoarse + (ind_ref[ind - 1] - 1) * m->ngridmax;
+        for (int ivar = 1; ivar <= 5; ivar++)
+          for (int i = 0; i < ngrid; i++) uu[(size_t)(ivar - 1) * nv + i] = *UOLD(m, iskip_ref + ind_grid_ref[i], ivar);
+        if (bt / 10 == 0) {
+          for (int ivar = 1; ivar <= 5; ivar++) {
+            const double sw = (ivar > 1 && ivar < 5) ? gs[ivar - 2] : 1.0;
+            for (int i = 0; i < ngrid; i++) *UOLD(m, iskip + ind_grid[i], ivar) = uu[(size_t)(ivar - 1) * nv + i] * sw;
+          }
+        } else {
+          for (int i = 0; i < ngrid; i++) { /* remove kinetic energy (:168-176) */
+            double ekin = 0.0;
+            const double d = fmaxd(uu[i], p->smallr);
+            for (int idim = 1; idim <= 3; idim++) {
+              const double v = uu[(size_t)idim * nv + i] / d;
+              ekin = ekin + 0.5 * d * (v * v);
+            }
+            uu[(size_t)4 * nv + i] = uu[(size_t)4 * nv + i] - ekin;
+          }
+          for (int ivar = 1; ivar <= 5; ivar++)
+            for (int i = 0; i < ngrid; i++) *UOLD(m, iskip + ind_grid[i], ivar) = uu[(size_t)(ivar - 1) * nv + i];
+          for (int i = 0; i < ngrid; i++) { /* add back kinetic energy (:194-202) */
+            const int cell = iskip + ind_grid[i];
+            double ekin = 0.0;
+            const double d = fmaxd(*UOLD(m, cell, 1), p->smallr);
+            for (int idim = 1; idim <= 3; idim++) {
+              const double v = *UOLD(m, cell, idim + 1) / d;
+              ekin = ekin + 0.5 * d * (v * v);
+            }
+            *UOLD(m, cell, 5) = *UOLD(m, cell, 5) + ekin;
+          }
+        }
+      }
+    }
+  }
+  free(ind_grid); free(ind_grid_ref); free(uu);
+  return rc;
 }
 
 int orc_coarse_step(const orc_params *p, orc_mesh *m) {

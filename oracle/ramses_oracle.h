@@ -62,6 +62,15 @@ typedef struct orc_mesh {
   int64_t cell_updates; /* leaf-cell updates accumulated by orc_coarse_step */
   int32_t nthreads;     /* OpenMP threads for the flux phase (0 = default) */
   double *divu, *enew;  /* divu(1:ncell), enew(1:ncell); used when pressure_fix */
+  /* physical boundaries (amr/amr_commons.f90 boundary(ibound,ilevel),
+   * hydro/read_hydro_params.f90:310-420); nboundary = 0: periodic box */
+  int32_t nx_loc;                /* icoarse_max-icoarse_min+1 (0: nx)         */
+  int32_t nboundary;
+  const int32_t *boundary_type;  /* [nboundary]: 1-6 wall, 11-16 free          */
+  const int64_t *bound_off;      /* [nlevelmax*nboundary+1]: the grids of
+                                    (ilevel, ibound) are bound_igrid[off[k]..off[k+1])
+                                    with k = (ilevel-1)*nboundary + ibound-1   */
+  const int32_t *bound_igrid;
 } orc_mesh;
 
 #ifdef __cplusplus
@@ -90,6 +99,9 @@ int orc_upload_fine(const orc_params *p, orc_mesh *m, int ilevel);
 
 /* amr_step.f90 hydro call sequence for one coarse step (levelmin .. finest),
  * followed by the restriction of levels levelmin-1..1 (adaptive_loop.f90). */
+/* make_boundary_hydro(ilevel): hydro/hydro_boundary.f90:5-260 (wall and
+ * free boundaries; imposed ones return -1). */
+int orc_make_boundary_hydro(const orc_params *p, orc_mesh *m, int ilevel);
 int orc_coarse_step(const orc_params *p, orc_mesh *m);
 
 /* nbors_utils.f90:5-194 for one father cell: the 27 neighbouring father

@@ -101,6 +101,10 @@ struct Level {
   double dx = 0.0;
   bool complete = false;
   bool tables_built = false;
+  // physical boundaries: per region (boundary order), the (boundary oct,
+  // reference oct) pairs of this level, igrid-1 each, at [boff[r], boff[r+1])
+  std::vector<int64_t> h_boff;
+  int32_t* d_bpair = nullptr;
 };
 
 // sorted (key, igrid) lookup of one level's octs
@@ -154,6 +158,14 @@ struct rb_context {
   bool have_tree = false;
   bool have_state = false;
   bool clock_valid = false;
+  // physical boundaries (make_boundary_hydro): region types and the
+  // host's boundary(ibound,ilevel) lists, kept for tree re-syncs
+  std::vector<int32_t> btype;
+  std::vector<int64_t> boff;        // [nlevelmax*nb+1] as rb_set_boundary's numbb
+  std::vector<int32_t> bgrid;
+  std::vector<int8_t> is_bnd;       // [ngridmax] 1 for a boundary oct
+  double* d_bbuf = nullptr;         // [largest region][8][5] staging of one fill
+  int64_t bbuf_cap = 0;
   // host copies of the tree (Fortran layout)
   std::vector<int32_t> son, father, nbor;
   std::vector<int64_t> coords;      // [ngridmax*3] oct coordinates at its level

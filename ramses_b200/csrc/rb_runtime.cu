@@ -122,17 +122,31 @@ void free_tree(rb_context* c) {
   for (int l = 0; l <= RB_MAXLEVEL + 1; l++) {
     free_level_tables(c->lv[l]);
     dfree(c->lv[l].d_active);
+    dfree(c->lv[l].d_bpair);
+    c->lv[l].h_boff.clear();
     c->lv[l].noct = 0;
     c->lv[l].h_active.clear();
   }
   c->have_tree = false;
 }
 
-int default_shape(const rb_context* c, const Level& L) {
-  (void)c;
-  if (L.complete && L.noct >= 64 * 148) return 4;   // 8x8x8 cells
-  if (L.noct >= 8 * 64) return 1;                   // 4x4x4 cells
-  return 0;                                         // single oct
+// With physical boundaries a tile must not hold both octs of the box and
+// boundary octs: along a bounded axis the tile's octs must divide the
+// 2^(l-1) octs of one coarse cell.
+bool shape_fits(const rb_context* c, int l, int shape) {
+  const rb::TileShape sh = rb::kTileShapes[shape];
+  const int64_t h = (int64_t)1 << (l - 1);
+  const int to[3] = {sh.tx / 2, sh.ty / 2, sh.tz / 2};
+  for (int32_t bt : c->btype)
+    if (h % to[(bt % 10 - 1) / 2] != 0) return false;
+  return true;
+}
+
+int default_shape(const rb_context* c, int l, const Level& L) {
+  int s = 0;                                            // single oct
+  if (L.complete && L.noct >= 64 * 148) s = 4;          // 8x8x8 cells
+  else if (L.noct >= 8 * 64) s = 1;                     // 4x4x4 cells
+  return shape_fits(c, l, s) ? s : 0;
 }
 
 // Device cell of nbor(igrid,j), j = 1..6, for the level's octs in active
@@ -174,7 +188,9 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   Level& L = c->lv[l];
   free_level_tables(L);
   if (L.noct == 0) return RB_OK;
-  if (L.shape < 0) L.shape = default_shape(c, L);
+  if (L.shape < 0) L.shape = default_shape(c, l, L);
+  if (!shape_fits(c, l, L.shape))
+    return fail(RB_ERR_INVALID, "level %d: tile shape %d spans the box face and the boundary layer", l, L.shape);
   const rb::TileShape sh = rb::kTileShapes[L.shape];
   const int TOX = sh.tx / 2, TOY = sh.ty / 2, TOZ = sh.tz / 2;
   const int BX = TOX + 2, BY = TOY + 2, BZ = TOZ + 2, NBLK = BX * BY * BZ;
@@ -292,7 +308,11 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
       }
     for (int z = 0; z < TOZ; z++)
       for (int y = 0; y < TOY; y++)
-        for (int x = 0; x < TOX; x++) inner[x + TOX * (y + TOY * z)] = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))] >= 0;
+        for (int x = 0; x < TOX; x++) {
+          const int32_t g = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))];
+          if (g >= 0 && c->is_bnd[g]) return fail(RB_ERR_TREE, "level %d: a tile holds a boundary oct", l);
+          inner[x + TOX * (y + TOY * z)] = g >= 0;
+        }
     for (int bz = 0; bz < BZ; bz++)
       for (int by = 0; by < BY; by++)
         for (int bx = 0; bx < BX; bx++) {
@@ -396,6 +416,49 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   return RB_OK;
 }
 
+// make_boundary_hydro's pairs (hydro/hydro_boundary.f90:118-137): for each
+// boundary oct of each region, the reference oct son(nbor(igrid,inbor)) across
+// the region's face towards the box.
+int build_boundary_pairs(rb_context* c) {
+  const int nb = (int)c->btype.size();
+  const int ngm = c->mp.ngridmax;
+  int64_t cap = 0;
+  for (int l = 1; l <= c->mp.nlevelmax; l++) {
+    Level& L = c->lv[l];
+    dfree(L.d_bpair);
+    L.h_boff.assign((size_t)nb + 1, 0);
+    if (nb == 0) continue;
+    std::vector<int32_t> pairs;
+    for (int ib = 0; ib < nb; ib++) {
+      const int dir = c->btype[ib] % 10;
+      const int inbor = (dir & 1) ? dir + 1 : dir - 1;  // the side towards the box
+      const int64_t k = (int64_t)(l - 1) * nb + ib;
+      for (int64_t i = c->boff[k]; i < c->boff[k + 1]; i++) {
+        const int32_t g = c->bgrid[i];
+        const int64_t nc = c->nbor[(size_t)(inbor - 1) * ngm + (g - 1)];
+        if (nc < 1 || nc > c->ncell) return fail(RB_ERR_TREE, "boundary grid %d: nbor(%d) out of range", g, inbor);
+        const int32_t ref = c->son[nc - 1];
+        if (ref < 1 || ref > ngm || c->level_of[ref - 1] != l)
+          return fail(RB_ERR_TREE, "boundary grid %d (level %d) has no reference grid towards the box", g, l);
+        pairs.push_back(g - 1);
+        pairs.push_back(ref - 1);
+      }
+      L.h_boff[ib + 1] = (int64_t)pairs.size() / 2;
+      cap = std::max(cap, L.h_boff[ib + 1] - L.h_boff[ib]);
+    }
+    if (!pairs.empty()) {
+      RB_TRY(dalloc(&L.d_bpair, pairs.size()));
+      RB_TRY(h2d(c, L.d_bpair, pairs.data(), pairs.size() * 4));
+    }
+  }
+  if (cap > c->bbuf_cap) {
+    dfree(c->d_bbuf);
+    RB_TRY(dalloc(&c->d_bbuf, (size_t)cap * 40));
+    c->bbuf_cap = cap;
+  }
+  return RB_OK;
+}
+
 int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
                    const int32_t* numbl, const int32_t* active) {
   if (!son || !father || !nbor || !numbl || !active) return fail(RB_ERR_INVALID, "null tree array");
@@ -407,6 +470,7 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
   c->nbor.assign(nbor, nbor + (size_t)6 * ngm);
   c->coords.assign((size_t)ngm * 3, 0);
   c->level_of.assign((size_t)ngm, 0);
+  c->is_bnd.assign((size_t)ngm, 0);
   c->idx.assign(RB_MAXLEVEL + 2, OctIndex());
   std::vector<OctIndex>& idx = c->idx;
   int64_t off = 0;
@@ -419,14 +483,25 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
     off += n;
     L.noct = n;
     if (n) c->finest = l;
-    L.dx = std::pow(0.5, l) * (c->mp.boxlen / (double)c->mp.nx);
+    L.dx = std::pow(0.5, l) * (c->mp.boxlen / (double)(c->mp.nx_loc > 0 ? c->mp.nx_loc : c->mp.nx));
     OctIndex& I = idx[l];
     I.nx = (int64_t)c->mp.nx << (l - 1);
     I.ny = (int64_t)c->mp.ny << (l - 1);
     I.nz = (int64_t)c->mp.nz << (l - 1);
     I.v.reserve(n);
-    for (int32_t g : L.h_active) {
-      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "active grid %d out of range", g);
+    // the level's active octs, then its boundary octs (found by the stencil
+    // lookups, never updated)
+    std::vector<int32_t> octs(L.h_active);
+    const int nb = (int)c->btype.size();
+    for (int ib = 0; ib < nb; ib++) {
+      const int64_t k = (int64_t)(l - 1) * nb + ib;
+      octs.insert(octs.end(), c->bgrid.begin() + c->boff[k], c->bgrid.begin() + c->boff[k + 1]);
+    }
+    for (size_t o = 0; o < octs.size(); o++) {
+      const int32_t g = octs[o];
+      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "%s grid %d out of range", o < (size_t)n ? "active" : "boundary", g);
+      if (c->level_of[g - 1] != 0) return fail(RB_ERR_TREE, "grid %d listed twice", g);
+      if (o >= (size_t)n) c->is_bnd[g - 1] = 1;
       const int64_t fc = father[g - 1];
       int64_t* x = &c->coords[(size_t)(g - 1) * 3];
       if (l == 1) {
@@ -477,6 +552,7 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
   RB_CUDA(cudaStreamSynchronize(c->stream));
   c->h_corr_slot.assign((size_t)ngm, -1);
   for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(build_level_tables(c, l, idx));
+  RB_TRY(build_boundary_pairs(c));
   c->have_tree = true;
   c->clock_valid = false;
   return RB_OK;
@@ -570,6 +646,24 @@ int upload_fine_impl(rb_context* c, int l) {
   rb::upload_fine_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
       c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->hp, c->gate);
   RB_CUDA(cudaGetLastError());
+  return RB_OK;
+}
+
+// make_boundary_hydro(l) (hydro/hydro_boundary.f90:5-260): the boundary
+// regions in order, each in two launches (stage, write).
+int boundary_impl(rb_context* c, int l) {
+  const Level& L = c->lv[l];
+  if (c->btype.empty() || L.h_boff.empty()) return RB_OK;
+  for (size_t ib = 0; ib < c->btype.size(); ib++) {
+    const int64_t n = L.h_boff[ib + 1] - L.h_boff[ib];
+    if (n == 0) continue;
+    for (int phase = 0; phase < 2; phase++) {
+      rb::boundary_fill_kernel<<<grid_for(n * 8, 256), 256, 0, c->stream>>>(
+          c->d_uold, L.d_bpair + 2 * L.h_boff[ib], n, c->ncell, c->mp.ncoarse, c->btype[ib], c->hp.smallr,
+          c->d_bbuf, phase, c->gate);
+      RB_CUDA(cudaGetLastError());
+    }
+  }
   return RB_OK;
 }
 
@@ -767,6 +861,7 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   RB_TRY(godunov_impl(c, l, c->dtnew[l], false));
   c->cell_updates += c->lv[l].leaf_cells;
   RB_TRY(set_uold_upload_impl(c, l, nullptr, c->dtnew[l]));
+  RB_TRY(boundary_impl(c, l));  // amr_step.f90:515
   if (l > c->mp.levelmin) {
     if (c->mp.nsubcycle[l - 1] == 1) c->dtnew[l - 1] = c->dtnew[l];
     if (icount == 2) c->dtnew[l - 1] = c->dtold[l] + c->dtnew[l];
@@ -807,6 +902,7 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   RB_CUDA(cudaGetLastError());
   RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l));
   RB_TRY(set_uold_upload_impl(c, l, s + RB_S_DTNEW + l, 0.0));
+  RB_TRY(boundary_impl(c, l));
   if (l > c->mp.levelmin && (c->mp.nsubcycle[l - 1] == 1 || icount == 2)) {
     rb::sched_end_kernel<<<1, 1, 0, c->stream>>>(s, l, c->mp.nsubcycle[l - 1] == 1 ? 1 : 0, icount);
     RB_CUDA(cudaGetLastError());
@@ -1013,7 +1109,7 @@ int rb_destroy(rb_context* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_tree(c);
   dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son);
-  dfree(c->d_divu); dfree(c->d_enew);
+  dfree(c->d_divu); dfree(c->d_enew); dfree(c->d_bbuf);
   dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
   dfree(c->d_flag);
   if (c->h_red) cudaFreeHost(c->h_red);
@@ -1034,6 +1130,48 @@ int rb_sync_tree(rb_context* c, const int32_t* son, const int32_t* father, const
   int rc = sync_tree_impl(c, son, father, nbor, numbl, active_igrid);
   if (rc) free_tree(c);
   return rc;
+}
+
+int rb_set_boundary(rb_context* c, int32_t nboundary, const int32_t* boundary_type, const int32_t* numbb,
+                    const int32_t* boundary_igrid) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (nboundary < 0 || nboundary > 6) return fail(RB_ERR_INVALID, "nboundary=%d must be 0..6", nboundary);
+  if (nboundary > 0 && (!boundary_type || !numbb || !boundary_igrid))
+    return fail(RB_ERR_INVALID, "null boundary array");
+  std::vector<int32_t> bt(boundary_type, boundary_type + nboundary);
+  for (int32_t t : bt)
+    if (!((t >= 1 && t <= 6) || (t >= 11 && t <= 16)))
+      return fail(RB_ERR_INVALID, "boundary_type %d not supported (walls 1-6, free 11-16; imposed 21-26 are not)", t);
+  const int nl = c->mp.nlevelmax;
+  std::vector<int64_t> off((size_t)nl * nboundary + 1, 0);
+  for (int l = 1; l <= nl; l++)
+    for (int ib = 0; ib < nboundary; ib++) {
+      const int64_t k = (int64_t)(l - 1) * nboundary + ib;
+      const int32_t n = numbb[ib + (int64_t)nboundary * (l - 1)];
+      if (n < 0 || n > c->mp.ngridmax) return fail(RB_ERR_INVALID, "numbb(%d,%d)=%d out of range", ib + 1, l, n);
+      off[k + 1] = off[k] + n;
+    }
+  c->btype = bt;
+  c->boff = off;
+  c->bgrid.assign(boundary_igrid, boundary_igrid + off.back());
+  if (!c->have_tree) return RB_OK;
+  // re-index the synchronised tree with the new boundary octs
+  std::vector<int32_t> son(c->son), father(c->father), nbor(c->nbor), numbl(nl), act;
+  for (int l = 1; l <= nl; l++) {
+    numbl[l - 1] = c->lv[l].noct;
+    act.insert(act.end(), c->lv[l].h_active.begin(), c->lv[l].h_active.end());
+  }
+  int rc = sync_tree_impl(c, son.data(), father.data(), nbor.data(), numbl.data(), act.data());
+  if (rc) free_tree(c);
+  return rc;
+}
+
+int rb_make_boundary_hydro(rb_context* c, int l) {
+  RB_TRY(check_level(c, l));
+  RB_TRY(sync_oct(c));
+  RB_TRY(boundary_impl(c, l));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  return RB_OK;
 }
 
 static int upload_impl(rb_context* c, const double* h, double* d) {
@@ -1304,7 +1442,7 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
   double* keep_unew = c->d_unew;
   for (int s = 0; s < rb::kNumTileShapes; s++) {
     const size_t smem = c->precision == RB_PREC_MIXED ? rb::tile_smem_mixed(s) : rb::tile_smem_f64(s);
-    if (smem > 227 * 1024) continue;
+    if (smem > 227 * 1024 || !shape_fits(c, l, s)) continue;
     L.shape = s;
     RB_TRY(build_level_tables(c, l, c->idx));
     if (L.ninterp) {
@@ -1348,7 +1486,9 @@ static int uniform_run_tiles(rb_context* c, int nsteps, int use_graph, double* t
   c->dense_valid = false;
   const int lf = c->finest;
   Level& L = c->lv[lf];
-  if (lf < 1 || !L.complete || L.leaf_cells != (int64_t)L.noct * 8)
+  // (with physical boundaries the level covers the box, not the extended
+  // coarse grid, and the run takes the amr_step sequence below)
+  if (lf < 1 || (!L.complete && c->btype.empty()) || L.leaf_cells != (int64_t)L.noct * 8)
     return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
   for (int l = 1; l < lf; l++)
     if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
@@ -1693,13 +1833,16 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
   if (nsteps < 0) return fail(RB_ERR_INVALID, "nsteps must be >= 0");
   const int lf = c->finest;
   Level& L = c->lv[lf];
-  if (lf < 1 || !L.complete || L.leaf_cells != (int64_t)L.noct * 8)
+  // (with physical boundaries the level covers the box, not the extended
+  // coarse grid, and the run takes the amr_step sequence below)
+  if (lf < 1 || (!L.complete && c->btype.empty()) || L.leaf_cells != (int64_t)L.noct * 8)
     return fail(RB_ERR_STATE, "rb_uniform_run needs a complete, unrefined finest level");
   for (int l = 1; l < lf; l++)
     if (c->lv[l].leaf_cells != 0) return fail(RB_ERR_STATE, "level %d has leaf cells: not a uniform grid", l);
   // with pressure_fix the pdV term and the energy fix come between the update
-  // and the next CFL condition: the amr_step sequence, step by step
-  if (c->hp.pressure_fix) {
+  // and the next CFL condition, and physical boundaries refill their ghost
+  // octs after each step: the amr_step sequence, step by step
+  if (c->hp.pressure_fix || !c->btype.empty()) {
     if (t_io) c->t = *t_io;
     for (int s = 0; s < nsteps; s++) RB_TRY(rb_coarse_step(c, nullptr, nullptr));
     if (t_io) *t_io = c->t;
@@ -1716,7 +1859,8 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
 
 int rb_get_uniform_info(rb_context* c, int* method, int* shape, int* hz, int* items) {
   if (!c) return fail(RB_ERR_INVALID, "null context");
-  const int m = (c->uniform_method == 0 && c->hp.slope_type != 3 && c->hp.difmag == 0.0) ? 0 : 1;
+  const int m =
+      (c->uniform_method == 0 && c->hp.slope_type != 3 && c->hp.difmag == 0.0 && c->btype.empty()) ? 0 : 1;
   if (method) *method = m;
   if (shape) *shape = m == 0 ? c->stream_shape : (c->finest ? c->lv[c->finest].shape : -1);
   if (hz) *hz = m == 0 ? c->stream_hz : 0;

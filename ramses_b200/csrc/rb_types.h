@@ -68,6 +68,10 @@ typedef struct rb_mesh_params {
   int32_t nvector;             /* host vector-sweep width (batch order)    */
   double boxlen;
   int32_t nsubcycle[RB_MAXLEVEL + 1]; /* index = level (1-based)          */
+  int32_t nx_loc;              /* icoarse_max-icoarse_min+1: coarse cells   */
+                               /* across the box without boundary layers   */
+                               /* (dx = 0.5**l * boxlen/nx_loc); 0: nx     */
+  int32_t pad_;                /* zero                                     */
 } rb_mesh_params;
 
 #endif

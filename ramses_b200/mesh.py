@@ -46,10 +46,47 @@ class Octree:
     nbor: np.ndarray         # int32 [6, ngridmax]  (Fortran nbor(ngridmax,6))
     active: list             # active[l] = int32 array of 1-based igrids, l=1..nlevelmax
     coords: list             # coords[l] = int64 (n,3) oct coordinates at level l
+    # physical boundaries (hydro/read_hydro_params.f90:310-420): the coarse
+    # grid carries one layer of boundary coarse cells per bounded side; their
+    # octs are listed per boundary region, not in ``active``
+    nx_loc: int = 0                      # icoarse_max-icoarse_min+1 (0: nx)
+    offset: tuple = (0, 0, 0)            # (icoarse_min, jcoarse_min, kcoarse_min)
+    boundary_type: list = dataclasses.field(default_factory=list)   # [nboundary] codes
+    boundary: list = dataclasses.field(default_factory=list)        # [ib][l] int32 igrids
+    bcoords: list = dataclasses.field(default_factory=list)         # [ib][l] (n,3) coords
 
     @property
     def ncell(self) -> int:
         return self.ncoarse + 8 * self.ngridmax
+
+    @property
+    def scale(self) -> float:
+        """boxlen / nx_loc: the length of one coarse cell (amr/init_amr.f90:44)."""
+        return self.boxlen / (self.nx_loc or self.nx)
+
+    def boundary_concat(self):
+        """(boundary_type int32[nb], off int64[nlevelmax*nb+1], igrid int32[])
+        with the grids of (level l, region ib) at [off[k], off[k+1]),
+        k = (l-1)*nb + ib (0-based ib)."""
+        nb = len(self.boundary_type)
+        off = np.zeros(self.nlevelmax * nb + 1, dtype=np.int64)
+        parts = []
+        for l in range(1, self.nlevelmax + 1):
+            for ib in range(nb):
+                g = self.boundary[ib][l] if l < len(self.boundary[ib]) else np.zeros(0, np.int32)
+                k = (l - 1) * nb + ib
+                off[k + 1] = off[k] + len(g)
+                parts.append(g)
+        cat = np.concatenate(parts) if parts else np.zeros(0, np.int32)
+        return np.asarray(self.boundary_type, np.int32), off, cat.astype(np.int32)
+
+    def boundary_octs(self, level: int):
+        """(igrid int64[n], coords[n,3]) of the boundary octs of ``level``."""
+        g = [self.boundary[ib][level] for ib in range(len(self.boundary)) if level < len(self.boundary[ib])]
+        c = [self.bcoords[ib][level] for ib in range(len(self.bcoords)) if level < len(self.bcoords[ib])]
+        if not g:
+            return np.zeros(0, np.int64), np.zeros((0, 3), np.int64)
+        return np.concatenate(g).astype(np.int64), np.concatenate(c)
 
     def noct(self, level: int) -> int:
         return len(self.active[level]) if level < len(self.active) else 0
@@ -76,7 +113,7 @@ class Octree:
         [z, y, x] (only valid for a complete level)."""
         n = 2 ** level
         a = self.active[level]
-        c = self.coords[level]
+        c = self.coords[level] - np.asarray(self.offset, np.int64) * 2 ** (level - 1)
         if len(a) != (n // 2) ** 3:
             raise ValueError("level %d is not complete" % level)
         out = np.zeros((n, n, n), dtype=np.int64)
@@ -86,16 +123,22 @@ class Octree:
             out[2 * c[:, 2] + iz, 2 * c[:, 1] + iy, 2 * c[:, 0] + ix] = cell
         return out
 
-    def cell_centres(self, level: int):
-        """(cells[1-based], x[n,3]) for every cell of the octs of ``level``."""
+    def cell_centres(self, level: int, boundary: bool = True):
+        """(cells[1-based], x[n,3]) for every cell of the octs of ``level``
+        (with ``boundary``, the boundary octs' cells too), x in user units
+        measured from the box corner (init_flow_fine.f90's skip_loc)."""
         a = self.active[level].astype(np.int64)
         c = self.coords[level]
-        dx = self.boxlen / self.nx * 0.5 ** level
+        if boundary and self.boundary:
+            bg, bc = self.boundary_octs(level)
+            a, c = np.concatenate([a, bg]), np.concatenate([c, bc])
+        dx = self.scale * 0.5 ** level
+        skip = np.asarray(self.offset, np.float64) * self.scale
         cells, xs = [], []
         for ind in range(8):
             off = np.array([ind & 1, (ind >> 1) & 1, (ind >> 2) & 1])
             cells.append(self.ncoarse + ind * self.ngridmax + a)
-            xs.append((2 * c + off + 0.5) * dx)
+            xs.append((2 * c + off + 0.5) * dx - skip)
         return np.concatenate(cells), np.concatenate(xs)
 
 
@@ -319,3 +362,134 @@ def union_refine(*fns) -> Callable[[int, np.ndarray], np.ndarray]:
             out |= f(level, cells)
         return out
     return refine
+
+
+# RAMSES boundary_type codes (hydro/read_hydro_params.f90:355-410): side
+# 1..6 = -x,+x,-y,+y,-z,+z; + 0 for walls (bound_type 1), + 10 for free
+# (zero-gradient, bound_type 2) boundaries.
+BOUND_KINDS = {"reflexive": 0, "outflow": 10}
+
+
+def add_boundaries(tree: Octree, bounds: Sequence[Optional[str]]) -> Octree:
+    """Embed a single-coarse-cell tree (``build_tree``) in RAMSES's extended
+    coarse grid with physical boundaries: per axis, ``bounds[d]`` is None
+    (periodic) or "outflow" / "reflexive" on both sides, which adds one
+    boundary coarse cell per side (nx = 3 for a bounded x). The boundary
+    coarse cells are refined down to levelmin like every coarse cell
+    (amr/refine_utils.f90:86-95); they hold no finer octs, so refinement
+    must stay clear of the box faces (the nesting check below fails
+    otherwise). Boundary regions are ordered -x, +x, -y, +y, -z, +z over the
+    bounded axes; a region spans the coarse cells of its side over the full
+    extent of the axes before it and the interior of the axes after it, as
+    the usual &BOUNDARY_PARAMS do: the later regions cover the edges and
+    corners, whose reference grids then lie in regions filled before."""
+    if tree.nx != 1 or tree.ny != 1 or tree.nz != 1 or tree.boundary:
+        raise ValueError("add_boundaries takes a single-coarse-cell periodic tree")
+    b = [1 if bounds[d] else 0 for d in range(3)]
+    for d in range(3):
+        if bounds[d] and bounds[d] not in BOUND_KINDS:
+            raise ValueError("unknown boundary kind %r" % bounds[d])
+    ext = np.array([1 + 2 * b[0], 1 + 2 * b[1], 1 + 2 * b[2]], np.int64)
+    lmin, lmax = tree.levelmin, tree.nlevelmax
+    regions = []  # (type, axis, side)
+    for d in range(3):
+        if b[d]:
+            for side in (0, 1):
+                regions.append((BOUND_KINDS[bounds[d]] + 2 * d + side + 1, d, side))
+    # oct sets per level in extended coordinates, tagged -1 (interior) or region
+    sets = {}
+    for l in range(1, lmax + 1):
+        h = 2 ** (l - 1)  # octs per coarse cell along an axis
+        inner = tree.coords[l] + np.asarray(b, np.int64) * h if tree.noct(l) else np.zeros((0, 3), np.int64)
+        tags = [np.full(len(inner), -1, np.int64)]
+        allc = [inner]
+        if l <= lmin:
+            g = np.stack(np.meshgrid(np.arange(ext[0] * h), np.arange(ext[1] * h), np.arange(ext[2] * h),
+                                     indexing="ij"), -1).reshape(-1, 3)
+            cc = g // h  # coarse cell of each oct
+            interior = np.ones(len(g), bool)
+            for d in range(3):
+                if b[d]:
+                    interior &= (cc[:, d] >= 1) & (cc[:, d] <= ext[d] - 2)
+            g, cc = g[~interior], cc[~interior]
+            tag = np.full(len(g), -2, np.int64)
+            for ir, (_, d, side) in enumerate(regions):
+                on = cc[:, d] == (0 if side == 0 else ext[d] - 1)
+                for d2 in range(d + 1, 3):  # interior of the axes after this one
+                    if b[d2]:
+                        on &= (cc[:, d2] >= 1) & (cc[:, d2] <= ext[d2] - 2)
+                tag[(tag == -2) & on] = ir
+            assert np.all(tag >= 0)
+            allc.append(g)
+            tags.append(tag)
+        sets[l] = (np.concatenate(allc), np.concatenate(tags))
+    return _assemble_ext(sets, ext, b, regions, lmin, lmax, tree.boxlen)
+
+
+def _assemble_ext(sets, ext, b, regions, levelmin, nlevelmax, boxlen) -> Octree:
+    nx, ny, nz = (int(e) for e in ext)
+    ncoarse = nx * ny * nz
+    ngridmax = int(sum(len(sets[l][0]) for l in sets))
+    son = np.zeros(ncoarse + 8 * ngridmax, dtype=np.int32)
+    father = np.zeros(ngridmax, dtype=np.int32)
+    nbor = np.zeros((6, ngridmax), dtype=np.int32)
+    active = [np.zeros(0, np.int32) for _ in range(nlevelmax + 1)]
+    coords = [np.zeros((0, 3), np.int64) for _ in range(nlevelmax + 1)]
+    bnd = [[np.zeros(0, np.int32) for _ in range(nlevelmax + 1)] for _ in regions]
+    bco = [[np.zeros((0, 3), np.int64) for _ in range(nlevelmax + 1)] for _ in regions]
+
+    def key(c, l):
+        X, Y = nx * 2 ** (l - 1), ny * 2 ** (l - 1)
+        return c[:, 0] + X * (c[:, 1] + Y * c[:, 2])
+
+    g0 = 0
+    lookup = None  # level l-1: (sorted keys, igrid)
+    for l in range(1, nlevelmax + 1):
+        oc, tag = sets.get(l, (np.zeros((0, 3), np.int64), np.zeros(0, np.int64)))
+        if len(oc) == 0:
+            break
+        E = ext * 2 ** (l - 1)  # octs per axis at level l; cells at level l-1
+        if l == 1:
+            order = np.lexsort((oc[:, 0], oc[:, 1], oc[:, 2]))
+        else:
+            ks, igr = lookup
+            pos = np.searchsorted(ks, key(oc // 2, l - 1))
+            pg = igr[pos]
+            slot = (oc[:, 0] & 1) + 2 * (oc[:, 1] & 1) + 4 * (oc[:, 2] & 1)
+            order = np.lexsort((slot, pg))
+        oc, tag = oc[order], tag[order]
+        ig = np.arange(g0 + 1, g0 + 1 + len(oc), dtype=np.int64)
+
+        def cell_of(cc):
+            cc = cc % E
+            if l == 1:
+                return 1 + cc[:, 0] + nx * (cc[:, 1] + ny * cc[:, 2])
+            ks, igr = lookup
+            k = key(cc // 2, l - 1)
+            pos = np.searchsorted(ks, k)
+            if np.any(pos >= len(ks)) or np.any(ks[np.minimum(pos, len(ks) - 1)] != k):
+                raise ValueError("refinement reaches the boundary layer at level %d "
+                                 "(no boundary octs below levelmin)" % l)
+            slot = (cc[:, 0] & 1) + 2 * (cc[:, 1] & 1) + 4 * (cc[:, 2] & 1)
+            return ncoarse + slot * ngridmax + igr[pos]
+
+        fc = cell_of(oc)
+        father[ig - 1] = fc
+        son[fc - 1] = ig
+        for j in range(6):
+            step = np.zeros(3, np.int64)
+            step[j // 2] = 1 if (j % 2) else -1
+            nbor[j, ig - 1] = cell_of(oc + step)
+        active[l] = ig[tag == -1].astype(np.int32)
+        coords[l] = oc[tag == -1]
+        for ir in range(len(regions)):
+            bnd[ir][l] = ig[tag == ir].astype(np.int32)
+            bco[ir][l] = oc[tag == ir]
+        k = key(oc, l)
+        srt = np.argsort(k)
+        lookup = (k[srt], ig[srt])
+        g0 += len(oc)
+    return Octree(nx=nx, ny=ny, nz=nz, ncoarse=ncoarse, ngridmax=ngridmax, nlevelmax=nlevelmax,
+                  levelmin=levelmin, boxlen=float(boxlen), son=son, father=father, nbor=nbor,
+                  active=active, coords=coords, nx_loc=1, offset=tuple(b),
+                  boundary_type=[r[0] for r in regions], boundary=bnd, bcoords=bco)

@@ -25,6 +25,7 @@ module rb_b200
      integer(c_int32_t) :: nx, ny, nz, ncoarse, ngridmax, nlevelmax, levelmin, nvector
      real(c_double) :: boxlen
      integer(c_int32_t) :: nsubcycle(0:32)
+     integer(c_int32_t) :: nx_loc, pad_
   end type rb_mesh_params_t
 
   type, bind(c) :: rb_refine_params_t
@@ -48,6 +49,17 @@ module rb_b200
        type(c_ptr), value :: ctx
        integer(c_int32_t), intent(in) :: son(*), father(*), nbor(*), numbl(*), active(*)
      end function rb_sync_tree
+     integer(c_int) function rb_set_boundary(ctx, nb, btype, numbb, igrid) bind(c, name='rb_set_boundary')
+       import :: c_int, c_ptr, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), value :: nb
+       integer(c_int32_t), intent(in) :: btype(*), numbb(*), igrid(*)
+     end function rb_set_boundary
+     integer(c_int) function rb_make_boundary_hydro(ctx, ilevel) bind(c, name='rb_make_boundary_hydro')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: ilevel
+     end function rb_make_boundary_hydro
      integer(c_int) function rb_upload_state(ctx, uold) bind(c, name='rb_upload_state')
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: ctx
@@ -142,6 +154,7 @@ contains
     mp%nx = nx; mp%ny = ny; mp%nz = nz; mp%ncoarse = ncoarse; mp%ngridmax = ngridmax
     mp%nlevelmax = nlevelmax; mp%levelmin = levelmin; mp%nvector = nvector
     mp%boxlen = boxlen
+    mp%nx_loc = icoarse_max - icoarse_min + 1; mp%pad_ = 0
     mp%nsubcycle = 2
     do l = 1, min(nlevelmax, 32)
        mp%nsubcycle(l) = nsubcycle(l)
@@ -154,9 +167,9 @@ contains
   subroutine rb_b200_push
     use amr_commons
     use hydro_commons
-    integer(c_int32_t), allocatable :: numbl(:), act(:)
+    integer(c_int32_t), allocatable :: numbl(:), act(:), numbb(:,:), bgrid(:), btype(:)
     integer(c_int64_t) :: stamp
-    integer :: l, i, n
+    integer :: l, i, n, ib
     call rb_b200_init
     stamp = 0
     do l = 1, nlevelmax
@@ -180,8 +193,31 @@ contains
              act(n) = active(l)%igrid(i)
           end do
        end do
+       ! physical boundaries: boundary(ibound,ilevel)%igrid, level by level
+       allocate(numbb(max(nboundary, 1), nlevelmax))
+       n = 0
+       do l = 1, nlevelmax
+          do ib = 1, nboundary
+             numbb(ib, l) = boundary(ib, l)%ngrid
+             n = n + boundary(ib, l)%ngrid
+          end do
+       end do
+       allocate(bgrid(max(n, 1)), btype(max(nboundary, 1)))
+       btype = 0
+       if (nboundary > 0) btype(1:nboundary) = boundary_type(1:nboundary)
+       n = 0
+       do l = 1, nlevelmax
+          do ib = 1, nboundary
+             do i = 1, boundary(ib, l)%ngrid
+                n = n + 1
+                bgrid(n) = boundary(ib, l)%igrid(i)
+             end do
+          end do
+       end do
+       call rb_b200_check(rb_set_boundary(rb_ctx, int(nboundary, c_int32_t), btype, numbb, bgrid), &
+            & 'rb_set_boundary')
        call rb_b200_check(rb_sync_tree(rb_ctx, son, father, nbor, numbl, act), 'rb_sync_tree')
-       deallocate(numbl, act)
+       deallocate(numbl, act, numbb, bgrid, btype)
        rb_tree_stamp = stamp
     end if
     call rb_b200_check(rb_upload_state(rb_ctx, uold), 'rb_upload_state')

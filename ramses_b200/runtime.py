@@ -47,7 +47,8 @@ class MeshParamsC(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
                 ("ncoarse", ctypes.c_int32), ("ngridmax", ctypes.c_int32), ("nlevelmax", ctypes.c_int32),
                 ("levelmin", ctypes.c_int32), ("nvector", ctypes.c_int32), ("boxlen", ctypes.c_double),
-                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1))]
+                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1)), ("nx_loc", ctypes.c_int32),
+                ("pad_", ctypes.c_int32)]
 
 
 class RBError(RuntimeError):
@@ -69,6 +70,8 @@ _PROTOS = {
                                  ctypes.POINTER(ctypes.c_void_p)]),
     "rb_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rb_sync_tree": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32, _P32]),
+    "rb_set_boundary": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, _P32, _P32, _P32]),
+    "rb_make_boundary_hydro": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_upload_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_pressure_fix": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
@@ -159,6 +162,7 @@ def mesh_params_c(tree: Octree, nsubcycle: Optional[Sequence[int]] = None, nvect
     m.ncoarse, m.ngridmax = tree.ncoarse, tree.ngridmax
     m.nlevelmax, m.levelmin, m.nvector = tree.nlevelmax, tree.levelmin, nvector
     m.boxlen = tree.boxlen
+    m.nx_loc = getattr(tree, "nx_loc", 0)
     ns = list(nsubcycle) if nsubcycle is not None else [2] * (MAXLEVEL + 1)
     for i in range(MAXLEVEL + 1):
         m.nsubcycle[i] = ns[i] if i < len(ns) else 2
@@ -196,6 +200,11 @@ class Solver:
         self.sync_tree()
         if uold is not None:
             self.upload_state(uold)
+            # physical boundaries: one fill per level, as init_flow_fine does
+            # (hydro/init_flow_fine.f90:19)
+            if tree.boundary_type:
+                for l in range(1, tree.nlevelmax + 1):
+                    self.make_boundary_hydro(l)
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -225,8 +234,15 @@ class Solver:
         nbor = np.ascontiguousarray(t.nbor, np.int32)
         numbl = np.array([t.noct(l) for l in range(1, t.nlevelmax + 1)], np.int32)
         act, _ = t.active_concat()
+        bt, boff, bg = t.boundary_concat()
+        numbb = np.diff(boff).astype(np.int32)
+        _check(load().rb_set_boundary(self._h, len(bt), _ptr(bt, _P32), _ptr(numbb, _P32), _ptr(bg, _P32)),
+               "rb_set_boundary")
         _check(load().rb_sync_tree(self._h, _ptr(son, _P32), _ptr(father, _P32), _ptr(nbor, _P32),
                                    _ptr(numbl, _P32), _ptr(act, _P32)), "rb_sync_tree")
+
+    def make_boundary_hydro(self, ilevel: int):
+        _check(load().rb_make_boundary_hydro(self._h, ilevel), "rb_make_boundary_hydro")
 
     def upload_state(self, uold: np.ndarray):
         u = np.ascontiguousarray(uold, np.float64)
