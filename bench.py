@@ -63,6 +63,8 @@ def parse():
                          "(profiling runs replay the autotuned choice without its probe launches)")
     ap.add_argument("--pressure-fix", type=float, default=None, metavar="BETA",
                     help="AMR runs with pressure_fix on and beta_fix=BETA (the dual-energy fix)")
+    ap.add_argument("--periodic", action="store_true",
+                    help="Sedov AMR run on a periodic box instead of outflow boundaries")
     ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
                     help="instead of the headline, time device-scheduled coarse steps (rb_run) on a static AMR "
                          "tree: sedov = Sedov levels 6-9 refined on a shell, clumps = blast-clump levels 7-10")
@@ -265,7 +267,7 @@ def leaf_cell_index(tree):
     return np.concatenate(out)
 
 
-def amr_workload(name):
+def amr_workload(name, periodic=False):
     """Static AMR trees of the Sedov and blast-clump configurations.
     sedov: levels 6-9; levels 7-9 on a shell of radius 0.25 around the box
     centre (where the shock of E=1 in rho=1 sits near t=0.02) plus the
@@ -293,6 +295,15 @@ def amr_workload(name):
         desc = ("blast-clump: 32 seeded clumps (contrast 100) + Sedov E=10, levels 7-10 (static: gradient 0.05 "
                 "of the initial state), hllc, slope_type=2, courant 0.8, nsubcycle 2")
     tree = mesh.build_tree(lmin, lmax, ref)
+    if name == "sedov" and not periodic:
+        # outflow (free, bound_type 2) boundaries on all six faces: one layer
+        # of boundary coarse cells, refined to levelmin, refilled after every
+        # levelmin step
+        tree = mesh.add_boundaries(tree, ("outflow",) * 3)
+        desc += ", outflow boundaries on all faces (%d boundary octs)" % sum(
+            len(g[l]) for g in tree.boundary for l in range(1, lmax + 1))
+    else:
+        desc += ", periodic"
     return tree, hp, ics.fill_all_levels(tree, prim, hp.gamma), desc
 
 
@@ -302,7 +313,7 @@ def run_amr(args):
     from ramses_b200 import runtime
     runtime.load()
     t0 = time.perf_counter()
-    tree, hp, u, desc = amr_workload(args.amr)
+    tree, hp, u, desc = amr_workload(args.amr, args.periodic)
     if args.pressure_fix is not None:
         hp.pressure_fix = True
         hp.beta_fix = args.pressure_fix
