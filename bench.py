@@ -333,7 +333,8 @@ def run_amr(args):
         s.synchronize()
         sync = {"sync_tree_s": t1s - t0s, "upload_state_s": time.perf_counter() - t1s}
         for l in levels:
-            s.set_tile_shape(l, args.tile_shape)  # -1: autotuned per level
+            if l >= tree.levelmin:  # the stepped levels
+                s.set_tile_shape(l, args.tile_shape)  # -1: autotuned per level
         s.run(max_steps=args.warmup)
         s.synchronize()
         before = s.cell_updates

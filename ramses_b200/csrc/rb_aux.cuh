@@ -810,7 +810,7 @@ static __global__ void dense_to_oct_kernel(const double* __restrict__ d, double*
 }
 
 // make_boundary_hydro for one boundary region (hydro/hydro_boundary.f90:
-// 118-208), thread = (boundary oct, cell). Boundary type bt: side
+// 118-208), one (boundary oct, cell) per grid-stride iteration. Boundary type bt: side
 // dir = bt % 10 (1..6 = -x,+x,-y,+y,-z,+z), walls bt < 10, free boundaries
 // 11..16. Cell ind of the boundary oct takes cell ind_ref of the reference oct:
 // the mirror cell across the face (walls) or the cell of the reference oct
@@ -823,48 +823,48 @@ static __global__ void boundary_fill_kernel(double* __restrict__ u, const int32_
                                      int64_t ncell, int32_t ncoarse, int bt, double smallr,
                                      double* __restrict__ buf, int phase, const double* __restrict__ gate) {
   RB_GATE(gate);
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n * 8) return;
-  const int64_t p = i >> 3;
-  const int ind = (int)(i & 7);  // ind - 1
   const int a = (bt % 10 - 1) >> 1;  // axis of the face
   const bool wall = bt < 10;
-  double q[5];
-  double* b = buf + (size_t)i * 5;
-  if (phase == 0) {
-    const int side = (bt % 10 - 1) & 1;  // 0: lower face, 1: upper face
-    const int ind_ref = wall ? (ind ^ (1 << a)) : (side ? (ind | (1 << a)) : (ind & ~(1 << a)));
-    const int64_t rc = ncoarse + 8 * (int64_t)pairs[2 * p + 1] + ind_ref;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * 8; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i >> 3;
+    const int ind = (int)(i & 7);  // ind - 1
+    double q[5];
+    double* b = buf + (size_t)i * 5;
+    if (phase == 0) {
+      const int side = (bt % 10 - 1) & 1;  // 0: lower face, 1: upper face
+      const int ind_ref = wall ? (ind ^ (1 << a)) : (side ? (ind | (1 << a)) : (ind & ~(1 << a)));
+      const int64_t rc = ncoarse + 8 * (int64_t)pairs[2 * p + 1] + ind_ref;
 #pragma unroll
-    for (int v = 0; v < 5; v++) q[v] = u[v * ncell + rc];
-    if (wall) {
-      q[1 + a] = q[1 + a] * -1.0;
+      for (int v = 0; v < 5; v++) q[v] = u[v * ncell + rc];
+      if (wall) {
+        q[1 + a] = q[1 + a] * -1.0;
+      } else {
+        double ekin = 0.0;
+        const double d = fmx(q[0], smallr);
+        for (int idim = 1; idim <= 3; idim++) {
+          const double vel = q[idim] / d;
+          ekin = ekin + 0.5 * d * (vel * vel);
+        }
+        q[4] = q[4] - ekin;
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++) b[v] = q[v];
     } else {
-      double ekin = 0.0;
-      const double d = fmx(q[0], smallr);
-      for (int idim = 1; idim <= 3; idim++) {
-        const double vel = q[idim] / d;
-        ekin = ekin + 0.5 * d * (vel * vel);
+      const int64_t gc = ncoarse + 8 * (int64_t)pairs[2 * p] + ind;
+#pragma unroll
+      for (int v = 0; v < 5; v++) q[v] = b[v];
+      if (!wall) {
+        double ekin = 0.0;
+        const double d = fmx(q[0], smallr);
+        for (int idim = 1; idim <= 3; idim++) {
+          const double vel = q[idim] / d;
+          ekin = ekin + 0.5 * d * (vel * vel);
+        }
+        q[4] = q[4] + ekin;
       }
-      q[4] = q[4] - ekin;
+#pragma unroll
+      for (int v = 0; v < 5; v++) u[v * ncell + gc] = q[v];
     }
-#pragma unroll
-    for (int v = 0; v < 5; v++) b[v] = q[v];
-  } else {
-    const int64_t gc = ncoarse + 8 * (int64_t)pairs[2 * p] + ind;
-#pragma unroll
-    for (int v = 0; v < 5; v++) q[v] = b[v];
-    if (!wall) {
-      double ekin = 0.0;
-      const double d = fmx(q[0], smallr);
-      for (int idim = 1; idim <= 3; idim++) {
-        const double vel = q[idim] / d;
-        ekin = ekin + 0.5 * d * (vel * vel);
-      }
-      q[4] = q[4] + ekin;
-    }
-#pragma unroll
-    for (int v = 0; v < 5; v++) u[v * ncell + gc] = q[v];
   }
 }
 

@@ -125,3 +125,23 @@ def test_mixed_close_to_fp64(cuda_lib):
         idx = tree.cell_index(5) - 1
         ra, rb_ = a.download_state()[0][idx], b.download_state()[0][idx]
         assert np.abs(ra - rb_).sum() / np.abs(ra).sum() < 1e-5
+
+
+def test_large_region_fill_bitwise(cuda_lib, oracle_lib):
+    """Regions larger than one launch's threads (levelmin 6: the z regions
+    hold 294,912 octs each)."""
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+    tree = mesh.add_boundaries(mesh.build_tree(6, 6, None), ("outflow", "reflexive", "outflow"))
+    assert max(len(g[6]) for g in tree.boundary) > 148 * 32 * 256 // 8
+    u = ics.fill_all_levels(tree, ics.sedov_prim(6), hp.gamma)
+    rng = np.random.default_rng(5)
+    for ib in range(len(tree.boundary_type)):
+        g = tree.boundary[ib][6].astype(np.int64)
+        cells = (tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + g[None, :]).reshape(-1)
+        u[:, cells - 1] = 1.0 + rng.random((5, len(cells)))
+    orc = oracle.OracleRun(tree, hp, u)
+    with runtime.Solver(tree, hp, uold=u) as s:
+        check(tree, s.download_state(), orc.uold)
+        orc.coarse_step()
+        s.coarse_step()
+        check(tree, s.download_state(), orc.uold)
