@@ -63,6 +63,8 @@ def parse():
                          "(profiling runs replay the autotuned choice without its probe launches)")
     ap.add_argument("--pressure-fix", type=float, default=None, metavar="BETA",
                     help="AMR runs with pressure_fix on and beta_fix=BETA (the dual-energy fix)")
+    ap.add_argument("--scheme", choices=["muscl", "plmde"], default="muscl",
+                    help="predictor of the headline workload (plmde runs the run-time scheme variant)")
     ap.add_argument("--periodic", action="store_true",
                     help="Sedov AMR run on a periodic box instead of outflow boundaries")
     ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
@@ -86,20 +88,21 @@ def make_solver(runtime, tree, hp, precision, u, args):
     return s
 
 
-def workload(level, seed):
+def workload(level, seed, scheme="muscl"):
     from ramses_b200 import ics, mesh
     from ramses_b200.params import HydroParams
-    hp = HydroParams(gamma=1.001, riemann="hllc", slope_type=2, courant_factor=0.8)
+    hp = HydroParams(gamma=1.001, riemann="hllc", slope_type=2, courant_factor=0.8, scheme=scheme)
     tree = mesh.uniform_tree(level)
     q = ics.turbulent_box_prim_grid(2 ** level, seed=seed, gamma=hp.gamma)
     u = ics.fill_uniform_level_from_grid(tree, level, q, hp.gamma)
     return tree, hp, u
 
 
-def config_dict(level, n_gpus):
+def config_dict(level, n_gpus, scheme="muscl"):
     n = 2 ** level
     return {"workload": "turbulent box %d^3 uniform (levelmin=levelmax=%d), periodic, hllc, slope_type=2, "
-                        "gamma=1.001, Mach 5, courant 0.8" % (n, level),
+                        "gamma=1.001, Mach 5, courant 0.8%s" % (n, level, "" if scheme == "muscl" else
+                                                                ", scheme=" + scheme),
             "cells": n ** 3, "riemann": "hllc", "slope_type": 2, "precision": "fp32-mixed",
             "l2_policy": "inputs larger than L2 (state %.0f MB per copy > 126 MB L2)" % (n ** 3 * 40 / 1e6),
             "parallelism": "replicas" if n_gpus > 1 else "single-gpu"}
@@ -226,13 +229,13 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    tree, hp, u = workload(args.level, args.seed)
+    tree, hp, u = workload(args.level, args.seed, args.scheme)
     nocts = min(args.cpu_sample_octs, tree.noct(args.level))
     value, cores, desc = cpu_sample(tree, hp, u, nocts, args.steps, args.warmup)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": nocts * 8 / value * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_dict(args.level, 1) | {"precision": "fp64", "sample_octs": nocts},
+            "config": config_dict(args.level, 1, args.scheme) | {"precision": "fp64", "sample_octs": nocts},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -431,7 +434,7 @@ def main():
     runtime.load()
     runtime.select_device(local)
 
-    tree, hp, u = workload(args.level, args.seed)
+    tree, hp, u = workload(args.level, args.seed, args.scheme)
     level = args.level
     cells = tree.leaf_cells(level)
 
@@ -524,7 +527,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": run_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": config_dict(level, world),
+            "config": config_dict(level, world, args.scheme),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "steps": args.e2e_steps,
                     "path": "rb_upload_state + rb_uniform_run(1) + rb_download_state, pinned host buffers"},

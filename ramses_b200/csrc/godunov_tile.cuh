@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
   cp_async_commit();
 
   // ---- A. gather + ctoprim ------------------------------------------------
-  const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
+  const int slope_type = ST >= 0 ? ST % 10 : a.hp.slope_type;
   const bool slope27 = (slope_type == 3);
   // the 27-point slopes and the corner divergence of difmag read the edge and
   // corner cells of the stencil too
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       }
     }
     Prim<R> sp[3], sm[3];
-    trace_sel<R, RS>(q0, dq, c, dtd, sp, sm, mask);
+    trace_sel<R, RS, ST>(q0, dq, c, dtd, sp, sm, mask);
     // store: qm of direction d at face index (coord+1), qp at face index coord
 #pragma unroll
     for (int d = 0; d < 3; d++) {

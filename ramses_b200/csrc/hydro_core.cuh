@@ -333,11 +333,16 @@ __device__ __forceinline__ void trace_plmde_cell(const Prim<R>& q, const R dq[5]
   }
 }
 
-// The predictor of the scheme: MUSCL-Hancock, or PLMDE in the run-time
-// variant (RS == 0) when c.scheme says so.
-template <typename R, int RS>
+// The predictor of the scheme: PLMDE in the compiled PLMDE variants
+// (ST >= 10, slope type ST % 10), chosen from c.scheme in the run-time
+// variant (RS == 0), MUSCL-Hancock otherwise.
+template <typename R, int RS, int ST = -1>
 __device__ __forceinline__ void trace_sel(const Prim<R>& q, const R dq[5][3], const Consts<R>& c, const R dtd[3],
                                           Prim<R> qp[3], Prim<R> qm[3], unsigned dirmask) {
+  if constexpr (ST >= 10) {
+    trace_plmde_cell<R>(q, dq, c.gamma, c.smallr, dtd, qp, qm, dirmask);
+    return;
+  }
   if constexpr (RS == 0) {
     if (c.scheme == RB_SCHEME_PLMDE) {
       trace_plmde_cell<R>(q, dq, c.gamma, c.smallr, dtd, qp, qm, dirmask);

@@ -114,7 +114,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
   const int64_t vstr = plane * a.nz;
   const Consts<R> c = make_consts<R>(a.hp);
   const double dt = *a.dt_dev;
-  const int slope_type = ST >= 0 ? ST : a.hp.slope_type;
+  const int slope_type = ST >= 0 ? ST % 10 : a.hp.slope_type;
   const R dtdx = (R)(dt / a.dx);
   const R dtd[3] = {dtdx, dtdx, dtdx};
 
@@ -229,7 +229,7 @@ __device__ __forceinline__ void stream_step_body(const StreamArgs& a, const int 
     }
     // the ring columns (whole warps after the interior ones) solve no z face
     Prim<R> sp[3], sm[3];
-    trace_sel<R, RS>(q_0, dq, c, dtd, sp, sm, inner ? 7u : 3u);
+    trace_sel<R, RS, ST>(q_0, dq, c, dtd, sp, sm, inner ? 7u : 3u);
     if (valid) {
       const int o = slot;
       xm[o] = sm[0].r; xm[NC + o] = sm[0].u; xm[2 * NC + o] = sm[0].v; xm[3 * NC + o] = sm[0].w; xm[4 * NC + o] = sm[0].p;
