@@ -127,3 +127,32 @@ def test_mesh_builder_rules():
                 po = cc // 2
                 keys = tree.coords[l - 1]
                 assert ((keys == po).all(axis=1)).any()
+
+
+def test_boundary_tree_layout():
+    """mesh.add_boundaries: RAMSES's extended coarse grid (one boundary coarse
+    cell per bounded side), regions ordered -x,+x,-y,+y,-z,+z with the later
+    regions covering edges and corners, every boundary oct's reference oct
+    (son(nbor(igrid,inbor))) present at its level, cell centres measured from
+    the box corner."""
+    import numpy as np
+
+    from ramses_b200 import mesh
+    t = mesh.add_boundaries(mesh.build_tree(3, 3, None), ("outflow", None, "reflexive"))
+    assert (t.nx, t.ny, t.nz, t.nx_loc, t.offset) == (3, 1, 3, 1, (1, 0, 1))
+    assert t.boundary_type == [11, 12, 5, 6]
+    # x regions: the x column over the interior z; z regions: all x
+    assert [len(g[3]) for g in t.boundary] == [64, 64, 192, 192]
+    for ib, bt in enumerate(t.boundary_type):
+        d = bt % 10
+        inbor = d + 1 if d % 2 else d - 1
+        for l in range(1, 4):
+            g = t.boundary[ib][l]
+            ref = t.son[t.nbor[inbor - 1, g - 1] - 1]
+            assert np.all(ref > 0)
+    cells, x = t.cell_centres(3, boundary=False)
+    assert x.min() > 0 and x.max() < 1 and len(cells) == 8 * 64
+    _, xb = t.cell_centres(3)
+    assert xb[:, 0].min() < 0 and xb[:, 2].max() > 1 and np.all((xb[:, 1] > 0) & (xb[:, 1] < 1))
+    with pytest.raises(ValueError):
+        mesh.add_boundaries(mesh.build_tree(3, 3, None), ("inflow", None, None))

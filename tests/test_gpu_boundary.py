@@ -145,3 +145,20 @@ def test_large_region_fill_bitwise(cuda_lib, oracle_lib):
         orc.coarse_step()
         s.coarse_step()
         check(tree, s.download_state(), orc.uold)
+
+
+def test_boundary_argument_checks(cuda_lib):
+    """Imposed boundaries are rejected; a tile shape that would hold octs of
+    the box and of the boundary layer is refused."""
+    import ctypes
+    tree, hp, u = tube(3)
+    with runtime.Solver(tree, hp, uold=u) as s:
+        L = runtime.load()
+        bt = np.array([21], np.int32)
+        nb = np.zeros(tree.nlevelmax, np.int32)
+        g = np.zeros(1, np.int32)
+        P = ctypes.POINTER(ctypes.c_int32)
+        rc = L.rb_set_boundary(s._h, 1, bt.ctypes.data_as(P), nb.ctypes.data_as(P), g.ctypes.data_as(P))
+        assert rc == 1  # RB_ERR_INVALID
+        with pytest.raises(runtime.RBError):
+            s.set_tile_shape(1, 3)  # 4x4x2 octs on a level with one oct per coarse cell
