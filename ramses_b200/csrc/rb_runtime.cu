@@ -55,6 +55,8 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
     return fail(RB_ERR_INVALID, "bad ngridmax/levelmin/nlevelmax");
   if (mp->nvector < 1) return fail(RB_ERR_INVALID, "nvector must be positive");
   if (!(mp->boxlen > 0.0)) return fail(RB_ERR_INVALID, "boxlen must be positive");
+  if (mp->nx_loc < 0 || mp->nx_loc > mp->nx)
+    return fail(RB_ERR_INVALID, "nx_loc=%d must lie in 0..nx (0: nx)", mp->nx_loc);
   return RB_OK;
 }
 
