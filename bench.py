@@ -317,6 +317,9 @@ def run_amr(args):
     runtime.load()
     t0 = time.perf_counter()
     tree, hp, u, desc = amr_workload(args.amr, args.periodic)
+    if args.scheme != "muscl":
+        hp.scheme = args.scheme
+        desc += ", scheme=" + args.scheme
     if args.pressure_fix is not None:
         hp.pressure_fix = True
         hp.beta_fix = args.pressure_fix
