@@ -112,3 +112,16 @@ def test_mixed_close_to_fp64(cuda_lib, path):
         _, ra = leaf_values(tree, a.download_state())
         _, rb_ = leaf_values(tree, b.download_state())
         assert np.abs(ra[0] - rb_[0]).sum() / np.abs(ra[0]).sum() < 1e-5
+
+
+def test_compiled_variant_with_pressure_fix_bitwise(cuda_lib, oracle_lib):
+    """hllc + minmod + PLMDE with the dual-energy fix: the compiled PLMDE
+    variant of the pressure_fix tile kernel."""
+    tree, hp, u = sedov_amr(3, 5)
+    hp = _plm(hp, pressure_fix=True, beta_fix=0.5)
+    orc = oracle.OracleRun(tree, hp, u)
+    with runtime.Solver(tree, hp, uold=u) as s:
+        for _ in range(3):
+            orc.coarse_step()
+            s.coarse_step()
+        np.testing.assert_array_equal(s.download_state(), orc.uold)
