@@ -72,8 +72,9 @@ int rb_sync_tree(rb_context *ctx, const int32_t *son, const int32_t *father, con
  * boundary(ibound,ilevel)%igrid concatenated level by level, boundary by
  * boundary within a level. The boundary octs are found by the stencil
  * gathers and never updated; mesh params nx_loc gives the coarse cells
- * across the box. Before or after rb_sync_tree (a synchronised tree is
- * re-indexed). nboundary = 0 restores a periodic box. */
+ * across the box. Call it before rb_sync_tree, which takes the lists with
+ * the tree; a tree synchronised earlier is dropped and must be synchronised
+ * again. nboundary = 0 restores a periodic box. */
 int rb_set_boundary(rb_context *ctx, int32_t nboundary, const int32_t *boundary_type, const int32_t *numbb,
                     const int32_t *boundary_igrid);
 /* make_boundary_hydro(ilevel): fill the boundary octs of ilevel from their

@@ -1156,16 +1156,9 @@ int rb_set_boundary(rb_context* c, int32_t nboundary, const int32_t* boundary_ty
   c->btype = bt;
   c->boff = off;
   c->bgrid.assign(boundary_igrid, boundary_igrid + off.back());
-  if (!c->have_tree) return RB_OK;
-  // re-index the synchronised tree with the new boundary octs
-  std::vector<int32_t> son(c->son), father(c->father), nbor(c->nbor), numbl(nl), act;
-  for (int l = 1; l <= nl; l++) {
-    numbl[l - 1] = c->lv[l].noct;
-    act.insert(act.end(), c->lv[l].h_active.begin(), c->lv[l].h_active.end());
-  }
-  int rc = sync_tree_impl(c, son.data(), father.data(), nbor.data(), numbl.data(), act.data());
-  if (rc) free_tree(c);
-  return rc;
+  // the lists belong to the next rb_sync_tree: a synchronised tree is dropped
+  if (c->have_tree) free_tree(c);
+  return RB_OK;
 }
 
 int rb_make_boundary_hydro(rb_context* c, int l) {
