@@ -233,6 +233,14 @@ int rb_server_submit_dense(rb_server *srv, int32_t nx, int32_t ny, int32_t nz, d
 int rb_server_submit_octree(rb_server *srv, const rb_mesh_params *mp, const int32_t *son, const int32_t *father,
                             const int32_t *nbor, const int32_t *numbl, const int32_t *active_igrid,
                             const double *uold, double t_end, int64_t max_steps, double *result, int64_t *id);
+/* The same with physical boundaries (rb_set_boundary's lists, kept by the
+ * caller until the request completes); the boundary octs are filled once at
+ * admission and after every level step. */
+int rb_server_submit_octree_bounded(rb_server *srv, const rb_mesh_params *mp, const int32_t *son,
+                                    const int32_t *father, const int32_t *nbor, const int32_t *numbl,
+                                    const int32_t *active_igrid, int32_t nboundary, const int32_t *boundary_type,
+                                    const int32_t *numbb, const int32_t *boundary_igrid, const double *uold,
+                                    double t_end, int64_t max_steps, double *result, int64_t *id);
 /* Admit, enqueue one round of steps, retire finished problems. Up to max_ids
  * completed request ids are written to done_ids (the rest on later calls). */
 int rb_server_progress(rb_server *srv, int64_t *done_ids, int max_ids, int *ndone);

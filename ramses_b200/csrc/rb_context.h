@@ -203,4 +203,6 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp);
 int run_async_begin(rb_context* c, double t_end, int64_t max_coarse);
 int run_async_chunk(rb_context* c, int chunk, bool use_graph);
 int run_async_end(rb_context* c, int64_t* coarse_out);
+// make_boundary_hydro of every level, queued on the context's stream (rb_runtime.cu)
+int make_boundary_all(rb_context* c);
 }  // namespace rbi

@@ -669,6 +669,11 @@ int boundary_impl(rb_context* c, int l) {
   return RB_OK;
 }
 
+int make_boundary_all(rb_context* c) {
+  for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(boundary_impl(c, l));
+  return RB_OK;
+}
+
 // Write the dense mirror of the finest level back into the oct layout and
 // restrict it to the coarser levels (amr_step.f90:442, adaptive_loop.f90),
 // when the dense mirror is ahead.

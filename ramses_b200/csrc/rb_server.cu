@@ -53,6 +53,8 @@ struct Request {
   // octree
   rb_mesh_params mp{};
   const int32_t *son = nullptr, *father = nullptr, *nbor = nullptr, *numbl = nullptr, *active = nullptr;
+  int32_t nboundary = 0;  // physical boundaries of an octree problem (rb_set_boundary's lists)
+  const int32_t *btype = nullptr, *numbb = nullptr, *bgrid = nullptr;
   rb_context* ctx = nullptr;
   cudaEvent_t ev = nullptr;
   bool chunk_in_flight = false;
@@ -214,8 +216,10 @@ int admit_tree(rb_server* s, Request* r) {
   r->ctx = c;
   s->in_use += r->bytes;
   int rc;
-  if ((rc = rb_sync_tree(c, r->son, r->father, r->nbor, r->numbl, r->active)) ||
-      (rc = rb_upload_state(c, r->h_in)) || (rc = run_async_begin(c, r->t_end, r->max_steps))) {
+  if ((r->nboundary && (rc = rb_set_boundary(c, r->nboundary, r->btype, r->numbb, r->bgrid))) ||
+      (rc = rb_sync_tree(c, r->son, r->father, r->nbor, r->numbl, r->active)) ||
+      (rc = rb_upload_state(c, r->h_in)) || (r->nboundary && (rc = make_boundary_all(c))) ||
+      (rc = run_async_begin(c, r->t_end, r->max_steps))) {
     release_tree(s, r);
     return rc;
   }
@@ -562,6 +566,20 @@ int rb_server_submit_octree(rb_server* s, const rb_mesh_params* mp, const int32_
   s->all[r->id] = r;
   s->queue.push_back(r);
   *id_out = r->id;
+  return RB_OK;
+}
+
+int rb_server_submit_octree_bounded(rb_server* s, const rb_mesh_params* mp, const int32_t* son,
+                                    const int32_t* father, const int32_t* nbor, const int32_t* numbl,
+                                    const int32_t* active, int32_t nboundary, const int32_t* boundary_type,
+                                    const int32_t* numbb, const int32_t* boundary_igrid, const double* uold,
+                                    double t_end, int64_t max_steps, double* result, int64_t* id_out) {
+  if (nboundary < 0 || nboundary > 6 || (nboundary > 0 && (!boundary_type || !numbb || !boundary_igrid)))
+    return fail(RB_ERR_INVALID, "bad boundary lists");
+  RB_TRY(rb_server_submit_octree(s, mp, son, father, nbor, numbl, active, uold, t_end, max_steps, result, id_out));
+  Request* r = s->all[*id_out];
+  r->nboundary = nboundary;
+  r->btype = boundary_type; r->numbb = numbb; r->bgrid = boundary_igrid;
   return RB_OK;
 }
 

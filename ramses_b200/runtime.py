@@ -105,6 +105,9 @@ _PROTOS = {
                                               _PD, _P64]),
     "rb_server_submit_octree": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MeshParamsC), _P32, _P32, _P32,
                                                _P32, _P32, _PD, ctypes.c_double, ctypes.c_int64, _PD, _P64]),
+    "rb_server_submit_octree_bounded": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MeshParamsC), _P32, _P32,
+                                                       _P32, _P32, _P32, ctypes.c_int32, _P32, _P32, _P32, _PD,
+                                                       ctypes.c_double, ctypes.c_int64, _PD, _P64]),
     "rb_server_progress": (ctypes.c_int, [ctypes.c_void_p, _P64, ctypes.c_int, _P32]),
     "rb_server_request_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, _P32, _PD, _P64, _P64, _PD]),
     "rb_server_cancel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),

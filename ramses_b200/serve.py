@@ -129,11 +129,13 @@ class Server:
         u = np.ascontiguousarray(uold, np.float64)
         out = np.empty_like(u)
         rid = ctypes.c_int64()
-        _check(load().rb_server_submit_octree(self._h, ctypes.byref(mp), _ptr(son, _P32), _ptr(father, _P32),
-                                              _ptr(nbor, _P32), _ptr(numbl, _P32), _ptr(act, _P32), _ptr(u, _PD),
-                                              float(t_end), int(max_steps), _ptr(out, _PD), ctypes.byref(rid)),
-               "rb_server_submit_octree")
-        self._keep[rid.value] = (mp, son, father, nbor, numbl, act, u, out)
+        bt, boff, bg = tree.boundary_concat()
+        numbb = np.diff(boff).astype(np.int32)
+        _check(load().rb_server_submit_octree_bounded(
+            self._h, ctypes.byref(mp), _ptr(son, _P32), _ptr(father, _P32), _ptr(nbor, _P32), _ptr(numbl, _P32),
+            _ptr(act, _P32), len(bt), _ptr(bt, _P32), _ptr(numbb, _P32), _ptr(bg, _P32), _ptr(u, _PD),
+            float(t_end), int(max_steps), _ptr(out, _PD), ctypes.byref(rid)), "rb_server_submit_octree_bounded")
+        self._keep[rid.value] = (mp, son, father, nbor, numbl, act, bt, numbb, bg, u, out)
         self.results[rid.value] = out
         return rid.value
 
@@ -245,9 +247,11 @@ def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 
                   outflow: bool = False) -> BuiltRequest:
     """Initial state of a request. Uniform requests become dense grids; AMR
     requests a static octree refined on the relative density/pressure
-    gradients of the initial state. outflow: the tube of a uniform request
-    has outflow (zero-gradient) boundaries in x instead of a periodic box."""
-    prim = _prim_fn(spec, hp.gamma, outflow and spec.extra == 0)
+    gradients of the initial state. outflow: a tube request has outflow
+    (zero-gradient) boundaries in x instead of a periodic box (uniform
+    requests in the z-streaming kernel's plane loads, AMR requests as free
+    boundary regions of the octree)."""
+    prim = _prim_fn(spec, hp.gamma, outflow and (spec.extra == 0 or spec.kind == "tube"))
     lmin = spec.levelmin
     if spec.extra == 0:
         tree = mesh.uniform_tree(lmin)
@@ -265,6 +269,8 @@ def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 
     if spec.kind == "sedov":
         ref = mesh.union_refine(ref, mesh.sphere_refine((0.5, 0.5, 0.5), 2.5 * 0.5 ** (lmin + spec.extra)))
     tree = mesh.build_tree(lmin, lmin + spec.extra, ref)
+    if outflow and spec.kind == "tube":
+        tree = mesh.add_boundaries(tree, ("outflow", None, None))
     return BuiltRequest(spec, tree=tree, uold=ics.fill_all_levels(tree, prim, hp.gamma))
 
 

@@ -189,3 +189,29 @@ def test_outflow_mixed_close_to_fp64(cuda_lib):
     # nothing re-entered through the x boundaries: the far left and right
     # states are still the initial ones
     assert r64[0, 0, 0] == pytest.approx(1.0, abs=1e-10) and r64[0, 0, -1] == pytest.approx(0.125, abs=1e-10)
+
+
+def test_outflow_octree_tube_request_equals_run(cuda_lib, oracle_lib):
+    """An AMR shock-tube request with outflow boundaries in x (free boundary
+    regions of the octree): the served state equals rb_run's and, in the box
+    and the boundary layers next to it, the oracle's."""
+    import oracle
+    spec = serve.RequestSpec("tube", 16, 1, {"rho_l": 2.0, "p_l": 3.0, "u_l": 0.4, "rho_r": 0.5, "p_r": 0.2,
+                                             "u_r": -0.3})
+    b = serve.build_request(spec, HP, outflow=True)
+    tree, u = b.tree, b.uold
+    assert tree.boundary_type == [11, 12]
+    with runtime.Solver(tree, HP, uold=u) as s:
+        n = s.run(max_steps=6)
+        ref = s.download_state()
+    with serve.Server(HP, precision="fp64") as srv:
+        rid = srv.submit_octree(tree, u, max_steps=6)
+        srv.drain()
+        assert srv.info(rid)["steps"] == n == 6
+        np.testing.assert_array_equal(srv.results[rid], ref)
+    orc = oracle.OracleRun(tree, HP, u)
+    for _ in range(6):
+        orc.coarse_step()
+    from test_gpu_boundary import determined_cells
+    c = determined_cells(tree) - 1
+    np.testing.assert_array_equal(ref[:, c], orc.uold[:, c])
