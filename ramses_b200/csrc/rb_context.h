@@ -16,6 +16,7 @@
 
 #include "../../include/ramses_b200.h"
 #include "godunov_tile.cuh"
+#include "rb_error.h"
 #include "rb_aux.cuh"
 #include "stream_kernel.cuh"
 #include "tile_launch.h"
@@ -24,32 +25,6 @@ namespace rbi {
 
 // host-side Fortran MIN with the same tie rule as the device and the oracle
 inline double rb_min_host(double a, double b) { return a < b ? a : (b < a ? b : a); }
-
-inline thread_local std::string g_last_error;
-
-inline int fail(int code, const char* fmt, ...) {
-  char buf[1024];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  g_last_error = buf;
-  return code;
-}
-
-#define RB_CUDA(call)                                                                        \
-  do {                                                                                       \
-    cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
-      return fail(RB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
-                  __LINE__);                                                                 \
-  } while (0)
-
-#define RB_TRY(expr)       \
-  do {                     \
-    int rc_ = (expr);      \
-    if (rc_) return rc_;   \
-  } while (0)
 
 template <typename T>
 int dalloc(T** p, size_t n) {

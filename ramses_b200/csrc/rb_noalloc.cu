@@ -20,11 +20,11 @@
 // Compiled with --fmad=false like the rest of the FP64 code.
 #include <cuda_runtime.h>
 
-#include <cstdio>
 #include <mutex>
 
 #include "../../include/ramses_b200.h"
 #include "hydro_core.cuh"
+#include "rb_error.h"
 
 #define RB_NOALLOC_NT 256
 #define RB_NOALLOC_MAX_BLOCKS 65536
@@ -112,15 +112,19 @@ __global__ void __launch_bounds__(1024) noalloc_cfl_final(const double* __restri
 
 extern "C" int rb_courant_cells_noalloc(const rb_hydro_params* hp, const double* d_u, int64_t ncell,
                                         int64_t stride, double dx, double dt_in, double* d_out, void* stream) {
-  if (!hp || !d_u || !d_out) return RB_ERR_INVALID;
-  if (ncell < 1 || stride < ncell || !(dx > 0.0)) return RB_ERR_INVALID;
-  if (ncell > RB_NOALLOC_MAX_CELLS) {
-    fprintf(stderr, "rb_courant_cells_noalloc: %lld cells exceed the fixed scratch capacity of %lld cells\n",
-            (long long)ncell, (long long)RB_NOALLOC_MAX_CELLS);
-    return RB_ERR_CAPACITY;
-  }
+  using rbi::fail;
+  if (!hp || !d_u || !d_out) return fail(RB_ERR_INVALID, "rb_courant_cells_noalloc: null argument");
+  if (ncell < 1 || stride < ncell || !(dx > 0.0))
+    return fail(RB_ERR_INVALID, "rb_courant_cells_noalloc: need ncell >= 1, stride >= ncell and dx > 0 "
+                "(ncell=%lld, stride=%lld, dx=%g)", (long long)ncell, (long long)stride, dx);
+  if (ncell > RB_NOALLOC_MAX_CELLS)
+    return fail(RB_ERR_CAPACITY, "rb_courant_cells_noalloc: %lld cells exceed the fixed scratch capacity of %lld "
+                "cells", (long long)ncell, (long long)RB_NOALLOC_MAX_CELLS);
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RB_ERR_NO_DEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return fail(RB_ERR_NO_DEVICE, "rb_courant_cells_noalloc: no usable current CUDA device");
+  }
   double* scratch;
   {
     std::lock_guard<std::mutex> lock(g_mu);
@@ -128,9 +132,11 @@ extern "C" int rb_courant_cells_noalloc(const rb_hydro_params* hp, const double*
       // the host-side name g_cfl_scratch is not a device address: look it up
       // once per device, with that device current
       void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_cfl_scratch) != cudaSuccess || !p) {
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_cfl_scratch);
+      if (e != cudaSuccess || !p) {
         cudaGetLastError();
-        return RB_ERR_CUDA;
+        return fail(RB_ERR_CUDA, "rb_courant_cells_noalloc: cudaGetSymbolAddress of the scratch array failed: %s",
+                    cudaGetErrorString(e));
       }
       g_scratch_ptr[dev] = static_cast<double*>(p);
     }
@@ -141,5 +147,7 @@ extern "C" int rb_courant_cells_noalloc(const rb_hydro_params* hp, const double*
   noalloc_cfl_partial<<<nblk, RB_NOALLOC_NT, 0, s>>>(d_u, ncell, stride, dx, *hp, scratch);
   const double dt0 = hp->courant_factor * dx / hp->smallc;
   noalloc_cfl_final<<<1, 1024, 0, s>>>(scratch, nblk, dt_in, dt0, d_out);
-  return cudaGetLastError() == cudaSuccess ? RB_OK : RB_ERR_CUDA;
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(RB_ERR_CUDA, "rb_courant_cells_noalloc: launch failed: %s", cudaGetErrorString(e));
+  return RB_OK;
 }

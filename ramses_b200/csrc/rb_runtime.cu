@@ -698,6 +698,7 @@ inline void oct_changed(rb_context* c) {
 
 bool stream_shape_fits(const rb_context* c, int s) {
   const int tx = rb::kStreamShapes[s][0], ty = rb::kStreamShapes[s][1];
+  if (rb::kStreamShapeV2[s] && (c->precision != RB_PREC_MIXED || !rb::stream2_supports(c->hp))) return false;
   return c->dnx % tx == 0 && c->dny % ty == 0 && c->dnx >= tx && c->dny >= ty;
 }
 int stream_items_of(const rb_context* c, int s, int hz) {
@@ -731,9 +732,10 @@ int dense_prepare(rb_context* c) {
   }
   RB_TRY(dalloc(&c->d_cbase, cb.size()));
   RB_TRY(h2d(c, c->d_cbase, cb.data(), cb.size() * 8));
-  // default column shape: the widest of 16x16, 16x8, 8x8 that divides the grid
+  // default column shape: the FP32-mixed kernel of stream2_kernel.cuh where
+  // it applies, else the widest of 16x16, 16x8, 8x8 that divides the grid
   int shape = -1;
-  for (int s : {2, 1, 0})
+  for (int s : {6, 2, 1, 0})
     if (stream_shape_fits(c, s)) { shape = s; break; }
   c->stream_shape = shape;
   if (shape >= 0) {

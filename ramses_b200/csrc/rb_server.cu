@@ -75,7 +75,7 @@ struct rb_server {
   int device = 0;
   int64_t budget = 0, in_use = 0;
   int steps_per_round = 8;
-  int shape = 1;  // column shape of the batched kernel (16x8)
+  int shape = 1;  // column shape of the batched kernel (16x8; 6: stream2_batch_kernel)
   cudaStream_t stream = nullptr;  // dense batch stream
   cudaStream_t copy = nullptr;    // result downloads
   int64_t next_id = 1;
@@ -433,6 +433,9 @@ int rb_server_create(const rb_hydro_params* hp, int precision, int64_t hbm_budge
   s->hp = *hp;
   s->precision = precision;
   s->steps_per_round = steps_per_round;
+  // FP32-mixed schemes that stream2_supports batch with stream2_batch_kernel
+  // (the kernel rb_uniform_run picks by default for them)
+  if (precision == RB_PREC_MIXED && rb::stream2_supports(*hp)) s->shape = 6;
   auto bail = [&](int rc) {
     rb_server_destroy(s);
     return rc;
@@ -576,8 +579,23 @@ int rb_server_submit_octree_bounded(rb_server* s, const rb_mesh_params* mp, cons
                                     double t_end, int64_t max_steps, double* result, int64_t* id_out) {
   if (nboundary < 0 || nboundary > 6 || (nboundary > 0 && (!boundary_type || !numbb || !boundary_igrid)))
     return fail(RB_ERR_INVALID, "bad boundary lists");
+  // the boundary-fill tables the admission also allocates: one
+  // (boundary oct, reference oct) pair (8 B) and one staged oct state
+  // (8 cells x 5 variables, 320 B) per boundary oct
+  int64_t nbocts = 0;
+  for (int l = 1; l <= mp->nlevelmax; l++)
+    for (int ib = 0; ib < nboundary; ib++) {
+      const int32_t n = numbb[ib + (int64_t)nboundary * (l - 1)];
+      if (n < 0 || n > mp->ngridmax) return fail(RB_ERR_INVALID, "numbb(%d,%d)=%d out of range", ib + 1, l, n);
+      nbocts += n;
+    }
+  const int64_t bbytes = nbocts * (8 + 320);
+  if (tree_bytes(*mp) + bbytes > s->budget)
+    return fail(RB_ERR_CAPACITY, "request needs about %lld bytes, the budget is %lld",
+                (long long)(tree_bytes(*mp) + bbytes), (long long)s->budget);
   RB_TRY(rb_server_submit_octree(s, mp, son, father, nbor, numbl, active, uold, t_end, max_steps, result, id_out));
   Request* r = s->all[*id_out];
+  r->bytes += bbytes;
   r->nboundary = nboundary;
   r->btype = boundary_type; r->numbb = numbb; r->bgrid = boundary_igrid;
   return RB_OK;

@@ -2,6 +2,7 @@
 // --fmad=false: no multiply-add is contracted, so every flux and update is
 // bit-identical to the reference's operation order.
 #define RB_TILE_REAL double
+#define RB_TILE_IS_MIXED 0
 #define RB_TILE_LAUNCH launch_tile_f64
 #define RB_TILE_SMEM tile_smem_f64
 #define RB_STREAM_LAUNCH launch_stream_f64

@@ -2,6 +2,7 @@
 // fluxes in FP32 (contracted, fast division); conservative->primitive and the
 // conservative accumulation into unew stay FP64.
 #define RB_TILE_REAL float
+#define RB_TILE_IS_MIXED 1
 #define RB_TILE_LAUNCH launch_tile_mixed
 #define RB_TILE_SMEM tile_smem_mixed
 #define RB_STREAM_LAUNCH launch_stream_mixed

@@ -113,7 +113,7 @@ def turbulent_box_prim_grid(n: int, seed: int = 2024, mach: float = 5.0, sigma: 
     def grf():
         re = rng.standard_normal(shape)
         im = rng.standard_normal(shape)
-        f = np.fft.irfftn((re + 1j * im) * amp, s=(n, n, n))
+        f = np.fft.irfftn((re + 1j * im) * amp, s=(n, n, n), axes=(0, 1, 2))
         return f
 
     g = grf()
@@ -130,7 +130,7 @@ def turbulent_box_prim_grid(n: int, seed: int = 2024, mach: float = 5.0, sigma: 
     k2[k2 == 0] = 1.0
     kdotv = kx * vh[0] + ky * vh[1] + kz * vh[2]
     vh = [vh[0] - kx * kdotv / k2, vh[1] - ky * kdotv / k2, vh[2] - kz * kdotv / k2]
-    v = [np.fft.irfftn(c, s=(n, n, n)) for c in vh]
+    v = [np.fft.irfftn(c, s=(n, n, n), axes=(0, 1, 2)) for c in vh]
     c_s = np.sqrt(gamma * p_over_rho)
     vrms = np.sqrt(np.mean(v[0] ** 2 + v[1] ** 2 + v[2] ** 2))
     scale = mach * c_s / vrms

@@ -23,6 +23,11 @@ LIB_PATH = PKG / "lib" / "libramses_b200.so"
 RB_PREC_FP64 = 0
 RB_PREC_MIXED = 1
 MAXLEVEL = 32
+# z-streaming column shapes (TX, TY, CTAs per SM of register budget), as
+# kStreamShapes in csrc/tile_launch.h; STREAM2_SHAPES run stream2_step_kernel
+# (FP32-mixed, HLLC with minmod or moncen slopes)
+STREAM_SHAPES = [(8, 8, 1), (16, 8, 1), (16, 16, 1), (16, 8, 2), (8, 8, 4), (16, 8, 3), (16, 8, 2)]
+STREAM2_SHAPES = (5, 6)
 
 _P32 = ctypes.POINTER(ctypes.c_int32)
 _P64 = ctypes.POINTER(ctypes.c_int64)
@@ -360,10 +365,10 @@ class Solver:
         _check(load().rb_get_uniform_info(self._h, *[ctypes.byref(x) for x in v]), "rb_get_uniform_info")
         method, shape, hz, items = (x.value for x in v)
         if method == 0:
-            dims = ([(8, 8, 1), (16, 8, 1), (16, 16, 1), (16, 8, 2), (8, 8, 4)][shape]
-                    if 0 <= shape < 5 else (0, 0, 0))
-            kern = "stream_step_kernel<%s,%d,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
-                "float" if self.precision == "mixed" else "double", dims[0], dims[1], dims[2], hz, items)
+            dims = STREAM_SHAPES[shape] if 0 <= shape < len(STREAM_SHAPES) else (0, 0, 0)
+            name = "stream2_step_kernel" if shape in STREAM2_SHAPES else "stream_step_kernel"
+            kern = "%s<%s,%d,%d,%d> (z-streaming, hz=%d, %d CTAs)" % (
+                name, "float" if self.precision == "mixed" else "double", dims[0], dims[1], dims[2], hz, items)
         else:
             kern = "godunov_tile_kernel<%s> shape %d (%d tiles)" % (
                 "float" if self.precision == "mixed" else "double", shape, items)

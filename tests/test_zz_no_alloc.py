@@ -64,3 +64,5 @@ def test_noalloc_rejects_sizes_beyond_capacity(cuda_lib):
     rc = runtime.load().rb_courant_cells_noalloc(ctypes.byref(hpc), ctypes.c_void_p(16), big, big, 0.1, 1.0,
                                                   ctypes.c_void_p(16), None)
     assert rc == 8  # RB_ERR_CAPACITY, returned before anything touches the device
+    msg = runtime.load().rb_last_error().decode()
+    assert "capacity" in msg and str(big) in msg, msg
