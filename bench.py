@@ -196,6 +196,27 @@ def ncu_traffic(method):
     return None
 
 
+def opcount_figures():
+    """Operation counts per cell update of the turbulent-box scheme (hllc,
+    moncen) from the committed summary profiles/opcount_hllc_moncen_turb.md:
+    {'algorithmic_ops_per_cell_update': ..., 'algorithmic_fp64_flops_per_cell_update': ...}."""
+    f = ROOT / "profiles" / "opcount_hllc_moncen_turb.md"
+    out = {}
+    if f.exists():
+        for ln in f.read_text().splitlines():
+            k, _, v = ln.partition(":")
+            if k.strip() in ("algorithmic_ops_per_cell_update", "algorithmic_fp64_flops_per_cell_update",
+                             "reference_fp64_flops_per_cell_update"):
+                try:
+                    out[k.strip()] = float(v.strip().split()[0])
+                except (ValueError, IndexError):
+                    pass
+    return out
+
+
+FP64_NOMINAL_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12   # FP64 FMA lanes per SM x SMs x 2 x max clock
+
+
 def cpu_sample(tree, hp, u, nocts, reps, warmup):
     """Time the oracle's hydro step (courant_fine, set_unew, godunov_fine,
     set_uold) on the first ``nocts`` octs (Morton order) of the finest level,
@@ -526,6 +547,17 @@ def main():
     peak, peak_kind = hbm_peak()
     achieved = BYTES_PER_CELL_UPDATE * cells / (kern_ms / 1e3) / 1e9
     traffic = ncu_traffic(args.method)
+    # issue ceiling: one instruction per counted operation at full issue
+    # (148 SMs x 4 schedulers x 32 threads per cycle at the sampled SM clock)
+    ops = opcount_figures()
+    clk_sum = clk.summary()
+    sm_hz = (clk_sum.get("sm_mhz") or 1965.0) * 1e6
+    issue_ceiling = None
+    if "algorithmic_ops_per_cell_update" in ops:
+        t_issue = ops["algorithmic_ops_per_cell_update"] * cells / (148 * 4 * 32 * sm_hz)
+        t_hbm = BYTES_PER_CELL_UPDATE * cells / (peak * 1e9)
+        issue_ceiling = min(1.0, t_hbm / t_issue)
+    f64_flops = ops.get("algorithmic_fp64_flops_per_cell_update")
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nocts = min(args.cpu_sample_octs, tree.noct(level))
@@ -545,13 +577,22 @@ def main():
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": mixed_kernel + " (fused godunov + update + CFL partials)",
                          "bytes_per_cell_update": BYTES_PER_CELL_UPDATE, "kernel_ms": kern_ms,
-                         "peak_kind": peak_kind},
+                         "peak_kind": peak_kind, "issue_ceiling_frac": issue_ceiling,
+                         "algorithmic_ops_per_cell_update": ops.get("algorithmic_ops_per_cell_update"),
+                         "issue_ceiling_note": "HBM time over the issue time of the algorithmic operation "
+                                               "count at one instruction per operation "
+                                               "(profiles/opcount_hllc_moncen_turb.md)"},
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clk_sum,
             "gpu_launches": 2 * args.steps,
             "fp64": {"value": f64_value, "ms_per_step": f64_ms / args.steps, "kernel_ms": f64_kern,
                      "kernel": f64_kernel,
-                     "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak},
+                     "roofline_frac": BYTES_PER_CELL_UPDATE * cells / (f64_kern / 1e3) / 1e9 / peak,
+                     "algorithmic_tflops": (f64_flops * cells / (f64_kern / 1e3) / 1e12) if f64_flops else None,
+                     "flop_frac": (f64_flops * cells / (f64_kern / 1e3) / 1e12 / FP64_NOMINAL_TFLOPS
+                                   if f64_flops else None),
+                     "flop_peak": "nominal FP64 %.1f TFLOP/s (64 FMA lanes/SM, 148 SMs, 1.965 GHz)"
+                                  % FP64_NOMINAL_TFLOPS},
             "mixed_over_fp64": value / f64_value,
             "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,
                          "mixed_vs_fp64": errs,

@@ -61,7 +61,13 @@ int rb_destroy(rb_context *ctx);
 
 /* Upload the octree (son, father, nbor as RAMSES stores them) and the active
  * grid lists: numbl[l-1] octs at level l, concatenated 1-based igrids in
- * active_igrid. Builds the device tile and interpolation tables. */
+ * active_igrid. Builds the device tile and interpolation tables. On a
+ * re-sync with a state resident (and no newer host state noted), the octs
+ * that are new since the previous tree (a level they did not have, or
+ * another father cell) get make_grid_fine's state on the device: the
+ * interpol_hydro prolongation of their father cell and its getnborfather
+ * neighbours, level by level (amr/refine_utils.f90:590-948,
+ * hydro/interpol_hydro.f90:268-444), so a remesh needs no state upload. */
 int rb_sync_tree(rb_context *ctx, const int32_t *son, const int32_t *father, const int32_t *nbor,
                  const int32_t *numbl, const int32_t *active_igrid);
 
@@ -86,6 +92,39 @@ int rb_make_boundary_hydro(rb_context *ctx, int ilevel);
 /* Fortran-layout uold(ncell,5) host <-> device mirror of uold. */
 int rb_upload_state(rb_context *ctx, const double *uold);
 int rb_download_state(rb_context *ctx, double *uold);
+
+/* Residency protocol of the drop-in boundary. The reference keeps uold and
+ * the tree in host memory and every hydro routine reads them there
+ * (amr/amr_step.f90:320-445); here the device copy stays authoritative across
+ * hydro calls, and host code that reads or writes uold or changes the tree
+ * says so:
+ *   rb_note_tree_changed: the host changed son/father/nbor/active or the
+ *     boundary lists (refine_fine, amr/refine_utils.f90:332-585; load_balance
+ *     and defrag, amr/load_balance.f90); bumps a generation counter.
+ *   rb_note_host_state_written: the host wrote uold (initial conditions,
+ *     restart, load balancing); the host copy is the newer one.
+ *   rb_ensure_device: before a device hydro call: re-synchronises the tree
+ *     (rb_set_boundary + rb_sync_tree) when the generation changed, then
+ *     uploads uold only when the host copy is newer (or none is resident).
+ *     The tree and boundary arrays are read only when a re-sync is due, which
+ *     rb_tree_needs_sync tells (a caller may pass placeholders otherwise).
+ *   rb_ensure_host: before host code reads uold (output, flag criteria
+ *     evaluated on the host): downloads only when the device copy is newer.
+ * Every device call that writes uold (set_uold, upload_fine,
+ * make_boundary_hydro, coarse steps, runs, new-oct prolongation) makes the
+ * device copy the newer one; rb_upload_state / rb_download_state make them
+ * equal. rb_transfer_stats reports the uold bytes moved each way, the tree
+ * synchronisations and the octs prolonged on the device. */
+int rb_note_tree_changed(rb_context *ctx);
+int rb_note_host_state_written(rb_context *ctx);
+int rb_tree_needs_sync(rb_context *ctx, int32_t *needed);
+int rb_ensure_device(rb_context *ctx, const int32_t *son, const int32_t *father, const int32_t *nbor,
+                     const int32_t *numbl, const int32_t *active_igrid, int32_t nboundary,
+                     const int32_t *boundary_type, const int32_t *numbb, const int32_t *boundary_igrid,
+                     const double *uold);
+int rb_ensure_host(rb_context *ctx, double *uold);
+int rb_transfer_stats(rb_context *ctx, int64_t *h2d_state_bytes, int64_t *d2h_state_bytes, int64_t *tree_syncs,
+                      int64_t *octs_prolonged);
 /* Same for unew (for callers that interleave host work with a level step). */
 int rb_upload_unew(rb_context *ctx, const double *unew);
 int rb_download_unew(rb_context *ctx, double *unew);

@@ -139,6 +139,21 @@ def unsplit(hp, uin, gravin, dx, dt, ngrid=None):
     return flux, tmp
 
 
+def interpol_hydro(hp, u1):
+    """interpol_hydro (hydro/interpol_hydro.f90:268-444) of nn father cells:
+    u1 (nn, 7, 5) = father cell and its 6 getnborfather neighbours,
+    conservative; returns u2 (nn, 8, 5), the 8 children."""
+    u1 = np.asarray(u1, np.float64)
+    nn = u1.shape[0]
+    a = np.ascontiguousarray(np.transpose(u1, (2, 1, 0)))  # Fortran u1(nn,7,5)
+    out = np.zeros((5, 8, nn))
+    p = params_struct(hp)
+    rc = lib().orc_interpol_hydro(ctypes.byref(p), _ptr(a, _PD), _ptr(out, _PD), nn)
+    if rc:
+        raise RuntimeError("orc_interpol_hydro failed: %d" % rc)
+    return np.transpose(out, (2, 1, 0))
+
+
 def dense_step(hp, u, boxlen=1.0, bc_outflow=0, nvector=32):
     """One coarse step of a complete level given as conservative
     [5, nz, ny, nx] (advanced in place); returns dt. bc_outflow: bit d set

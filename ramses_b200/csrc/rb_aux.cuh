@@ -208,6 +208,29 @@ static __global__ void interp_blocks_kernel(const double* __restrict__ uold, con
     for (int v = 0; v < 5; v++) out[v * stride + (int64_t)e * 8 + ind] = u2[ind][v];
 }
 
+// The state of octs created by refinement (make_grid_fine,
+// amr/refine_utils.f90:590-948, through interpol_hydro,
+// hydro/interpol_hydro.f90:268-444): the 8 children of each new oct prolonged
+// from its father cell and that cell's 6 getnborfather neighbours
+// (cells7[e][0..6], device cell indices) and written into the oct's cells.
+// Father cells are one level coarser than the new octs, so no thread reads a
+// cell another thread writes.
+static __global__ void prolong_new_octs_kernel(double* __restrict__ uold, const int32_t* __restrict__ cells7,
+                                               const int32_t* __restrict__ octs, int32_t n, int64_t ncell,
+                                               int64_t ncoarse, rb_hydro_params hp) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double u1[7][5], u2[8][5];
+  for (int j = 0; j < 7; j++) {
+    const int64_t dc = cells7[(int64_t)e * 7 + j];
+    for (int v = 0; v < 5; v++) u1[j][v] = uold[v * ncell + dc];
+  }
+  interp_children(u1, hp, u2);
+  const int64_t base = ncoarse + 8 * (int64_t)octs[e];   // octs[e] = igrid - 1
+  for (int ind = 0; ind < 8; ind++)
+    for (int v = 0; v < 5; v++) uold[v * ncell + base + ind] = u2[ind][v];
+}
+
 // Fine-to-coarse correction (godunov_fine.f90:798-908), applied target by
 // target with the contributions in the reference's sweep order: by vector
 // batch of the contributing oct, then direction, then left before right, and

@@ -163,6 +163,13 @@ struct rb_context {
   bool dense_valid = false;         // the dense mirror holds the newest state of `finest`
   bool oct_stale = false;           // the oct layout of `finest` lags the dense mirror
   int stream_shape = -1, stream_hz = 0, stream_items = 0;
+  // residency protocol of the drop-in boundary: which copy of uold is newer
+  // (0: host and device agree, 1: the device's, 2: the host's), the host's
+  // tree generation and the one last synchronised, and the transfer counters
+  int state_newer = 2;
+  bool prev_tree_valid = false;     // level_of/father describe the last synchronised tree
+  int64_t tree_gen = 0, synced_gen = -1;
+  int64_t h2d_state_bytes = 0, d2h_state_bytes = 0, tree_syncs = 0, octs_prolonged = 0;
   // scheduler state (amr_commons dtnew/dtold, t, nstep)
   double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
   double t = 0.0;

@@ -185,6 +185,49 @@ int ensure_nres6(rb_context* c, Level& L) {
   return RB_OK;
 }
 
+// getnborfather (amr/nbors_utils.f90:404-525): the level-(l-1) cell f
+// (Fortran index) and its 6 face neighbours (-x,+x,-y,+y,-z,+z) at level
+// l-1, or the coarser cell nbor(...) where that neighbour oct does not exist.
+// Needs c->idx[l-1] and c->idx[l] of the current tree.
+void father_nbor_cells(const rb_context* c, int l, int64_t f, int64_t cells[7]) {
+  cells[0] = f;
+  if (l == 1) {
+    const int64_t nx = c->mp.nx, ny = c->mp.ny, nz = c->mp.nz, nxny = nx * ny;
+    const int64_t ib[3] = {nx - 1, ny - 1, nz - 1};
+    const int64_t s1[3] = {1, nx, nxny};
+    const int64_t s2[3] = {nx - 1, (ny - 1) * nx, (nz - 1) * nxny};
+    int64_t ix[3];
+    ix[2] = (f - 1) / nxny;
+    ix[1] = (f - 1 - ix[2] * nxny) / nx;
+    ix[0] = (f - 1 - ix[1] * nx - ix[2] * nxny);
+    for (int d = 0; d < 3; d++) {
+      cells[2 * d + 1] = ix[d] > 0 ? f - s1[d] : f + s2[d];
+      cells[2 * d + 2] = ix[d] < ib[d] ? f + s1[d] : f - s2[d];
+    }
+    return;
+  }
+  const OctIndex& P = c->idx[l - 1];
+  const int64_t cnx = c->idx[l].nx, cny = c->idx[l].ny, cnz = c->idx[l].nz;
+  const int64_t r = f - 1 - c->mp.ncoarse;
+  const int32_t pg = (int32_t)(r % c->mp.ngridmax) + 1;
+  const int pos = (int)(r / c->mp.ngridmax);
+  const int cc[3] = {pos & 1, (pos >> 1) & 1, (pos >> 2) & 1};
+  const int64_t* pc = &c->coords[(size_t)(pg - 1) * 3];
+  for (int j = 1; j <= 6; j++) {
+    const int d = (j - 1) / 2, plus = (j - 1) & 1;
+    int64_t q[3] = {2 * pc[0] + cc[0], 2 * pc[1] + cc[1], 2 * pc[2] + cc[2]};
+    q[d] += plus ? 1 : -1;
+    const int32_t g = P.find(q[0] >> 1, q[1] >> 1, q[2] >> 1);
+    if (g > 0) {
+      const int64_t cx = ((q[0] % cnx) + cnx) % cnx, cy = ((q[1] % cny) + cny) % cny, cz = ((q[2] % cnz) + cnz) % cnz;
+      const int ind = 1 + (int)(cx & 1) + 2 * (int)(cy & 1) + 4 * (int)(cz & 1);
+      cells[j] = fcell(c, ind, g);
+    } else {
+      cells[j] = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (pg - 1)];
+    }
+  }
+}
+
 // Build the godunov tile / prolongation / correction tables of level l.
 int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   Level& L = c->lv[l];
@@ -245,41 +288,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     const int32_t e = (int32_t)interp_of.size();
     interp_of.emplace(f, e);
     int64_t cells[7];
-    cells[0] = f;
-    // getnborfather (nbors_utils.f90:404-525)
-    if (l == 1) {
-      const int64_t nx = c->mp.nx, ny = c->mp.ny, nz = c->mp.nz, nxny = nx * ny;
-      const int64_t ib[3] = {nx - 1, ny - 1, nz - 1};
-      const int64_t s1[3] = {1, nx, nxny};
-      const int64_t s2[3] = {nx - 1, (ny - 1) * nx, (nz - 1) * nxny};
-      int64_t ix[3];
-      ix[2] = (f - 1) / nxny;
-      ix[1] = (f - 1 - ix[2] * nxny) / nx;
-      ix[0] = (f - 1 - ix[1] * nx - ix[2] * nxny);
-      for (int d = 0; d < 3; d++) {
-        cells[2 * d + 1] = ix[d] > 0 ? f - s1[d] : f + s2[d];
-        cells[2 * d + 2] = ix[d] < ib[d] ? f + s1[d] : f - s2[d];
-      }
-    } else {
-      const int64_t r = f - 1 - c->mp.ncoarse;
-      const int32_t pg = (int32_t)(r % c->mp.ngridmax) + 1;
-      const int pos = (int)(r / c->mp.ngridmax);
-      const int cc[3] = {pos & 1, (pos >> 1) & 1, (pos >> 2) & 1};
-      const int64_t* pc = &c->coords[(size_t)(pg - 1) * 3];
-      for (int j = 1; j <= 6; j++) {
-        const int d = (j - 1) / 2, plus = (j - 1) & 1;
-        int64_t q[3] = {2 * pc[0] + cc[0], 2 * pc[1] + cc[1], 2 * pc[2] + cc[2]};
-        q[d] += plus ? 1 : -1;
-        const int32_t g = P->find(q[0] >> 1, q[1] >> 1, q[2] >> 1);
-        if (g > 0) {
-          const int64_t cx = ((q[0] % cnx) + cnx) % cnx, cy = ((q[1] % cny) + cny) % cny, cz = ((q[2] % cnz) + cnz) % cnz;
-          const int ind = 1 + (int)(cx & 1) + 2 * (int)(cy & 1) + 4 * (int)(cz & 1);
-          cells[j] = fcell(c, ind, g);
-        } else {
-          cells[j] = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (pg - 1)];
-        }
-      }
-    }
+    father_nbor_cells(c, l, f, cells);
     for (int j = 0; j < 7; j++) interp7.push_back((int32_t)dev_of_fortran(c, cells[j]));
     *code = -2 - e;
     return RB_OK;
@@ -461,9 +470,59 @@ int build_boundary_pairs(rb_context* c) {
   return RB_OK;
 }
 
+int sync_oct(rb_context* c);
+
+// After a re-sync: the octs that are new since the previous tree (a level
+// they did not have, or another father cell) get the state make_grid_fine
+// gives them, prolonged on the device in level order, so that a remeshed
+// tree needs no state upload.
+int prolong_new_octs(rb_context* c, const std::vector<int8_t>& old_level, const std::vector<int32_t>& old_father) {
+  for (int l = 2; l <= c->mp.nlevelmax; l++) {
+    const Level& L = c->lv[l];
+    std::vector<int32_t> octs, cells7;
+    for (int32_t g : L.h_active) {
+      if (old_level[g - 1] == l && old_father[g - 1] == c->father[g - 1]) continue;
+      int64_t cells[7];
+      father_nbor_cells(c, l, c->father[g - 1], cells);
+      for (int j = 0; j < 7; j++) {
+        if (cells[j] < 1 || cells[j] > c->ncell) return fail(RB_ERR_TREE, "grid %d: prolongation cell out of range", g);
+        cells7.push_back((int32_t)dev_of_fortran(c, cells[j]));
+      }
+      octs.push_back(g - 1);
+    }
+    if (octs.empty()) continue;
+    int32_t *d_octs = nullptr, *d_cells = nullptr;
+    int rc = dalloc(&d_octs, octs.size());
+    if (!rc) rc = dalloc(&d_cells, cells7.size());
+    if (!rc) rc = h2d(c, d_octs, octs.data(), octs.size() * 4);
+    if (!rc) rc = h2d(c, d_cells, cells7.data(), cells7.size() * 4);
+    if (!rc) {
+      rb::prolong_new_octs_kernel<<<(int)((octs.size() + 127) / 128), 128, 0, c->stream>>>(
+          c->d_uold, d_cells, d_octs, (int32_t)octs.size(), c->ncell, c->mp.ncoarse, c->hp);
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) rc = fail(RB_ERR_CUDA, "prolongation of new octs failed: %s", cudaGetErrorString(e));
+    }
+    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(RB_ERR_CUDA, "prolongation sync failed");
+    dfree(d_octs);
+    dfree(d_cells);
+    if (rc) return rc;
+    c->octs_prolonged += (int64_t)octs.size();
+  }
+  return RB_OK;
+}
+
 int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
                    const int32_t* numbl, const int32_t* active) {
   if (!son || !father || !nbor || !numbl || !active) return fail(RB_ERR_INVALID, "null tree array");
+  // a state held in the dense mirror goes back to the oct layout first
+  if (c->have_tree) RB_TRY(sync_oct(c));
+  // the previous tree (still in level_of/father after an rb_set_boundary
+  // dropped it) decides which octs are new
+  const bool prolong = c->prev_tree_valid && c->have_state && c->state_newer != 2;
+  std::vector<int8_t> old_level;
+  std::vector<int32_t> old_father;
+  if (prolong) { old_level = c->level_of; old_father = c->father; }
+  c->prev_tree_valid = false;
   free_tree(c);
   const int64_t ncell = c->ncell;
   const int ngm = c->mp.ngridmax;
@@ -556,7 +615,13 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
   for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(build_level_tables(c, l, idx));
   RB_TRY(build_boundary_pairs(c));
   c->have_tree = true;
+  c->prev_tree_valid = true;
   c->clock_valid = false;
+  c->tree_syncs++;
+  if (prolong) {
+    RB_TRY(prolong_new_octs(c, old_level, old_father));
+    if (c->state_newer == 0) c->state_newer = 1;
+  }
   return RB_OK;
 }
 
@@ -694,6 +759,11 @@ int sync_oct(rb_context* c) {
 inline void oct_changed(rb_context* c) {
   c->dense_valid = false;
   c->clock_valid = false;
+}
+
+// A device call wrote uold: the device copy is now the newer one.
+inline void dev_wrote(rb_context* c) {
+  if (c->have_state) c->state_newer = 1;
 }
 
 bool stream_shape_fits(const rb_context* c, int s) {
@@ -1138,6 +1208,7 @@ int rb_sync_tree(rb_context* c, const int32_t* son, const int32_t* father, const
   if (!c) return fail(RB_ERR_INVALID, "null context");
   int rc = sync_tree_impl(c, son, father, nbor, numbl, active_igrid);
   if (rc) free_tree(c);
+  else c->synced_gen = c->tree_gen;  // the device now holds the host's current tree
   return rc;
 }
 
@@ -1163,14 +1234,20 @@ int rb_set_boundary(rb_context* c, int32_t nboundary, const int32_t* boundary_ty
   c->btype = bt;
   c->boff = off;
   c->bgrid.assign(boundary_igrid, boundary_igrid + off.back());
-  // the lists belong to the next rb_sync_tree: a synchronised tree is dropped
-  if (c->have_tree) free_tree(c);
+  // the lists belong to the next rb_sync_tree: a synchronised tree is
+  // dropped (the state it held in a dense mirror goes back to the octs), and
+  // the tree it leaves behind is what that sync compares against
+  if (c->have_tree) {
+    RB_TRY(sync_oct(c));
+    free_tree(c);
+  }
   return RB_OK;
 }
 
 int rb_make_boundary_hydro(rb_context* c, int l) {
   RB_TRY(check_level(c, l));
   RB_TRY(sync_oct(c));
+  dev_wrote(c);
   RB_TRY(boundary_impl(c, l));
   RB_CUDA(cudaStreamSynchronize(c->stream));
   return RB_OK;
@@ -1200,12 +1277,62 @@ int rb_upload_state(rb_context* c, const double* uold) {
   c->have_state = true;
   c->oct_stale = false;  // overwritten entirely
   oct_changed(c);
+  c->state_newer = 0;
+  c->h2d_state_bytes += c->ncell * 5 * (int64_t)sizeof(double);
   return RB_OK;
 }
 int rb_download_state(rb_context* c, double* uold) {
   if (!c) return fail(RB_ERR_INVALID, "null context");
   RB_TRY(sync_oct(c));
-  return download_impl(c, c->d_uold, uold);
+  RB_TRY(download_impl(c, c->d_uold, uold));
+  if (c->have_state) c->state_newer = 0;
+  c->d2h_state_bytes += c->ncell * 5 * (int64_t)sizeof(double);
+  return RB_OK;
+}
+
+// ---- residency protocol of the drop-in boundary ----
+int rb_note_tree_changed(rb_context* c) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  c->tree_gen++;
+  return RB_OK;
+}
+int rb_note_host_state_written(rb_context* c) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  c->state_newer = 2;
+  return RB_OK;
+}
+int rb_tree_needs_sync(rb_context* c, int32_t* needed) {
+  if (!c || !needed) return fail(RB_ERR_INVALID, "null argument");
+  *needed = (!c->have_tree || c->synced_gen != c->tree_gen) ? 1 : 0;
+  return RB_OK;
+}
+int rb_ensure_device(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
+                     const int32_t* numbl, const int32_t* active_igrid, int32_t nboundary,
+                     const int32_t* boundary_type, const int32_t* numbb, const int32_t* boundary_igrid,
+                     const double* uold) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!c->have_tree || c->synced_gen != c->tree_gen) {
+    RB_TRY(rb_set_boundary(c, nboundary, boundary_type, numbb, boundary_igrid));
+    RB_TRY(rb_sync_tree(c, son, father, nbor, numbl, active_igrid));
+    c->synced_gen = c->tree_gen;
+  }
+  if (!c->have_state || c->state_newer == 2) RB_TRY(rb_upload_state(c, uold));
+  return RB_OK;
+}
+int rb_ensure_host(rb_context* c, double* uold) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!uold) return fail(RB_ERR_INVALID, "null uold");
+  if (c->have_state && c->state_newer == 1) RB_TRY(rb_download_state(c, uold));
+  return RB_OK;
+}
+int rb_transfer_stats(rb_context* c, int64_t* h2d_state_bytes, int64_t* d2h_state_bytes, int64_t* tree_syncs,
+                      int64_t* octs_prolonged) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (h2d_state_bytes) *h2d_state_bytes = c->h2d_state_bytes;
+  if (d2h_state_bytes) *d2h_state_bytes = c->d2h_state_bytes;
+  if (tree_syncs) *tree_syncs = c->tree_syncs;
+  if (octs_prolonged) *octs_prolonged = c->octs_prolonged;
+  return RB_OK;
 }
 int rb_upload_unew(rb_context* c, const double* unew) { return upload_impl(c, unew, c ? c->d_unew : nullptr); }
 int rb_download_pressure_fix(rb_context* c, double* divu, double* enew) {
@@ -1232,12 +1359,14 @@ int rb_set_uold(rb_context* c, int l) {
   RB_TRY(check_level(c, l));
   RB_TRY(sync_oct(c));
   oct_changed(c);
+  dev_wrote(c);
   return set_uold_impl(c, l);
 }
 int rb_upload_fine(rb_context* c, int l) {
   RB_TRY(check_level(c, l));
   RB_TRY(sync_oct(c));
   oct_changed(c);
+  dev_wrote(c);
   return upload_fine_impl(c, l);
 }
 
@@ -1263,6 +1392,7 @@ int rb_coarse_step(rb_context* c, double* t_io, double* dtnew_out) {
   if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
   RB_TRY(sync_oct(c));
   oct_changed(c);
+  dev_wrote(c);
   if (t_io) c->t = *t_io;
   c->mass_tot = c->ekin_tot = c->eint_tot = 0.0;
   RB_TRY(amr_step_impl(c, c->mp.levelmin, 1));
@@ -1282,6 +1412,7 @@ int rb_run(rb_context* c, int max_steps, double t_end, int use_graph, double* t_
   if (max_steps < 0) return fail(RB_ERR_INVALID, "max_steps=%d must be non-negative", max_steps);
   if (std::isnan(t_end)) return fail(RB_ERR_INVALID, "t_end is NaN");
   if (t_io) c->t = *t_io;
+  dev_wrote(c);
   struct GateScope {
     rb_context* c;
     ~GateScope() { c->gate = nullptr; }
@@ -1833,6 +1964,7 @@ int rb_uniform_run(rb_context* c, int nsteps, int use_graph, double* t_io, doubl
   if (!c) return fail(RB_ERR_INVALID, "null context");
   if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
   if (nsteps < 0) return fail(RB_ERR_INVALID, "nsteps must be >= 0");
+  if (nsteps > 0) dev_wrote(c);
   const int lf = c->finest;
   Level& L = c->lv[lf];
   // (with physical boundaries the level covers the box, not the extended

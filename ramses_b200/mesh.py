@@ -153,12 +153,14 @@ def _neighbourhood(cells: np.ndarray) -> np.ndarray:
 
 def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
                refine: Optional[Callable[[int, np.ndarray], np.ndarray]] = None,
-               boxlen: float = 1.0, nexpand: int = 1) -> Octree:
+               boxlen: float = 1.0, nexpand: int = 1, spare: int = 0) -> Octree:
     """Build a periodic single-coarse-cell (nx=ny=nz=1) octree.
 
     ``refine(level, cell_coords[n,3]) -> bool[n]`` flags level-``level``
     cells (level >= levelmin) for refinement; flags are expanded by
-    ``nexpand`` cells and closed under the nesting rule.
+    ``nexpand`` cells and closed under the nesting rule. ``spare`` free
+    grids are reserved beyond the octs built (ngridmax, room for
+    ``remesh``).
     """
     if nlevelmax is None:
         nlevelmax = levelmin
@@ -221,13 +223,13 @@ def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
         fc = fc[np.isin(_keys(fc // 2, n // 2), parent_keys)]
         refined[l] = fc
         oct_coords[l + 1] = fc
-    return _assemble(oct_coords, levelmin, nlevelmax, boxlen)
+    return _assemble(oct_coords, levelmin, nlevelmax, boxlen, spare)
 
 
-def _assemble(oct_coords, levelmin, nlevelmax, boxlen) -> Octree:
+def _assemble(oct_coords, levelmin, nlevelmax, boxlen, spare=0) -> Octree:
     ncoarse = 1
     counts = [len(oct_coords.get(l, ())) for l in range(1, nlevelmax + 1)]
-    ngridmax = int(sum(counts))
+    ngridmax = int(sum(counts)) + int(spare)
     ncell = ncoarse + 8 * ngridmax
     son = np.zeros(ncell, dtype=np.int32)
     father = np.zeros(ngridmax, dtype=np.int32)
@@ -289,6 +291,93 @@ def _assemble(oct_coords, levelmin, nlevelmax, boxlen) -> Octree:
     return Octree(nx=1, ny=1, nz=1, ncoarse=ncoarse, ngridmax=ngridmax,
                   nlevelmax=nlevelmax, levelmin=levelmin, boxlen=float(boxlen),
                   son=son, father=father, nbor=nbor, active=active, coords=coords)
+
+
+def remesh(old: Octree, oct_coords) -> Octree:
+    """The tree that refine_fine leaves behind (amr/refine_utils.f90:332-948)
+    when the octs of level l become ``oct_coords[l]`` (n,3 oct coordinates):
+    an oct present before and after keeps its igrid and its place in the
+    level's active list; killed octs free their igrids (kill_grid); new octs
+    take free igrids in ascending order and are appended to the list in
+    (parent igrid, child slot) order (make_grid_fine). ngridmax and the cell
+    numbering are unchanged, so the old tree needs spare grids
+    (``build_tree(spare=...)``). Single-coarse-cell periodic trees."""
+    if old.ncoarse != 1 or old.boundary_type:
+        raise ValueError("remesh: single-coarse-cell periodic trees only")
+    L = old.nlevelmax
+    ngm, ncoarse = old.ngridmax, old.ncoarse
+    new_sets = [np.zeros((0, 3), np.int64)] + [np.asarray(oct_coords.get(l, np.zeros((0, 3), np.int64)),
+                                                          np.int64).reshape(-1, 3) for l in range(1, L + 1)]
+    keep = {}          # level -> (bool mask over the old active list)
+    used = np.zeros(ngm + 1, bool)
+    for l in range(1, L + 1):
+        if old.noct(l) == 0:
+            keep[l] = np.zeros(0, bool)
+            continue
+        n = 2 ** (l - 1)
+        k_old = _keys(old.coords[l], n)
+        k_new = _keys(new_sets[l], n) if len(new_sets[l]) else np.zeros(0, np.int64)
+        keep[l] = np.isin(k_old, k_new)
+        used[old.active[l][keep[l]]] = True
+    free = [g for g in range(1, ngm + 1) if not used[g]]
+    fi = 0
+    son = np.zeros(ncoarse + 8 * ngm, np.int32)
+    father = np.zeros(ngm, np.int32)
+    nbor = np.zeros((6, ngm), np.int32)
+    active = [np.zeros(0, np.int32) for _ in range(L + 1)]
+    coords = [np.zeros((0, 3), np.int64) for _ in range(L + 1)]
+    parent_lookup = None
+    for l in range(1, L + 1):
+        oc_new = new_sets[l]
+        if len(oc_new) == 0:
+            break
+        n = 2 ** (l - 1)
+        surv_g = old.active[l][keep[l]] if old.noct(l) else np.zeros(0, np.int32)
+        surv_c = old.coords[l][keep[l]] if old.noct(l) else np.zeros((0, 3), np.int64)
+        k_surv = _keys(surv_c, n) if len(surv_c) else np.zeros(0, np.int64)
+        born = oc_new[~np.isin(_keys(oc_new, n), k_surv)]
+        if l > 1 and len(born):
+            keys_sorted, igr = parent_lookup
+            pos = np.searchsorted(keys_sorted, _keys(born // 2, 2 ** (l - 2)))
+            slot = (born[:, 0] & 1) + 2 * (born[:, 1] & 1) + 4 * (born[:, 2] & 1)
+            born = born[np.lexsort((slot, igr[pos]))]
+        if fi + len(born) > len(free):
+            raise ValueError("remesh: ngridmax=%d too small" % ngm)
+        born_g = np.array(free[fi:fi + len(born)], np.int64)
+        fi += len(born)
+        ig = np.concatenate([surv_g.astype(np.int64), born_g])
+        oc = np.concatenate([surv_c, born]) if len(born) else surv_c
+        active[l] = ig.astype(np.int32)
+        coords[l] = oc
+        if l == 1:
+            father[ig - 1] = 1
+            nbor[:, ig - 1] = 1
+            son[0] = int(ig[0])
+        else:
+            keys_sorted, igr = parent_lookup
+            nl = 2 ** (l - 1)
+
+            def cell_of(cc):
+                cc = cc % nl
+                k = _keys(cc // 2, nl // 2)
+                pos = np.searchsorted(keys_sorted, k)
+                if np.any(pos >= len(keys_sorted)) or np.any(keys_sorted[np.minimum(pos, len(keys_sorted) - 1)] != k):
+                    raise ValueError("remesh: refinement map violates the nesting rule at level %d" % l)
+                slot = (cc[:, 0] & 1) + 2 * (cc[:, 1] & 1) + 4 * (cc[:, 2] & 1)
+                return ncoarse + slot * ngm + igr[pos]
+
+            fcell = cell_of(oc)
+            father[ig - 1] = fcell
+            son[fcell - 1] = ig
+            for j in range(6):
+                step = np.zeros(3, np.int64)
+                step[j // 2] = 1 if (j % 2) else -1
+                nbor[j, ig - 1] = cell_of(oc + step)
+        k = _keys(oc, n)
+        srt = np.argsort(k)
+        parent_lookup = (k[srt], ig[srt])
+    return Octree(nx=1, ny=1, nz=1, ncoarse=ncoarse, ngridmax=ngm, nlevelmax=L, levelmin=old.levelmin,
+                  boxlen=old.boxlen, son=son, father=father, nbor=nbor, active=active, coords=coords)
 
 
 def uniform_tree(level: int, boxlen: float = 1.0) -> Octree:

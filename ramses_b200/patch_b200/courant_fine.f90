@@ -17,7 +17,7 @@ subroutine courant_fine(ilevel)
   real(c_double)::dt_loc,mass_loc,ekin_loc,eint_loc
   real(kind=8)::mass_all,ekin_all,eint_all,dt_all
   if(numbtot(1,ilevel)==0)return
-  call rb_b200_push
+  call rb_b200_device
   dt_loc=dtnew(ilevel)
   call rb_b200_check(rb_courant_fine(rb_ctx, int(ilevel, c_int), dt_loc, mass_loc, ekin_loc, eint_loc), &
        & 'courant_fine')

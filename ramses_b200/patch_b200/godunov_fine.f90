@@ -1,6 +1,7 @@
 !###########################################################
 ! B200 replacement of hydro/godunov_fine.f90 for the PATCH mechanism:
-! godunov_fine, set_unew and set_uold run on the GPU through rb_b200.
+! godunov_fine, set_unew and set_uold run on the GPU through rb_b200, on the
+! device-resident uold (rb_b200_device before each call).
 ! Same call sites and semantics as the reference (pure hydro: no Poisson
 ! source terms, no pressure_fix, no momentum feedback, one MPI rank).
 !###########################################################
@@ -12,7 +13,7 @@ subroutine godunov_fine(ilevel)
   integer::ilevel
   if(numbtot(1,ilevel)==0)return
   if(static)return
-  call rb_b200_push
+  call rb_b200_device
   call rb_b200_check(rb_godunov_fine(rb_ctx, int(ilevel, c_int), real(dtnew(ilevel), c_double)), 'godunov_fine')
 end subroutine godunov_fine
 !###########################################################
@@ -23,7 +24,7 @@ subroutine set_unew(ilevel)
   implicit none
   integer::ilevel
   if(numbtot(1,ilevel)==0)return
-  call rb_b200_init
+  call rb_b200_device
   call rb_b200_check(rb_set_unew(rb_ctx, int(ilevel, c_int)), 'set_unew')
 end subroutine set_unew
 !###########################################################
@@ -39,12 +40,11 @@ subroutine set_uold(ilevel)
      call clean_stop
   end if
   ! with pressure_fix, rb_set_uold adds the pdV term to enew and repairs the
-  ! total energy on the device (add_pdv_source_terms and the fix of set_uold)
+  ! total energy on the device (add_pdv_source_terms and the fix of set_uold);
+  ! uold stays on the device (amr_step's upload_fine that follows is wrapped
+  ! to the device too, wrap_b200.f90)
+  call rb_b200_device
   call rb_b200_check(rb_set_uold(rb_ctx, int(ilevel, c_int)), 'set_uold')
-  ! restriction to the coarser level on the device; the host's own
-  ! upload_fine, called next by amr_step, recomputes the same values
-  call rb_b200_check(rb_upload_fine(rb_ctx, int(ilevel, c_int)), 'upload_fine')
-  call rb_b200_pull
 end subroutine set_uold
 !###########################################################
 subroutine add_gravity_source_terms(ilevel)

@@ -3,8 +3,7 @@
 ! whose refinement uses the gradient criterion only (err_grad_d, err_grad_p,
 ! err_grad_u of &REFINE_PARAMS; no Jeans or geometric criterion, NENER=0):
 ! the criterion is evaluated on the device state and only the flags come
-! back, one byte per cell of the level. Under the push/pull protocol of
-! rb_b200 the host owns uold between calls, so the state is pushed first.
+! back, one byte per cell of the level; uold stays on the device.
 !###########################################################
 subroutine hydro_flag(ilevel)
   use amr_commons
@@ -17,7 +16,7 @@ subroutine hydro_flag(ilevel)
   if(ilevel==nlevelmax)return
   if(numbtot(1,ilevel)==0)return
   if(err_grad_d==-1.0.and.err_grad_p==-1.0.and.err_grad_u==-1.0)return
-  call rb_b200_push
+  call rb_b200_device
   rp%err_grad_d=err_grad_d; rp%err_grad_p=err_grad_p; rp%err_grad_u=err_grad_u
   rp%floor_d=floor_d; rp%floor_u=floor_u; rp%floor_p=floor_p
   ! flag1 is allocated (0:ncell): pass flag1(0) so that C indexes by icell

@@ -4,10 +4,21 @@
 ! (son, father, nbor, active, uold) and its &HYDRO_PARAMS namelist; this
 ! module mirrors them on the GPU and converts the namelist strings to codes.
 !
-! Synchronisation protocol (correct whatever the host does between calls):
-!   rb_b200_push : host -> device (tree if it changed, then uold); called at
-!                  the start of courant_fine and godunov_fine;
-!   rb_b200_pull : device -> host uold; called at the end of set_uold.
+! Residency protocol: the device copy of uold stays authoritative across
+! hydro calls. The library knows which copy is newer (every device call that
+! writes uold makes it the device's); the host says when it changed the
+! tree or wrote uold:
+!   rb_b200_device : before a device hydro call (courant_fine, set_unew,
+!                    godunov_fine, set_uold, upload_fine, make_boundary_hydro,
+!                    hydro_flag): re-synchronises the tree when the host
+!                    changed it (the library prolongs the new octs on the
+!                    device), uploads uold only when the host copy is newer;
+!   rb_b200_host   : before host code reads uold (dump_all, load_balance,
+!                    flag criteria evaluated on the host): downloads only when
+!                    the device copy is newer;
+!   rb_b200_tree_changed / rb_b200_host_wrote : called by the wrappers of
+!                    refine_fine, load_balance and defrag (wrap_b200.f90,
+!                    linked with -Wl,--wrap).
 ! unew lives on the device only between set_unew and set_uold.
 !###########################################################
 module rb_b200
@@ -34,7 +45,6 @@ module rb_b200
   end type rb_refine_params_t
 
   type(c_ptr), save :: rb_ctx = c_null_ptr
-  integer(c_int64_t), save :: rb_tree_stamp = -1
 
   interface
      integer(c_int) function rb_create(hp, mp, precision, ctx) bind(c, name='rb_create')
@@ -106,6 +116,33 @@ module rb_b200
        integer(c_int32_t), dimension(*) :: flag1
        integer(c_int64_t) :: nflag_added
      end function rb_hydro_flag
+     integer(c_int) function rb_note_tree_changed(ctx) bind(c, name='rb_note_tree_changed')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+     end function rb_note_tree_changed
+     integer(c_int) function rb_note_host_state_written(ctx) bind(c, name='rb_note_host_state_written')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+     end function rb_note_host_state_written
+     integer(c_int) function rb_tree_needs_sync(ctx, needed) bind(c, name='rb_tree_needs_sync')
+       import :: c_int, c_ptr, c_int32_t
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), intent(out) :: needed
+     end function rb_tree_needs_sync
+     integer(c_int) function rb_ensure_device(ctx, son, father, nbor, numbl, active, nb, btype, numbb, bgrid, &
+          & uold) bind(c, name='rb_ensure_device')
+       import :: c_int, c_ptr, c_int32_t, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int32_t), intent(in) :: son(*), father(*), nbor(*), numbl(*), active(*)
+       integer(c_int32_t), value :: nb
+       integer(c_int32_t), intent(in) :: btype(*), numbb(*), bgrid(*)
+       real(c_double), intent(in) :: uold(*)
+     end function rb_ensure_device
+     integer(c_int) function rb_ensure_host(ctx, uold) bind(c, name='rb_ensure_host')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       real(c_double), intent(inout) :: uold(*)
+     end function rb_ensure_host
      type(c_ptr) function rb_last_error() bind(c, name='rb_last_error')
        import :: c_ptr
      end function rb_last_error
@@ -136,6 +173,10 @@ contains
     type(rb_mesh_params_t) :: mp
     integer :: l
     if (c_associated(rb_ctx)) return
+    if (no_inflow) then
+       write(*,*) 'rb_b200: no_inflow is not supported by the device boundary fill'
+       call clean_stop
+    end if
     hp%gamma = gamma; hp%smallr = smallr; hp%smallc = smallc
     hp%courant_factor = courant_factor; hp%slope_theta = slope_theta
     hp%slope_type = slope_type; hp%scheme = 0; hp%pressure_fix = 0
@@ -162,70 +203,79 @@ contains
     call rb_b200_check(rb_create(hp, mp, 0_c_int, rb_ctx), 'rb_create')
   end subroutine rb_b200_init
 
-  ! host -> device: the tree (when any level's oct count or the son array
-  ! changed) and the whole uold
-  subroutine rb_b200_push
+  ! before a device hydro call: the tree when the host changed it (the tree
+  ! arrays are gathered only then), uold when the host copy is newer
+  subroutine rb_b200_device
     use amr_commons
     use hydro_commons
     integer(c_int32_t), allocatable :: numbl(:), act(:), numbb(:,:), bgrid(:), btype(:)
-    integer(c_int64_t) :: stamp
+    integer(c_int32_t) :: need, dummy(1)
     integer :: l, i, n, ib
     call rb_b200_init
-    stamp = 0
-    do l = 1, nlevelmax
-       stamp = stamp * 31 + active(l)%ngrid
-    end do
-    do i = 1, ncoarse + twotondim * ngridmax, 97
-       stamp = stamp * 7 + son(i)
-    end do
-    if (stamp /= rb_tree_stamp) then
-       allocate(numbl(nlevelmax))
-       n = 0
-       do l = 1, nlevelmax
-          numbl(l) = active(l)%ngrid
-          n = n + active(l)%ngrid
-       end do
-       allocate(act(max(n, 1)))
-       n = 0
-       do l = 1, nlevelmax
-          do i = 1, active(l)%ngrid
-             n = n + 1
-             act(n) = active(l)%igrid(i)
-          end do
-       end do
-       ! physical boundaries: boundary(ibound,ilevel)%igrid, level by level
-       allocate(numbb(max(nboundary, 1), nlevelmax))
-       n = 0
-       do l = 1, nlevelmax
-          do ib = 1, nboundary
-             numbb(ib, l) = boundary(ib, l)%ngrid
-             n = n + boundary(ib, l)%ngrid
-          end do
-       end do
-       allocate(bgrid(max(n, 1)), btype(max(nboundary, 1)))
-       btype = 0
-       if (nboundary > 0) btype(1:nboundary) = boundary_type(1:nboundary)
-       n = 0
-       do l = 1, nlevelmax
-          do ib = 1, nboundary
-             do i = 1, boundary(ib, l)%ngrid
-                n = n + 1
-                bgrid(n) = boundary(ib, l)%igrid(i)
-             end do
-          end do
-       end do
-       call rb_b200_check(rb_set_boundary(rb_ctx, int(nboundary, c_int32_t), btype, numbb, bgrid), &
-            & 'rb_set_boundary')
-       call rb_b200_check(rb_sync_tree(rb_ctx, son, father, nbor, numbl, act), 'rb_sync_tree')
-       deallocate(numbl, act, numbb, bgrid, btype)
-       rb_tree_stamp = stamp
+    call rb_b200_check(rb_tree_needs_sync(rb_ctx, need), 'rb_tree_needs_sync')
+    if (need == 0) then
+       dummy = 0
+       call rb_b200_check(rb_ensure_device(rb_ctx, son, father, nbor, dummy, dummy, 0_c_int32_t, dummy, &
+            & dummy, dummy, uold), 'rb_ensure_device')
+       return
     end if
-    call rb_b200_check(rb_upload_state(rb_ctx, uold), 'rb_upload_state')
-  end subroutine rb_b200_push
+    allocate(numbl(nlevelmax))
+    n = 0
+    do l = 1, nlevelmax
+       numbl(l) = active(l)%ngrid
+       n = n + active(l)%ngrid
+    end do
+    allocate(act(max(n, 1)))
+    n = 0
+    do l = 1, nlevelmax
+       do i = 1, active(l)%ngrid
+          n = n + 1
+          act(n) = active(l)%igrid(i)
+       end do
+    end do
+    ! physical boundaries: boundary(ibound,ilevel)%igrid, level by level
+    allocate(numbb(max(nboundary, 1), nlevelmax))
+    n = 0
+    do l = 1, nlevelmax
+       do ib = 1, nboundary
+          numbb(ib, l) = boundary(ib, l)%ngrid
+          n = n + boundary(ib, l)%ngrid
+       end do
+    end do
+    allocate(bgrid(max(n, 1)), btype(max(nboundary, 1)))
+    btype = 0
+    if (nboundary > 0) btype(1:nboundary) = boundary_type(1:nboundary)
+    n = 0
+    do l = 1, nlevelmax
+       do ib = 1, nboundary
+          do i = 1, boundary(ib, l)%ngrid
+             n = n + 1
+             bgrid(n) = boundary(ib, l)%igrid(i)
+          end do
+       end do
+    end do
+    call rb_b200_check(rb_ensure_device(rb_ctx, son, father, nbor, numbl, act, int(nboundary, c_int32_t), &
+         & btype, numbb, bgrid, uold), 'rb_ensure_device')
+    deallocate(numbl, act, numbb, bgrid, btype)
+  end subroutine rb_b200_device
 
-  subroutine rb_b200_pull
+  ! before host code reads uold
+  subroutine rb_b200_host
     use hydro_commons
-    call rb_b200_check(rb_download_state(rb_ctx, uold), 'rb_download_state')
-  end subroutine rb_b200_pull
+    if (.not. c_associated(rb_ctx)) return
+    call rb_b200_check(rb_ensure_host(rb_ctx, uold), 'rb_ensure_host')
+  end subroutine rb_b200_host
+
+  ! the host changed son/father/nbor/active or the boundary lists
+  subroutine rb_b200_tree_changed
+    call rb_b200_init
+    call rb_b200_check(rb_note_tree_changed(rb_ctx), 'rb_note_tree_changed')
+  end subroutine rb_b200_tree_changed
+
+  ! the host wrote uold
+  subroutine rb_b200_host_wrote
+    call rb_b200_init
+    call rb_b200_check(rb_note_host_state_written(rb_ctx), 'rb_note_host_state_written')
+  end subroutine rb_b200_host_wrote
 
 end module rb_b200

@@ -79,6 +79,13 @@ _PROTOS = {
     "rb_make_boundary_hydro": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_upload_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_note_tree_changed": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_note_host_state_written": (ctypes.c_int, [ctypes.c_void_p]),
+    "rb_tree_needs_sync": (ctypes.c_int, [ctypes.c_void_p, _P32]),
+    "rb_ensure_device": (ctypes.c_int, [ctypes.c_void_p, _P32, _P32, _P32, _P32, _P32, ctypes.c_int32, _P32, _P32,
+                                        _P32, _PD]),
+    "rb_ensure_host": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_transfer_stats": (ctypes.c_int, [ctypes.c_void_p, _P64, _P64, _P64, _P64]),
     "rb_download_pressure_fix": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
     "rb_upload_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
@@ -251,6 +258,49 @@ class Solver:
 
     def make_boundary_hydro(self, ilevel: int):
         _check(load().rb_make_boundary_hydro(self._h, ilevel), "rb_make_boundary_hydro")
+
+    # ---- residency protocol of the drop-in boundary ----
+    def note_tree_changed(self, tree: Optional[Octree] = None):
+        """The host changed the tree (refine_fine, load_balance, defrag)."""
+        if tree is not None:
+            self.tree = tree
+        _check(load().rb_note_tree_changed(self._h), "rb_note_tree_changed")
+
+    def note_host_state_written(self):
+        _check(load().rb_note_host_state_written(self._h), "rb_note_host_state_written")
+
+    def ensure_device(self, uold: np.ndarray):
+        """Before a device hydro call: re-sync the tree if the host changed
+        it, upload uold only if the host copy is the newer one."""
+        t = self.tree
+        son = np.ascontiguousarray(t.son, np.int32)
+        father = np.ascontiguousarray(t.father, np.int32)
+        nbor = np.ascontiguousarray(t.nbor, np.int32)
+        numbl = np.array([t.noct(l) for l in range(1, t.nlevelmax + 1)], np.int32)
+        act, _ = t.active_concat()
+        bt, boff, bg = t.boundary_concat()
+        numbb = np.diff(boff).astype(np.int32)
+        u = np.ascontiguousarray(uold, np.float64)
+        assert u.shape == (5, t.ncell)
+        _check(load().rb_ensure_device(self._h, _ptr(son, _P32), _ptr(father, _P32), _ptr(nbor, _P32),
+                                       _ptr(numbl, _P32), _ptr(act, _P32), len(bt), _ptr(bt, _P32),
+                                       _ptr(numbb, _P32), _ptr(bg, _P32), _ptr(u, _PD)), "rb_ensure_device")
+
+    def tree_needs_sync(self) -> bool:
+        n = ctypes.c_int32()
+        _check(load().rb_tree_needs_sync(self._h, ctypes.byref(n)), "rb_tree_needs_sync")
+        return bool(n.value)
+
+    def ensure_host(self, uold: np.ndarray):
+        """Before host code reads uold: download it if the device copy is newer."""
+        assert uold.dtype == np.float64 and uold.flags.c_contiguous and uold.shape == (5, self.tree.ncell)
+        _check(load().rb_ensure_host(self._h, _ptr(uold, _PD)), "rb_ensure_host")
+
+    def transfer_stats(self) -> dict:
+        v = [ctypes.c_int64() for _ in range(4)]
+        _check(load().rb_transfer_stats(self._h, *[ctypes.byref(x) for x in v]), "rb_transfer_stats")
+        return dict(zip(("h2d_state_bytes", "d2h_state_bytes", "tree_syncs", "octs_prolonged"),
+                        (x.value for x in v)))
 
     def upload_state(self, uold: np.ndarray):
         u = np.ascontiguousarray(uold, np.float64)

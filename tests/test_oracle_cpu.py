@@ -13,6 +13,8 @@ from ramses_b200.params import HydroParams
 import exact_riemann
 from helpers import leaf_values, random_blocks, sedov_amr, sedov_uniform
 
+ROOT = Path(__file__).resolve().parent.parent
+
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
@@ -563,3 +565,25 @@ def test_boundary_amr_runs_and_conserves_inside():
         run.coarse_step()
     _, a1 = leaf_values(tree, run.uold)
     assert abs(a1[0].sum() - a0[0].sum()) <= 1e-13 * a0[0].sum()
+
+
+def test_operation_counts_of_the_oracle_stages():
+    """oracle/opcount.cpp counts the oracle's own arithmetic: the conservative
+    update is 30 additions per cell (3 directions x 5 variables x 2), HLLC
+    takes two square roots per face, and the committed summary's totals are
+    the ones the harness prints."""
+    from oracle import opcount
+    c = opcount.counts(3, 2)
+    assert c["update_per_cell"]["add"] == 30 and c["update_per_cell"]["mul"] == 0
+    assert c["riemann_per_face"]["sqrt"] == 2
+    assert c["ctoprim_per_cell"]["div"] >= 1 and c["ctoprim_per_cell"]["sqrt"] == 1
+    a = c["algorithmic_per_cell_update"]
+    # per cell: ctoprim + slopes + trace + 3 faces (Riemann and scaling) + update + cmpdt
+    parts = ["ctoprim_per_cell", "uslope_per_cell", "trace3d_per_cell", "update_per_cell", "cmpdt_per_cell"]
+    flops = sum(c[k]["flops"] for k in parts) + 3 * (c["riemann_per_face"]["flops"] + c["flux_scale_per_face"]["flops"])
+    assert abs(a["flops"] - flops) < 1e-3
+    # godunov_fine's 6^3 stencil per oct does several times the algorithmic work
+    assert c["reference_dense_step_per_cell_update"]["flops"] > 4 * a["flops"]
+    summary = (ROOT / "profiles" / "opcount_hllc_moncen_turb.md").read_text()
+    assert "algorithmic_fp64_flops_per_cell_update: %.1f" % a["flops"] in summary
+    assert "algorithmic_ops_per_cell_update: %.1f" % opcount.total_ops(a) in summary
