@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
                     help="instead of the headline, time device-scheduled coarse steps (rb_run) on a static AMR "
                          "tree: sedov = Sedov levels 6-9 refined on a shell, clumps = blast-clump levels 7-10")
+    ap.add_argument("--serve-requests", type=int, default=48,
+                    help="requests of the bounded serving pass (0: none)")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
                     help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
@@ -245,6 +247,37 @@ def cpu_sample(tree, hp, u, nocts, reps, warmup):
     desc = ("oracle (C restatement, OpenMP %d threads) hydro step on %d of %d octs (%d cells, Morton-contiguous) "
             "of the same workload, %d timed repetitions" % (cores, nocts, tree.noct(level), cells, len(times)))
     return value, cores, desc
+
+
+def serving_pass(nreq, rate=100.0, seed=0):
+    """A bounded pass of the ensemble-serving workload: ``nreq`` seeded
+    requests (shock tubes along x with outflow boundaries and Sedov blasts on
+    32^3 / 64^3 base grids with 0..1 extra levels, to t = 0.1) arriving as a
+    Poisson process, through the FP32-mixed serving engine; beside it the
+    same stream served one at a time by the plain FP64 path (measured service
+    times replayed through a FIFO queue with the same arrivals)."""
+    from ramses_b200 import serve
+    from ramses_b200.params import HydroParams
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+    specs = serve.draw_requests(nreq, seed, (32, 64), 1)
+    t0 = time.perf_counter()
+    reqs = [serve.build_request(sp, hp, outflow=True) for sp in specs]
+    build_s = time.perf_counter() - t0
+    arrivals = serve.poisson_arrivals(nreq, rate, seed + 1)
+    with serve.Server(hp, precision="mixed") as srv:
+        res = serve.run_stream(srv, reqs, arrivals, 0.1, keep_results=False)
+    base = serve.one_at_a_time(reqs, hp, 0.1, "fp64")
+    comp = serve.fifo_completion(arrivals, base["service_s"])
+    b = serve.percentiles(comp - arrivals)
+    return {"workload": "%d requests (tubes with outflow in x, Sedov), 32^3/64^3 base grids +0..1 levels, t_end=0.1, "
+                        "Poisson %g req/s, seed %d" % (nreq, rate, seed),
+            "dense_requests": sum(r.is_dense for r in reqs), "amr_requests": sum(not r.is_dense for r in reqs),
+            "p50_s": res["latency_s"]["p50"], "p99_s": res["latency_s"]["p99"],
+            "updates_per_s": res["cell_updates_per_s"], "cell_updates": res["cell_updates"],
+            "makespan_s": res["makespan_s"], "precision": "fp32-mixed", "ic_build_s": build_s,
+            "one_at_a_time_fp64": {"p50_s": b["p50"], "p99_s": b["p99"],
+                                   "updates_per_s": base["cell_updates"] / float(sum(base["service_s"])),
+                                   "makespan_s": float(comp[-1] - arrivals[0])}}
 
 
 def run_reference(args):
@@ -558,6 +591,9 @@ def main():
         t_hbm = BYTES_PER_CELL_UPDATE * cells / (peak * 1e9)
         issue_ceiling = min(1.0, t_hbm / t_issue)
     f64_flops = ops.get("algorithmic_fp64_flops_per_cell_update")
+    serving = None
+    if world == 1 and args.serve_requests > 0:
+        serving = serving_pass(args.serve_requests)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         nocts = min(args.cpu_sample_octs, tree.noct(level))
@@ -594,6 +630,7 @@ def main():
                      "flop_peak": "nominal FP64 %.1f TFLOP/s (64 FMA lanes/SM, 148 SMs, 1.965 GHz)"
                                   % FP64_NOMINAL_TFLOPS},
             "mixed_over_fp64": value / f64_value,
+            "serving": serving,
             "accuracy": {"l1_rho_mixed_vs_fp64": l1_rho, "linf_rel_rho_mixed_vs_fp64": linf_rho,
                          "mixed_vs_fp64": errs,
                          "steps_compared": acc_steps,

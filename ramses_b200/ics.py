@@ -54,8 +54,12 @@ def sedov_prim(level: int, boxlen: float = 1.0, rho0: float = 1.0, p0: float = 1
     dx = boxlen * 0.5 ** level
     n = 2 ** level
     c = np.asarray(centre) * boxlen
-    idx = (np.arange(n) + 0.5) * dx
-    X, Y, Z = np.meshgrid(idx, idx, idx, indexing="ij")
+    # the cells within radius_cells of the centre lie in a window of
+    # indices around it: count them there (same distance expression)
+    lo = np.maximum(np.floor(c / dx - radius_cells - 2).astype(np.int64), 0)
+    hi = np.minimum(np.ceil(c / dx + radius_cells + 2).astype(np.int64), n)
+    ax = [(np.arange(lo[d], hi[d]) + 0.5) * dx for d in range(3)]
+    X, Y, Z = np.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
     r = np.sqrt(((X - c[0]) / dx) ** 2 + ((Y - c[1]) / dx) ** 2 + ((Z - c[2]) / dx) ** 2)
     ncell = int(np.count_nonzero(r < radius_cells))
     p_in = (gamma - 1.0) * energy / (ncell * dx ** 3)

@@ -243,8 +243,29 @@ class BuiltRequest:
         return self.dense is not None
 
 
+def _tree_key(spec: RequestSpec, refine_threshold: float, outflow: bool):
+    """Requests whose initial refinement is the same share one octree: a
+    Sedov blast's gradient flags are its blast region for every E of the mix
+    (the deposited pressure exceeds the ambient 1e-5 by orders of magnitude),
+    a tube's are its interface planes whenever the density or pressure step
+    passes the relative-gradient threshold there (hydro_refine's
+    |f(i+1)-f(i-1)| / (|f(i+1)|+|f(i)|+|f(i-1)|) at the two cells beside the
+    step), else none."""
+    if spec.kind == "sedov":
+        return ("sedov", spec.n, spec.extra, refine_threshold)
+    p = spec.params
+
+    def step_err(a, b):
+        return abs(b - a) / (abs(a) + abs(b) + min(abs(a), abs(b)))
+    refined = max(step_err(p["rho_l"], p["rho_r"]), step_err(p["p_l"], p["p_r"])) > refine_threshold
+    return ("tube", spec.n, spec.extra, refine_threshold, bool(outflow), refined)
+
+
+_TREE_CACHE: dict = {}
+
+
 def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 0.1,
-                  outflow: bool = False) -> BuiltRequest:
+                  outflow: bool = False, cache: bool = True) -> BuiltRequest:
     """Initial state of a request. Uniform requests become dense grids; AMR
     requests a static octree refined on the relative density/pressure
     gradients of the initial state. outflow: a tube request has outflow
@@ -276,9 +297,14 @@ def build_request(spec: RequestSpec, hp: HydroParams, refine_threshold: float = 
         def ref(level, cells):
             n = 2 ** level
             return np.asarray(grad(level, cells), bool) & (cells[:, 0] >= 4) & (cells[:, 0] < n - 4)
-    tree = mesh.build_tree(lmin, lmin + spec.extra, ref)
-    if outflow and spec.kind == "tube":
-        tree = mesh.add_boundaries(tree, ("outflow", None, None))
+    key = _tree_key(spec, refine_threshold, outflow)
+    tree = _TREE_CACHE.get(key) if cache else None
+    if tree is None:
+        tree = mesh.build_tree(lmin, lmin + spec.extra, ref)
+        if outflow and spec.kind == "tube":
+            tree = mesh.add_boundaries(tree, ("outflow", None, None))
+        if cache:
+            _TREE_CACHE[key] = tree
     return BuiltRequest(spec, tree=tree, uold=ics.fill_all_levels(tree, prim, hp.gamma))
 
 
@@ -313,9 +339,11 @@ def percentiles(x: Sequence[float]) -> dict:
 
 
 def run_stream(server: Server, reqs: Sequence[BuiltRequest], arrivals: Sequence[float], t_end: float,
-               timeout_s: float = 3600.0) -> dict:
+               timeout_s: float = 3600.0, keep_results: bool = True) -> dict:
     """Serve ``reqs`` arriving at ``arrivals`` (seconds from start) in real
-    time; time-to-solution = result in host memory - arrival."""
+    time; time-to-solution = result in host memory - arrival. With
+    ``keep_results`` False each result array is dropped once its request is
+    done (long streams)."""
     order = np.argsort(arrivals, kind="stable")
     t0 = time.perf_counter()
     arrive, finish, ids = {}, {}, {}
@@ -333,6 +361,8 @@ def run_stream(server: Server, reqs: Sequence[BuiltRequest], arrivals: Sequence[
             k += 1
         for rid in server.progress():
             finish[ids[rid]] = time.perf_counter() - t0
+            if not keep_results:
+                server.results.pop(rid, None)
         if server.stats()["active"] == 0 and server.stats()["queued"] == 0 and k < n:
             time.sleep(max(0.0, min(0.002, arrivals[order[k]] - (time.perf_counter() - t0))))
         if time.perf_counter() - t0 > timeout_s:
@@ -356,7 +386,7 @@ def one_at_a_time(reqs: Sequence[BuiltRequest], hp: HydroParams, t_end: float, p
     request on the GPU at a time (the FP64 z-streaming step for dense
     problems, device-scheduled coarse steps as Solver.run for AMR ones),
     submission to result in host memory. Returns the service times."""
-    service, updates = [], 0
+    service, updates, per = [], 0, []
     with Server(hp, precision=precision) as srv:
         for b in reqs:
             t0 = time.perf_counter()
@@ -364,8 +394,10 @@ def one_at_a_time(reqs: Sequence[BuiltRequest], hp: HydroParams, t_end: float, p
                    else srv.submit_octree(b.tree, b.uold, t_end=t_end))
             srv.drain()
             service.append(time.perf_counter() - t0)
-            updates += srv.info(rid)["cell_updates"]
-    return {"service_s": service, "cell_updates": updates}
+            per.append(srv.info(rid)["cell_updates"])
+            updates += per[-1]
+            srv.results.pop(rid, None)
+    return {"service_s": service, "cell_updates": updates, "cell_updates_each": per}
 
 
 def main(argv=None):
@@ -383,19 +415,30 @@ def main(argv=None):
     ap.add_argument("--baseline", action="store_true", help="also serve the stream one at a time with plain FP64")
     ap.add_argument("--periodic-tubes", action="store_true",
                     help="tubes in a periodic box instead of outflow boundaries in x")
+    ap.add_argument("--ic-pool", type=int, default=0,
+                    help="build only this many distinct initial states; request i takes state i mod N "
+                         "(long streams: host memory and set-up time)")
     args = ap.parse_args(argv)
     hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
     specs = draw_requests(args.requests, args.seed, [int(x) for x in args.sizes.split(",")], args.max_extra)
     t0 = time.perf_counter()
-    reqs = [build_request(s, hp, outflow=not args.periodic_tubes) for s in specs]
+    npool = args.ic_pool if args.ic_pool > 0 else len(specs)
+    pool = [build_request(s, hp, outflow=not args.periodic_tubes) for s in specs[:npool]]
+    reqs = [pool[i % npool] for i in range(len(specs))]
     build_s = time.perf_counter() - t0
     rates = [float(r) for r in args.rates.split(",")] if args.rates else [args.rate]
-    base = one_at_a_time(reqs, hp, args.t_end, "fp64") if args.baseline else None
+    base = None
+    if args.baseline:
+        # a request's service time is a function of its initial state: the
+        # pool's are measured, request i takes the time of state i mod N
+        pb = one_at_a_time(pool, hp, args.t_end, "fp64")
+        base = {"service_s": [pb["service_s"][i % npool] for i in range(len(reqs))],
+                "cell_updates": int(sum(pb["cell_updates_each"][i % npool] for i in range(len(reqs))))}
     sweep = []
     for rate in rates:
         arrivals = poisson_arrivals(len(reqs), rate, args.seed + 1)
         with Server(hp, precision=args.precision, steps_per_round=args.steps_per_round) as srv:
-            res = run_stream(srv, reqs, arrivals, args.t_end)
+            res = run_stream(srv, reqs, arrivals, args.t_end, keep_results=npool == len(reqs))
             launches = srv.stats()["batch_launches"]
         row = {"rate_per_s": rate, "latency_s": res["latency_s"], "makespan_s": res["makespan_s"],
                "cell_updates_per_s": res["cell_updates_per_s"], "cell_updates": res["cell_updates"],
@@ -409,8 +452,9 @@ def main(argv=None):
                                          "cell_updates_per_s": base["cell_updates"] / float(sum(base["service_s"])),
                                          "cell_updates": base["cell_updates"]}
         sweep.append(row)
-    out = {"workload": "ensemble serving: %d requests (%s), Poisson %s req/s, t_end=%g, seed %d"
-           % (len(reqs), args.sizes, ",".join("%g" % r for r in rates), args.t_end, args.seed),
+    out = {"workload": "ensemble serving: %d requests (%s, +0..%d levels), Poisson %s req/s, t_end=%g, seed %d%s"
+           % (len(reqs), args.sizes, args.max_extra, ",".join("%g" % r for r in rates), args.t_end, args.seed,
+              ", initial states from a pool of %d" % npool if npool < len(reqs) else ""),
            "precision": args.precision, "ic_build_s": build_s,
            "dense_requests": sum(r.is_dense for r in reqs), "amr_requests": sum(not r.is_dense for r in reqs)}
     if len(sweep) == 1:
