@@ -286,6 +286,14 @@ class Solver:
                                        _ptr(numbl, _P32), _ptr(act, _P32), len(bt), _ptr(bt, _P32),
                                        _ptr(numbb, _P32), _ptr(bg, _P32), _ptr(u, _PD)), "rb_ensure_device")
 
+    def write_snapshot(self, outdir, nout: int, nstep_coarse: int = 0):
+        """dump_all's amr/hydro files of the current state (downloaded from the
+        device) in RAMSES's output format: ramses_b200.snapshot."""
+        from . import snapshot
+        u = self.download_state()
+        return snapshot.write_snapshot(outdir, nout, self.tree, u, self.hp.gamma, self.hp.smallr, t=self.t,
+                                       nstep_coarse=nstep_coarse)
+
     def tree_needs_sync(self) -> bool:
         n = ctypes.c_int32()
         _check(load().rb_tree_needs_sync(self._h, ctypes.byref(n)), "rb_tree_needs_sync")

@@ -2,14 +2,18 @@
 known-answer table (tests/hydro/sod-tube/sod-tube-ana.dat: index, x, u, rho,
 P, e at t=0.245, gamma=1.4, left (1,0,1), right (0.125,0,0.1), interface at
 x=0.5). Every 4th row is kept (x, u, rho, P). Run once where the reference
-tree is available; the CSV is committed."""
+tree is available; the CSV is committed.
+
+    python tests/golden/make_sod_fixture.py <reference>/tests/hydro/sod-tube/sod-tube-ana.dat
+"""
 import sys
 from pathlib import Path
 
 import numpy as np
 
-SRC = Path(sys.argv[1] if len(sys.argv) > 1 else
-           "/root/reference/tests/hydro/sod-tube/sod-tube-ana.dat")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_sod_fixture.py <path of the reference's tests/hydro/sod-tube/sod-tube-ana.dat>")
+SRC = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent / "sod_tube_ana.csv"
 
 d = np.loadtxt(SRC)
