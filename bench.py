@@ -181,11 +181,16 @@ def hbm_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(method):
+def ncu_traffic(method, kernel=""):
     """DRAM bytes per launch of the dominant FP32-mixed kernel on this
-    workload, from the committed ncu summary (line
+    workload, from the committed ncu summary of that kernel (line
     'traffic_bytes_per_launch: N')."""
-    name = "stream_step_mixed_turb256.md" if method == "stream" else "godunov_tile_mixed_turb256.md"
+    if method != "stream":
+        name = "godunov_tile_mixed_turb256.md"
+    elif kernel.startswith("stream2_step_kernel"):
+        name = "stream2_step_mixed_turb256.md"
+    else:
+        name = "stream_step_mixed_turb256.md"
     f = ROOT / "profiles" / name
     if not f.exists():
         return None
@@ -579,7 +584,7 @@ def main():
 
     peak, peak_kind = hbm_peak()
     achieved = BYTES_PER_CELL_UPDATE * cells / (kern_ms / 1e3) / 1e9
-    traffic = ncu_traffic(args.method)
+    traffic = ncu_traffic(args.method, mixed_kernel)
     # issue ceiling: one instruction per counted operation at full issue
     # (148 SMs x 4 schedulers x 32 threads per cycle at the sampled SM clock)
     ops = opcount_figures()
