@@ -162,6 +162,14 @@ def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
     grids are reserved beyond the octs built (ngridmax, room for
     ``remesh``).
     """
+    return _assemble(oct_sets(levelmin, nlevelmax, refine, nexpand), levelmin, nlevelmax or levelmin, boxlen, spare)
+
+
+def oct_sets(levelmin: int, nlevelmax: Optional[int] = None,
+             refine: Optional[Callable[[int, np.ndarray], np.ndarray]] = None, nexpand: int = 1) -> dict:
+    """The oct coordinates of every level (dict level -> (n, 3)) of the tree
+    that ``build_tree`` assembles: ``refine`` flags, expanded by ``nexpand``
+    cells, closed under the nesting rule."""
     if nlevelmax is None:
         nlevelmax = levelmin
     if not (1 <= levelmin <= nlevelmax <= MAXLEVEL - 1):
@@ -223,7 +231,53 @@ def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
         fc = fc[np.isin(_keys(fc // 2, n // 2), parent_keys)]
         refined[l] = fc
         oct_coords[l + 1] = fc
-    return _assemble(oct_coords, levelmin, nlevelmax, boxlen, spare)
+    return oct_coords
+
+
+def flag_refine(tree: "Octree", flag1: np.ndarray) -> Callable[[int, np.ndarray], np.ndarray]:
+    """A ``refine`` callback for ``oct_sets`` from per-cell flags of a tree
+    (flag1[icell], icell the Fortran cell index, as hydro_flag sets them):
+    a level-l cell is flagged when it is a cell of the tree and flagged, or
+    when it is refined and one of its children is (so that refined regions
+    shrink only from their finest level, one level per remesh)."""
+    lookups = {}
+    for l in range(1, tree.nlevelmax + 1):
+        if tree.noct(l) == 0:
+            continue
+        n = 2 ** (l - 1)
+        k = _keys(tree.coords[l], n)
+        srt = np.argsort(k)
+        lookups[l] = (k[srt], np.asarray(tree.active[l], np.int64)[srt])
+
+    def cells_of(level, cells):
+        """Fortran cell indices of level-``level`` cells (0 where absent)."""
+        if level not in lookups:
+            return np.zeros(len(cells), np.int64)
+        ks, ig = lookups[level]
+        n = 2 ** (level - 1)
+        k = _keys(cells // 2, n)
+        pos = np.minimum(np.searchsorted(ks, k), len(ks) - 1)
+        ok = ks[pos] == k
+        ind = (cells[:, 0] & 1) + 2 * (cells[:, 1] & 1) + 4 * (cells[:, 2] & 1)
+        return np.where(ok, tree.ncoarse + ind * tree.ngridmax + ig[pos], 0)
+
+    def refine(level, cells):
+        c = cells_of(level, cells)
+        have = c > 0
+        flag = np.zeros(len(cells), bool)
+        flag[have] = flag1[c[have]] != 0
+        if level + 1 <= tree.nlevelmax:
+            son = np.zeros(len(cells), np.int64)
+            son[have] = tree.son[c[have] - 1]
+            kids = son > 0
+            if kids.any():
+                g = son[kids]
+                sub = np.zeros(len(g), bool)
+                for ind in range(8):
+                    sub |= tree.son[tree.ncoarse + ind * tree.ngridmax + g - 1] > 0
+                flag[np.nonzero(kids)[0][sub]] = True
+        return flag
+    return refine
 
 
 def _assemble(oct_coords, levelmin, nlevelmax, boxlen, spare=0) -> Octree:
