@@ -71,6 +71,14 @@ def parse():
     ap.add_argument("--amr", choices=["sedov", "clumps"], default=None,
                     help="instead of the headline, time device-scheduled coarse steps (rb_run) on a static AMR "
                          "tree: sedov = Sedov levels 6-9 refined on a shell, clumps = blast-clump levels 7-10")
+    ap.add_argument("--remesh", type=int, default=0, metavar="K",
+                    help="with --amr sedov: the dynamic run of config 1, remeshed from the device's refinement "
+                         "flags every K coarse steps until --t-end (periodic box)")
+    ap.add_argument("--t-end", type=float, default=0.05, help="end time of the --remesh run")
+    ap.add_argument("--remesh-spare", type=int, default=1500000,
+                    help="free grids reserved for the --remesh run's growing tree")
+    ap.add_argument("--remesh-wall", type=float, default=600.0,
+                    help="host wall-time budget (s) of the --remesh run: it reports where it stopped")
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests of the bounded serving pass (0: none)")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
@@ -370,6 +378,111 @@ def amr_workload(name, periodic=False):
     return tree, hp, ics.fill_all_levels(tree, prim, hp.gamma), desc
 
 
+def run_remesh(args):
+    """Config 1 with its refinement criterion, remeshed while it runs: Sedov
+    (E=1, rho=1, P=1e-5) on levels 6-9, hllc, slope 1, courant 0.8,
+    nsubcycle 2, refined from hydro_flag on the device (err_grad_d =
+    err_grad_p = 0.1, the criterion of hydro/hydro_flag.f90) every K coarse
+    steps until t_end. The tree is the host's (refine_fine's stand-in,
+    mesh.refine_from_flags: surviving octs keep their igrids); each remesh
+    re-syncs the library's mirror (levels whose inputs are unchanged keep
+    their tables) and prolongs the new octs on the device, so no state crosses
+    PCIe. Periodic box: the host remesher keeps igrids on single-coarse-cell
+    periodic trees, and the blast stays clear of the faces until t = 0.05
+    (shock radius ~0.35 of a unit box). Reports the hydro throughput and the
+    per-remesh cost of the flags, the host remesh and the re-sync."""
+    from ramses_b200 import ics, mesh, runtime
+    from ramses_b200.params import HydroParams, RefineParams
+    runtime.load()
+    lmin, lmax, K = 6, 9, args.remesh
+    hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+    rp = RefineParams(err_grad_d=0.1, err_grad_p=0.1)
+    prim = ics.sedov_prim(lmax)
+
+    def fields(x):
+        q = prim(x)
+        return [q[0], q[4]]
+    t0 = time.perf_counter()
+    ref = mesh.union_refine(mesh.gradient_refine(fields, [0.1, 0.1]),
+                            mesh.sphere_refine((0.5, 0.5, 0.5), 2.5 * 0.5 ** lmax))
+    tree = mesh.build_tree(lmin, lmax, ref, spare=args.remesh_spare)
+    u = ics.fill_all_levels(tree, prim, hp.gamma)
+    build_s = time.perf_counter() - t0
+    prec = args.only or "mixed"
+    s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
+    hydro_ms, flag_s, host_s, sync_s = 0.0, 0.0, 0.0, 0.0
+    coarse, remeshes, updates0 = 0, 0, s.cell_updates
+    syncs = []
+    max_coarse = args.steps if args.steps > 0 else 1 << 30
+    stop = None
+    wall0 = time.perf_counter()
+    with ClockSampler(0) as clk:
+        while s.t < args.t_end and coarse < max_coarse and time.perf_counter() - wall0 < args.remesh_wall:
+            n = s.run(t_end=args.t_end, max_steps=min(K, max_coarse - coarse))
+            s.synchronize()
+            hydro_ms += s.last_run_ms()
+            coarse += n
+            if n == 0 or s.t >= args.t_end or coarse >= max_coarse:
+                break
+            a = time.perf_counter()
+            flag1 = s.flag_tree(rp)
+            b = time.perf_counter()
+            try:
+                new = mesh.refine_from_flags(s.tree, flag1)
+            except ValueError as e:   # the tree outgrew ngridmax: report where the run stopped
+                stop = str(e)
+                break
+            c = time.perf_counter()
+            pro0 = s.transfer_stats()["octs_prolonged"]
+            s.sync_tree(new)
+            s.synchronize()
+            d = time.perf_counter()
+            st = s.sync_stats()
+            st["octs_prolonged"] = s.transfer_stats()["octs_prolonged"] - pro0
+            st["octs"] = int(sum(new.noct(l) for l in range(1, lmax + 1)))
+            syncs.append(st)
+            flag_s += b - a
+            host_s += c - b
+            sync_s += d - c
+            remeshes += 1
+            if remeshes % 10 == 0:
+                print("remesh %d: coarse %d t=%.3e octs %d, flags %.1f ms, host %.0f ms, sync %.1f ms (%d built)"
+                      % (remeshes, coarse, s.t, st["octs"], 1e3 * (b - a), 1e3 * (c - b), 1e3 * (d - c),
+                         st["levels_built"]), file=sys.stderr, flush=True)
+    wall = time.perf_counter() - wall0
+    if stop is None:
+        stop = ("t_end reached" if s.t >= args.t_end else "coarse-step cap" if coarse >= max_coarse
+                else "wall-time budget")
+    tr = s.tree
+    levels = [l for l in range(1, tr.nlevelmax + 1) if tr.noct(l)]
+    upd = s.cell_updates - updates0
+    xfer = s.transfer_stats()
+    s.close()
+    mean = lambda k: float(np.mean([x[k] for x in syncs])) if syncs else 0.0
+    line = {"metric": METRIC, "value": upd / (hydro_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": coarse,
+            "warmup": 0, "ms_per_step": hydro_ms / max(coarse, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "Sedov E=1, rho=1, P=1e-5, levels 6-9 remeshed every %d coarse steps from "
+                                   "hydro_flag (err_grad_d=err_grad_p=0.1) to t=%g, hllc, slope_type=1, courant "
+                                   "0.8, nsubcycle 2, periodic" % (K, args.t_end),
+                       "precision": prec, "path": "rb_run between remeshes; rb_hydro_flag, host remesh, "
+                                                  "rb_sync_tree with device prolongation at each remesh",
+                       "tree_build_s": build_s},
+            "t": s.t, "stopped": stop, "coarse_steps": coarse, "final_octs_per_level": {l: tr.noct(l) for l in levels},
+            "final_leaf_cells": int(sum(tr.leaf_cells(l) for l in levels)),
+            "remesh": {"count": remeshes, "every_coarse_steps": K,
+                       "flag_ms_mean": 1e3 * flag_s / max(remeshes, 1),
+                       "host_remesh_ms_mean": 1e3 * host_s / max(remeshes, 1),
+                       "sync_ms_mean": 1e3 * sync_s / max(remeshes, 1),
+                       "sync_phases_ms_mean": {k: mean(k) for k in ("index_ms", "tables_ms", "boundary_ms",
+                                                                     "prolong_ms")},
+                       "levels_built_mean": mean("levels_built"), "levels_reused_mean": mean("levels_reused"),
+                       "octs_prolonged_mean": mean("octs_prolonged"), "octs_mean": mean("octs"),
+                       "state_h2d_bytes": xfer["h2d_state_bytes"], "state_d2h_bytes": xfer["d2h_state_bytes"]},
+            "hydro_s": hydro_ms / 1e3, "wall_s": wall, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def run_amr(args):
     """Leaf-cell updates/s of rb_run (device-scheduled coarse steps from CUDA
     graphs) on a static AMR tree, FP32-mixed and FP64."""
@@ -480,6 +593,10 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.amr and args.remesh > 0:
+        if args.amr != "sedov":
+            raise SystemExit("--remesh runs the Sedov configuration")
+        return run_remesh(args)
     if args.amr:
         return run_amr(args)
     from ramses_b200 import runtime

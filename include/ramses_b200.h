@@ -125,6 +125,17 @@ int rb_ensure_device(rb_context *ctx, const int32_t *son, const int32_t *father,
 int rb_ensure_host(rb_context *ctx, double *uold);
 int rb_transfer_stats(rb_context *ctx, int64_t *h2d_state_bytes, int64_t *d2h_state_bytes, int64_t *tree_syncs,
                       int64_t *octs_prolonged);
+/* The last tree synchronisation (rb_sync_tree, or the one rb_ensure_device
+ * ran): ms[5] host wall time of the whole sync, of the per-level position
+ * indexes (with the son mirror), of the level tables, of the boundary pairs
+ * and of the device prolongation of new octs; the levels whose tables were
+ * rebuilt and those kept. A re-sync keeps a level's tables when their inputs
+ * are unchanged: the level's active list and boundary octs, the positions and
+ * nbor rows of the octs of that level and the next coarser one, and son of the
+ * coarser level's cells (compared exactly). Replaces the per-remesh rebuild
+ * that refine_fine's callers would otherwise pay (amr/refine_utils.f90:332-948
+ * changes the tree; make_grid_fine's new octs are prolonged on the device). */
+int rb_sync_stats(rb_context *ctx, double *ms, int32_t *levels_built, int32_t *levels_reused);
 /* Same for unew (for callers that interleave host work with a level step). */
 int rb_upload_unew(rb_context *ctx, const double *unew);
 int rb_download_unew(rb_context *ctx, double *unew);

@@ -45,6 +45,13 @@ static __global__ void permute_d2f_kernel(const double* __restrict__ d, double* 
     f[i] = d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)];
   }
 }
+// d[idx[i]] = v[i]: the son entries that changed in a tree re-sync
+static __global__ void scatter_son_kernel(int32_t* __restrict__ d, const int64_t* __restrict__ idx,
+                                          const int32_t* __restrict__ v, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[idx[i]] = v[i];
+}
+
 static __global__ void permute_son_kernel(const int32_t* __restrict__ f, int32_t* __restrict__ d, int64_t ncell,
                                    int32_t ncoarse, int32_t ngridmax) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += (int64_t)gridDim.x * blockDim.x)

@@ -55,6 +55,7 @@ struct Level {
   std::vector<int32_t> h_active;  // igrid (1-based), host order
   int32_t* d_active = nullptr;    // igrid-1
   int shape = -1;
+  bool shape_user = false;        // shape set by rb_set_tile_shape (else re-chosen at every table build)
   int ntile = 0;
   int32_t* d_tile_blk = nullptr;
   int32_t* d_tile_corr_off = nullptr; // [ntile+1] first correction face entry of each tile (null: none)
@@ -80,6 +81,8 @@ struct Level {
   // reference oct) pairs of this level, igrid-1 each, at [boff[r], boff[r+1])
   std::vector<int64_t> h_boff;
   int32_t* d_bpair = nullptr;
+  // the level's boundary octs (all regions, in region order) of the last sync
+  std::vector<int32_t> h_bnd;
 };
 
 // sorted (key, igrid) lookup of one level's octs
@@ -170,6 +173,15 @@ struct rb_context {
   bool prev_tree_valid = false;     // level_of/father describe the last synchronised tree
   int64_t tree_gen = 0, synced_gen = -1;
   int64_t h2d_state_bytes = 0, d2h_state_bytes = 0, tree_syncs = 0, octs_prolonged = 0;
+  // tree re-syncs: a level whose table inputs did not change keeps its
+  // tables (tables_kept: the last tree's tables are still allocated, with
+  // the boundary region types they were built for); wall time of the phases
+  // of the last sync (ms: total, per-level index, level tables, boundary
+  // pairs, new-oct prolongation) and its levels rebuilt / reused
+  bool tables_kept = false;
+  std::vector<int32_t> tables_btype;
+  double sync_ms[5] = {0, 0, 0, 0, 0};
+  int32_t levels_built = 0, levels_reused = 0;
   // scheduler state (amr_commons dtnew/dtold, t, nstep)
   double dtnew[RB_MAXLEVEL + 2] = {0}, dtold[RB_MAXLEVEL + 2] = {0};
   double t = 0.0;

@@ -7,6 +7,11 @@
 // (amr/amr_step.f90:320-445) that drives the level kernels on one stream.
 // Compiled with --fmad=false (FP64 kernels bit-identical to the reference
 // operation order).
+#include <atomic>
+#include <chrono>
+#include <mutex>
+#include <thread>
+
 #include "rb_context.h"
 
 using namespace rbi;
@@ -118,19 +123,66 @@ void free_dense(rb_context* c) {
   c->stream_shape = -1;
 }
 
-void free_tree(rb_context* c) {
+// Drop the synchronised tree. With keep_tables the per-level tables, active
+// lists (host and device) and boundary lists stay allocated (tables_kept) for
+// the next rb_sync_tree, which reuses the levels whose inputs did not change.
+void free_tree(rb_context* c, bool keep_tables = false) {
   drop_graph(c);
   free_dense(c);
+  const bool keep = keep_tables && (c->have_tree || c->tables_kept);
   for (int l = 0; l <= RB_MAXLEVEL + 1; l++) {
-    free_level_tables(c->lv[l]);
-    dfree(c->lv[l].d_active);
-    dfree(c->lv[l].d_bpair);
-    c->lv[l].h_boff.clear();
-    c->lv[l].noct = 0;
-    c->lv[l].h_active.clear();
+    Level& L = c->lv[l];
+    dfree(L.d_bpair);
+    L.h_boff.clear();
+    if (keep) continue;
+    dfree(L.d_active);
+    free_level_tables(L);
+    L.noct = 0;
+    L.h_active.clear();
+    L.h_bnd.clear();
   }
+  c->tables_kept = keep;
   c->have_tree = false;
 }
+
+// Run f(begin, end) over [0, n) on up to hardware_concurrency host threads
+// (one chunk each; small ranges run on the calling thread).
+template <typename F>
+void parallel_for(int64_t n, int64_t min_chunk, F&& f) {
+  int64_t nt = std::max(1u, std::thread::hardware_concurrency());
+  nt = std::min<int64_t>(std::min<int64_t>(nt, 32), std::max<int64_t>(1, n / std::max<int64_t>(1, min_chunk)));
+  if (nt <= 1) {
+    f((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  th.reserve((size_t)nt);
+  for (int64_t t = 0; t < nt; t++) th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt); });
+  for (auto& x : th) x.join();
+}
+
+// first error of a parallel region, reported through fail() on the calling
+// thread afterwards (the last-error string is thread-local)
+struct ParError {
+  std::atomic<bool> set{false};
+  std::mutex m;
+  int code = RB_OK;
+  std::string msg;
+  void record(int code_, const char* fmt, ...) {
+    if (set.load()) return;
+    std::lock_guard<std::mutex> g(m);
+    if (set.load()) return;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    code = code_;
+    msg = buf;
+    set.store(true);
+  }
+  int report() const { return set.load() ? fail(code, "%s", msg.c_str()) : RB_OK; }
+};
 
 // With physical boundaries a tile must not hold both octs of the box and
 // boundary octs: along a bounded axis the tile's octs must divide the
@@ -228,12 +280,36 @@ void father_nbor_cells(const rb_context* c, int l, int64_t f, int64_t cells[7]) 
   }
 }
 
+// RB_SYNC_TRACE=1 in the environment: the host time of each part of a level
+// table build goes to stderr (the tree re-sync's cost breakdown).
+bool sync_trace() {
+  static const bool on = [] {
+    const char* v = std::getenv("RB_SYNC_TRACE");
+    return v && v[0] && v[0] != '0';
+  }();
+  return on;
+}
+struct PhaseClock {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  std::string line;
+  void mark(const char* what) {
+    if (!sync_trace()) return;
+    const auto t1 = std::chrono::steady_clock::now();
+    char b[64];
+    snprintf(b, sizeof b, " %s %.2f", what, std::chrono::duration<double, std::milli>(t1 - t0).count());
+    line += b;
+    t0 = t1;
+  }
+};
+
 // Build the godunov tile / prolongation / correction tables of level l.
 int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   Level& L = c->lv[l];
+  PhaseClock pc;
   free_level_tables(L);
+  pc.mark("free");
   if (L.noct == 0) return RB_OK;
-  if (L.shape < 0) L.shape = default_shape(c, l, L);
+  if (L.shape < 0 || !L.shape_user) L.shape = default_shape(c, l, L);
   if (!shape_fits(c, l, L.shape))
     return fail(RB_ERR_INVALID, "level %d: tile shape %d spans the box face and the boundary layer", l, L.shape);
   const rb::TileShape sh = rb::kTileShapes[L.shape];
@@ -257,90 +333,116 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
               [](const auto& a, const auto& b) { return a.first < b.first; });
   }
   L.ntile = (int)tiles.size();
+  pc.mark("tiles");
   std::vector<int32_t> blk((size_t)L.ntile * NBLK, -1);
-  std::unordered_map<int64_t, int32_t> interp_of;  // father Fortran cell -> entry
-  std::vector<int32_t> interp7;
   const OctIndex* P = l >= 2 ? &idx[l - 1] : nullptr;
   // level l-1 cells per dimension
   const int64_t cnx = I.nx, cny = I.ny, cnz = I.nz;
-  auto father_cell_of_pos = [&](int64_t x, int64_t y, int64_t z, int64_t* fc) -> int {
-    // level-(l-1) cell at coordinates (x,y,z) (a level-l oct position)
+  ParError perr;
+  // level-(l-1) cell at coordinates (x,y,z) (a level-l oct position), 0 if absent
+  auto father_cell_of_pos = [&](int64_t x, int64_t y, int64_t z) -> int64_t {
     x = ((x % cnx) + cnx) % cnx;
     y = ((y % cny) + cny) % cny;
     z = ((z % cnz) + cnz) % cnz;
-    if (l == 1) {
-      *fc = 1 + x + c->mp.nx * (y + (int64_t)c->mp.ny * z);
-      return RB_OK;
-    }
+    if (l == 1) return 1 + x + c->mp.nx * (y + (int64_t)c->mp.ny * z);
     const int32_t pg = P->find(x >> 1, y >> 1, z >> 1);
-    if (pg <= 0)
-      return fail(RB_ERR_TREE, "level %d: father cell (%lld,%lld,%lld) of a needed neighbour block does not exist "
+    if (pg <= 0) {
+      perr.record(RB_ERR_TREE, "level %d: father cell (%lld,%lld,%lld) of a needed neighbour block does not exist "
                   "(refinement rule violated)", l, (long long)x, (long long)y, (long long)z);
+      return 0;
+    }
     const int ind = 1 + (int)(x & 1) + 2 * (int)(y & 1) + 4 * (int)(z & 1);
-    *fc = fcell(c, ind, pg);
-    return RB_OK;
+    return fcell(c, ind, pg);
   };
-  auto make_interp = [&](int64_t x, int64_t y, int64_t z, int32_t* code) -> int {
-    int64_t f;
-    RB_TRY(father_cell_of_pos(x, y, z, &f));
-    auto it = interp_of.find(f);
-    if (it != interp_of.end()) { *code = -2 - it->second; return RB_OK; }
-    const int32_t e = (int32_t)interp_of.size();
-    interp_of.emplace(f, e);
-    int64_t cells[7];
-    father_nbor_cells(c, l, f, cells);
-    for (int j = 0; j < 7; j++) interp7.push_back((int32_t)dev_of_fortran(c, cells[j]));
-    *code = -2 - e;
-    return RB_OK;
-  };
-  std::vector<char> inner((size_t)TOX * TOY * TOZ);
-  for (int t = 0; t < L.ntile; t++) {
-    const int64_t ox0 = tiles[t].second[0] * TOX, oy0 = tiles[t].second[1] * TOY, oz0 = tiles[t].second[2] * TOZ;
-    int32_t* B = &blk[(size_t)t * NBLK];
-    const bool x_inside = ox0 - 1 >= 0 && ox0 - 1 + BX <= I.nx;
-    for (int bz = 0; bz < BZ; bz++)
-      for (int by = 0; by < BY; by++) {
-        int32_t* row = B + BX * (by + BY * bz);
-        if (x_inside) {
-          // one search per row of blocks: the row's positions are
-          // consecutive keys, so its octs follow each other in I.v
-          const int64_t k0 = I.key(ox0 - 1, oy0 - 1 + by, oz0 - 1 + bz);
-          auto it = std::lower_bound(I.v.begin(), I.v.end(), std::make_pair(k0, (int32_t)INT32_MIN));
-          for (int bx = 0; bx < BX; bx++) {
-            while (it != I.v.end() && it->first < k0 + bx) ++it;
-            row[bx] = (it != I.v.end() && it->first == k0 + bx) ? it->second - 1 : -1;
-          }
-        } else {
-          for (int bx = 0; bx < BX; bx++) {
-            const int32_t g = I.find(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
-            row[bx] = g > 0 ? g - 1 : -1;
+  // pass 1, tiles in parallel: the source of every block of each tile's
+  // stencil box; an absent block that an oct of the tile needs is marked
+  // with its father cell f as -1 - f (prolongation entries are numbered in
+  // pass 2)
+  parallel_for(L.ntile, 256, [&](int64_t t0, int64_t t1) {
+    std::vector<char> inner((size_t)TOX * TOY * TOZ);
+    for (int64_t t = t0; t < t1 && !perr.set.load(); t++) {
+      const int64_t ox0 = tiles[t].second[0] * TOX, oy0 = tiles[t].second[1] * TOY, oz0 = tiles[t].second[2] * TOZ;
+      int32_t* B = &blk[(size_t)t * NBLK];
+      const bool x_inside = ox0 - 1 >= 0 && ox0 - 1 + BX <= I.nx;
+      for (int bz = 0; bz < BZ; bz++)
+        for (int by = 0; by < BY; by++) {
+          int32_t* row = B + BX * (by + BY * bz);
+          if (x_inside) {
+            // one search per row of blocks: the row's positions are
+            // consecutive keys, so its octs follow each other in I.v
+            const int64_t k0 = I.key(ox0 - 1, oy0 - 1 + by, oz0 - 1 + bz);
+            auto it = std::lower_bound(I.v.begin(), I.v.end(), std::make_pair(k0, (int32_t)INT32_MIN));
+            for (int bx = 0; bx < BX; bx++) {
+              while (it != I.v.end() && it->first < k0 + bx) ++it;
+              row[bx] = (it != I.v.end() && it->first == k0 + bx) ? it->second - 1 : -1;
+            }
+          } else {
+            for (int bx = 0; bx < BX; bx++) {
+              const int32_t g = I.find(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
+              row[bx] = g > 0 ? g - 1 : -1;
+            }
           }
         }
-      }
-    for (int z = 0; z < TOZ; z++)
-      for (int y = 0; y < TOY; y++)
-        for (int x = 0; x < TOX; x++) {
-          const int32_t g = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))];
-          if (g >= 0 && c->is_bnd[g]) return fail(RB_ERR_TREE, "level %d: a tile holds a boundary oct", l);
-          inner[x + TOX * (y + TOY * z)] = g >= 0;
-        }
-    for (int bz = 0; bz < BZ; bz++)
-      for (int by = 0; by < BY; by++)
-        for (int bx = 0; bx < BX; bx++) {
-          int32_t& code = B[bx + BX * (by + BY * bz)];
-          if (code >= 0) continue;
-          bool needed = false;
-          for (int dz = -1; dz <= 1 && !needed; dz++)
-            for (int dy = -1; dy <= 1 && !needed; dy++)
-              for (int dx = -1; dx <= 1 && !needed; dx++) {
-                const int ix = bx - 1 + dx, iy = by - 1 + dy, iz = bz - 1 + dz;
-                if (ix < 0 || iy < 0 || iz < 0 || ix >= TOX || iy >= TOY || iz >= TOZ) continue;
-                needed = inner[ix + TOX * (iy + TOY * iz)];
-              }
-          if (needed) RB_TRY(make_interp(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz, &code));
-        }
-  }
-  L.ninterp = (int)interp_of.size();
+      for (int z = 0; z < TOZ; z++)
+        for (int y = 0; y < TOY; y++)
+          for (int x = 0; x < TOX; x++) {
+            const int32_t g = B[(x + 1) + BX * ((y + 1) + BY * (z + 1))];
+            if (g >= 0 && c->is_bnd[g]) {
+              perr.record(RB_ERR_TREE, "level %d: a tile holds a boundary oct", l);
+              return;
+            }
+            inner[x + TOX * (y + TOY * z)] = g >= 0;
+          }
+      for (int bz = 0; bz < BZ; bz++)
+        for (int by = 0; by < BY; by++)
+          for (int bx = 0; bx < BX; bx++) {
+            int32_t& code = B[bx + BX * (by + BY * bz)];
+            if (code >= 0) continue;
+            bool needed = false;
+            for (int dz = -1; dz <= 1 && !needed; dz++)
+              for (int dy = -1; dy <= 1 && !needed; dy++)
+                for (int dx = -1; dx <= 1 && !needed; dx++) {
+                  const int ix = bx - 1 + dx, iy = by - 1 + dy, iz = bz - 1 + dz;
+                  if (ix < 0 || iy < 0 || iz < 0 || ix >= TOX || iy >= TOY || iz >= TOZ) continue;
+                  needed = inner[ix + TOX * (iy + TOY * iz)];
+                }
+            if (!needed) continue;
+            const int64_t f = father_cell_of_pos(ox0 - 1 + bx, oy0 - 1 + by, oz0 - 1 + bz);
+            if (f <= 0) return;
+            code = (int32_t)(-1 - f);
+          }
+    }
+  });
+  RB_TRY(perr.report());
+  pc.mark("pass1");
+  // pass 2: one prolongation entry per distinct father cell (ascending f),
+  // the blocks' codes -2 - entry
+  std::vector<int32_t> fcells;
+  for (int32_t code : blk)
+    if (code <= -2) fcells.push_back(-1 - code);
+  std::sort(fcells.begin(), fcells.end());
+  fcells.erase(std::unique(fcells.begin(), fcells.end()), fcells.end());
+  parallel_for((int64_t)blk.size(), 1 << 16, [&](int64_t b0, int64_t b1) {
+    for (int64_t b = b0; b < b1; b++) {
+      const int32_t code = blk[b];
+      if (code > -2) continue;
+      const int32_t e = (int32_t)(std::lower_bound(fcells.begin(), fcells.end(), -1 - code) - fcells.begin());
+      blk[b] = -2 - e;
+    }
+  });
+  pc.mark("pass2");
+  // pass 3, entries in parallel: the father cell and its getnborfather
+  // neighbours of every entry
+  std::vector<int32_t> interp7(fcells.size() * 7);
+  parallel_for((int64_t)fcells.size(), 1024, [&](int64_t e0, int64_t e1) {
+    for (int64_t e = e0; e < e1; e++) {
+      int64_t cells[7];
+      father_nbor_cells(c, l, fcells[e], cells);
+      for (int j = 0; j < 7; j++) interp7[(size_t)e * 7 + j] = (int32_t)dev_of_fortran(c, cells[j]);
+    }
+  });
+  pc.mark("pass3");
+  L.ninterp = (int)fcells.size();
   RB_TRY(dalloc(&L.d_tile_blk, blk.size()));
   RB_TRY(h2d(c, L.d_tile_blk, blk.data(), blk.size() * 4));
   if (L.ninterp) {
@@ -348,6 +450,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(h2d(c, L.d_interp7, interp7.data(), interp7.size() * 4));
     RB_TRY(dalloc(&L.d_interp_buf, (size_t)L.ninterp * 8 * 5));
   }
+  pc.mark("upload");
   // --- fine-to-coarse corrections (godunov_fine.f90:798-908)
   struct Contrib { int64_t tgt; int64_t batch; int face; int slot; };
   std::vector<Contrib> cons;
@@ -398,6 +501,7 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   // this level's entries of the per-oct correction slot table
   for (int32_t g : L.h_active) c->h_corr_slot[g - 1] = -1;
   for (size_t i = 0; i + 1 < h_slot_upd.size(); i += 2) c->h_corr_slot[h_slot_upd[i]] = h_slot_upd[i + 1];
+  pc.mark("corr");
   // per tile, the faces whose fluxes the fine-to-coarse correction reads:
   // entries (oct position in the tile | face << 8, slot), tile t's in
   // [off[t], off[t+1]), so that the godunov kernel stores only those
@@ -423,6 +527,10 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
     RB_TRY(h2d(c, L.d_tile_corr, ent.data(), ent.size() * 4));
   }
   if (c->hp.pressure_fix) RB_TRY(ensure_nres6(c, L));
+  pc.mark("tilecorr");
+  if (sync_trace())
+    fprintf(stderr, "[rb sync] level %d: %d octs, %d tiles, %d entries, %d slots; ms:%s\n", l, L.noct, L.ntile,
+            L.ninterp, L.nslot, pc.line.c_str());
   L.tables_built = true;
   return RB_OK;
 }
@@ -473,15 +581,16 @@ int build_boundary_pairs(rb_context* c) {
 int sync_oct(rb_context* c);
 
 // After a re-sync: the octs that are new since the previous tree (a level
-// they did not have, or another father cell) get the state make_grid_fine
-// gives them, prolonged on the device in level order, so that a remeshed
-// tree needs no state upload.
-int prolong_new_octs(rb_context* c, const std::vector<int8_t>& old_level, const std::vector<int32_t>& old_father) {
+// they did not have, or another father cell; born[l], igrids) get the state
+// make_grid_fine gives them, prolonged on the device in level order, so that
+// a remeshed tree needs no state upload.
+int prolong_new_octs(rb_context* c, const std::vector<std::vector<int32_t>>& born) {
   for (int l = 2; l <= c->mp.nlevelmax; l++) {
-    const Level& L = c->lv[l];
+    if (born[l].empty()) continue;
     std::vector<int32_t> octs, cells7;
-    for (int32_t g : L.h_active) {
-      if (old_level[g - 1] == l && old_father[g - 1] == c->father[g - 1]) continue;
+    octs.reserve(born[l].size());
+    cells7.reserve(born[l].size() * 7);
+    for (int32_t g : born[l]) {
       int64_t cells[7];
       father_nbor_cells(c, l, c->father[g - 1], cells);
       for (int j = 0; j < 7; j++) {
@@ -490,7 +599,6 @@ int prolong_new_octs(rb_context* c, const std::vector<int8_t>& old_level, const 
       }
       octs.push_back(g - 1);
     }
-    if (octs.empty()) continue;
     int32_t *d_octs = nullptr, *d_cells = nullptr;
     int rc = dalloc(&d_octs, octs.size());
     if (!rc) rc = dalloc(&d_cells, cells7.size());
@@ -511,60 +619,110 @@ int prolong_new_octs(rb_context* c, const std::vector<int8_t>& old_level, const 
   return RB_OK;
 }
 
+// A re-sync is incremental when the previous tree's host mirrors and level
+// tables are still held (same boundary region types): the host mirrors are
+// updated over the octs of the old and new trees only (not over ngridmax),
+// the device son mirror receives the entries that changed, and a level keeps
+// its tables (tiles, prolongation entries, corrections, nbor6/nres6), its
+// position index and its device active list when their inputs are unchanged.
+// Level l's tables are a function of: its active list (whose order fixes the
+// nvector batches of the corrections) and boundary octs, the positions and
+// nbor rows of the octs of levels l and l-1, and son of the level-(l-1) cells
+// (of the coarse cells for l = 1); all compared exactly, not sampled.
 int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, const int32_t* nbor,
                    const int32_t* numbl, const int32_t* active) {
   if (!son || !father || !nbor || !numbl || !active) return fail(RB_ERR_INVALID, "null tree array");
+  using clk = std::chrono::steady_clock;
+  auto ms_since = [](clk::time_point t0) { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
+  const clk::time_point t_start = clk::now();
   // a state held in the dense mirror goes back to the oct layout first
   if (c->have_tree) RB_TRY(sync_oct(c));
+  const int NL = c->mp.nlevelmax;
+  const int64_t ncell = c->ncell;
+  const int ngm = c->mp.ngridmax;
   // the previous tree (still in level_of/father after an rb_set_boundary
   // dropped it) decides which octs are new
   const bool prolong = c->prev_tree_valid && c->have_state && c->state_newer != 2;
-  std::vector<int8_t> old_level;
-  std::vector<int32_t> old_father;
-  if (prolong) { old_level = c->level_of; old_father = c->father; }
+  const bool incremental = c->prev_tree_valid && (c->have_tree || c->tables_kept) && c->tables_btype == c->btype &&
+                           c->son.size() == (size_t)ncell && c->level_of.size() == (size_t)ngm;
+  std::vector<std::vector<int32_t>> old_active(RB_MAXLEVEL + 2), old_bnd(RB_MAXLEVEL + 2);
+  if (incremental)
+    for (int l = 1; l <= NL; l++) {
+      old_active[l].swap(c->lv[l].h_active);
+      old_bnd[l].swap(c->lv[l].h_bnd);
+    }
   c->prev_tree_valid = false;
-  free_tree(c);
-  const int64_t ncell = c->ncell;
-  const int ngm = c->mp.ngridmax;
-  c->son.assign(son, son + ncell);
-  c->father.assign(father, father + ngm);
-  c->nbor.assign(nbor, nbor + (size_t)6 * ngm);
-  c->coords.assign((size_t)ngm * 3, 0);
-  c->level_of.assign((size_t)ngm, 0);
-  c->is_bnd.assign((size_t)ngm, 0);
-  c->idx.assign(RB_MAXLEVEL + 2, OctIndex());
-  std::vector<OctIndex>& idx = c->idx;
+  free_tree(c, incremental);
+  // the new lists
   int64_t off = 0;
   c->finest = 0;
-  for (int l = 1; l <= c->mp.nlevelmax; l++) {
+  const int nb = (int)c->btype.size();
+  for (int l = 1; l <= NL; l++) {
     Level& L = c->lv[l];
     const int n = numbl[l - 1];
-    if (n < 0 || n > ngm) return fail(RB_ERR_INVALID, "numbl(%d)=%d out of range", l, n);
+    if (n < 0 || n > ngm || off + n > (int64_t)ngm) return fail(RB_ERR_INVALID, "numbl(%d)=%d out of range", l, n);
     L.h_active.assign(active + off, active + off + n);
     off += n;
     L.noct = n;
     if (n) c->finest = l;
     L.dx = std::pow(0.5, l) * (c->mp.boxlen / (double)(c->mp.nx_loc > 0 ? c->mp.nx_loc : c->mp.nx));
-    OctIndex& I = idx[l];
-    I.nx = (int64_t)c->mp.nx << (l - 1);
-    I.ny = (int64_t)c->mp.ny << (l - 1);
-    I.nz = (int64_t)c->mp.nz << (l - 1);
-    I.v.reserve(n);
-    // the level's active octs, then its boundary octs (found by the stencil
-    // lookups, never updated)
-    std::vector<int32_t> octs(L.h_active);
-    const int nb = (int)c->btype.size();
+    L.h_bnd.clear();
     for (int ib = 0; ib < nb; ib++) {
       const int64_t k = (int64_t)(l - 1) * nb + ib;
-      octs.insert(octs.end(), c->bgrid.begin() + c->boff[k], c->bgrid.begin() + c->boff[k + 1]);
+      L.h_bnd.insert(L.h_bnd.end(), c->bgrid.begin() + c->boff[k], c->bgrid.begin() + c->boff[k + 1]);
     }
-    for (size_t o = 0; o < octs.size(); o++) {
-      const int32_t g = octs[o];
-      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "%s grid %d out of range", o < (size_t)n ? "active" : "boundary", g);
-      if (c->level_of[g - 1] != 0) return fail(RB_ERR_TREE, "grid %d listed twice", g);
-      if (o >= (size_t)n) c->is_bnd[g - 1] = 1;
-      const int64_t fc = father[g - 1];
-      int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+    for (int32_t g : L.h_active)
+      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "active grid %d out of range", g);
+    for (int32_t g : L.h_bnd)
+      if (g < 1 || g > ngm) return fail(RB_ERR_INVALID, "boundary grid %d out of range", g);
+  }
+  // octs new since the previous tree, judged against it before any mirror
+  // is overwritten
+  std::vector<std::vector<int32_t>> born(RB_MAXLEVEL + 2);
+  if (prolong)
+    for (int l = 2; l <= NL; l++)
+      for (int32_t g : c->lv[l].h_active)
+        if (c->level_of[g - 1] != l || c->father[g - 1] != father[g - 1]) born[l].push_back(g);
+  // per level: its octs changed (lists, positions, nbor rows) / son of its
+  // cells changed; son of the coarse cells changed
+  std::vector<char> oct_dirty(RB_MAXLEVEL + 2, incremental ? 0 : 1), cell_dirty(RB_MAXLEVEL + 2, incremental ? 0 : 1);
+  bool coarse_dirty = !incremental;
+  std::vector<int64_t> son_idx;   // device cells whose son changed, and the values
+  std::vector<int32_t> son_val;
+  if (incremental) {
+    for (int l = 1; l <= NL; l++) {
+      if (c->lv[l].h_active != old_active[l] || c->lv[l].h_bnd != old_bnd[l]) oct_dirty[l] = 1;
+      for (int32_t g : old_active[l]) { c->level_of[g - 1] = 0; c->is_bnd[g - 1] = 0; }
+      for (int32_t g : old_bnd[l]) { c->level_of[g - 1] = 0; c->is_bnd[g - 1] = 0; }
+    }
+    for (int64_t i = 0; i < c->mp.ncoarse; i++)
+      if (c->son[i] != son[i]) {
+        coarse_dirty = true;
+        son_idx.push_back(i);
+        son_val.push_back(son[i]);
+        c->son[i] = son[i];
+      }
+  } else {
+    c->son.assign(son, son + ncell);
+    c->father.assign(father, father + ngm);
+    c->nbor.assign(nbor, nbor + (size_t)6 * ngm);
+    c->coords.assign((size_t)ngm * 3, 0);
+    c->level_of.assign((size_t)ngm, 0);
+    c->is_bnd.assign((size_t)ngm, 0);
+    c->h_corr_slot.assign((size_t)ngm, -1);
+  }
+  // positions (from the father chain, level by level), level and boundary
+  // marks; in the incremental case also the nbor rows, father and the son
+  // entries of the octs' cells, compared with the previous tree's
+  for (int l = 1; l <= NL; l++) {
+    Level& L = c->lv[l];
+    const size_t n = L.h_active.size(), nall = n + L.h_bnd.size();
+    for (size_t o = 0; o < nall; o++) {
+      const int32_t g = o < n ? L.h_active[o] : L.h_bnd[o - n];
+      const size_t gi = (size_t)(g - 1);
+      if (c->level_of[gi] != 0) return fail(RB_ERR_TREE, "grid %d listed twice", g);
+      const int64_t fc = father[gi];
+      int64_t x[3];
       if (l == 1) {
         if (fc < 1 || fc > c->mp.ncoarse) return fail(RB_ERR_TREE, "level-1 grid %d father %lld is not coarse", g, (long long)fc);
         x[0] = (fc - 1) % c->mp.nx;
@@ -581,47 +739,140 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
         x[1] = 2 * px[1] + ((pos >> 1) & 1);
         x[2] = 2 * px[2] + ((pos >> 2) & 1);
       }
-      c->level_of[g - 1] = (int8_t)l;
-      I.v.push_back({I.key(x[0], x[1], x[2]), g});
+      int64_t* xc = &c->coords[gi * 3];
+      if (incremental) {
+        if (xc[0] != x[0] || xc[1] != x[1] || xc[2] != x[2]) oct_dirty[l] = 1;
+        for (int j = 0; j < 6; j++) {
+          const size_t k = (size_t)j * ngm + gi;
+          if (c->nbor[k] != nbor[k]) { oct_dirty[l] = 1; c->nbor[k] = nbor[k]; }
+        }
+        c->father[gi] = father[gi];
+        for (int ind = 1; ind <= 8; ind++) {
+          const int64_t cf = fcell(c, ind, g) - 1;
+          if (c->son[cf] != son[cf]) {
+            cell_dirty[l] = 1;
+            son_idx.push_back(dev_of_fortran(c, cf + 1));
+            son_val.push_back(son[cf]);
+            c->son[cf] = son[cf];
+          }
+        }
+      }
+      xc[0] = x[0]; xc[1] = x[1]; xc[2] = x[2];
+      c->level_of[gi] = (int8_t)l;
+      if (o >= n) c->is_bnd[gi] = 1;
     }
-    std::sort(I.v.begin(), I.v.end());
-    for (size_t i = 1; i < I.v.size(); i++)
-      if (I.v[i].first == I.v[i - 1].first) return fail(RB_ERR_TREE, "level %d: two octs at one position", l);
-    L.complete = (int64_t)n == I.nx * I.ny * I.nz;
+  }
+  // the position indexes of the changed levels, sorted in parallel
+  c->idx.resize(RB_MAXLEVEL + 2);
+  {
+    ParError perr;
+    parallel_for(NL, 1, [&](int64_t l0, int64_t l1) {
+      for (int64_t l = l0 + 1; l <= l1; l++) {
+        if (!oct_dirty[l]) continue;
+        const Level& L = c->lv[l];
+        OctIndex& I = c->idx[l];
+        I.v.clear();
+        I.nx = (int64_t)c->mp.nx << (l - 1);
+        I.ny = (int64_t)c->mp.ny << (l - 1);
+        I.nz = (int64_t)c->mp.nz << (l - 1);
+        I.v.reserve(L.h_active.size() + L.h_bnd.size());
+        for (int32_t g : L.h_active) {
+          const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+          I.v.push_back({I.key(x[0], x[1], x[2]), g});
+        }
+        for (int32_t g : L.h_bnd) {
+          const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+          I.v.push_back({I.key(x[0], x[1], x[2]), g});
+        }
+        std::sort(I.v.begin(), I.v.end());
+        for (size_t i = 1; i < I.v.size(); i++)
+          if (I.v[i].first == I.v[i - 1].first) perr.record(RB_ERR_TREE, "level %d: two octs at one position", (int)l);
+      }
+    });
+    RB_TRY(perr.report());
+  }
+  // per level: completeness, leaf cells, device active list (re-uploaded
+  // only when the list changed)
+  for (int l = 1; l <= NL; l++) {
+    Level& L = c->lv[l];
+    const int n = L.noct;
+    L.complete = (int64_t)n == c->idx[l].nx * c->idx[l].ny * c->idx[l].nz;
     int64_t leaf = 0;
     int refined = 0;
     for (int32_t g : L.h_active)
       for (int ind = 1; ind <= 8; ind++) {
-        const int32_t s = son[fcell(c, ind, g) - 1];
-        leaf += (s == 0);
-        refined |= (s > 0);
+        const int32_t sv = son[fcell(c, ind, g) - 1];
+        leaf += (sv == 0);
+        refined |= (sv > 0);
       }
     L.leaf_cells = leaf;
     L.has_refined = refined;
-    if (n) {
-      std::vector<int32_t> a0(n);
-      for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
-      RB_TRY(dalloc(&L.d_active, (size_t)n));
-      RB_TRY(h2d(c, L.d_active, a0.data(), (size_t)n * 4));
+    const bool same_list = incremental && L.h_active == old_active[l] && (L.d_active || n == 0);
+    if (!same_list) {
+      dfree(L.d_active);
+      if (n) {
+        std::vector<int32_t> a0(n);
+        for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
+        RB_TRY(dalloc(&L.d_active, (size_t)n));
+        RB_TRY(h2d(c, L.d_active, a0.data(), (size_t)n * 4));
+      }
     }
   }
-  // son mirror (device layout) and the per-oct correction slot table
-  RB_TRY(h2d(c, c->d_stage, son, ncell * 4));
-  rb::permute_son_kernel<<<grid_for(ncell, 256), 256, 0, c->stream>>>((const int32_t*)c->d_stage, c->d_son, ncell,
-                                                                      c->mp.ncoarse, ngm);
-  RB_CUDA(cudaGetLastError());
-  RB_CUDA(cudaStreamSynchronize(c->stream));
-  c->h_corr_slot.assign((size_t)ngm, -1);
-  for (int l = 1; l <= c->mp.nlevelmax; l++) RB_TRY(build_level_tables(c, l, idx));
+  // son mirror (device layout): the whole array, or the entries that changed
+  if (!incremental) {
+    RB_TRY(h2d(c, c->d_stage, son, ncell * 4));
+    rb::permute_son_kernel<<<grid_for(ncell, 256), 256, 0, c->stream>>>((const int32_t*)c->d_stage, c->d_son, ncell,
+                                                                        c->mp.ncoarse, ngm);
+    RB_CUDA(cudaGetLastError());
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+  } else if (!son_idx.empty()) {
+    const int64_t m = (int64_t)son_idx.size();
+    // staging: indexes then values in the (5 * ncell doubles) stage buffer
+    if ((size_t)m * 12 > (size_t)ncell * 40) return fail(RB_ERR_TREE, "son diff larger than the staging buffer");
+    int64_t* d_idx = reinterpret_cast<int64_t*>(c->d_stage);
+    int32_t* d_val = reinterpret_cast<int32_t*>(d_idx + m);
+    RB_TRY(h2d(c, d_idx, son_idx.data(), (size_t)m * 8));
+    RB_TRY(h2d(c, d_val, son_val.data(), (size_t)m * 4));
+    rb::scatter_son_kernel<<<grid_for(m, 256), 256, 0, c->stream>>>(c->d_son, d_idx, d_val, m);
+    RB_CUDA(cudaGetLastError());
+    RB_CUDA(cudaStreamSynchronize(c->stream));
+  }
+  c->sync_ms[1] = ms_since(t_start);
+  const clk::time_point t_tables = clk::now();
+  c->levels_built = c->levels_reused = 0;
+  for (int l = 1; l <= NL; l++) {
+    Level& L = c->lv[l];
+    const bool keep = incremental && L.tables_built && L.noct > 0 && !oct_dirty[l] &&
+                      (l == 1 ? !coarse_dirty : (!oct_dirty[l - 1] && !cell_dirty[l - 1]));
+    if (keep) {
+      c->levels_reused++;
+      continue;
+    }
+    RB_TRY(build_level_tables(c, l, c->idx));
+    if (L.noct) c->levels_built++;
+  }
+  c->sync_ms[2] = ms_since(t_tables);
+  const clk::time_point t_bnd = clk::now();
   RB_TRY(build_boundary_pairs(c));
+  c->sync_ms[3] = ms_since(t_bnd);
   c->have_tree = true;
+  c->tables_kept = false;
+  c->tables_btype = c->btype;
   c->prev_tree_valid = true;
   c->clock_valid = false;
   c->tree_syncs++;
+  const clk::time_point t_pro = clk::now();
   if (prolong) {
-    RB_TRY(prolong_new_octs(c, old_level, old_father));
+    RB_TRY(prolong_new_octs(c, born));
     if (c->state_newer == 0) c->state_newer = 1;
   }
+  c->sync_ms[4] = ms_since(t_pro);
+  c->sync_ms[0] = ms_since(t_start);
+  if (sync_trace())
+    fprintf(stderr, "[rb sync] %s: total %.2f ms (index %.2f, tables %.2f, boundary pairs %.2f, prolongation %.2f), "
+            "%d levels built, %d kept, %zu son entries changed\n", incremental ? "incremental" : "full",
+            c->sync_ms[0], c->sync_ms[1], c->sync_ms[2], c->sync_ms[3], c->sync_ms[4], c->levels_built,
+            c->levels_reused, son_idx.size());
   return RB_OK;
 }
 
@@ -1239,7 +1490,7 @@ int rb_set_boundary(rb_context* c, int32_t nboundary, const int32_t* boundary_ty
   // the tree it leaves behind is what that sync compares against
   if (c->have_tree) {
     RB_TRY(sync_oct(c));
-    free_tree(c);
+    free_tree(c, true);  // the level tables stay for the comparison in the sync
   }
   return RB_OK;
 }
@@ -1332,6 +1583,14 @@ int rb_transfer_stats(rb_context* c, int64_t* h2d_state_bytes, int64_t* d2h_stat
   if (d2h_state_bytes) *d2h_state_bytes = c->d2h_state_bytes;
   if (tree_syncs) *tree_syncs = c->tree_syncs;
   if (octs_prolonged) *octs_prolonged = c->octs_prolonged;
+  return RB_OK;
+}
+int rb_sync_stats(rb_context* c, double* ms, int32_t* levels_built, int32_t* levels_reused) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (ms)
+    for (int i = 0; i < 5; i++) ms[i] = c->sync_ms[i];
+  if (levels_built) *levels_built = c->levels_built;
+  if (levels_reused) *levels_reused = c->levels_reused;
   return RB_OK;
 }
 int rb_upload_unew(rb_context* c, const double* unew) { return upload_impl(c, unew, c ? c->d_unew : nullptr); }
@@ -1565,6 +1824,7 @@ int rb_set_tile_shape(rb_context* c, int l, int shape) {
   if (shape >= rb::kNumTileShapes) return fail(RB_ERR_INVALID, "tile shape %d out of range", shape);
   drop_graph(c);
   RB_TRY(sync_oct(c));
+  L.shape_user = true;
   if (shape >= 0 || L.noct == 0) {
     L.shape = shape >= 0 ? shape : L.shape;
     return build_level_tables(c, l, c->idx);

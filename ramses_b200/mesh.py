@@ -146,9 +146,46 @@ def _keys(c: np.ndarray, n: int) -> np.ndarray:
     return c[:, 0] + n * (c[:, 1] + n * c[:, 2])
 
 
+def _unique(x: np.ndarray) -> np.ndarray:
+    """Sorted unique values (sort-based: much faster than numpy's hashing
+    unique on large int64 key arrays)."""
+    x = np.sort(np.asarray(x).ravel())
+    if len(x) < 2:
+        return x
+    return x[np.concatenate(([True], x[1:] != x[:-1]))]
+
+
+def _isin(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Boolean mask of the entries of ``a`` present in ``b`` (sort and
+    binary search)."""
+    a = np.asarray(a)
+    bs = _unique(b)
+    if len(bs) == 0:
+        return np.zeros(a.shape, bool)
+    pos = np.minimum(np.searchsorted(bs, a), len(bs) - 1)
+    return bs[pos] == a
+
+
 def _neighbourhood(cells: np.ndarray) -> np.ndarray:
     offs = np.array([[i, j, k] for k in (-1, 0, 1) for j in (-1, 0, 1) for i in (-1, 0, 1)])
     return (cells[:, None, :] + offs[None, :, :]).reshape(-1, 3)
+
+
+def _dilated_keys(cells: np.ndarray, n: int) -> np.ndarray:
+    """Sorted unique keys of the cells within one cell (26-neighbourhood,
+    periodic in n) of ``cells``: three separable one-axis dilations, each
+    followed by a unique (a third of the sorting work of the 27-point
+    expansion)."""
+    k = _unique(_keys(cells % n, n))
+    for d in range(3):
+        c = np.stack([k % n, (k // n) % n, k // (n * n)], 1)
+        parts = []
+        for s in (-1, 0, 1):
+            cc = c.copy()
+            cc[:, d] = (cc[:, d] + s) % n
+            parts.append(_keys(cc, n))
+        k = _unique(np.concatenate(parts))
+    return k
 
 
 def build_tree(levelmin: int, nlevelmax: Optional[int] = None,
@@ -193,10 +230,9 @@ def oct_sets(levelmin: int, nlevelmax: Optional[int] = None,
         for _ in range(nexpand if l >= levelmin else 0):
             if len(fc) == 0:
                 break
-            nb = _neighbourhood(fc) % n
-            k = np.unique(_keys(nb, n))
+            k = _dilated_keys(fc, n)
             ck = _keys(cells, n)
-            fc = cells[np.isin(ck, k)]
+            fc = cells[_isin(ck, k)]
         refined[l] = fc
         oct_coords[l + 1] = fc.copy()
         if len(fc) == 0:
@@ -211,9 +247,11 @@ def oct_sets(levelmin: int, nlevelmax: Optional[int] = None,
         if len(fc) == 0:
             continue
         n = 2 ** l
-        need = np.unique(_keys((_neighbourhood(fc) % n) // 2, n // 2))
+        kd = _dilated_keys(fc, n)
+        dc = np.stack([kd % n, (kd // n) % n, kd // (n * n)], 1)
+        need = _unique(_keys(dc // 2, n // 2))
         have = _keys(refined[l - 1], n // 2)
-        missing = np.setdiff1d(need, have)
+        missing = need[~_isin(need, have)]
         if len(missing):
             nn = n // 2
             mc = np.stack([missing % nn, (missing // nn) % nn, missing // (nn * nn)], 1)
@@ -228,7 +266,7 @@ def oct_sets(levelmin: int, nlevelmax: Optional[int] = None,
             oct_coords[l + 1] = np.zeros((0, 3), np.int64)
             continue
         parent_keys = _keys(oct_coords[l], n // 2)
-        fc = fc[np.isin(_keys(fc // 2, n // 2), parent_keys)]
+        fc = fc[_isin(_keys(fc // 2, n // 2), parent_keys)]
         refined[l] = fc
         oct_coords[l + 1] = fc
     return oct_coords
@@ -371,9 +409,9 @@ def remesh(old: Octree, oct_coords) -> Octree:
         n = 2 ** (l - 1)
         k_old = _keys(old.coords[l], n)
         k_new = _keys(new_sets[l], n) if len(new_sets[l]) else np.zeros(0, np.int64)
-        keep[l] = np.isin(k_old, k_new)
+        keep[l] = _isin(k_old, k_new)
         used[old.active[l][keep[l]]] = True
-    free = [g for g in range(1, ngm + 1) if not used[g]]
+    free = np.nonzero(~used[1:])[0] + 1
     fi = 0
     son = np.zeros(ncoarse + 8 * ngm, np.int32)
     father = np.zeros(ngm, np.int32)
@@ -389,7 +427,7 @@ def remesh(old: Octree, oct_coords) -> Octree:
         surv_g = old.active[l][keep[l]] if old.noct(l) else np.zeros(0, np.int32)
         surv_c = old.coords[l][keep[l]] if old.noct(l) else np.zeros((0, 3), np.int64)
         k_surv = _keys(surv_c, n) if len(surv_c) else np.zeros(0, np.int64)
-        born = oc_new[~np.isin(_keys(oc_new, n), k_surv)]
+        born = oc_new[~_isin(_keys(oc_new, n), k_surv)]
         if l > 1 and len(born):
             keys_sorted, igr = parent_lookup
             pos = np.searchsorted(keys_sorted, _keys(born // 2, 2 ** (l - 2)))
@@ -397,7 +435,7 @@ def remesh(old: Octree, oct_coords) -> Octree:
             born = born[np.lexsort((slot, igr[pos]))]
         if fi + len(born) > len(free):
             raise ValueError("remesh: ngridmax=%d too small" % ngm)
-        born_g = np.array(free[fi:fi + len(born)], np.int64)
+        born_g = free[fi:fi + len(born)].astype(np.int64)
         fi += len(born)
         ig = np.concatenate([surv_g.astype(np.int64), born_g])
         oc = np.concatenate([surv_c, born]) if len(born) else surv_c
@@ -432,6 +470,17 @@ def remesh(old: Octree, oct_coords) -> Octree:
         parent_lookup = (k[srt], ig[srt])
     return Octree(nx=1, ny=1, nz=1, ncoarse=ncoarse, ngridmax=ngm, nlevelmax=L, levelmin=old.levelmin,
                   boxlen=old.boxlen, son=son, father=father, nbor=nbor, active=active, coords=coords)
+
+
+def refine_from_flags(old: Octree, flag1: np.ndarray, nexpand: int = 1) -> Octree:
+    """The host's remesh from cell flags (flag_fine -> refine_fine): the
+    flagged cells of every level from levelmin (flag1[icell], Fortran cell
+    index, as hydro_flag sets them) are refined, expanded by ``nexpand``
+    cells and closed under the nesting rule (``oct_sets``); refined regions
+    shrink from their finest level; the new tree keeps the igrids of the
+    octs that survive (``remesh``)."""
+    sets = oct_sets(old.levelmin, old.nlevelmax, flag_refine(old, np.asarray(flag1)), nexpand)
+    return remesh(old, sets)
 
 
 def uniform_tree(level: int, boxlen: float = 1.0) -> Octree:

@@ -86,6 +86,7 @@ _PROTOS = {
                                         _P32, _PD]),
     "rb_ensure_host": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_transfer_stats": (ctypes.c_int, [ctypes.c_void_p, _P64, _P64, _P64, _P64]),
+    "rb_sync_stats": (ctypes.c_int, [ctypes.c_void_p, _PD, _P32, _P32]),
     "rb_download_pressure_fix": (ctypes.c_int, [ctypes.c_void_p, _PD, _PD]),
     "rb_upload_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_unew": (ctypes.c_int, [ctypes.c_void_p, _PD]),
@@ -310,6 +311,16 @@ class Solver:
         return dict(zip(("h2d_state_bytes", "d2h_state_bytes", "tree_syncs", "octs_prolonged"),
                         (x.value for x in v)))
 
+    def sync_stats(self) -> dict:
+        """Phases of the last tree synchronisation (host ms) and the levels
+        whose tables were rebuilt or kept."""
+        ms = (ctypes.c_double * 5)()
+        built, reused = ctypes.c_int32(), ctypes.c_int32()
+        _check(load().rb_sync_stats(self._h, ms, ctypes.byref(built), ctypes.byref(reused)), "rb_sync_stats")
+        d = dict(zip(("total_ms", "index_ms", "tables_ms", "boundary_ms", "prolong_ms"), list(ms)))
+        d.update(levels_built=built.value, levels_reused=reused.value)
+        return d
+
     def upload_state(self, uold: np.ndarray):
         u = np.ascontiguousarray(uold, np.float64)
         assert u.shape == (5, self.tree.ncell)
@@ -413,6 +424,17 @@ class Solver:
         _check(load().rb_hydro_flag(self._h, int(ilevel), ctypes.byref(r), _ptr(f, _P32), ctypes.byref(n)),
                "rb_hydro_flag")
         return f, n.value
+
+    def flag_tree(self, rp) -> np.ndarray:
+        """hydro_flag on the device for every level from levelmin to
+        nlevelmax-1 (flag_fine's criterion): one flag array (int32, ncell+1
+        entries, index = Fortran cell index) for the host's remesh."""
+        t = self.tree
+        f = np.zeros(t.ncell + 1, np.int32)
+        for l in range(t.levelmin, t.nlevelmax):
+            if t.noct(l):
+                self.hydro_flag(l, rp, f)
+        return f
 
     def set_stream_shape(self, shape: int, hz: int):
         """Fix the z-streaming column shape and z extent (no autotuning)."""

@@ -79,3 +79,38 @@ def fingerprint(tree, u, gamma):
     return {"density": math.fsum(np.log10(np.abs(rho))), "velocity_x": math.fsum(np.abs(v[0])),
             "velocity_y": math.fsum(np.abs(v[1])), "velocity_z": math.fsum(np.abs(v[2])),
             "pressure": math.fsum(np.log10(np.abs(p)))}
+
+
+def oct_cells(tree):
+    """Fortran indices of every cell of the tree's active octs (all levels)."""
+    return np.concatenate([(tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + tree.active[l][None, :]).ravel()
+                           for l in range(1, tree.nlevelmax + 1) if tree.noct(l)])
+
+
+def oracle_prolong_born(old, new, u, hp):
+    """make_grid_fine's state for the octs of ``new`` that ``old`` did not
+    have at that level under the same father (refine_fine's new octs,
+    amr/refine_utils.f90:590-948): interpol_hydro of the father cell and its
+    getnborfather neighbours (hydro/interpol_hydro.f90:268-444), level by
+    level so that an oct born under a new oct reads its state. The oracle
+    restatement; ``u`` is the Fortran-layout state on the pre-remesh tree
+    (cell numbering is unchanged by the remesh)."""
+    import oracle
+    u = np.array(u, np.float64, copy=True)
+    old_level = np.zeros(old.ngridmax + 1, np.int64)
+    for l in range(1, old.nlevelmax + 1):
+        if old.noct(l):
+            old_level[old.active[l]] = l
+    for l in range(2, new.nlevelmax + 1):
+        if not new.noct(l):
+            continue
+        g = new.active[l].astype(np.int64)
+        born = g[(old_level[g] != l) | (old.father[g - 1] != new.father[g - 1])]
+        if not len(born):
+            continue
+        orc = oracle.OracleRun(new, hp, u)
+        cells7 = np.stack([orc.getnborfather(int(new.father[b - 1]), l - 1) for b in born])
+        u8 = oracle.interpol_hydro(hp, u[:, cells7 - 1].transpose(1, 2, 0))   # (n, 8, 5)
+        for ind in range(8):
+            u[:, new.ncoarse + ind * new.ngridmax + born - 1] = u8[:, ind, :].T
+    return u
