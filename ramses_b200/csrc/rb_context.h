@@ -42,6 +42,32 @@ void dfree(T*& p) {
   if (p) cudaFree((void*)p);
   p = nullptr;
 }
+// Grow-only device buffer from a memory pool, ordered on `stream`: at least
+// n elements (a quarter more when it has to grow); a smaller request keeps
+// the allocation. The pool keeps freed memory (its release threshold is
+// unbounded), so growing a table during a tree re-sync does not go through
+// cudaMalloc/cudaFree, which cost up to hundreds of ms there.
+template <typename T>
+int dreserve(cudaMemPool_t pool, cudaStream_t stream, T** p, size_t* cap, size_t n) {
+  if (n <= *cap && (*p || n == 0)) return RB_OK;
+  if (*p) cudaFreeAsync((void*)*p, stream);
+  *p = nullptr;
+  *cap = 0;
+  const size_t m = n + n / 4;
+  cudaError_t e = cudaMallocFromPoolAsync((void**)p, m * sizeof(T), pool, stream);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return fail(RB_ERR_NOMEM, "device table allocation of %zu bytes failed: %s", m * sizeof(T), cudaGetErrorString(e));
+  }
+  *cap = m;
+  return RB_OK;
+}
+template <typename T>
+void drelease(cudaStream_t stream, T*& p, size_t& cap) {
+  if (p) cudaFreeAsync((void*)p, stream);
+  p = nullptr;
+  cap = 0;
+}
 
 inline int grid_for(int64_t n, int nt, int cap = 148 * 32) {
   int64_t g = (n + nt - 1) / nt;
@@ -73,6 +99,12 @@ struct Level {
   int32_t* d_contrib = nullptr;
   int32_t* d_nbor6 = nullptr;     // [noct][6] device cell of nbor(igrid,j) (hydro_flag)
   int64_t* d_nres6 = nullptr;     // [noct][6] nbor(igrid,j) resolved to the neighbouring oct (pressure_fix pdV)
+  bool nbor6_ok = false, nres6_ok = false;  // d_nbor6 / d_nres6 hold this tree's values
+  // capacities (elements) of the device buffers: they only grow, so a
+  // re-sync reuses the allocations (no cudaFree/cudaMalloc per remesh)
+  size_t cap_active = 0, cap_tile_blk = 0, cap_tile_corr = 0, cap_tile_corr_off = 0, cap_interp7 = 0,
+         cap_interp_buf = 0, cap_corr_flux = 0, cap_corr_tmp = 0, cap_tgt = 0, cap_tgt_off = 0, cap_contrib = 0,
+         cap_nbor6 = 0, cap_nres6 = 0, cap_bpair = 0;
   int64_t leaf_cells = 0;
   double dx = 0.0;
   bool complete = false;
@@ -112,6 +144,7 @@ struct rb_context {
   int device = 0;
   int64_t ncell = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t table_pool = nullptr;  // the level tables' device buffers (grow-only, kept across re-syncs)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
   double* d_uold = nullptr;

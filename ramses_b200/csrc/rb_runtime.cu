@@ -7,6 +7,8 @@
 // (amr/amr_step.f90:320-445) that drives the level kernels on one stream.
 // Compiled with --fmad=false (FP64 kernels bit-identical to the reference
 // operation order).
+#include <sched.h>
+
 #include <atomic>
 #include <chrono>
 #include <mutex>
@@ -87,19 +89,25 @@ inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
   return spread(x) | spread(y) << 1 | spread(z) << 2;
 }
 
-void free_level_tables(Level& L) {
-  dfree(L.d_tile_blk);
-  dfree(L.d_tile_corr);
-  dfree(L.d_tile_corr_off);
-  dfree(L.d_interp7);
-  dfree(L.d_interp_buf);
-  dfree(L.d_corr_flux);
-  dfree(L.d_corr_tmp);
-  dfree(L.d_tgt);
-  dfree(L.d_tgt_off);
-  dfree(L.d_contrib);
-  dfree(L.d_nbor6);
-  dfree(L.d_nres6);
+// Invalidate a level's tables; with release the device buffers are freed
+// too (else they are kept for the next build, which reuses them).
+void free_level_tables(rb_context* c, Level& L, bool release = false) {
+  if (release) {
+    cudaStream_t st = c->stream;
+    drelease(st, L.d_tile_blk, L.cap_tile_blk);
+    drelease(st, L.d_tile_corr, L.cap_tile_corr);
+    drelease(st, L.d_tile_corr_off, L.cap_tile_corr_off);
+    drelease(st, L.d_interp7, L.cap_interp7);
+    drelease(st, L.d_interp_buf, L.cap_interp_buf);
+    drelease(st, L.d_corr_flux, L.cap_corr_flux);
+    drelease(st, L.d_corr_tmp, L.cap_corr_tmp);
+    drelease(st, L.d_tgt, L.cap_tgt);
+    drelease(st, L.d_tgt_off, L.cap_tgt_off);
+    drelease(st, L.d_contrib, L.cap_contrib);
+    drelease(st, L.d_nbor6, L.cap_nbor6);
+    drelease(st, L.d_nres6, L.cap_nres6);
+  }
+  L.nbor6_ok = L.nres6_ok = false;
   L.ntile = L.ninterp = L.nslot = L.ntgt = 0;
   L.tables_built = false;
 }
@@ -132,11 +140,11 @@ void free_tree(rb_context* c, bool keep_tables = false) {
   const bool keep = keep_tables && (c->have_tree || c->tables_kept);
   for (int l = 0; l <= RB_MAXLEVEL + 1; l++) {
     Level& L = c->lv[l];
-    dfree(L.d_bpair);
     L.h_boff.clear();
     if (keep) continue;
-    dfree(L.d_active);
-    free_level_tables(L);
+    drelease(c->stream, L.d_bpair, L.cap_bpair);
+    drelease(c->stream, L.d_active, L.cap_active);
+    free_level_tables(c, L, true);
     L.noct = 0;
     L.h_active.clear();
     L.h_bnd.clear();
@@ -145,12 +153,26 @@ void free_tree(rb_context* c, bool keep_tables = false) {
   c->have_tree = false;
 }
 
-// Run f(begin, end) over [0, n) on up to hardware_concurrency host threads
-// (one chunk each; small ranges run on the calling thread).
+// Host threads for the table builds: the CPUs this process may run on
+// (its affinity mask; a container's limit, not the machine's core count),
+// at most 32.
+int64_t host_threads() {
+  static const int64_t n = [] {
+    cpu_set_t set;
+    int64_t k = 0;
+    if (sched_getaffinity(0, sizeof set, &set) == 0) k = CPU_COUNT(&set);
+    if (k < 1) k = std::max(1u, std::thread::hardware_concurrency());
+    return std::min<int64_t>(k, 32);
+  }();
+  return n;
+}
+
+// Run f(begin, end) over [0, n) on up to host_threads() threads (one chunk
+// each; small ranges run on the calling thread).
 template <typename F>
 void parallel_for(int64_t n, int64_t min_chunk, F&& f) {
-  int64_t nt = std::max(1u, std::thread::hardware_concurrency());
-  nt = std::min<int64_t>(std::min<int64_t>(nt, 32), std::max<int64_t>(1, n / std::max<int64_t>(1, min_chunk)));
+  int64_t nt = host_threads();
+  nt = std::min<int64_t>(nt, std::max<int64_t>(1, n / std::max<int64_t>(1, min_chunk)));
   if (nt <= 1) {
     f((int64_t)0, n);
     return;
@@ -159,6 +181,33 @@ void parallel_for(int64_t n, int64_t min_chunk, F&& f) {
   th.reserve((size_t)nt);
   for (int64_t t = 0; t < nt; t++) th.emplace_back([&f, n, nt, t] { f(n * t / nt, n * (t + 1) / nt); });
   for (auto& x : th) x.join();
+}
+
+// std::sort on up to host_threads() threads: chunks sorted in
+// parallel, then merged pairwise. The order is that of std::sort for a
+// comparator with no ties (a strict total order), as every caller uses.
+template <typename T, typename Cmp>
+void parallel_sort(std::vector<T>& v, Cmp cmp) {
+  const int64_t n = (int64_t)v.size();
+  const int64_t nt = host_threads();
+  if (n < (1 << 16) || nt < 2) {
+    std::sort(v.begin(), v.end(), cmp);
+    return;
+  }
+  int64_t p2 = 1;
+  while (p2 * 2 <= nt) p2 *= 2;
+  std::vector<int64_t> b((size_t)p2 + 1);
+  for (int64_t i = 0; i <= p2; i++) b[i] = n * i / p2;
+  parallel_for(p2, 1, [&](int64_t c0, int64_t c1) {
+    for (int64_t i = c0; i < c1; i++) std::sort(v.begin() + b[i], v.begin() + b[i + 1], cmp);
+  });
+  for (int64_t w = 1; w < p2; w *= 2)
+    parallel_for(p2 / (2 * w), 1, [&](int64_t m0, int64_t m1) {
+      for (int64_t m = m0; m < m1; m++) {
+        const int64_t i = m * 2 * w;
+        std::inplace_merge(v.begin() + b[i], v.begin() + b[i + w], v.begin() + b[i + 2 * w], cmp);
+      }
+    });
 }
 
 // first error of a parallel region, reported through fail() on the calling
@@ -206,15 +255,16 @@ int default_shape(const rb_context* c, int l, const Level& L) {
 // Device cell of nbor(igrid,j), j = 1..6, for the level's octs in active
 // order (hydro_flag and the pdV term of pressure_fix).
 int ensure_nbor6(rb_context* c, Level& L) {
-  if (L.d_nbor6 || !L.noct) return RB_OK;
+  if (L.nbor6_ok || !L.noct) return RB_OK;
   std::vector<int32_t> nb((size_t)L.noct * 6);
   for (int i = 0; i < L.noct; i++) {
     const int g = L.h_active[i];
     for (int j = 0; j < 6; j++)
       nb[(size_t)i * 6 + j] = (int32_t)dev_of_fortran(c, c->nbor[(size_t)j * c->mp.ngridmax + (g - 1)]);
   }
-  RB_TRY(dalloc(&L.d_nbor6, nb.size()));
+  RB_TRY(dreserve(c->table_pool, c->stream, &L.d_nbor6, &L.cap_nbor6, nb.size()));
   RB_TRY(h2d(c, L.d_nbor6, nb.data(), nb.size() * sizeof(int32_t)));
+  L.nbor6_ok = true;
   return RB_OK;
 }
 
@@ -222,7 +272,7 @@ int ensure_nbor6(rb_context* c, Level& L) {
 // cell of child 0 of the neighbouring oct at this level where it exists,
 // else -(device cell of the coarse neighbour) - 1.
 int ensure_nres6(rb_context* c, Level& L) {
-  if (L.d_nres6 || !L.noct) return RB_OK;
+  if (L.nres6_ok || !L.noct) return RB_OK;
   std::vector<int64_t> nr((size_t)L.noct * 6);
   for (int i = 0; i < L.noct; i++) {
     const int g = L.h_active[i];
@@ -232,8 +282,9 @@ int ensure_nres6(rb_context* c, Level& L) {
       nr[(size_t)i * 6 + j] = gn > 0 ? (int64_t)c->mp.ncoarse + 8 * (int64_t)(gn - 1) : -dev_of_fortran(c, fcell) - 1;
     }
   }
-  RB_TRY(dalloc(&L.d_nres6, nr.size()));
+  RB_TRY(dreserve(c->table_pool, c->stream, &L.d_nres6, &L.cap_nres6, nr.size()));
   RB_TRY(h2d(c, L.d_nres6, nr.data(), nr.size() * sizeof(int64_t)));
+  L.nres6_ok = true;
   return RB_OK;
 }
 
@@ -306,7 +357,7 @@ struct PhaseClock {
 int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   Level& L = c->lv[l];
   PhaseClock pc;
-  free_level_tables(L);
+  free_level_tables(c, L);
   pc.mark("free");
   if (L.noct == 0) return RB_OK;
   if (L.shape < 0 || !L.shape_user) L.shape = default_shape(c, l, L);
@@ -317,20 +368,22 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   const int BX = TOX + 2, BY = TOY + 2, BZ = TOZ + 2, NBLK = BX * BY * BZ;
   const OctIndex& I = idx[l];
   // --- tiles: unique tile coordinates of the level's octs, Morton ordered
-  std::vector<std::pair<uint64_t, std::array<int64_t, 3>>> tiles;
+  std::vector<std::pair<uint64_t, std::array<int64_t, 3>>> tiles((size_t)L.noct);
   {
-    std::vector<uint64_t> seen;
-    seen.reserve(L.noct);
-    std::unordered_map<uint64_t, int> tmap;
-    tmap.reserve(L.noct * 2 / (TOX * TOY * TOZ) + 16);
-    for (int32_t g : L.h_active) {
-      const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
-      const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
-      const uint64_t m = morton3(tx, ty, tz);
-      if (tmap.emplace(m, 0).second) tiles.push_back({m, {tx, ty, tz}});
-    }
-    std::sort(tiles.begin(), tiles.end(),
-              [](const auto& a, const auto& b) { return a.first < b.first; });
+    parallel_for(L.noct, 1 << 14, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++) {
+        const int64_t* x = &c->coords[(size_t)(L.h_active[i] - 1) * 3];
+        const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
+        tiles[i] = {morton3(tx, ty, tz), {tx, ty, tz}};
+      }
+    });
+    // the Morton key is unique per tile position: octs of one tile tie on
+    // the key and are equal entries, so a sort by key then a unique by key
+    // gives the same list whatever the order of equal entries
+    parallel_sort(tiles, [](const auto& a, const auto& b) { return a.first < b.first; });
+    tiles.erase(std::unique(tiles.begin(), tiles.end(),
+                            [](const auto& a, const auto& b) { return a.first == b.first; }),
+                tiles.end());
   }
   L.ntile = (int)tiles.size();
   pc.mark("tiles");
@@ -418,9 +471,21 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   // pass 2: one prolongation entry per distinct father cell (ascending f),
   // the blocks' codes -2 - entry
   std::vector<int32_t> fcells;
-  for (int32_t code : blk)
-    if (code <= -2) fcells.push_back(-1 - code);
-  std::sort(fcells.begin(), fcells.end());
+  {
+    const int64_t nb = (int64_t)blk.size();
+    const int nch = 64;
+    std::vector<std::vector<int32_t>> part(nch);
+    parallel_for(nch, 1, [&](int64_t c0, int64_t c1) {
+      for (int64_t ch = c0; ch < c1; ch++)
+        for (int64_t b = nb * ch / nch; b < nb * (ch + 1) / nch; b++)
+          if (blk[b] <= -2) part[ch].push_back(-1 - blk[b]);
+    });
+    size_t tot = 0;
+    for (auto& v : part) tot += v.size();
+    fcells.reserve(tot);
+    for (auto& v : part) fcells.insert(fcells.end(), v.begin(), v.end());
+  }
+  parallel_sort(fcells, [](int32_t a, int32_t b) { return a < b; });
   fcells.erase(std::unique(fcells.begin(), fcells.end()), fcells.end());
   parallel_for((int64_t)blk.size(), 1 << 16, [&](int64_t b0, int64_t b1) {
     for (int64_t b = b0; b < b1; b++) {
@@ -443,87 +508,130 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   });
   pc.mark("pass3");
   L.ninterp = (int)fcells.size();
-  RB_TRY(dalloc(&L.d_tile_blk, blk.size()));
+  RB_TRY(dreserve(c->table_pool, c->stream, &L.d_tile_blk, &L.cap_tile_blk, blk.size()));
   RB_TRY(h2d(c, L.d_tile_blk, blk.data(), blk.size() * 4));
   if (L.ninterp) {
-    RB_TRY(dalloc(&L.d_interp7, interp7.size()));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_interp7, &L.cap_interp7, interp7.size()));
     RB_TRY(h2d(c, L.d_interp7, interp7.data(), interp7.size() * 4));
-    RB_TRY(dalloc(&L.d_interp_buf, (size_t)L.ninterp * 8 * 5));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_interp_buf, &L.cap_interp_buf, (size_t)L.ninterp * 8 * 5));
   }
   pc.mark("upload");
   // --- fine-to-coarse corrections (godunov_fine.f90:798-908)
   struct Contrib { int64_t tgt; int64_t batch; int face; int slot; };
-  std::vector<Contrib> cons;
-  std::vector<int32_t> slot_of((size_t)L.noct, -1);
-  int nslot = 0;
-  std::vector<int32_t> h_slot_upd;  // (igrid-1, slot) pairs
-  std::vector<uint8_t> slot_faces;  // faces of each slot that border an unrefined coarser cell
-  for (int p = 0; p < L.noct; p++) {
-    const int32_t g = L.h_active[p];
-    int slot = -1;
-    for (int j = 1; j <= 6; j++) {
-      const int64_t nc = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (g - 1)];
-      if (nc < 1 || nc > c->ncell) return fail(RB_ERR_TREE, "nbor(%d,%d)=%lld out of range", g, j, (long long)nc);
-      if (c->son[nc - 1] == 0) {
-        if (slot < 0) { slot = nslot++; slot_faces.push_back(0); }
-        slot_faces[slot] |= (uint8_t)(1u << (j - 1));
-        cons.push_back({dev_of_fortran(c, nc), p / c->mp.nvector, j - 1, slot});
+  // per oct (active order) the faces bordering an unrefined coarser cell;
+  // slots are numbered in active order, contributions laid out in that
+  // order too (prefix sums), so the tables do not depend on the threads
+  std::vector<uint8_t> fmask((size_t)L.noct, 0);
+  {
+    ParError perr;
+    parallel_for(L.noct, 1 << 14, [&](int64_t p0, int64_t p1) {
+      for (int64_t p = p0; p < p1; p++) {
+        const int32_t g = L.h_active[p];
+        uint8_t m = 0;
+        for (int j = 1; j <= 6; j++) {
+          const int64_t nc = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (g - 1)];
+          if (nc < 1 || nc > c->ncell) {
+            perr.record(RB_ERR_TREE, "nbor(%d,%d)=%lld out of range", g, j, (long long)nc);
+            return;
+          }
+          if (c->son[nc - 1] == 0) m |= (uint8_t)(1u << (j - 1));
+        }
+        fmask[p] = m;
       }
-    }
-    if (slot >= 0) { h_slot_upd.push_back(g - 1); h_slot_upd.push_back(slot); }
+    });
+    RB_TRY(perr.report());
   }
+  std::vector<int32_t> slot_at((size_t)L.noct + 1, 0), con_at((size_t)L.noct + 1, 0);
+  for (int p = 0; p < L.noct; p++) {
+    slot_at[p + 1] = slot_at[p] + (fmask[p] != 0);
+    con_at[p + 1] = con_at[p] + __builtin_popcount(fmask[p]);
+  }
+  const int nslot = slot_at[L.noct];
+  std::vector<Contrib> cons((size_t)con_at[L.noct]);
+  std::vector<uint8_t> slot_faces((size_t)nslot);  // faces of each slot that border an unrefined coarser cell
+  parallel_for(L.noct, 1 << 14, [&](int64_t p0, int64_t p1) {
+    for (int64_t p = p0; p < p1; p++) {
+      const uint8_t m = fmask[p];
+      if (!m) continue;
+      const int32_t g = L.h_active[p];
+      const int slot = slot_at[p];
+      slot_faces[slot] = m;
+      int k = con_at[p];
+      for (int j = 1; j <= 6; j++)
+        if (m >> (j - 1) & 1) {
+          const int64_t nc = c->nbor[(size_t)(j - 1) * c->mp.ngridmax + (g - 1)];
+          cons[k++] = {dev_of_fortran(c, nc), p / c->mp.nvector, j - 1, slot};
+        }
+    }
+  });
   L.nslot = nslot;
   if (nslot) {
-    std::stable_sort(cons.begin(), cons.end(), [](const Contrib& a, const Contrib& b) {
+    // (target, face) is unique (a coarse cell has one contributing fine oct
+    // per face direction); the slot, which follows the active order, breaks
+    // any tie as the generation order would
+    parallel_sort(cons, [](const Contrib& a, const Contrib& b) {
       if (a.tgt != b.tgt) return a.tgt < b.tgt;
       if (a.batch != b.batch) return a.batch < b.batch;
-      return a.face < b.face;  // direction, then left (even) before right (odd)
+      if (a.face != b.face) return a.face < b.face;  // direction, then left (even) before right (odd)
+      return a.slot < b.slot;
     });
-    std::vector<int32_t> tgt, off, contrib;
+    std::vector<int32_t> tgt, off, contrib(cons.size());
     for (size_t i = 0; i < cons.size(); i++) {
       if (i == 0 || cons[i].tgt != cons[i - 1].tgt) {
         tgt.push_back((int32_t)cons[i].tgt);
         off.push_back((int32_t)i);
       }
-      contrib.push_back(cons[i].slot * 6 + cons[i].face);
+      contrib[i] = cons[i].slot * 6 + cons[i].face;
     }
     off.push_back((int32_t)cons.size());
     L.ntgt = (int)tgt.size();
-    RB_TRY(dalloc(&L.d_tgt, tgt.size()));
-    RB_TRY(dalloc(&L.d_tgt_off, off.size()));
-    RB_TRY(dalloc(&L.d_contrib, contrib.size()));
-    RB_TRY(dalloc(&L.d_corr_flux, (size_t)nslot * 120));
-    if (c->hp.pressure_fix) RB_TRY(dalloc(&L.d_corr_tmp, (size_t)nslot * 48));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_tgt, &L.cap_tgt, tgt.size()));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_tgt_off, &L.cap_tgt_off, off.size()));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_contrib, &L.cap_contrib, contrib.size()));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_corr_flux, &L.cap_corr_flux, (size_t)nslot * 120));
+    if (c->hp.pressure_fix) RB_TRY(dreserve(c->table_pool, c->stream, &L.d_corr_tmp, &L.cap_corr_tmp, (size_t)nslot * 48));
     RB_TRY(h2d(c, L.d_tgt, tgt.data(), tgt.size() * 4));
     RB_TRY(h2d(c, L.d_tgt_off, off.data(), off.size() * 4));
     RB_TRY(h2d(c, L.d_contrib, contrib.data(), contrib.size() * 4));
   }
   // this level's entries of the per-oct correction slot table
-  for (int32_t g : L.h_active) c->h_corr_slot[g - 1] = -1;
-  for (size_t i = 0; i + 1 < h_slot_upd.size(); i += 2) c->h_corr_slot[h_slot_upd[i]] = h_slot_upd[i + 1];
+  parallel_for(L.noct, 1 << 14, [&](int64_t p0, int64_t p1) {
+    for (int64_t p = p0; p < p1; p++) c->h_corr_slot[L.h_active[p] - 1] = fmask[p] ? slot_at[p] : -1;
+  });
   pc.mark("corr");
   // per tile, the faces whose fluxes the fine-to-coarse correction reads:
   // entries (oct position in the tile | face << 8, slot), tile t's in
   // [off[t], off[t+1]), so that the godunov kernel stores only those
   if (nslot) {
     const int NOCT = TOX * TOY * TOZ;
-    std::vector<int32_t> off((size_t)L.ntile + 1, 0), ent;
-    for (int t = 0; t < L.ntile; t++) {
+    std::vector<int32_t> off((size_t)L.ntile + 1, 0);
+    auto tile_entries = [&](int t, int32_t* out) {  // entries of tile t (written when out != null)
       const int32_t* B = &blk[(size_t)t * NBLK];
-      off[t] = (int32_t)(ent.size() / 2);
+      int k = 0;
       for (int o = 0; o < NOCT; o++) {
         const int ox = o % TOX, oy = (o / TOX) % TOY, oz = o / (TOX * TOY);
         const int32_t code = B[(ox + 1) + BX * ((oy + 1) + BY * (oz + 1))];
         if (code < 0 || c->h_corr_slot[code] < 0) continue;
         const int32_t slot = c->h_corr_slot[code];
         for (int f = 0; f < 6; f++)
-          if (slot_faces[slot] >> f & 1) { ent.push_back(o | f << 8); ent.push_back(slot); }
+          if (slot_faces[slot] >> f & 1) {
+            if (out) { out[2 * k] = o | f << 8; out[2 * k + 1] = slot; }
+            k++;
+          }
       }
-    }
-    off[L.ntile] = (int32_t)(ent.size() / 2);
-    RB_TRY(dalloc(&L.d_tile_corr_off, off.size()));
+      return k;
+    };
+    parallel_for(L.ntile, 1024, [&](int64_t t0, int64_t t1) {
+      for (int64_t t = t0; t < t1; t++) off[t + 1] = tile_entries((int)t, nullptr);
+    });
+    for (int t = 0; t < L.ntile; t++) off[t + 1] += off[t];
+    std::vector<int32_t> ent((size_t)off[L.ntile] * 2);
+    parallel_for(L.ntile, 1024, [&](int64_t t0, int64_t t1) {
+      for (int64_t t = t0; t < t1; t++) tile_entries((int)t, ent.data() + 2 * (size_t)off[t]);
+    });
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_tile_corr_off, &L.cap_tile_corr_off, off.size()));
     RB_TRY(h2d(c, L.d_tile_corr_off, off.data(), off.size() * 4));
-    RB_TRY(dalloc(&L.d_tile_corr, ent.size()));
+    RB_TRY(dreserve(c->table_pool, c->stream, &L.d_tile_corr, &L.cap_tile_corr, ent.size()));
     RB_TRY(h2d(c, L.d_tile_corr, ent.data(), ent.size() * 4));
   }
   if (c->hp.pressure_fix) RB_TRY(ensure_nres6(c, L));
@@ -544,7 +652,6 @@ int build_boundary_pairs(rb_context* c) {
   int64_t cap = 0;
   for (int l = 1; l <= c->mp.nlevelmax; l++) {
     Level& L = c->lv[l];
-    dfree(L.d_bpair);
     L.h_boff.assign((size_t)nb + 1, 0);
     if (nb == 0) continue;
     std::vector<int32_t> pairs;
@@ -566,7 +673,7 @@ int build_boundary_pairs(rb_context* c) {
       cap = std::max(cap, L.h_boff[ib + 1] - L.h_boff[ib]);
     }
     if (!pairs.empty()) {
-      RB_TRY(dalloc(&L.d_bpair, pairs.size()));
+      RB_TRY(dreserve(c->table_pool, c->stream, &L.d_bpair, &L.cap_bpair, pairs.size()));
       RB_TRY(h2d(c, L.d_bpair, pairs.data(), pairs.size() * 4));
     }
   }
@@ -599,21 +706,17 @@ int prolong_new_octs(rb_context* c, const std::vector<std::vector<int32_t>>& bor
       }
       octs.push_back(g - 1);
     }
-    int32_t *d_octs = nullptr, *d_cells = nullptr;
-    int rc = dalloc(&d_octs, octs.size());
-    if (!rc) rc = dalloc(&d_cells, cells7.size());
-    if (!rc) rc = h2d(c, d_octs, octs.data(), octs.size() * 4);
-    if (!rc) rc = h2d(c, d_cells, cells7.data(), cells7.size() * 4);
-    if (!rc) {
-      rb::prolong_new_octs_kernel<<<(int)((octs.size() + 127) / 128), 128, 0, c->stream>>>(
-          c->d_uold, d_cells, d_octs, (int32_t)octs.size(), c->ncell, c->mp.ncoarse, c->hp);
-      const cudaError_t e = cudaGetLastError();
-      if (e != cudaSuccess) rc = fail(RB_ERR_CUDA, "prolongation of new octs failed: %s", cudaGetErrorString(e));
-    }
-    if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = fail(RB_ERR_CUDA, "prolongation sync failed");
-    dfree(d_octs);
-    dfree(d_cells);
-    if (rc) return rc;
+    // octs and cells in the staging buffer (8 ints per new oct, at most
+    // ngridmax octs: within its 40 bytes per cell)
+    int32_t* d_octs = reinterpret_cast<int32_t*>(c->d_stage);
+    int32_t* d_cells = d_octs + octs.size();
+    RB_TRY(h2d(c, d_octs, octs.data(), octs.size() * 4));
+    RB_TRY(h2d(c, d_cells, cells7.data(), cells7.size() * 4));
+    rb::prolong_new_octs_kernel<<<(int)((octs.size() + 127) / 128), 128, 0, c->stream>>>(
+        c->d_uold, d_cells, d_octs, (int32_t)octs.size(), c->ncell, c->mp.ncoarse, c->hp);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(RB_ERR_CUDA, "prolongation of new octs failed: %s", cudaGetErrorString(e));
+    RB_CUDA(cudaStreamSynchronize(c->stream));
     c->octs_prolonged += (int64_t)octs.size();
   }
   return RB_OK;
@@ -713,83 +816,109 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
   }
   // positions (from the father chain, level by level), level and boundary
   // marks; in the incremental case also the nbor rows, father and the son
-  // entries of the octs' cells, compared with the previous tree's
-  for (int l = 1; l <= NL; l++) {
-    Level& L = c->lv[l];
-    const size_t n = L.h_active.size(), nall = n + L.h_bnd.size();
-    for (size_t o = 0; o < nall; o++) {
-      const int32_t g = o < n ? L.h_active[o] : L.h_bnd[o - n];
-      const size_t gi = (size_t)(g - 1);
-      if (c->level_of[gi] != 0) return fail(RB_ERR_TREE, "grid %d listed twice", g);
-      const int64_t fc = father[gi];
-      int64_t x[3];
-      if (l == 1) {
-        if (fc < 1 || fc > c->mp.ncoarse) return fail(RB_ERR_TREE, "level-1 grid %d father %lld is not coarse", g, (long long)fc);
-        x[0] = (fc - 1) % c->mp.nx;
-        x[1] = ((fc - 1) / c->mp.nx) % c->mp.ny;
-        x[2] = (fc - 1) / ((int64_t)c->mp.nx * c->mp.ny);
-      } else {
-        const int64_t r = fc - 1 - c->mp.ncoarse;
-        if (r < 0 || r >= (int64_t)8 * ngm) return fail(RB_ERR_TREE, "grid %d father %lld out of range", g, (long long)fc);
-        const int32_t pg = (int32_t)(r % ngm) + 1;
-        const int pos = (int)(r / ngm);
-        if (c->level_of[pg - 1] != l - 1) return fail(RB_ERR_TREE, "grid %d: father grid %d is not at level %d", g, pg, l - 1);
-        const int64_t* px = &c->coords[(size_t)(pg - 1) * 3];
-        x[0] = 2 * px[0] + (pos & 1);
-        x[1] = 2 * px[1] + ((pos >> 1) & 1);
-        x[2] = 2 * px[2] + ((pos >> 2) & 1);
-      }
-      int64_t* xc = &c->coords[gi * 3];
-      if (incremental) {
-        if (xc[0] != x[0] || xc[1] != x[1] || xc[2] != x[2]) oct_dirty[l] = 1;
-        for (int j = 0; j < 6; j++) {
-          const size_t k = (size_t)j * ngm + gi;
-          if (c->nbor[k] != nbor[k]) { oct_dirty[l] = 1; c->nbor[k] = nbor[k]; }
-        }
-        c->father[gi] = father[gi];
-        for (int ind = 1; ind <= 8; ind++) {
-          const int64_t cf = fcell(c, ind, g) - 1;
-          if (c->son[cf] != son[cf]) {
-            cell_dirty[l] = 1;
-            son_idx.push_back(dev_of_fortran(c, cf + 1));
-            son_val.push_back(son[cf]);
-            c->son[cf] = son[cf];
+  // entries of the octs' cells, compared with the previous tree's. Levels in
+  // order (a level reads its parents' positions), the octs of a level on all
+  // host threads (each oct writes only its own entries).
+  {
+    const int nch = 64;
+    std::vector<std::vector<int64_t>> part_idx(nch);
+    std::vector<std::vector<int32_t>> part_val(nch);
+    for (int l = 1; l <= NL; l++) {
+      Level& L = c->lv[l];
+      const size_t n = L.h_active.size();
+      const int64_t nall = (int64_t)(n + L.h_bnd.size());
+      ParError perr;
+      std::atomic<bool> odirty{false}, cdirty{false};
+      parallel_for(nch, 1, [&](int64_t c0, int64_t c1) {
+        for (int64_t ch = c0; ch < c1; ch++) {
+          bool od = false, cd = false;
+          for (int64_t o = nall * ch / nch; o < nall * (ch + 1) / nch; o++) {
+            const int32_t g = (size_t)o < n ? L.h_active[o] : L.h_bnd[o - n];
+            const size_t gi = (size_t)(g - 1);
+            if (c->level_of[gi] != 0) { perr.record(RB_ERR_TREE, "grid %d listed twice", g); return; }
+            const int64_t fc = father[gi];
+            int64_t x[3];
+            if (l == 1) {
+              if (fc < 1 || fc > c->mp.ncoarse) {
+                perr.record(RB_ERR_TREE, "level-1 grid %d father %lld is not coarse", g, (long long)fc);
+                return;
+              }
+              x[0] = (fc - 1) % c->mp.nx;
+              x[1] = ((fc - 1) / c->mp.nx) % c->mp.ny;
+              x[2] = (fc - 1) / ((int64_t)c->mp.nx * c->mp.ny);
+            } else {
+              const int64_t r = fc - 1 - c->mp.ncoarse;
+              if (r < 0 || r >= (int64_t)8 * ngm) {
+                perr.record(RB_ERR_TREE, "grid %d father %lld out of range", g, (long long)fc);
+                return;
+              }
+              const int32_t pg = (int32_t)(r % ngm) + 1;
+              const int pos = (int)(r / ngm);
+              if (c->level_of[pg - 1] != l - 1) {
+                perr.record(RB_ERR_TREE, "grid %d: father grid %d is not at level %d", g, pg, l - 1);
+                return;
+              }
+              const int64_t* px = &c->coords[(size_t)(pg - 1) * 3];
+              x[0] = 2 * px[0] + (pos & 1);
+              x[1] = 2 * px[1] + ((pos >> 1) & 1);
+              x[2] = 2 * px[2] + ((pos >> 2) & 1);
+            }
+            int64_t* xc = &c->coords[gi * 3];
+            if (incremental) {
+              if (xc[0] != x[0] || xc[1] != x[1] || xc[2] != x[2]) od = true;
+              for (int j = 0; j < 6; j++) {
+                const size_t k = (size_t)j * ngm + gi;
+                if (c->nbor[k] != nbor[k]) { od = true; c->nbor[k] = nbor[k]; }
+              }
+              c->father[gi] = father[gi];
+              for (int ind = 1; ind <= 8; ind++) {
+                const int64_t cf = fcell(c, ind, g) - 1;
+                if (c->son[cf] != son[cf]) {
+                  cd = true;
+                  part_idx[ch].push_back(dev_of_fortran(c, cf + 1));
+                  part_val[ch].push_back(son[cf]);
+                  c->son[cf] = son[cf];
+                }
+              }
+            }
+            xc[0] = x[0]; xc[1] = x[1]; xc[2] = x[2];
+            c->level_of[gi] = (int8_t)l;
+            if ((size_t)o >= n) c->is_bnd[gi] = 1;
           }
+          if (od) odirty.store(true);
+          if (cd) cdirty.store(true);
         }
-      }
-      xc[0] = x[0]; xc[1] = x[1]; xc[2] = x[2];
-      c->level_of[gi] = (int8_t)l;
-      if (o >= n) c->is_bnd[gi] = 1;
+      });
+      RB_TRY(perr.report());
+      if (odirty.load()) oct_dirty[l] = 1;
+      if (cdirty.load()) cell_dirty[l] = 1;
+    }
+    for (int ch = 0; ch < nch; ch++) {
+      son_idx.insert(son_idx.end(), part_idx[ch].begin(), part_idx[ch].end());
+      son_val.insert(son_val.end(), part_val[ch].begin(), part_val[ch].end());
     }
   }
-  // the position indexes of the changed levels, sorted in parallel
+  // the position indexes of the changed levels (sorted on all host threads)
   c->idx.resize(RB_MAXLEVEL + 2);
-  {
-    ParError perr;
-    parallel_for(NL, 1, [&](int64_t l0, int64_t l1) {
-      for (int64_t l = l0 + 1; l <= l1; l++) {
-        if (!oct_dirty[l]) continue;
-        const Level& L = c->lv[l];
-        OctIndex& I = c->idx[l];
-        I.v.clear();
-        I.nx = (int64_t)c->mp.nx << (l - 1);
-        I.ny = (int64_t)c->mp.ny << (l - 1);
-        I.nz = (int64_t)c->mp.nz << (l - 1);
-        I.v.reserve(L.h_active.size() + L.h_bnd.size());
-        for (int32_t g : L.h_active) {
-          const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
-          I.v.push_back({I.key(x[0], x[1], x[2]), g});
-        }
-        for (int32_t g : L.h_bnd) {
-          const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
-          I.v.push_back({I.key(x[0], x[1], x[2]), g});
-        }
-        std::sort(I.v.begin(), I.v.end());
-        for (size_t i = 1; i < I.v.size(); i++)
-          if (I.v[i].first == I.v[i - 1].first) perr.record(RB_ERR_TREE, "level %d: two octs at one position", (int)l);
+  for (int l = 1; l <= NL; l++) {
+    if (!oct_dirty[l]) continue;
+    const Level& L = c->lv[l];
+    OctIndex& I = c->idx[l];
+    I.nx = (int64_t)c->mp.nx << (l - 1);
+    I.ny = (int64_t)c->mp.ny << (l - 1);
+    I.nz = (int64_t)c->mp.nz << (l - 1);
+    const size_t n = L.h_active.size(), nall = n + L.h_bnd.size();
+    I.v.resize(nall);
+    parallel_for((int64_t)nall, 1 << 14, [&](int64_t o0, int64_t o1) {
+      for (int64_t o = o0; o < o1; o++) {
+        const int32_t g = (size_t)o < n ? L.h_active[o] : L.h_bnd[o - n];
+        const int64_t* x = &c->coords[(size_t)(g - 1) * 3];
+        I.v[o] = {I.key(x[0], x[1], x[2]), g};
       }
     });
-    RB_TRY(perr.report());
+    parallel_sort(I.v, [](const std::pair<int64_t, int32_t>& a, const std::pair<int64_t, int32_t>& b) { return a < b; });
+    for (size_t i = 1; i < I.v.size(); i++)
+      if (I.v[i].first == I.v[i - 1].first) return fail(RB_ERR_TREE, "level %d: two octs at one position", l);
   }
   // per level: completeness, leaf cells, device active list (re-uploaded
   // only when the list changed)
@@ -808,14 +937,11 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
     L.leaf_cells = leaf;
     L.has_refined = refined;
     const bool same_list = incremental && L.h_active == old_active[l] && (L.d_active || n == 0);
-    if (!same_list) {
-      dfree(L.d_active);
-      if (n) {
-        std::vector<int32_t> a0(n);
-        for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
-        RB_TRY(dalloc(&L.d_active, (size_t)n));
-        RB_TRY(h2d(c, L.d_active, a0.data(), (size_t)n * 4));
-      }
+    if (!same_list && n) {
+      std::vector<int32_t> a0(n);
+      for (int i = 0; i < n; i++) a0[i] = L.h_active[i] - 1;
+      RB_TRY(dreserve(c->table_pool, c->stream, &L.d_active, &L.cap_active, (size_t)n));
+      RB_TRY(h2d(c, L.d_active, a0.data(), (size_t)n * 4));
     }
   }
   // son mirror (device layout): the whole array, or the entries that changed
@@ -1407,6 +1533,21 @@ int rb_create(const rb_hydro_params* hp, const rb_mesh_params* mp, int precision
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess)
     return bail(fail(RB_ERR_CUDA, "stream/event creation failed"));
+  {
+    // the level tables' pool: freed blocks stay in it for the next re-sync
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = c->device;
+    uint64_t keep_all = UINT64_MAX;
+    if (cudaMemPoolCreate(&c->table_pool, &props) != cudaSuccess) {
+      c->table_pool = nullptr;
+      return bail(fail(RB_ERR_CUDA, "memory pool creation failed"));
+    }
+    if (cudaMemPoolSetAttribute(c->table_pool, cudaMemPoolAttrReleaseThreshold, &keep_all) != cudaSuccess)
+      return bail(fail(RB_ERR_CUDA, "memory pool set-up failed"));
+  }
   int rc;
   if ((rc = dalloc(&c->d_uold, (size_t)c->ncell * 5)) || (rc = dalloc(&c->d_unew, (size_t)c->ncell * 5)) ||
       (rc = dalloc(&c->d_son, (size_t)c->ncell)) ||
@@ -1438,6 +1579,9 @@ int rb_destroy(rb_context* c) {
   if (!c) return RB_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_tree(c);
+  if (c->stream) cudaStreamSynchronize(c->stream);  // the tables' pool frees are stream-ordered
+  if (c->table_pool) cudaMemPoolDestroy(c->table_pool);
+  c->table_pool = nullptr;
   dfree(c->d_uold); dfree(c->d_unew); dfree(c->d_son);
   dfree(c->d_divu); dfree(c->d_enew); dfree(c->d_bbuf);
   dfree(c->d_stage); dfree(c->d_partial); dfree(c->d_red); dfree(c->d_clock); dfree(c->d_sched);
