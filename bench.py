@@ -81,6 +81,8 @@ def parse():
                     help="host wall-time budget (s) of the --remesh run: it reports where it stopped")
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests of the bounded serving pass (0: none)")
+    ap.add_argument("--tile-order", type=int, default=0, choices=[0, 1],
+                    help="AMR runs: launch order of the tiles (0 3D Morton, 1 z slabs)")
     ap.add_argument("--method", choices=["stream", "tiles"], default="stream",
                     help="uniform-level kernel: z-streaming over a dense mirror, or godunov_fine oct tiles")
     return ap.parse_args()
@@ -502,6 +504,7 @@ def run_amr(args):
     out, states = {}, {}
     for prec in ([args.only] if args.only else ["mixed", "fp64"]):
         s = runtime.Solver(tree, hp, precision=prec, uold=u, nsubcycle=[2] * 33)
+        s.set_tile_order(args.tile_order)
         # the cost of a remeshing round trip through the drop-in boundary: a
         # full tree re-sync (tables rebuilt on the host) and a state upload
         t0s = time.perf_counter()

@@ -184,6 +184,12 @@ int rb_cell_updates(rb_context *ctx, int64_t *out);
 int rb_set_tile_shape(rb_context *ctx, int ilevel, int shape);
 int rb_get_tile_shape(rb_context *ctx, int ilevel, int *shape);
 int rb_tile_shape_info(int shape, int *tx, int *ty, int *tz, int *nthreads);
+/* Launch order of every level's tiles (one CTA each): 0 (default) a 3D Morton
+ * curve over the tile positions; 1 z slabs one tile thick, a 2D Morton curve
+ * inside each, so that the CTAs resident at once cover neighbouring slabs and
+ * the stencil halos a tile reads were read by a tile of the slab before it.
+ * The results do not depend on the order. */
+int rb_set_tile_order(rb_context *ctx, int order);
 
 /* unsplit with the reference's argument list and Fortran layouts
  * (umuscl.f90:22-38): uin(nvector,-1:4,-1:4,-1:4,5),

@@ -44,7 +44,9 @@ struct TileArgs {
   int32_t has_refined;                  // any son>0 among this level's cells
   int32_t dx_pow2;                      // dx is an exact power of two
   int32_t fused;                        // 1: unew = uold + fluxes (set_unew fused) and
-                                        //    CFL partials of the new state
+                                        //    CFL partials of the new state; 2: unew = uold +
+                                        //    fluxes only (a level without finer octs, whose
+                                        //    unew holds no fine-to-coarse correction)
   double dt, dx, inv_dx;
   const double* __restrict__ dt_dev;    // if non-null, dt is read here
   double* __restrict__ partial;         // fused: [ntile][4] (min dt, mass, E, eint)
@@ -478,7 +480,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
 #pragma unroll
     for (int v = 0; v < 5; v++) {
       const R* Fv = F + v * NF;
-      double un = a.fused ? __ldcg(a.uold + v * ncell + dc) : a.unew[v * ncell + dc];
+      double un = a.fused ? __ldcg(a.uold + v * ncell + dc) : a.unew[v * ncell + dc];  // set_unew's value
       un = un + ((double)Fv[fxl] - (double)Fv[fxl + 1]);
       un = un + ((double)Fv[fyl] - (double)Fv[fyl + TX]);
       un = un + ((double)Fv[fzl] - (double)Fv[fzl + TX * TY]);
@@ -512,7 +514,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       a.divu[dc] = dv;
       a.enew[dc] = en;
     }
-    if (a.fused) {
+    if (a.fused == 1) {
       // courant_fine on the updated state (the next step's CFL condition);
       // the level minimum of dt_cell is dt_cell(maximum wave speed)
       const double ir = 1.0 / fmx(unv[0], a.hp.smallr);
@@ -522,7 +524,7 @@ __global__ void __launch_bounds__(NT) godunov_tile_kernel(TileArgs a) {
       smax = fmx(smax, sizeof(R) == 8 ? cfl_speed(unv, a.hp) : cfl_speed_fast(unv, a.hp));
     }
   }
-  if (a.fused) {
+  if (a.fused == 1) {
     __shared__ double red[4][NT / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

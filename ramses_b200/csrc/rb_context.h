@@ -199,6 +199,7 @@ struct rb_context {
   bool dense_valid = false;         // the dense mirror holds the newest state of `finest`
   bool oct_stale = false;           // the oct layout of `finest` lags the dense mirror
   int stream_shape = -1, stream_hz = 0, stream_items = 0;
+  int tile_order = 0;               // launch order of a level's tiles: 0 3D Morton, 1 z slabs
   // residency protocol of the drop-in boundary: which copy of uold is newer
   // (0: host and device agree, 1: the device's, 2: the host's), the host's
   // tree generation and the one last synchronised, and the transfer counters

@@ -76,6 +76,19 @@ inline int64_t dev_of_fortran(const rb_context* c, int64_t icell) {
   return c->mp.ncoarse + (r % c->mp.ngridmax) * 8 + r / c->mp.ngridmax;
 }
 
+inline uint64_t morton2(uint64_t x, uint64_t y) {
+  auto spread = [](uint64_t a) {
+    a &= 0x1fffff;
+    a = (a | a << 16) & 0x0000ffff0000ffffULL;
+    a = (a | a << 8) & 0x00ff00ff00ff00ffULL;
+    a = (a | a << 4) & 0x0f0f0f0f0f0f0f0fULL;
+    a = (a | a << 2) & 0x3333333333333333ULL;
+    a = (a | a << 1) & 0x5555555555555555ULL;
+    return a;
+  };
+  return spread(x) | spread(y) << 1;
+}
+
 inline uint64_t morton3(uint64_t x, uint64_t y, uint64_t z) {
   auto spread = [](uint64_t a) {
     a &= 0x1fffff;
@@ -374,10 +387,13 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
       for (int64_t i = i0; i < i1; i++) {
         const int64_t* x = &c->coords[(size_t)(L.h_active[i] - 1) * 3];
         const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
-        tiles[i] = {morton3(tx, ty, tz), {tx, ty, tz}};
+        // launch order of the tiles: a 3D Morton curve, or z slabs one tile
+        // thick with a 2D Morton curve inside each (rb_set_tile_order)
+        const uint64_t key = c->tile_order == 1 ? ((uint64_t)tz << 42 | morton2(tx, ty)) : morton3(tx, ty, tz);
+        tiles[i] = {key, {tx, ty, tz}};
       }
     });
-    // the Morton key is unique per tile position: octs of one tile tie on
+    // the order key is unique per tile position: octs of one tile tie on
     // the key and are equal entries, so a sort by key then a unique by key
     // gives the same list whatever the order of equal entries
     parallel_sort(tiles, [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -1233,7 +1249,12 @@ int launch_tile(rb_context* c, int shape, const rb::TileArgs& a, int grid) {
   return RB_OK;
 }
 
-int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_dev = nullptr) {
+// fuse_unew: the level has no finer octs, so at godunov time its unew is
+// set_unew's copy of uold (no fine-to-coarse correction went into it); the
+// kernel then starts the update from uold and writes unew without reading it
+// (the caller skips set_unew's copy for the level). Same values bit for bit.
+int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_dev = nullptr,
+                 bool fuse_unew = false) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   if (!dt_dev && (!(dt > 0.0) || !std::isfinite(dt)))
@@ -1246,6 +1267,7 @@ int godunov_impl(rb_context* c, int l, double dt, bool timed, const double* dt_d
   }
   rb::TileArgs a = tile_args(c, L, dt);
   a.dt_dev = dt_dev;
+  if (fuse_unew) a.fused = 2;
   if (!dt_dev) c->dt_godunov[l] = dt;
   if (timed) RB_CUDA(cudaEventRecord(c->ev0, c->stream));
   RB_TRY(launch_tile(c, L.shape, a, L.ntile));
@@ -1291,7 +1313,9 @@ int amr_step_impl(rb_context* c, int l, int icount) {
   c->dtold[l] = c->dtnew[l];
   c->dtnew[l] = c->mp.boxlen / c->hp.smallc;
   double dt_all = c->dtnew[l], ma = 0, ek = 0, ei = 0;
-  RB_TRY(courant_impl(c, l, &dt_all, &ma, &ek, &ei, /*with_set_unew=*/true));
+  // a level without finer octs gets set_unew inside its godunov kernel
+  const bool fuse = !c->lv[l].has_refined;
+  RB_TRY(courant_impl(c, l, &dt_all, &ma, &ek, &ei, /*with_set_unew=*/!fuse));
   c->mass_tot += ma; c->ekin_tot += ek; c->eint_tot += ei;
   c->dtnew[l] = rb_min_host(c->dtnew[l], dt_all);
   if (l > c->mp.levelmin)
@@ -1314,7 +1338,7 @@ int amr_step_impl(rb_context* c, int l, int icount) {
     c->t += c->dtnew[l];
     c->nstep++;
   }
-  RB_TRY(godunov_impl(c, l, c->dtnew[l], false));
+  RB_TRY(godunov_impl(c, l, c->dtnew[l], false, nullptr, fuse));
   c->cell_updates += c->lv[l].leaf_cells;
   RB_TRY(set_uold_upload_impl(c, l, nullptr, c->dtnew[l]));
   RB_TRY(boundary_impl(c, l));  // amr_step.f90:515
@@ -1337,8 +1361,11 @@ int amr_step_dev(rb_context* c, int l, int icount) {
   double* s = c->d_sched;
   const int nblk = courant_blocks(c, l);
   auto k = c->precision == RB_PREC_MIXED ? rb::courant_partial_kernel<256, true> : rb::courant_partial_kernel<256, false>;
+  // + set_unew, which a level without finer octs gets in its godunov kernel
+  const bool fuse = !L.has_refined;
   k<<<nblk, 256, 0, c->stream>>>(c->d_uold, c->d_son, L.d_active, L.noct, c->ncell, c->mp.ncoarse, L.dx, c->hp,
-                                 c->d_partial, c->gate, c->d_unew, c->d_divu, c->d_enew);  // + set_unew
+                                 c->d_partial, c->gate, fuse ? nullptr : c->d_unew, fuse ? nullptr : c->d_divu,
+                                 fuse ? nullptr : c->d_enew);
   RB_CUDA(cudaGetLastError());
   const double nsub_prev = l > c->mp.levelmin ? (double)(float)c->mp.nsubcycle[l - 1] : 1.0;
   rb::sched_courant_kernel<<<1, RB_RED_NT, 0, c->stream>>>(
@@ -1356,7 +1383,7 @@ int amr_step_dev(rb_context* c, int l, int icount) {
     rb::sched_advance_kernel<<<1, 1, 0, c->stream>>>(s, l, 2, 1.0);
   }
   RB_CUDA(cudaGetLastError());
-  RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l));
+  RB_TRY(godunov_impl(c, l, 0.0, false, s + RB_S_DTNEW + l, fuse));
   RB_TRY(set_uold_upload_impl(c, l, s + RB_S_DTNEW + l, 0.0));
   RB_TRY(boundary_impl(c, l));
   if (l > c->mp.levelmin && (c->mp.nsubcycle[l - 1] == 1 || icount == 2)) {
@@ -1959,6 +1986,19 @@ int rb_unsplit(const rb_hydro_params* hp, const double* uin, const double* gravi
   if (e == cudaSuccess) e = cudaMemcpy(tmp, d_tmp, nfl * 6 * sizeof(double), cudaMemcpyDeviceToHost);
   dfree(d_uin); dfree(d_g); dfree(d_flux); dfree(d_tmp);
   if (e != cudaSuccess) return fail(RB_ERR_CUDA, "rb_unsplit: %s", cudaGetErrorString(e));
+  return RB_OK;
+}
+
+int rb_set_tile_order(rb_context* c, int order) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (order != 0 && order != 1) return fail(RB_ERR_INVALID, "tile order %d must be 0 (Morton) or 1 (z slabs)", order);
+  if (order == c->tile_order) return RB_OK;
+  c->tile_order = order;
+  if (!c->have_tree) return RB_OK;
+  drop_graph(c);
+  RB_TRY(sync_oct(c));
+  for (int l = 1; l <= c->mp.nlevelmax; l++)
+    if (c->lv[l].noct) RB_TRY(build_level_tables(c, l, c->idx));
   return RB_OK;
 }
 

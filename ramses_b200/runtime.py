@@ -100,6 +100,7 @@ _PROTOS = {
     "rb_hydro_flag": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(RefineParamsC), _P32, _P64]),
     "rb_cell_updates": (ctypes.c_int, [ctypes.c_void_p, _P64]),
     "rb_set_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "rb_set_tile_order": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_get_tile_shape": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _P32]),
     "rb_tile_shape_info": (ctypes.c_int, [ctypes.c_int, _P32, _P32, _P32, _P32]),
     "rb_unsplit": (ctypes.c_int, [ctypes.POINTER(HydroParamsC), _PD, _PD, _PD, _PD, _PD, ctypes.c_double,
@@ -457,6 +458,10 @@ class Solver:
 
     def set_tile_shape(self, ilevel: int, shape: int):
         _check(load().rb_set_tile_shape(self._h, ilevel, shape), "rb_set_tile_shape")
+
+    def set_tile_order(self, order: int):
+        """Launch order of the levels' tiles: 0 3D Morton, 1 z slabs."""
+        _check(load().rb_set_tile_order(self._h, int(order)), "rb_set_tile_order")
 
     def tile_shape(self, ilevel: int) -> int:
         s = ctypes.c_int32()

@@ -144,6 +144,22 @@ def test_amr_tile_shapes_identical(cuda_lib):
     np.testing.assert_array_equal(outs[0], outs[2])
 
 
+def test_amr_tile_orders_identical(cuda_lib):
+    """The tiles' launch order (3D Morton or z slabs) changes no result."""
+    tree, hp, u = sedov_amr(4, 6)
+    outs = []
+    for order in (0, 1):
+        with runtime.Solver(tree, hp, uold=u) as s:
+            s.set_tile_order(order)
+            for l in range(4, 7):
+                s.set_tile_shape(l, 1)
+            for _ in range(2):
+                s.coarse_step()
+            s.run(max_steps=2)
+            outs.append(s.download_state())
+    np.testing.assert_array_equal(outs[0], outs[1])
+
+
 def test_uniform_run_equals_coarse_steps(cuda_lib):
     tree, hp, u = turbulent_uniform(5)
     with runtime.Solver(tree, hp, uold=u) as a, runtime.Solver(tree, hp, uold=u) as b:
