@@ -484,33 +484,47 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   });
   RB_TRY(perr.report());
   pc.mark("pass1");
-  // pass 2: one prolongation entry per distinct father cell (ascending f),
-  // the blocks' codes -2 - entry
-  std::vector<int32_t> fcells;
+  // pass 2: one prolongation entry per distinct father cell, numbered in the
+  // order of first use (tile order, so that a tile's entries lie together in
+  // the interpolation buffer), the blocks' codes -2 - entry
+  std::vector<int32_t> fcells;   // entry -> father cell
   {
     const int64_t nb = (int64_t)blk.size();
     const int nch = 64;
-    std::vector<std::vector<int32_t>> part(nch);
+    std::vector<std::vector<std::pair<int32_t, int64_t>>> part(nch);   // (father cell, first block)
     parallel_for(nch, 1, [&](int64_t c0, int64_t c1) {
       for (int64_t ch = c0; ch < c1; ch++)
         for (int64_t b = nb * ch / nch; b < nb * (ch + 1) / nch; b++)
-          if (blk[b] <= -2) part[ch].push_back(-1 - blk[b]);
+          if (blk[b] <= -2) part[ch].push_back({-1 - blk[b], b});
     });
+    std::vector<std::pair<int32_t, int64_t>> fb;
     size_t tot = 0;
     for (auto& v : part) tot += v.size();
-    fcells.reserve(tot);
-    for (auto& v : part) fcells.insert(fcells.end(), v.begin(), v.end());
-  }
-  parallel_sort(fcells, [](int32_t a, int32_t b) { return a < b; });
-  fcells.erase(std::unique(fcells.begin(), fcells.end()), fcells.end());
-  parallel_for((int64_t)blk.size(), 1 << 16, [&](int64_t b0, int64_t b1) {
-    for (int64_t b = b0; b < b1; b++) {
-      const int32_t code = blk[b];
-      if (code > -2) continue;
-      const int32_t e = (int32_t)(std::lower_bound(fcells.begin(), fcells.end(), -1 - code) - fcells.begin());
-      blk[b] = -2 - e;
+    fb.reserve(tot);
+    for (auto& v : part) fb.insert(fb.end(), v.begin(), v.end());
+    parallel_sort(fb, [](const std::pair<int32_t, int64_t>& a, const std::pair<int32_t, int64_t>& b) { return a < b; });
+    // first use of each father cell, then the cells in the order of first use
+    std::vector<std::pair<int64_t, int32_t>> first;
+    for (size_t i = 0; i < fb.size(); i++)
+      if (i == 0 || fb[i].first != fb[i - 1].first) first.push_back({fb[i].second, fb[i].first});
+    parallel_sort(first, [](const std::pair<int64_t, int32_t>& a, const std::pair<int64_t, int32_t>& b) { return a < b; });
+    fcells.resize(first.size());
+    std::vector<std::pair<int32_t, int32_t>> entry_of(first.size());   // (father cell, entry), by cell
+    for (size_t e = 0; e < first.size(); e++) {
+      fcells[e] = first[e].second;
+      entry_of[e] = {first[e].second, (int32_t)e};
     }
-  });
+    parallel_sort(entry_of, [](const std::pair<int32_t, int32_t>& a, const std::pair<int32_t, int32_t>& b) { return a < b; });
+    parallel_for(nb, 1 << 16, [&](int64_t b0, int64_t b1) {
+      for (int64_t b = b0; b < b1; b++) {
+        const int32_t code = blk[b];
+        if (code > -2) continue;
+        const int32_t f = -1 - code;
+        const auto it = std::lower_bound(entry_of.begin(), entry_of.end(), std::make_pair(f, (int32_t)INT32_MIN));
+        blk[b] = -2 - it->second;
+      }
+    });
+  }
   pc.mark("pass2");
   // pass 3, entries in parallel: the father cell and its getnborfather
   // neighbours of every entry
