@@ -96,6 +96,31 @@ def test_amr_device_run_bitwise(cuda_lib, oracle_lib, riemann):
         check(tree, s.download_state(), orc.uold)
 
 
+def test_resync_with_boundaries_keeps_tables_and_results(cuda_lib, oracle_lib):
+    """A re-sync of the same bounded tree (rb_set_boundary then
+    rb_sync_tree, as the drop-in does after a host tree change) keeps every
+    level's tables, and the run stays bit-identical to the oracle; a re-sync
+    with other boundary types rebuilds them all."""
+    tree, hp, u = sedov_amr_bounded(("outflow",) * 3)
+    orc = oracle.OracleRun(tree, hp, u)
+    for _ in range(4):
+        orc.coarse_step()
+    nonempty = sum(1 for lvl in range(1, tree.nlevelmax + 1) if tree.noct(lvl))
+    with runtime.Solver(tree, hp, uold=u) as s:
+        assert s.run(max_steps=2) == 2
+        s.sync_tree(tree)
+        st = s.sync_stats()
+        assert st["levels_built"] == 0 and st["levels_reused"] == nonempty, st
+        assert s.transfer_stats()["octs_prolonged"] == 0
+        assert s.run(max_steps=2) == 2
+        check(tree, s.download_state(), orc.uold)
+    t2, hp2, u2 = sedov_amr_bounded(("reflexive",) * 3)
+    with runtime.Solver(tree, hp, uold=u) as s:
+        s.sync_tree(t2)   # same octs, walls instead of free boundaries
+        st = s.sync_stats()
+        assert st["levels_reused"] == 0 and st["levels_built"] == nonempty, st
+
+
 def test_amr_walls_pressure_fix_bitwise(cuda_lib, oracle_lib):
     tree, hp, u = sedov_amr_bounded(("reflexive",) * 3, pressure_fix=True, beta_fix=0.5)
     orc = oracle.OracleRun(tree, hp, u)
