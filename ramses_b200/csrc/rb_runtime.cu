@@ -381,18 +381,27 @@ int build_level_tables(rb_context* c, int l, const std::vector<OctIndex>& idx) {
   const int BX = TOX + 2, BY = TOY + 2, BZ = TOZ + 2, NBLK = BX * BY * BZ;
   const OctIndex& I = idx[l];
   // --- tiles: unique tile coordinates of the level's octs, Morton ordered
-  std::vector<std::pair<uint64_t, std::array<int64_t, 3>>> tiles((size_t)L.noct);
+  std::vector<std::pair<uint64_t, std::array<int64_t, 3>>> tiles;
   {
-    parallel_for(L.noct, 1 << 14, [&](int64_t i0, int64_t i1) {
-      for (int64_t i = i0; i < i1; i++) {
-        const int64_t* x = &c->coords[(size_t)(L.h_active[i] - 1) * 3];
-        const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
-        // launch order of the tiles: a 3D Morton curve, or z slabs one tile
-        // thick with a 2D Morton curve inside each (rb_set_tile_order)
-        const uint64_t key = c->tile_order == 1 ? ((uint64_t)tz << 42 | morton2(tx, ty)) : morton3(tx, ty, tz);
-        tiles[i] = {key, {tx, ty, tz}};
-      }
+    // the tile of every oct; runs of octs of one tile (siblings follow each
+    // other in an active list) are cut to one entry per chunk before the sort
+    const int nch = 64;
+    std::vector<std::vector<std::pair<uint64_t, std::array<int64_t, 3>>>> part(nch);
+    parallel_for(nch, 1, [&](int64_t c0, int64_t c1) {
+      for (int64_t ch = c0; ch < c1; ch++)
+        for (int64_t i = (int64_t)L.noct * ch / nch; i < (int64_t)L.noct * (ch + 1) / nch; i++) {
+          const int64_t* x = &c->coords[(size_t)(L.h_active[i] - 1) * 3];
+          const int64_t tx = x[0] / TOX, ty = x[1] / TOY, tz = x[2] / TOZ;
+          // launch order of the tiles: a 3D Morton curve, or z slabs one tile
+          // thick with a 2D Morton curve inside each (rb_set_tile_order)
+          const uint64_t key = c->tile_order == 1 ? ((uint64_t)tz << 42 | morton2(tx, ty)) : morton3(tx, ty, tz);
+          if (part[ch].empty() || part[ch].back().first != key) part[ch].push_back({key, {tx, ty, tz}});
+        }
     });
+    size_t tot = 0;
+    for (auto& v : part) tot += v.size();
+    tiles.reserve(tot);
+    for (auto& v : part) tiles.insert(tiles.end(), v.begin(), v.end());
     // the order key is unique per tile position: octs of one tile tie on
     // the key and are equal entries, so a sort by key then a unique by key
     // gives the same list whatever the order of equal entries
@@ -956,16 +965,22 @@ int sync_tree_impl(rb_context* c, const int32_t* son, const int32_t* father, con
     Level& L = c->lv[l];
     const int n = L.noct;
     L.complete = (int64_t)n == c->idx[l].nx * c->idx[l].ny * c->idx[l].nz;
-    int64_t leaf = 0;
-    int refined = 0;
-    for (int32_t g : L.h_active)
-      for (int ind = 1; ind <= 8; ind++) {
-        const int32_t sv = son[fcell(c, ind, g) - 1];
-        leaf += (sv == 0);
-        refined |= (sv > 0);
-      }
-    L.leaf_cells = leaf;
-    L.has_refined = refined;
+    std::atomic<int64_t> leaf{0};
+    std::atomic<int> refined{0};
+    parallel_for(n, 1 << 15, [&](int64_t i0, int64_t i1) {
+      int64_t lf = 0;
+      int rf = 0;
+      for (int64_t i = i0; i < i1; i++)
+        for (int ind = 1; ind <= 8; ind++) {
+          const int32_t sv = son[fcell(c, ind, L.h_active[i]) - 1];
+          lf += (sv == 0);
+          rf |= (sv > 0);
+        }
+      leaf += lf;
+      if (rf) refined.store(1);
+    });
+    L.leaf_cells = leaf.load();
+    L.has_refined = refined.load();
     const bool same_list = incremental && L.h_active == old_active[l] && (L.d_active || n == 0);
     if (!same_list && n) {
       std::vector<int32_t> a0(n);
