@@ -28,17 +28,35 @@ __device__ __forceinline__ int64_t dev_cell_of_fortran(int64_t icell /*1-based*/
   return ncoarse + ig * 8 + ind;
 }
 
-// Fortran uold(ncell,5) -> device layout (and back).
+// Fortran uold(ncell,5) -> device layout. The coarse cells keep their index;
+// oct cell ncoarse + ind*ngridmax + ig in Fortran (ind the child, ig =
+// igrid-1) is device cell ncoarse + ig*8 + ind. The loop runs in device
+// order, so a warp (4 octs x 8 children) writes 256 contiguous device bytes
+// and reads one 32-byte sector in each of the 8 Fortran rows; the nvar values
+// of a cell are in flight together.
 static __global__ void permute_f2d_kernel(const double* __restrict__ f, double* __restrict__ d, int64_t ncell,
-                                   int32_t ncoarse, int32_t ngridmax, int nvar) {
-  const int64_t n = ncell * nvar;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = i / ncell, icell = i % ncell + 1;
-    d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)] = f[i];
+                                          int32_t ncoarse, int32_t ngridmax, int nvar) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell; i += stride) {
+    int64_t fi = i;
+    if (i >= ncoarse) {
+      const int64_t r = i - ncoarse;
+      fi = ncoarse + (r & 7) * (int64_t)ngridmax + (r >> 3);
+    }
+    double x[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+      if (v < nvar) x[v] = f[v * ncell + fi];
+#pragma unroll
+    for (int v = 0; v < 5; v++)
+      if (v < nvar) d[v * ncell + i] = x[v];
   }
 }
+// Device layout -> Fortran: Fortran order (whole Fortran rows written), one
+// value per iteration; the device reads of a warp hit 32 octs' cells of one
+// child, and the other children's warps find those sectors in L2.
 static __global__ void permute_d2f_kernel(const double* __restrict__ d, double* __restrict__ f, int64_t ncell,
-                                   int32_t ncoarse, int32_t ngridmax, int nvar) {
+                                          int32_t ncoarse, int32_t ngridmax, int nvar) {
   const int64_t n = ncell * nvar;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t v = i / ncell, icell = i % ncell + 1;
@@ -186,11 +204,14 @@ static __global__ void copy_octs_kernel(const double* __restrict__ src, double* 
                                  const int32_t* __restrict__ active, int32_t noct, int64_t ncell,
                                  int32_t ncoarse, const double* __restrict__ gate) {
   RB_GATE(gate);
-  const int64_t n = (int64_t)noct * 8 * 5;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+  const int64_t n = (int64_t)noct * 8;  // one cell per iteration, its 5 variables in flight together
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t dc = ncoarse + (int64_t)active[r >> 3] * 8 + (r & 7);
-    dst[v * ncell + dc] = src[v * ncell + dc];
+    double u[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) u[v] = src[v * ncell + dc];
+#pragma unroll
+    for (int v = 0; v < 5; v++) dst[v * ncell + dc] = u[v];
   }
 }
 
@@ -816,26 +837,34 @@ static __global__ void oct_to_dense_kernel(const double* __restrict__ u, double*
                                     const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
                                     int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
                                     int64_t vstr) {
-  const int64_t n = (int64_t)noct * 8 * 5;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t o = r >> 3;
     const int ch = (int)(r & 7);
     const int64_t di = cbase[o] + (ch & 1) + (int64_t)nx * (((ch >> 1) & 1) + (int64_t)ny * (ch >> 2));
-    d[v * vstr + di] = u[v * ncell + oct0 + (int64_t)active[o] * 8 + ch];
+    const int64_t oc = oct0 + (int64_t)active[o] * 8 + ch;
+    double x[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) x[v] = u[v * ncell + oc];
+#pragma unroll
+    for (int v = 0; v < 5; v++) d[v * vstr + di] = x[v];
   }
 }
 static __global__ void dense_to_oct_kernel(const double* __restrict__ d, double* __restrict__ u,
                                     const int32_t* __restrict__ active, const int64_t* __restrict__ cbase,
                                     int32_t noct, int64_t ncell, int32_t oct0, int32_t nx, int32_t ny,
                                     int64_t vstr) {
-  const int64_t n = (int64_t)noct * 8 * 5;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t v = i / ((int64_t)noct * 8), r = i % ((int64_t)noct * 8);
+  const int64_t n = (int64_t)noct * 8;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t o = r >> 3;
     const int ch = (int)(r & 7);
     const int64_t di = cbase[o] + (ch & 1) + (int64_t)nx * (((ch >> 1) & 1) + (int64_t)ny * (ch >> 2));
-    u[v * ncell + oct0 + (int64_t)active[o] * 8 + ch] = d[v * vstr + di];
+    const int64_t oc = oct0 + (int64_t)active[o] * 8 + ch;
+    double x[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) x[v] = d[v * vstr + di];
+#pragma unroll
+    for (int v = 0; v < 5; v++) u[v * ncell + oc] = x[v];
   }
 }
 

@@ -61,6 +61,9 @@ int check_params(const rb_hydro_params* hp, const rb_mesh_params* mp) {
       mp->levelmin > mp->nlevelmax)
     return fail(RB_ERR_INVALID, "bad ngridmax/levelmin/nlevelmax");
   if (mp->nvector < 1) return fail(RB_ERR_INVALID, "nvector must be positive");
+  // device cell indices are held in 32 bits in the level tables and kernels
+  if ((int64_t)mp->ncoarse + 8 * (int64_t)mp->ngridmax >= (int64_t)INT32_MAX)
+    return fail(RB_ERR_INVALID, "ncoarse + 8*ngridmax must stay below 2^31 cells");
   if (!(mp->boxlen > 0.0)) return fail(RB_ERR_INVALID, "boxlen must be positive");
   if (mp->nx_loc < 0 || mp->nx_loc > mp->nx)
     return fail(RB_ERR_INVALID, "nx_loc=%d must lie in 0..nx (0: nx)", mp->nx_loc);
@@ -1066,7 +1069,7 @@ int check_level(rb_context* c, int l) {
 int set_unew_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
-  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
       c->d_uold, c->d_unew, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
   if (c->hp.pressure_fix) {
@@ -1106,7 +1109,7 @@ int set_uold_impl(rb_context* c, int l) {
   Level& L = c->lv[l];
   if (!L.noct) return RB_OK;
   if (c->hp.pressure_fix) RB_TRY(pdv_impl(c, l, nullptr, c->dt_godunov[l]));
-  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+  rb::copy_octs_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
       c->d_unew, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->gate);
   RB_CUDA(cudaGetLastError());
   if (c->hp.pressure_fix) RB_TRY(pf_fix_impl(c, l, nullptr, c->dt_godunov[l], 0));
@@ -1168,7 +1171,7 @@ int sync_oct(rb_context* c) {
   if (!c->oct_stale) return RB_OK;
   Level& L = c->lv[c->finest];
   const int64_t vstr = (int64_t)c->dnx * c->dny * c->dnz;
-  rb::dense_to_oct_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+  rb::dense_to_oct_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
       c->d_dense[c->dense_cur], c->d_uold, L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
       c->dny, vstr);
   RB_CUDA(cudaGetLastError());
@@ -1707,7 +1710,7 @@ int rb_make_boundary_hydro(rb_context* c, int l) {
 static int upload_impl(rb_context* c, const double* h, double* d) {
   if (!c || !h) return fail(RB_ERR_INVALID, "null argument");
   RB_CUDA(cudaMemcpyAsync(c->d_stage, h, (size_t)c->ncell * 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  rb::permute_f2d_kernel<<<grid_for(c->ncell * 5, 256), 256, 0, c->stream>>>(c->d_stage, d, c->ncell, c->mp.ncoarse,
+  rb::permute_f2d_kernel<<<grid_for(c->ncell, 256), 256, 0, c->stream>>>(c->d_stage, d, c->ncell, c->mp.ncoarse,
                                                                             c->mp.ngridmax, 5);
   RB_CUDA(cudaGetLastError());
   RB_CUDA(cudaStreamSynchronize(c->stream));
@@ -2225,7 +2228,7 @@ static int uniform_run_dense(rb_context* c, int nsteps, int use_graph, double* t
   if (t_io) c->t = *t_io;
   if (!c->dense_valid) {
     RB_TRY(sync_oct(c));
-    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
         c->d_uold, c->d_dense[c->dense_cur], L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
         c->dny, vstr);
     RB_CUDA(cudaGetLastError());
@@ -2347,7 +2350,7 @@ int rb_autotune_uniform(rb_context* c, int* shape_out, int* hz_out, float* ms_ou
   if (!c->dense_valid) {
     RB_TRY(sync_oct(c));
     const int64_t vstr = (int64_t)c->dnx * c->dny * c->dnz;
-    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 40, 256), 256, 0, c->stream>>>(
+    rb::oct_to_dense_kernel<<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
         c->d_uold, c->d_dense[c->dense_cur], L.d_active, c->d_cbase, L.noct, c->ncell, c->mp.ncoarse, c->dnx,
         c->dny, vstr);
     RB_CUDA(cudaGetLastError());
