@@ -43,3 +43,25 @@ def test_flags_grow_the_tree_and_reuse_igrids():
     used = np.concatenate([new.active[l] for l in range(1, 6) if new.noct(l)])
     assert len(np.unique(used)) == len(used) and used.max() <= new.ngridmax
     _check_nesting(new)
+
+
+def test_sorted_set_helpers_match_numpy():
+    """The sort-based set helpers of the tree builder (the hashing np.unique is
+    slow on large int64 key arrays) give numpy's answers."""
+    rng = np.random.default_rng(11)
+    for n in (0, 1, 5, 1000, 50000):
+        a = rng.integers(0, 4000, n)
+        b = rng.integers(0, 4000, max(n // 3, 1))
+        np.testing.assert_array_equal(mesh._unique(a), np.unique(a))
+        np.testing.assert_array_equal(mesh._isin(a, b), np.isin(a, b))
+    assert mesh._isin(np.arange(5), np.zeros(0, np.int64)).sum() == 0
+
+
+def test_separable_dilation_equals_the_27_point_neighbourhood():
+    """Three one-axis dilations give the periodic 26-neighbourhood of a cell
+    set, as the 27-point expansion does."""
+    rng = np.random.default_rng(5)
+    for n in (4, 16, 64):
+        cells = rng.integers(0, n, (200, 3))
+        want = np.unique(mesh._keys(mesh._neighbourhood(cells) % n, n))
+        np.testing.assert_array_equal(mesh._dilated_keys(cells, n), want)
