@@ -4,9 +4,12 @@ TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
 and ``bench.py``'s CPU-baseline / reference arm, as the checker. The product
 package ``ramses_b200`` never imports it.
 
-Parity status: restatement of the reference Fortran, pinned physically to the
-reference's Sod known-answer table; bit-level parity with the Fortran binary
-is unpinned (no Fortran compiler in the build image).
+Parity status: restatement of the reference Fortran. Its NDIM=1 companion
+(``ramses_oracle_1d.c``, ``run_1d``), which shares the Riemann solvers,
+reproduces the reference's own 1D AMR Sod regression checksums
+(tests/hydro/sod-tube/sod-tube-ref.dat); the 3D restatement is also pinned
+physically to the reference's Sod known-answer table. 3D bit-level parity
+with the Fortran binary is unpinned (no Fortran compiler in the build image).
 """
 from __future__ import annotations
 
@@ -22,6 +25,8 @@ BUILD = HERE / "_build"
 LIB_PATH = BUILD / "liboracle.so"
 SRC = HERE / "ramses_oracle.c"
 HDR = HERE / "ramses_oracle.h"
+SOURCES = [SRC, HERE / "ramses_oracle_1d.c"]
+HEADERS = [HDR, HERE / "ramses_oracle_1d.h"]
 CFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c11"]
 
 
@@ -29,10 +34,10 @@ def build(force: bool = False) -> Path:
     """Compile the oracle with gcc (no FMA contraction)."""
     BUILD.mkdir(exist_ok=True)
     if (not force and LIB_PATH.exists()
-            and LIB_PATH.stat().st_mtime >= max(SRC.stat().st_mtime, HDR.stat().st_mtime)):
+            and LIB_PATH.stat().st_mtime >= max(f.stat().st_mtime for f in SOURCES + HEADERS)):
         return LIB_PATH
     tmp = LIB_PATH.with_suffix(".so.tmp%d" % os.getpid())
-    subprocess.run(["gcc", *CFLAGS, str(SRC), "-o", str(tmp), "-lm"], check=True)
+    subprocess.run(["gcc", *CFLAGS, *map(str, SOURCES), "-o", str(tmp), "-lm"], check=True)
     os.replace(tmp, LIB_PATH)
     return LIB_PATH
 
@@ -87,6 +92,80 @@ class OrcMesh(ctypes.Structure):
                 ("boundary_type", _P32), ("bound_off", _P64), ("bound_igrid", _P32)]
 
 
+_NREG = 8
+
+
+class Orc1dParams(ctypes.Structure):
+    """orc1d_params (ramses_oracle_1d.h): the namelist of a 1D run."""
+    _fields_ = [("hydro", OrcParams), ("refine", OrcRefine),
+                ("levelmin", ctypes.c_int32), ("nlevelmax", ctypes.c_int32),
+                ("ngridmax", ctypes.c_int32), ("nexpand", ctypes.c_int32),
+                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1)),
+                ("boxlen", ctypes.c_double), ("tout", ctypes.c_double),
+                ("nboundary", ctypes.c_int32), ("bound_side", ctypes.c_int32 * 2),
+                ("bound_type", ctypes.c_int32 * 2), ("nregion", ctypes.c_int32),
+                ("x_center", ctypes.c_double * _NREG), ("length_x", ctypes.c_double * _NREG),
+                ("exp_region", ctypes.c_double * _NREG), ("d_region", ctypes.c_double * _NREG),
+                ("u_region", ctypes.c_double * _NREG), ("p_region", ctypes.c_double * _NREG),
+                ("max_coarse_steps", ctypes.c_int64)]
+
+
+class Orc1dResult(ctypes.Structure):
+    _fields_ = [("capacity", ctypes.c_int32), ("init_only", ctypes.c_int32),
+                ("x", _PD), ("level", _P32), ("u", _PD), ("ncell", ctypes.c_int32),
+                ("taken", ctypes.c_int32), ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
+                ("nstep_coarse", ctypes.c_int64), ("noct", ctypes.c_int32 * (MAXLEVEL + 1)),
+                ("message", ctypes.c_char * 160)]
+
+
+def run_1d(hp, refine, *, levelmin, nlevelmax, ngridmax, tout, regions, nsubcycle=None,
+           nexpand=1, boxlen=1.0, boundaries=(), max_coarse_steps=1_000_000, init_only=False,
+           capacity=1 << 16):
+    """A whole 1D (NDIM=1) RAMSES hydro run in the oracle (ramses_oracle_1d.c)
+    up to the snapshot of the first coarse step starting at t >= tout.
+
+    ``refine``: (err_grad_d, err_grad_p, err_grad_u), -1 for off (floors 1e-10);
+    ``regions``: [(x_center, length_x, d, u, p[, exp_region])] 'square' regions;
+    ``boundaries``: [(side, bound_type)] with side -1 (x min) / +1 (x max) and
+    bound_type 1 (reflexive) / 2 (outflow); empty: periodic;
+    ``nsubcycle``: per level from 1 (default 2 everywhere).
+    Returns the leaf cells (x, level, rho, rho u, E) and the run's clock."""
+    p = Orc1dParams()
+    p.hydro = params_struct(hp)
+    d, pr, uu = refine
+    p.refine = OrcRefine(d, pr, uu, 1e-10, 1e-10, 1e-10)
+    p.levelmin, p.nlevelmax, p.ngridmax, p.nexpand = levelmin, nlevelmax, ngridmax, nexpand
+    ns = list(nsubcycle or [])
+    for lvl in range(1, MAXLEVEL + 1):
+        p.nsubcycle[lvl] = ns[lvl - 1] if lvl - 1 < len(ns) else 2
+    p.boxlen, p.tout = boxlen, tout
+    p.nboundary = len(boundaries)
+    for i, (side, bt) in enumerate(boundaries):
+        p.bound_side[i], p.bound_type[i] = side, bt
+    if len(regions) > _NREG:
+        raise ValueError("at most %d regions" % _NREG)
+    p.nregion = len(regions)
+    for k, reg in enumerate(regions):
+        p.x_center[k], p.length_x[k], p.d_region[k], p.u_region[k], p.p_region[k] = reg[:5]
+        p.exp_region[k] = reg[5] if len(reg) > 5 else 2.0
+    p.max_coarse_steps = max_coarse_steps
+    x = np.zeros(capacity)
+    lv = np.zeros(capacity, np.int32)
+    u = np.zeros((capacity, 3))
+    r = Orc1dResult()
+    r.capacity, r.init_only = capacity, 1 if init_only else 0
+    r.x, r.level, r.u = _ptr(x, _PD), _ptr(lv, _P32), _ptr(u, _PD)
+    rc = lib().orc1d_run(ctypes.byref(p), ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError("orc1d_run failed (%d): %s" % (rc, r.message.decode()))
+    n = r.ncell
+    if n > capacity:
+        raise RuntimeError("more leaf cells than capacity")
+    return {"x": x[:n].copy(), "level": lv[:n].copy(), "u": u[:n].copy(), "t": r.t, "taken": bool(r.taken),
+            "nstep": r.nstep, "nstep_coarse": r.nstep_coarse,
+            "noct": [r.noct[lvl] for lvl in range(1, nlevelmax + 1)]}
+
+
 def _declare(L):
     P = ctypes.POINTER(OrcParams)
     M = ctypes.POINTER(OrcMesh)
@@ -107,6 +186,8 @@ def _declare(L):
     L.orc_dense_step.argtypes = [P, _PD, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, _PD]
     L.orc_hydro_flag.restype = ctypes.c_int64
+    L.orc_riemann_face.argtypes = [P, _PD, _PD, _PD]
+    L.orc1d_run.argtypes = [ctypes.POINTER(Orc1dParams), ctypes.POINTER(Orc1dResult)]
 
 
 def params_struct(hp) -> OrcParams:

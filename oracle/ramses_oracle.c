@@ -4,8 +4,11 @@
  * parity checker for the CUDA library and the timed CPU baseline; the
  * product library never links or calls it.
  *
- * Parity status: line-by-line restatement of the cited Fortran, pinned
- * physically against the reference's Sod known-answer table; bit-level
+ * Parity status: line-by-line restatement of the cited Fortran. Its Riemann
+ * solvers, driven by the NDIM=1 restatement of a whole AMR run
+ * (ramses_oracle_1d.c), reproduce the reference's 1D Sod regression
+ * checksums (tests/hydro/sod-tube/sod-tube-ref.dat); it is also pinned
+ * physically against the reference's Sod known-answer table. 3D bit-level
  * parity with the Fortran binary is unpinned (no Fortran compiler here).
  *
  * Every expression keeps the Fortran evaluation order (left-to-right for
@@ -485,6 +488,26 @@ static void riemann_hllc(const orc_params *p, const double *ql, const double *qr
     else fg[n] = ro * uo * qr[n];
   }
   fg[5] = uo * eo;
+}
+
+/* One Riemann problem of cmpflxm (umuscl.f90:791-803) in the face frame
+ * (rho, u_n, p, u_t1, u_t2), the solver chosen by p->riemann; fg[0..2] are
+ * the mass, normal-momentum and energy fluxes. The NDIM=1 restatement
+ * (ramses_oracle_1d.c) calls the same solvers with zero transverse
+ * velocities: every term they contribute adds an exact zero, so the three
+ * fluxes are those of the reference's nvar=3 build. */
+static void riemann_acoustic(const orc_params *p, const double *ql, const double *qr, double *fg);
+static void riemann_exact(const orc_params *p, const double *ql, const double *qr, double *fg);
+int orc_riemann_face(const orc_params *p, const double *ql, const double *qr, double *fg) {
+  double l[5] = {ql[0], ql[1], ql[2], ql[3], ql[4]}, r[5] = {qr[0], qr[1], qr[2], qr[3], qr[4]}, g[6];
+  if (p->riemann == ORC_RIEMANN_LLF) riemann_llf(p, l, r, g);
+  else if (p->riemann == ORC_RIEMANN_HLLC) riemann_hllc(p, l, r, g);
+  else if (p->riemann == ORC_RIEMANN_HLL) riemann_hll(p, l, r, g);
+  else if (p->riemann == ORC_RIEMANN_ACOUSTIC) riemann_acoustic(p, l, r, g);
+  else if (p->riemann == ORC_RIEMANN_EXACT) riemann_exact(p, l, r, g);
+  else return -1;
+  for (int n = 0; n < 6; n++) fg[n] = g[n];
+  return 0;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -6,10 +6,13 @@
  *
  * Parity status: the reference is Fortran and no Fortran compiler exists in
  * the build image, so this restatement could not be compiled against the
- * reference binary. It is pinned (a) line by line to the cited Fortran and
- * (b) physically against the reference's own Sod known-answer file
- * (tests/hydro/sod-tube/sod-tube-ana.dat); 3D bit-level parity with the
- * Fortran binary is unpinned.
+ * reference binary. It is pinned (a) line by line to the cited Fortran,
+ * (b) through its NDIM=1 companion (ramses_oracle_1d.c, which shares the
+ * Riemann solvers) to the reference's own regression checksums of the 1D
+ * AMR Sod run (tests/hydro/sod-tube/sod-tube-ref.dat: same tree, density and
+ * pressure sums to the last digit, velocity within 3.3e-16), and (c)
+ * physically to the reference's Sod known-answer file (sod-tube-ana.dat).
+ * 3D bit-level parity with the Fortran binary is unpinned.
  *
  * Array conventions follow the Fortran ones exactly (column-major, 1-based
  * cell / grid indices stored as int32):
@@ -125,6 +128,11 @@ int64_t orc_hydro_flag(const orc_params *p, const orc_refine *r, const orc_mesh 
  * outflow). u is advanced in place; dt_out receives the step's dt. */
 int orc_dense_step(const orc_params *p, double *u, int nx, int ny, int nz, double dx, double dt_max,
                    int bc_outflow, int nvector, double *dt_out);
+
+/* One Riemann problem of cmpflxm (umuscl.f90:791-803) in the face frame
+ * (rho, u_n, p, u_t1, u_t2) with the solver p->riemann: fg[0..2] mass,
+ * normal-momentum and energy fluxes (fg has room for 6). */
+int orc_riemann_face(const orc_params *p, const double *ql, const double *qr, double *fg);
 
 /* interpol_hydro.f90:268-444 for nn father stencils:
  * u1(nn,0:6,5) -> u2(nn,1:8,5), column-major with leading dim nn. */
