@@ -4,10 +4,11 @@ TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
 and ``bench.py``'s CPU-baseline / reference arm, as the checker. The product
 package ``ramses_b200`` never imports it.
 
-Parity status: restatement of the reference Fortran. Its NDIM=1 companion
-(``ramses_oracle_1d.c``, ``run_1d``), which shares the Riemann solvers,
-reproduces the reference's own 1D AMR Sod regression checksums
-(tests/hydro/sod-tube/sod-tube-ref.dat); the 3D restatement is also pinned
+Parity status: restatement of the reference Fortran. Its NDIM=1/2 companion
+(``ramses_oracle_amr.c``, ``run_amr``), which shares the Riemann solvers,
+reproduces the reference's own regression checksums of the 1D AMR Sod run
+and the 2D AMR implosion (tests/hydro/sod-tube, tests/hydro/implosion); the
+3D restatement is also pinned
 physically to the reference's Sod known-answer table. 3D bit-level parity
 with the Fortran binary is unpinned (no Fortran compiler in the build image).
 """
@@ -25,8 +26,8 @@ BUILD = HERE / "_build"
 LIB_PATH = BUILD / "liboracle.so"
 SRC = HERE / "ramses_oracle.c"
 HDR = HERE / "ramses_oracle.h"
-SOURCES = [SRC, HERE / "ramses_oracle_1d.c"]
-HEADERS = [HDR, HERE / "ramses_oracle_1d.h"]
+SOURCES = [SRC, HERE / "ramses_oracle_amr.c"]
+HEADERS = [HDR, HERE / "ramses_oracle_amr.h"]
 CFLAGS = ["-O2", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared", "-std=c11"]
 
 
@@ -93,75 +94,82 @@ class OrcMesh(ctypes.Structure):
 
 
 _NREG = 8
+_NBND = 4
 
 
-class Orc1dParams(ctypes.Structure):
-    """orc1d_params (ramses_oracle_1d.h): the namelist of a 1D run."""
-    _fields_ = [("hydro", OrcParams), ("refine", OrcRefine),
-                ("levelmin", ctypes.c_int32), ("nlevelmax", ctypes.c_int32),
-                ("ngridmax", ctypes.c_int32), ("nexpand", ctypes.c_int32),
-                ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1)),
-                ("boxlen", ctypes.c_double), ("tout", ctypes.c_double),
-                ("nboundary", ctypes.c_int32), ("bound_side", ctypes.c_int32 * 2),
-                ("bound_type", ctypes.c_int32 * 2), ("nregion", ctypes.c_int32),
-                ("x_center", ctypes.c_double * _NREG), ("length_x", ctypes.c_double * _NREG),
+class OrcAmrParams(ctypes.Structure):
+    """orc_amr_params (ramses_oracle_amr.h): the namelist of a 1D or 2D run."""
+    _fields_ = [("hydro", OrcParams), ("refine", OrcRefine), ("ndim", ctypes.c_int32),
+                ("levelmin", ctypes.c_int32), ("nlevelmax", ctypes.c_int32), ("ngridmax", ctypes.c_int32),
+                ("nexpand", ctypes.c_int32 * (MAXLEVEL + 1)), ("nsubcycle", ctypes.c_int32 * (MAXLEVEL + 1)),
+                ("boxlen", ctypes.c_double), ("tout", ctypes.c_double), ("nboundary", ctypes.c_int32),
+                ("ibound_min", ctypes.c_int32 * _NBND), ("ibound_max", ctypes.c_int32 * _NBND),
+                ("jbound_min", ctypes.c_int32 * _NBND), ("jbound_max", ctypes.c_int32 * _NBND),
+                ("bound_type", ctypes.c_int32 * _NBND), ("nregion", ctypes.c_int32),
+                ("x_center", ctypes.c_double * _NREG), ("y_center", ctypes.c_double * _NREG),
+                ("length_x", ctypes.c_double * _NREG), ("length_y", ctypes.c_double * _NREG),
                 ("exp_region", ctypes.c_double * _NREG), ("d_region", ctypes.c_double * _NREG),
-                ("u_region", ctypes.c_double * _NREG), ("p_region", ctypes.c_double * _NREG),
-                ("max_coarse_steps", ctypes.c_int64)]
+                ("u_region", ctypes.c_double * _NREG), ("v_region", ctypes.c_double * _NREG),
+                ("p_region", ctypes.c_double * _NREG), ("max_coarse_steps", ctypes.c_int64)]
 
 
-class Orc1dResult(ctypes.Structure):
+class OrcAmrResult(ctypes.Structure):
     _fields_ = [("capacity", ctypes.c_int32), ("init_only", ctypes.c_int32),
-                ("x", _PD), ("level", _P32), ("u", _PD), ("ncell", ctypes.c_int32),
+                ("pos", _PD), ("level", _P32), ("u", _PD), ("ncell", ctypes.c_int32),
                 ("taken", ctypes.c_int32), ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
                 ("nstep_coarse", ctypes.c_int64), ("noct", ctypes.c_int32 * (MAXLEVEL + 1)),
                 ("message", ctypes.c_char * 160)]
 
 
-def run_1d(hp, refine, *, levelmin, nlevelmax, ngridmax, tout, regions, nsubcycle=None,
-           nexpand=1, boxlen=1.0, boundaries=(), max_coarse_steps=1_000_000, init_only=False,
-           capacity=1 << 16):
-    """A whole 1D (NDIM=1) RAMSES hydro run in the oracle (ramses_oracle_1d.c)
+def run_amr(hp, refine, *, ndim, levelmin, nlevelmax, ngridmax, tout, regions, nsubcycle, nexpand,
+            boxlen=1.0, boundaries=(), max_coarse_steps=10_000_000, init_only=False, capacity=1 << 18):
+    """A whole 1D or 2D RAMSES hydro run in the oracle (ramses_oracle_amr.c)
     up to the snapshot of the first coarse step starting at t >= tout.
 
     ``refine``: (err_grad_d, err_grad_p, err_grad_u), -1 for off (floors 1e-10);
-    ``regions``: [(x_center, length_x, d, u, p[, exp_region])] 'square' regions;
-    ``boundaries``: [(side, bound_type)] with side -1 (x min) / +1 (x max) and
-    bound_type 1 (reflexive) / 2 (outflow); empty: periodic;
-    ``nsubcycle``: per level from 1 (default 2 everywhere).
-    Returns the leaf cells (x, level, rho, rho u, E) and the run's clock."""
-    p = Orc1dParams()
+    ``regions``: 'square' regions as dicts with x_center, length_x, d, p and
+    optionally y_center, length_y, u, v, exp_region (default 2);
+    ``boundaries``: (ibound_min, ibound_max, jbound_min, jbound_max,
+    bound_type) per region as in the namelist, bound_type 1 reflexive or 2
+    outflow; empty: periodic;
+    ``nsubcycle``, ``nexpand``: per level from level 1, as RAMSES holds them
+    after read_params (entry k of the namelist applies to levelmin + k - 1).
+    Returns the leaf cells (pos, level, conservative u) and the run's clock."""
+    p = OrcAmrParams()
     p.hydro = params_struct(hp)
     d, pr, uu = refine
     p.refine = OrcRefine(d, pr, uu, 1e-10, 1e-10, 1e-10)
-    p.levelmin, p.nlevelmax, p.ngridmax, p.nexpand = levelmin, nlevelmax, ngridmax, nexpand
-    ns = list(nsubcycle or [])
+    p.ndim, p.levelmin, p.nlevelmax, p.ngridmax = ndim, levelmin, nlevelmax, ngridmax
     for lvl in range(1, MAXLEVEL + 1):
-        p.nsubcycle[lvl] = ns[lvl - 1] if lvl - 1 < len(ns) else 2
+        p.nsubcycle[lvl] = nsubcycle[lvl - 1] if lvl - 1 < len(nsubcycle) else 2
+        p.nexpand[lvl] = nexpand[lvl - 1] if lvl - 1 < len(nexpand) else 1
     p.boxlen, p.tout = boxlen, tout
+    if len(boundaries) > _NBND or len(regions) > _NREG:
+        raise ValueError("too many boundary or initial-condition regions")
     p.nboundary = len(boundaries)
-    for i, (side, bt) in enumerate(boundaries):
-        p.bound_side[i], p.bound_type[i] = side, bt
-    if len(regions) > _NREG:
-        raise ValueError("at most %d regions" % _NREG)
+    for i, (imin, imax, jmin, jmax, bt) in enumerate(boundaries):
+        p.ibound_min[i], p.ibound_max[i], p.jbound_min[i], p.jbound_max[i], p.bound_type[i] = imin, imax, jmin, jmax, bt
     p.nregion = len(regions)
     for k, reg in enumerate(regions):
-        p.x_center[k], p.length_x[k], p.d_region[k], p.u_region[k], p.p_region[k] = reg[:5]
-        p.exp_region[k] = reg[5] if len(reg) > 5 else 2.0
+        p.x_center[k], p.length_x[k] = reg["x_center"], reg["length_x"]
+        p.y_center[k], p.length_y[k] = reg.get("y_center", 0.0), reg.get("length_y", 1.0)
+        p.exp_region[k] = reg.get("exp_region", 2.0)
+        p.d_region[k], p.p_region[k] = reg["d"], reg["p"]
+        p.u_region[k], p.v_region[k] = reg.get("u", 0.0), reg.get("v", 0.0)
     p.max_coarse_steps = max_coarse_steps
-    x = np.zeros(capacity)
+    pos = np.zeros((capacity, ndim))
     lv = np.zeros(capacity, np.int32)
-    u = np.zeros((capacity, 3))
-    r = Orc1dResult()
+    u = np.zeros((capacity, ndim + 2))
+    r = OrcAmrResult()
     r.capacity, r.init_only = capacity, 1 if init_only else 0
-    r.x, r.level, r.u = _ptr(x, _PD), _ptr(lv, _P32), _ptr(u, _PD)
-    rc = lib().orc1d_run(ctypes.byref(p), ctypes.byref(r))
+    r.pos, r.level, r.u = _ptr(pos, _PD), _ptr(lv, _P32), _ptr(u, _PD)
+    rc = lib().orc_amr_run(ctypes.byref(p), ctypes.byref(r))
     if rc != 0:
-        raise RuntimeError("orc1d_run failed (%d): %s" % (rc, r.message.decode()))
+        raise RuntimeError("orc_amr_run failed (%d): %s" % (rc, r.message.decode()))
     n = r.ncell
     if n > capacity:
         raise RuntimeError("more leaf cells than capacity")
-    return {"x": x[:n].copy(), "level": lv[:n].copy(), "u": u[:n].copy(), "t": r.t, "taken": bool(r.taken),
+    return {"pos": pos[:n].copy(), "level": lv[:n].copy(), "u": u[:n].copy(), "t": r.t, "taken": bool(r.taken),
             "nstep": r.nstep, "nstep_coarse": r.nstep_coarse,
             "noct": [r.noct[lvl] for lvl in range(1, nlevelmax + 1)]}
 
@@ -187,7 +195,7 @@ def _declare(L):
                                  ctypes.c_double, ctypes.c_int, ctypes.c_int, _PD]
     L.orc_hydro_flag.restype = ctypes.c_int64
     L.orc_riemann_face.argtypes = [P, _PD, _PD, _PD]
-    L.orc1d_run.argtypes = [ctypes.POINTER(Orc1dParams), ctypes.POINTER(Orc1dResult)]
+    L.orc_amr_run.argtypes = [ctypes.POINTER(OrcAmrParams), ctypes.POINTER(OrcAmrResult)]
 
 
 def params_struct(hp) -> OrcParams:

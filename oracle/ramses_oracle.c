@@ -5,9 +5,9 @@
  * product library never links or calls it.
  *
  * Parity status: line-by-line restatement of the cited Fortran. Its Riemann
- * solvers, driven by the NDIM=1 restatement of a whole AMR run
- * (ramses_oracle_1d.c), reproduce the reference's 1D Sod regression
- * checksums (tests/hydro/sod-tube/sod-tube-ref.dat); it is also pinned
+ * solvers, driven by the NDIM=1/2 restatement of a whole AMR run
+ * (ramses_oracle_amr.c), reproduce the reference's 1D Sod and 2D implosion
+ * regression checksums (tests/hydro/sod-tube, tests/hydro/implosion); it is also pinned
  * physically against the reference's Sod known-answer table. 3D bit-level
  * parity with the Fortran binary is unpinned (no Fortran compiler here).
  *
@@ -492,10 +492,11 @@ static void riemann_hllc(const orc_params *p, const double *ql, const double *qr
 
 /* One Riemann problem of cmpflxm (umuscl.f90:791-803) in the face frame
  * (rho, u_n, p, u_t1, u_t2), the solver chosen by p->riemann; fg[0..2] are
- * the mass, normal-momentum and energy fluxes. The NDIM=1 restatement
- * (ramses_oracle_1d.c) calls the same solvers with zero transverse
- * velocities: every term they contribute adds an exact zero, so the three
- * fluxes are those of the reference's nvar=3 build. */
+ * the mass, normal-momentum and energy fluxes, fg[3] the first transverse
+ * momentum flux. The NDIM=1/2 restatement (ramses_oracle_amr.c) calls the
+ * same solvers with the transverse velocities its build lacks set to zero:
+ * every term they contribute adds an exact zero, so the fluxes are those of
+ * the reference's nvar=3 and nvar=4 builds. */
 static void riemann_acoustic(const orc_params *p, const double *ql, const double *qr, double *fg);
 static void riemann_exact(const orc_params *p, const double *ql, const double *qr, double *fg);
 int orc_riemann_face(const orc_params *p, const double *ql, const double *qr, double *fg) {

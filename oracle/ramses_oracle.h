@@ -7,10 +7,10 @@
  * Parity status: the reference is Fortran and no Fortran compiler exists in
  * the build image, so this restatement could not be compiled against the
  * reference binary. It is pinned (a) line by line to the cited Fortran,
- * (b) through its NDIM=1 companion (ramses_oracle_1d.c, which shares the
- * Riemann solvers) to the reference's own regression checksums of the 1D
- * AMR Sod run (tests/hydro/sod-tube/sod-tube-ref.dat: same tree, density and
- * pressure sums to the last digit, velocity within 3.3e-16), and (c)
+ * (b) through its NDIM=1/2 companion (ramses_oracle_amr.c, which shares
+ * the Riemann solvers) to the reference's own regression checksums of the
+ * 1D AMR Sod run and the 2D AMR implosion (tests/hydro/sod-tube,
+ * tests/hydro/implosion: same trees, sums within the checker's 3e-13), and (c)
  * physically to the reference's Sod known-answer file (sod-tube-ana.dat).
  * 3D bit-level parity with the Fortran binary is unpinned.
  *
