@@ -110,7 +110,8 @@ class OrcAmrParams(ctypes.Structure):
                 ("length_x", ctypes.c_double * _NREG), ("length_y", ctypes.c_double * _NREG),
                 ("exp_region", ctypes.c_double * _NREG), ("d_region", ctypes.c_double * _NREG),
                 ("u_region", ctypes.c_double * _NREG), ("v_region", ctypes.c_double * _NREG),
-                ("p_region", ctypes.c_double * _NREG), ("max_coarse_steps", ctypes.c_int64)]
+                ("p_region", ctypes.c_double * _NREG), ("max_coarse_steps", ctypes.c_int64),
+                ("dt_force", _PD), ("dt_force_n", ctypes.c_int64)]
 
 
 class OrcAmrResult(ctypes.Structure):
@@ -118,11 +119,12 @@ class OrcAmrResult(ctypes.Structure):
                 ("pos", _PD), ("level", _P32), ("u", _PD), ("ncell", ctypes.c_int32),
                 ("taken", ctypes.c_int32), ("t", ctypes.c_double), ("nstep", ctypes.c_int64),
                 ("nstep_coarse", ctypes.c_int64), ("noct", ctypes.c_int32 * (MAXLEVEL + 1)),
-                ("message", ctypes.c_char * 160)]
+                ("message", ctypes.c_char * 160), ("dt_log", _PD), ("dt_cap", ctypes.c_int32)]
 
 
 def run_amr(hp, refine, *, ndim, levelmin, nlevelmax, ngridmax, tout, regions, nsubcycle, nexpand,
-            boxlen=1.0, boundaries=(), max_coarse_steps=10_000_000, init_only=False, capacity=1 << 18):
+            boxlen=1.0, boundaries=(), max_coarse_steps=10_000_000, init_only=False, capacity=1 << 18,
+            dt_force=None):
     """A whole 1D or 2D RAMSES hydro run in the oracle (ramses_oracle_amr.c)
     up to the snapshot of the first coarse step starting at t >= tout.
 
@@ -133,8 +135,11 @@ def run_amr(hp, refine, *, ndim, levelmin, nlevelmax, ngridmax, tout, regions, n
     bound_type) per region as in the namelist, bound_type 1 reflexive or 2
     outflow; empty: periodic;
     ``nsubcycle``, ``nexpand``: per level from level 1, as RAMSES holds them
-    after read_params (entry k of the namelist applies to levelmin + k - 1).
-    Returns the leaf cells (pos, level, conservative u) and the run's clock."""
+    after read_params (entry k of the namelist applies to levelmin + k - 1);
+    ``dt_force``: for one complete level, the time steps of the coarse steps
+    in place of courant_fine's.
+    Returns the leaf cells (pos, level, conservative u), the run's clock and
+    the dt of every completed coarse step (``dt``)."""
     p = OrcAmrParams()
     p.hydro = params_struct(hp)
     d, pr, uu = refine
@@ -157,12 +162,18 @@ def run_amr(hp, refine, *, ndim, levelmin, nlevelmax, ngridmax, tout, regions, n
         p.d_region[k], p.p_region[k] = reg["d"], reg["p"]
         p.u_region[k], p.v_region[k] = reg.get("u", 0.0), reg.get("v", 0.0)
     p.max_coarse_steps = max_coarse_steps
+    if dt_force is not None:
+        dtf = np.ascontiguousarray(dt_force, dtype=np.float64)
+        p.dt_force, p.dt_force_n = _ptr(dtf, _PD), len(dtf)
     pos = np.zeros((capacity, ndim))
     lv = np.zeros(capacity, np.int32)
     u = np.zeros((capacity, ndim + 2))
     r = OrcAmrResult()
     r.capacity, r.init_only = capacity, 1 if init_only else 0
     r.pos, r.level, r.u = _ptr(pos, _PD), _ptr(lv, _P32), _ptr(u, _PD)
+    ncap = int(min(max_coarse_steps, 1 << 20))
+    dts = np.full(ncap, np.nan)
+    r.dt_log, r.dt_cap = _ptr(dts, _PD), ncap
     rc = lib().orc_amr_run(ctypes.byref(p), ctypes.byref(r))
     if rc != 0:
         raise RuntimeError("orc_amr_run failed (%d): %s" % (rc, r.message.decode()))
@@ -171,7 +182,8 @@ def run_amr(hp, refine, *, ndim, levelmin, nlevelmax, ngridmax, tout, regions, n
         raise RuntimeError("more leaf cells than capacity")
     return {"pos": pos[:n].copy(), "level": lv[:n].copy(), "u": u[:n].copy(), "t": r.t, "taken": bool(r.taken),
             "nstep": r.nstep, "nstep_coarse": r.nstep_coarse,
-            "noct": [r.noct[lvl] for lvl in range(1, nlevelmax + 1)]}
+            "noct": [r.noct[lvl] for lvl in range(1, nlevelmax + 1)],
+            "dt": dts[:min(r.nstep_coarse, ncap)].copy()}
 
 
 def _declare(L):

@@ -1089,6 +1089,8 @@ static int amr_step(tamr *T, int ilevel, int icount, orc_amr_result *res) {
   courant_fine(T, ilevel);
   if (ilevel > T->levelmin)
     T->dtnew[ilevel] = fmind1(T->dtnew[ilevel - 1] / (double)(float)T->P->nsubcycle[ilevel - 1], T->dtnew[ilevel]);
+  if (ilevel == T->levelmin && T->P->dt_force && T->nstep_coarse < T->P->dt_force_n)
+    T->dtnew[ilevel] = T->P->dt_force[T->nstep_coarse];
   set_unew(T, ilevel);
   if (ilevel < T->nlevelmax) {
     if (T->numbl[ilevel + 1] > 0) {
@@ -1106,6 +1108,8 @@ static int amr_step(tamr *T, int ilevel, int icount, orc_amr_result *res) {
   } else {
     if (update_time(T, ilevel)) return 1;
   }
+  if (ilevel == T->levelmin && res->dt_log && T->nstep_coarse < res->dt_cap)
+    res->dt_log[T->nstep_coarse] = T->dtnew[ilevel];
   godunov_fine(T, ilevel);
   if (T->err) return 1;
   set_uold(T, ilevel);
@@ -1192,6 +1196,7 @@ static int setup_boundaries(tamr *T, const orc_amr_params *P) {
 }
 
 int orc_amr_run(const orc_amr_params *P, orc_amr_result *res) {
+  if (P && P->dt_force && P->levelmin != P->nlevelmax) return -1;
   if (!P || !res || (P->ndim != 1 && P->ndim != 2) || P->nlevelmax < 1 || P->nlevelmax > ORC_MAXLEVEL ||
       P->levelmin < 1 || P->levelmin > P->nlevelmax || P->ngridmax < 4 || P->nboundary < 0 ||
       P->nboundary > NB_MAX || P->nregion < 0 || P->nregion > ORC_AMR_MAXREGION)

@@ -36,6 +36,10 @@ typedef struct orc_amr_params {
   double d_region[ORC_AMR_MAXREGION], u_region[ORC_AMR_MAXREGION], v_region[ORC_AMR_MAXREGION];
   double p_region[ORC_AMR_MAXREGION];
   int64_t max_coarse_steps;
+  /* optional, for one complete level (levelmin = nlevelmax): the time step
+   * of coarse step k is dt_force[k] instead of courant_fine's, k < dt_force_n */
+  const double *dt_force;
+  int64_t dt_force_n;
 } orc_amr_params;
 
 typedef struct orc_amr_result {
@@ -50,6 +54,9 @@ typedef struct orc_amr_result {
   int64_t nstep, nstep_coarse;
   int32_t noct[ORC_MAXLEVEL + 1]; /* out: active grids per level */
   char message[160];
+  double *dt_log;    /* in (optional): the dt of each coarse step's levelmin
+                        godunov_fine, dt_cap entries at most */
+  int32_t dt_cap;
 } orc_amr_result;
 
 #ifdef __cplusplus

@@ -114,3 +114,108 @@ def oracle_prolong_born(old, new, u, hp):
         for ind in range(8):
             u[:, new.ncoarse + ind * new.ngridmax + born - 1] = u8[:, ind, :].T
     return u
+
+
+# ---- planar problems: the pinned 1D/2D whole-run oracle against the 3D path ----
+# The reference's pure-hydro regression setups (tests/hydro/sod-tube, 1D, and
+# tests/hydro/implosion, 2D) on one complete level with walls. On data that
+# is constant along the missing axes every transverse term of the 3D scheme
+# adds an exact zero, so a 3D run driven with the same time steps equals the
+# 1D/2D restatement bit for bit.
+PLANAR = {
+    "sod1d": {"ndim": 1, "gamma": 1.4,
+              "regions": [{"x_center": 0.25, "length_x": 0.5, "d": 1.0, "p": 1.0},
+                          {"x_center": 0.75, "length_x": 0.5, "d": 0.125, "p": 0.1}],
+              "boundaries": [(-1, -1, 0, 0, 1), (1, 1, 0, 0, 1)],
+              "bounds3d": ("reflexive", None, None)},
+    "implosion2d": {"ndim": 2, "gamma": 1.4,
+                    "regions": [{"x_center": 0.5, "y_center": 0.5, "length_x": 1.0, "length_y": 1.0,
+                                 "exp_region": 10.0, "d": 1.0, "p": 1.0},
+                                {"x_center": 0.0, "y_center": 0.0, "length_x": 1.0, "length_y": 1.0,
+                                 "exp_region": 1.0, "d": 0.125, "p": 0.4}],
+                    "boundaries": [(-1, -1, 0, 0, 1), (1, 1, 0, 0, 1), (-1, 1, 1, 1, 1), (-1, 1, -1, -1, 1)],
+                    "bounds3d": ("reflexive", "reflexive", None)},
+}
+
+
+PLANAR["sod1d_periodic"] = dict(PLANAR["sod1d"], boundaries=[], bounds3d=(None, None, None))
+PLANAR["implosion2d_periodic"] = dict(PLANAR["implosion2d"], boundaries=[], bounds3d=(None, None, None))
+
+
+def planar_lowdim_run(kind, level, nsteps, dt_force=None):
+    """The 1D/2D oracle on one complete level: (initial leaves, leaves after
+    nsteps coarse steps with the run's own CFL time steps or ``dt_force``,
+    the dts taken)."""
+    import oracle
+    c = PLANAR[kind]
+    hp = HydroParams(gamma=c["gamma"], riemann="hllc", slope_type=2, courant_factor=0.8,
+                     interpol_var=0, interpol_type=2)
+    kw = dict(ndim=c["ndim"], levelmin=level, nlevelmax=level, ngridmax=4 ** level + 64, tout=1e30,
+              regions=c["regions"], boundaries=c["boundaries"], nsubcycle=[1] * level, nexpand=[1] * level)
+    init = oracle.run_amr(hp, (-1.0, -1.0, -1.0), max_coarse_steps=0, **kw)
+    final = oracle.run_amr(hp, (-1.0, -1.0, -1.0), max_coarse_steps=nsteps, dt_force=dt_force, **kw)
+    assert final["nstep_coarse"] == nsteps and len(final["dt"]) == nsteps
+    return hp, init, final
+
+
+def _lowdim_grid(res, ndim, level):
+    """leaf cells -> dense [y][x][v] (ndim = 2) or [x][v] arrays"""
+    n = 2 ** level
+    idx = np.floor(res["pos"] * n).astype(np.int64)
+    if ndim == 1:
+        g = np.zeros((n, 3))
+        g[idx[:, 0]] = res["u"]
+    else:
+        g = np.zeros((n, n, 4))
+        g[idx[:, 1], idx[:, 0]] = res["u"]
+    return g
+
+
+def planar_tree(kind, level, init):
+    """The 3D tree with the kind's walls (periodic along the missing axes)
+    and uold with level ``level`` set from the 1D/2D initial leaves, the
+    coarser levels from the same regions at their cell centres."""
+    c = PLANAR[kind]
+    nd = c["ndim"]
+    tree = mesh.build_tree(level, level, None)
+    if any(c["bounds3d"]):
+        tree = mesh.add_boundaries(tree, c["bounds3d"])
+
+    def prim(x):
+        q = np.zeros((5, len(x)))
+        for r in c["regions"]:
+            xn = 2.0 * np.abs(x[:, 0] - r["x_center"]) / r["length_x"]
+            yn = 2.0 * np.abs(x[:, 1] - r.get("y_center", 0.0)) / r.get("length_y", 1.0) if nd > 1 else 0 * xn
+            en = r.get("exp_region", 2.0)
+            rr = (xn ** en + yn ** en) ** (1.0 / en) if en < 10 else np.maximum(xn, yn)
+            q[0] = np.where(rr < 1.0, r["d"], q[0])
+            q[4] = np.where(rr < 1.0, r["p"], q[4])
+        return q
+    u = ics.fill_all_levels(tree, prim, c["gamma"])
+    g = _lowdim_grid(init, nd, level)
+    idx = tree.cell_index(level)  # [z, y, x]
+    if nd == 1:
+        for v3, v1 in ((0, 0), (1, 1), (4, 2)):
+            u[v3, idx.reshape(-1, idx.shape[2]) - 1] = g[None, :, v1]
+        u[2:4, idx.reshape(-1) - 1] = 0.0
+    else:
+        for v3, v2 in ((0, 0), (1, 1), (2, 2), (4, 3)):
+            u[v3, idx - 1] = np.broadcast_to(g[None, :, :, v2], idx.shape)
+        u[3, idx.reshape(-1) - 1] = 0.0
+    return tree, u
+
+
+def planar_expected(kind, level, tree, final):
+    """(cells, expected uold[5, cells]) of level ``level`` from the 1D/2D
+    leaves, constant along the missing axes, zero momenta along them."""
+    nd = PLANAR[kind]["ndim"]
+    g = _lowdim_grid(final, nd, level)
+    idx = tree.cell_index(level)
+    exp = np.zeros((5,) + idx.shape)
+    if nd == 1:
+        for v3, v1 in ((0, 0), (1, 1), (4, 2)):
+            exp[v3] = g[None, None, :, v1]
+    else:
+        for v3, v2 in ((0, 0), (1, 1), (2, 2), (4, 3)):
+            exp[v3] = g[None, :, :, v2]
+    return idx.reshape(-1), exp.reshape(5, -1)
