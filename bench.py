@@ -677,10 +677,12 @@ def main():
     f64.close()
 
     # ---- end to end through the C ABI with host buffers ------------------
-    # every step: H2D of the full Fortran-layout state from pinned memory,
-    # the coarse step (CFL + fused update), D2H of the result state.
+    # every step: H2D of the step's input rows of the Fortran-layout uold
+    # (the finest level's octs, rb_upload_level_state) from pinned memory,
+    # the coarse step (CFL + fused update), D2H of the same rows of the
+    # result (rb_download_level_state).
     import ctypes
-    nbytes = 5 * tree.ncell * 8
+    nbytes = 5 * 8 * 8 * tree.noct(level)
     host = np.empty((5, tree.ncell))
     try:
         import torch
@@ -695,9 +697,9 @@ def main():
     mixed.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        mixed.upload_state(host)
+        mixed.upload_level_state(level, host)
         mixed.uniform_run(1, graph=False)
-        mixed.download_state(out=host)
+        mixed.download_level_state(level, host)
     mixed.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = rep.job_rate(cells * args.e2e_steps, e2e_s)
@@ -734,7 +736,8 @@ def main():
             "config": config_dict(level, world, args.scheme),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "steps": args.e2e_steps,
-                    "path": "rb_upload_state + rb_uniform_run(1) + rb_download_state, pinned host buffers"},
+                    "path": "rb_upload_level_state + rb_uniform_run(1) + rb_download_level_state "
+                            "(the finest level's rows of the Fortran-layout uold), pinned host buffers"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": mixed_kernel + " (fused godunov + update + CFL partials)",

@@ -92,6 +92,15 @@ int rb_make_boundary_hydro(rb_context *ctx, int ilevel);
 /* Fortran-layout uold(ncell,5) host <-> device mirror of uold. */
 int rb_upload_state(rb_context *ctx, const double *uold);
 int rb_download_state(rb_context *ctx, double *uold);
+/* Only the rows of uold(ncell,5) that belong to the octs of level ilevel
+ * (icell = ncoarse+(ind-1)*ngridmax+igrid, igrid in active(ilevel)%igrid:
+ * the cells the level routines read and write, e.g. set_uold,
+ * hydro/godunov_fine.f90:135-232), host <-> device; every other row keeps
+ * its value on both sides. One copy per run of consecutive igrids, variable
+ * and cell position. The tree and the whole state must have been uploaded
+ * once (rb_sync_tree, rb_upload_state). */
+int rb_upload_level_state(rb_context *ctx, int ilevel, const double *uold);
+int rb_download_level_state(rb_context *ctx, int ilevel, double *uold);
 
 /* Residency protocol of the drop-in boundary. The reference keeps uold and
  * the tree in host memory and every hydro routine reads them there

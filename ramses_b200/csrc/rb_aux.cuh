@@ -63,6 +63,26 @@ static __global__ void permute_d2f_kernel(const double* __restrict__ d, double* 
     f[i] = d[v * ncell + dev_cell_of_fortran(icell, ncoarse, ngridmax)];
   }
 }
+// The cells of one level's octs between the staging copy of uold in the
+// Fortran layout (f) and the device layout (d): thread i handles cell ind =
+// i % 8 of the oct act[i / 8] (igrid-1), so the device side is contiguous
+// and the Fortran side reads whole sectors of consecutive igrids.
+template <bool F2D>
+static __global__ void permute_level_kernel(double* __restrict__ f, double* __restrict__ d,
+                                            const int32_t* __restrict__ act, int64_t noct, int64_t ncell,
+                                            int32_t ncoarse, int32_t ngridmax) {
+  const int64_t n = noct * 8;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = act[i >> 3];
+    const int ind = (int)(i & 7);
+    const int64_t fi = ncoarse + (int64_t)ind * ngridmax + g, di = ncoarse + 8 * g + ind;
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+      if (F2D) d[v * ncell + di] = f[v * ncell + fi];
+      else f[v * ncell + fi] = d[v * ncell + di];
+    }
+  }
+}
 // d[idx[i]] = v[i]: the son entries that changed in a tree re-sync
 static __global__ void scatter_son_kernel(int32_t* __restrict__ d, const int64_t* __restrict__ idx,
                                           const int32_t* __restrict__ v, int64_t n) {

@@ -115,6 +115,10 @@ struct Level {
   int32_t* d_bpair = nullptr;
   // the level's boundary octs (all regions, in region order) of the last sync
   std::vector<int32_t> h_bnd;
+  // runs of consecutive igrids of h_active as (first igrid, count) pairs,
+  // for the level's uold transfers; valid for tree sync number runs_sync
+  std::vector<int32_t> runs;
+  int64_t runs_sync = -1;
 };
 
 // sorted (key, igrid) lookup of one level's octs

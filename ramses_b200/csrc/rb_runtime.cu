@@ -1744,6 +1744,78 @@ int rb_download_state(rb_context* c, double* uold) {
   return RB_OK;
 }
 
+// ---- one level's rows of uold ----
+// Runs of consecutive igrids of a level's active list, (first, count)
+// pairs, cached until the next tree sync.
+static const std::vector<int32_t>& level_runs(rb_context* c, int l) {
+  Level& L = c->lv[l];
+  if (L.runs_sync != c->tree_syncs) {
+    L.runs.clear();
+    const std::vector<int32_t>& a = L.h_active;
+    for (size_t i = 0; i < a.size();) {
+      size_t j = i + 1;
+      while (j < a.size() && a[j] == a[j - 1] + 1) j++;
+      L.runs.push_back(a[i]);
+      L.runs.push_back((int32_t)(j - i));
+      i = j;
+    }
+    L.runs_sync = c->tree_syncs;
+  }
+  return L.runs;
+}
+// The level's rows between the host array and the staging buffer, one copy
+// per run, variable and cell position (same offsets on both sides).
+static int level_rows_copy(rb_context* c, int l, double* h, bool to_device) {
+  const std::vector<int32_t>& runs = level_runs(c, l);
+  const size_t nc = (size_t)c->ncell;
+  for (size_t r = 0; r < runs.size(); r += 2) {
+    const size_t g0 = (size_t)runs[r] - 1, n = (size_t)runs[r + 1];
+    for (int v = 0; v < 5; v++)
+      for (int ind = 0; ind < 8; ind++) {
+        const size_t off = v * nc + (size_t)c->mp.ncoarse + (size_t)ind * c->mp.ngridmax + g0;
+        if (to_device)
+          RB_CUDA(cudaMemcpyAsync(c->d_stage + off, h + off, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        else
+          RB_CUDA(cudaMemcpyAsync(h + off, c->d_stage + off, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      }
+  }
+  return RB_OK;
+}
+static int check_level_transfer(rb_context* c, int ilevel, const void* uold) {
+  if (!c) return fail(RB_ERR_INVALID, "null context");
+  if (!uold) return fail(RB_ERR_INVALID, "null uold");
+  if (!c->have_tree || !c->have_state) return fail(RB_ERR_STATE, "tree and state must be uploaded first");
+  if (ilevel < 1 || ilevel > c->mp.nlevelmax) return fail(RB_ERR_INVALID, "ilevel=%d out of 1..%d", ilevel, c->mp.nlevelmax);
+  return RB_OK;
+}
+int rb_upload_level_state(rb_context* c, int ilevel, const double* uold) {
+  RB_TRY(check_level_transfer(c, ilevel, uold));
+  RB_TRY(sync_oct(c));  // the device's own newer cells first, so the rows not sent stay current
+  Level& L = c->lv[ilevel];
+  if (L.noct == 0) return RB_OK;
+  RB_TRY(level_rows_copy(c, ilevel, const_cast<double*>(uold), true));
+  rb::permute_level_kernel<true><<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_stage, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->mp.ngridmax);
+  RB_CUDA(cudaGetLastError());
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  oct_changed(c);
+  c->h2d_state_bytes += (int64_t)L.noct * 8 * 5 * (int64_t)sizeof(double);
+  return RB_OK;
+}
+int rb_download_level_state(rb_context* c, int ilevel, double* uold) {
+  RB_TRY(check_level_transfer(c, ilevel, uold));
+  RB_TRY(sync_oct(c));
+  Level& L = c->lv[ilevel];
+  if (L.noct == 0) return RB_OK;
+  rb::permute_level_kernel<false><<<grid_for((int64_t)L.noct * 8, 256), 256, 0, c->stream>>>(
+      c->d_stage, c->d_uold, L.d_active, L.noct, c->ncell, c->mp.ncoarse, c->mp.ngridmax);
+  RB_CUDA(cudaGetLastError());
+  RB_TRY(level_rows_copy(c, ilevel, uold, false));
+  RB_CUDA(cudaStreamSynchronize(c->stream));
+  c->d2h_state_bytes += (int64_t)L.noct * 8 * 5 * (int64_t)sizeof(double);
+  return RB_OK;
+}
+
 // ---- residency protocol of the drop-in boundary ----
 int rb_note_tree_changed(rb_context* c) {
   if (!c) return fail(RB_ERR_INVALID, "null context");

@@ -79,6 +79,8 @@ _PROTOS = {
     "rb_make_boundary_hydro": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rb_upload_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
     "rb_download_state": (ctypes.c_int, [ctypes.c_void_p, _PD]),
+    "rb_upload_level_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _PD]),
+    "rb_download_level_state": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _PD]),
     "rb_note_tree_changed": (ctypes.c_int, [ctypes.c_void_p]),
     "rb_note_host_state_written": (ctypes.c_int, [ctypes.c_void_p]),
     "rb_tree_needs_sync": (ctypes.c_int, [ctypes.c_void_p, _P32]),
@@ -334,6 +336,19 @@ class Solver:
         assert u.shape == (5, self.tree.ncell) and u.dtype == np.float64 and u.flags.c_contiguous
         _check(load().rb_download_state(self._h, _ptr(u, _PD)), "rb_download_state")
         return u
+
+    def upload_level_state(self, ilevel: int, uold: np.ndarray):
+        """The rows of level ``ilevel``'s octs from the Fortran-layout host
+        array (5, ncell); the device keeps every other row."""
+        assert uold.shape == (5, self.tree.ncell) and uold.dtype == np.float64 and uold.flags.c_contiguous
+        _check(load().rb_upload_level_state(self._h, ilevel, _ptr(uold, _PD)), "rb_upload_level_state")
+
+    def download_level_state(self, ilevel: int, out: np.ndarray) -> np.ndarray:
+        """The rows of level ``ilevel``'s octs into the Fortran-layout host
+        array ``out`` (5, ncell); its other rows are left as they are."""
+        assert out.shape == (5, self.tree.ncell) and out.dtype == np.float64 and out.flags.c_contiguous
+        _check(load().rb_download_level_state(self._h, ilevel, _ptr(out, _PD)), "rb_download_level_state")
+        return out
 
     def upload_unew(self, unew: np.ndarray):
         u = np.ascontiguousarray(unew, np.float64)

@@ -230,3 +230,55 @@ def test_host_writes_are_uploaded_once(cuda_lib):
         assert not back.any()
         s.download_state(back)
         np.testing.assert_array_equal(back, u2)
+
+
+@pytest.mark.parametrize("case", ["uniform", "amr"])
+def test_level_state_transfers_touch_only_the_level_rows(cuda_lib, case):
+    """rb_upload_level_state / rb_download_level_state move the rows of one
+    level's octs and leave every other row as it is on both sides; the AMR
+    level's igrids come in several runs."""
+    from helpers import sedov_uniform
+    if case == "uniform":
+        tree, hp, u = sedov_uniform(4)
+    else:  # a remeshed tree: the level's igrids recycled from the free list
+        hp = HydroParams(gamma=1.4, riemann="hllc", slope_type=1, courant_factor=0.8)
+        t1 = mesh.build_tree(3, 5, mesh.sphere_refine((0.5, 0.5, 0.5), 0.12), spare=3000)
+        tree = mesh.remesh(t1, mesh.oct_sets(3, 5, mesh.sphere_refine((0.56, 0.5, 0.5), 0.12)))
+        u = ics.fill_all_levels(tree, ics.sedov_prim(5), hp.gamma)
+    level = 4
+    a = tree.active[level].astype(np.int64)
+    rows = (tree.ncoarse + np.arange(8)[:, None] * tree.ngridmax + a[None, :]).reshape(-1) - 1
+    other = np.setdiff1d(np.arange(tree.ncell), rows)
+    if case == "amr":
+        assert np.count_nonzero(np.diff(np.sort(a)) != 1) >= 1
+    with runtime.Solver(tree, hp, uold=u) as s:
+        b0 = s.transfer_stats()
+        h = u.copy()
+        h[:, rows] *= 1.25
+        h[:, other] = np.nan
+        s.upload_level_state(level, h)
+        got = s.download_state()
+        np.testing.assert_array_equal(got[:, rows], h[:, rows])
+        np.testing.assert_array_equal(got[:, other], u[:, other])
+        out = np.full_like(u, -7.0)
+        s.download_level_state(level, out)
+        np.testing.assert_array_equal(out[:, rows], h[:, rows])
+        assert np.all(out[:, other] == -7.0)
+        b1 = s.transfer_stats()
+        nb = rows.size * 5 * 8
+        assert b1["h2d_state_bytes"] - b0["h2d_state_bytes"] == nb
+        assert b1["d2h_state_bytes"] - b0["d2h_state_bytes"] == nb + 5 * 8 * tree.ncell
+        if case == "uniform":  # after steps held in the dense mirror
+            s.uniform_run(2, graph=False)
+            full = s.download_state()
+            out2 = np.full_like(u, -7.0)
+            s.download_level_state(level, out2)
+            np.testing.assert_array_equal(out2[:, rows], full[:, rows])
+            s.upload_level_state(level, full)
+            s.uniform_run(1, graph=False)
+            ref = np.full_like(u, -7.0)
+            s.download_level_state(level, ref)
+        if case == "uniform":
+            with runtime.Solver(tree, hp, uold=full) as s2:
+                s2.uniform_run(1, graph=False)
+                np.testing.assert_array_equal(s2.download_state()[:, rows], ref[:, rows])
