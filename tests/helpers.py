@@ -142,13 +142,13 @@ PLANAR["sod1d_periodic"] = dict(PLANAR["sod1d"], boundaries=[], bounds3d=(None, 
 PLANAR["implosion2d_periodic"] = dict(PLANAR["implosion2d"], boundaries=[], bounds3d=(None, None, None))
 
 
-def planar_lowdim_run(kind, level, nsteps, dt_force=None):
+def planar_lowdim_run(kind, level, nsteps, dt_force=None, riemann="hllc", slope_type=2):
     """The 1D/2D oracle on one complete level: (initial leaves, leaves after
     nsteps coarse steps with the run's own CFL time steps or ``dt_force``,
     the dts taken)."""
     import oracle
     c = PLANAR[kind]
-    hp = HydroParams(gamma=c["gamma"], riemann="hllc", slope_type=2, courant_factor=0.8,
+    hp = HydroParams(gamma=c["gamma"], riemann=riemann, slope_type=slope_type, courant_factor=0.8,
                      interpol_var=0, interpol_type=2)
     kw = dict(ndim=c["ndim"], levelmin=level, nlevelmax=level, ngridmax=4 ** level + 64, tout=1e30,
               regions=c["regions"], boundaries=c["boundaries"], nsubcycle=[1] * level, nexpand=[1] * level)
