@@ -221,3 +221,27 @@ def test_implosion_checksums_within_reference_tolerance(implosion):
     errs = {k: rel_error(sol[k], ref[k]) for k in sol}
     bad = {k: (sol[k], ref[k], e) for k, e in errs.items() if e > fx["checker"]["tolerance"]}
     assert not bad, bad
+
+
+def test_namelist_parser_forms():
+    """The fixture generator's namelist reader on the value forms the
+    reference's test namelists use: r*value repeats, d exponents, strings,
+    logicals, indexed keys and comments."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("mkfix", GOLDEN / "make_regression_fixture.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    text = """header line
+&RUN_PARAMS
+hydro=.true.
+nsubcycle=3*1,2
+/
+&INIT_PARAMS
+region_type(1)='square'
+d_region=1.0,0.125d0 ! a comment
+/
+"""
+    g = mod.parse_namelist(text)
+    assert g["RUN_PARAMS"] == {"hydro": [True], "nsubcycle": [1.0, 1.0, 1.0, 2.0]}
+    assert g["INIT_PARAMS"]["region_type(1)"] == ["square"]
+    assert g["INIT_PARAMS"]["d_region"] == [1.0, 0.125]
